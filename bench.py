@@ -1,0 +1,351 @@
+"""Benchmark of the fem25 hot path on B200.
+
+Headline workload (one step): the batched assembly of 512 complex128 CSR
+systems (8 frequencies 0.2-1.6 Hz x 64 ky) of the 400x120 degree-4 mesh of a
+layered model -- the "CSR assemblies/s" half of the metric.  Each rank does
+the full 512-system batch (weak scaling, no data-path collective: the
+(omega, py) systems are independent).  Inputs (the per-mesh basis, 2.6 GB)
+and outputs (3.98 GB per system) are larger than L2, so no flush is needed.
+
+Also reported on the same line:
+  * plain_fp64: the per-(omega, py) FP64 element + gather kernels (systems/s)
+  * e2e: ASMBLE_DRIVER through the C ABI with host buffers (model upload from
+    pinned memory, COMPLEX*8 CDIST read back to pinned memory) -- systems/s
+  * gradient: exact adjoint gradient, elem.rhs/s, config-1 mesh, 32 sources
+  * roofline of the streaming kernel and the CPU baseline (the oracle).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "CSR assemblies/s & gradient elem·rhs/s, batched-TF32x3 vs plain FP64 at 1e-6 rel"
+UNIT = "assemblies/s"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(dev), f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, n in enumerate(names):
+                if "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def cpu_assembly_sample(cfg_idx, seconds_target=15.0, workers=None):
+    """The oracle (CPU restatement of ASMBLE_DRIVER) on the host cores: each
+    worker assembles a contiguous slice of elements of a different system;
+    returns equivalent full systems/s."""
+    import multiprocessing as mp
+    workers = workers or os.cpu_count()
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(workers) as pool:
+        # calibrate: one small slice per worker
+        per = 64
+        t0 = time.perf_counter()
+        r = pool.map(_cpu_worker, [(cfg_idx, w, per) for w in range(workers)])
+        nelem = r[0][1]
+        t_mean = max(sum(x[0] for x in r) / workers, 1e-9)
+        # size the measured sample to ~seconds_target of wall time per core
+        per = int(max(64, min(nelem, per / t_mean * seconds_target)))
+        t0 = time.perf_counter()
+        r = pool.map(_cpu_worker, [(cfg_idx, w, per) for w in range(workers)])
+        wall = time.perf_counter() - t0
+    done = per * workers
+    return {"value": done / nelem / wall, "unit": UNIT, "cores": workers, "kind": "port",
+            "sample": f"{done} of {nelem} elements (one slice per core, each a different (omega, py) "
+                      f"system of the 400x120 mesh), oracle ASMBLE_DRIVER restatement, "
+                      f"{wall:.1f} s wall, scaled by elements"}
+
+
+_CPU_CACHE = {}
+
+
+def _cpu_worker(arg):
+    cfg_idx, w, per = arg
+    import oracle
+    from fem25_b200 import synth
+    if cfg_idx not in _CPU_CACHE:
+        mesh, pairs, _ = synth.make_config(cfg_idx)
+        from fem25_b200 import graph_build
+        g = graph_build(mesh)
+        _CPU_CACHE[cfg_idx] = (mesh, pairs, g)
+    mesh, pairs, g = _CPU_CACHE[cfg_idx]
+    f, py = pairs[(w * 37) % len(pairs)]
+    lo = (w * 997) % max(1, mesh.nelem - per)
+    t0 = time.perf_counter()
+    oracle.asmble(mesh, g, "B", f, py, elo=lo, ehi=min(mesh.nelem, lo + per), want64=True)
+    return time.perf_counter() - t0, mesh.nelem
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from fem25_b200 import synth
+    c = synth.CONFIGS[1]
+    vals = []
+    base = None
+    cpu_assembly_sample(1, seconds_target=2.0)  # warm-up: worker start, mesh and graph set-up
+    for _ in range(args.steps):
+        base = cpu_assembly_sample(1, seconds_target=10.0)
+        vals.append(base["value"])
+    v = statistics.mean(vals)
+    base["value"] = v
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 512 / v * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded layered model, 400x120 mesh)",
+           "config": {"workload": "configs[1]: batched assembly, 400x120 deg-4 mesh, 8 f x 64 ky "
+                                  "= 512 complex128 CSR systems",
+                      "systems_per_step": 512, "nelem": 48000},
+           "cpu_baseline": base,
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nslots", type=int, default=16)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-grad", action="store_true")
+    ap.add_argument("--small", action="store_true", help="small mesh (profiling captures)")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from fem25_b200 import FEM25_PREC_FP64, Context, synth
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---------------- setup (untimed)
+    t_setup = time.perf_counter()
+    if args.small:
+        mesh, pairs, cfg = synth.make_config(1, nx=100, nz=40)
+    else:
+        mesh, pairs, cfg = synth.make_config(1)
+    ctx = Context(mesh, device=local)
+    nz = ctx.nzero
+    nsys = len(pairs)
+    freqs = [p[0] for p in pairs]
+    pys = [p[1] for p in pairs]
+    nslots = args.nslots
+    stride = 2 * nz
+    ring = torch.empty(nslots * stride, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    setup_s = time.perf_counter() - t_setup
+
+    def step():
+        ctx.assemble_batch("B", freqs, pys, ring, stride, nslots, stream=stream)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+
+    # ---------------- timed region: batched assembly
+    ctx.profile(True)
+    clk = Clocks(local)
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    kern_ms = []
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+        kern_ms.append(ctx.profile_ms(0))  # streaming kernel, events on the same stream
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(ms)
+    ms_step = ms / args.steps
+    value = nsys * args.steps * world / (ms / 1e3)
+    # streaming kernel roofline: algorithmic bytes = 16 * NNZ per system
+    kms = statistics.mean(kern_ms)
+    peak, peak_kind = peaks()
+    achieved = 16.0 * nz * nsys / (kms / 1e3) / 1e9
+    launches_per_step = 2 * len(set(freqs)) + -(-nsys // min(16, nslots))
+
+    # ---------------- plain FP64 per-system path (device buffers)
+    o128 = torch.empty(nz, dtype=torch.complex128, device=dev)
+    o64 = torch.empty(nz, dtype=torch.complex64, device=dev)
+    for k in range(2):
+        ctx.assemble("B", freqs[k], pys[k], o128, o64, stream=stream)
+    torch.cuda.synchronize()
+    nplain = 16
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for k in range(nplain):
+        ctx.assemble("B", freqs[(k * 31) % nsys], pys[(k * 31) % nsys], o128, None, stream=stream)
+    p1.record(stream)
+    torch.cuda.synchronize()
+    plain_rate = nplain / (p0.elapsed_time(p1) / 1e3)
+    del o128, o64
+
+    # ---------------- e2e through the C ABI with host buffers
+    h_cdist = torch.empty(nz, dtype=torch.complex64, pin_memory=True)
+    h_e = torch.from_numpy(np.ascontiguousarray(mesh.ecoeff)).pin_memory()
+    h_d = torch.from_numpy(np.ascontiguousarray(mesh.dens)).pin_memory()
+    ne2e = 6
+    ctx.asmble_driver("B", freqs[0], pys[0], out=h_cdist)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(ne2e):
+        ctx.update_model(h_e.numpy(), h_d.numpy())
+        ctx.asmble_driver("B", freqs[(k * 17) % nsys], pys[(k * 17) % nsys], out=h_cdist)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = {"value": ne2e * world / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": int(h_e.numel() * 8 + h_d.numel() * 8),
+           "d2h_bytes_per_step": int(nz * 8),
+           "path": "fem25_update_model + fem25_asmble_driver (ASMBLE_DRIVER drop-in), "
+                   "COMPLEX*8 CDIST to pinned host memory"}
+    del h_cdist
+    # batched basis is rebuilt after update_model: restore it outside any timing
+    step()
+    torch.cuda.synchronize()
+
+    # ---------------- gradient (exact lambda/mu/rho, FP64), config-2 shape
+    grad = None
+    if not args.no_grad:
+        nsrc = 32
+        npool = 2
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(2027)
+        shape = (npool, nsrc, ctx.ndof)
+        u = torch.randn(shape, dtype=torch.complex128, device=dev, generator=gen)
+        lam = torch.randn(shape, dtype=torch.complex128, device=dev, generator=gen)
+        g = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=dev)
+        gp = pairs[::64][:npool]
+        ctx.gradient([p[0] for p in gp], [p[1] for p in gp], nsrc, u, lam, g, FEM25_PREC_FP64,
+                     stream=stream)
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        ctx.gradient([p[0] for p in gp], [p[1] for p in gp], nsrc, u, lam, g, FEM25_PREC_FP64,
+                     stream=stream)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        gms = g0.elapsed_time(g1)
+        nelem_phys = int(np.sum(mesh.cdomain != ord("A")))
+        units = mesh.nelem * nsrc * npool
+        grad = {"metric": "gradient elem·rhs/s", "unit": "elem·rhs/s",
+                "plain_fp64": units / (gms / 1e3), "ms": gms,
+                "units": f"{mesh.nelem} elements x {nsrc} sources x {npool} (omega,py) pairs "
+                         f"({nelem_phys} non-PML elements computed)",
+                "algorithmic_tflops_fp64": units * 547200 / (gms / 1e3) / 1e12}
+        del u, lam
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_assembly_sample(1, seconds_target=12.0)
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded layered model; no public dataset exists for this path)",
+           "config": {"workload": "configs[1]: batched assembly, 400x120 deg-4 mesh "
+                                  f"({mesh.nelem} elements, NDOF {ctx.ndof}, NNZ {nz}), "
+                                  f"8 f x 64 ky = {nsys} complex128 CSR systems per step",
+                      "systems_per_step": nsys, "nslots": nslots, "parallelism": f"replicas x{world}",
+                      "l2": "inputs (basis 2.6 GB) and outputs (4 GB/system) larger than L2",
+                      "setup_s": round(setup_s, 2)},
+           "plain_fp64": {"value": plain_rate, "unit": UNIT, "speedup_batched": value / world / plain_rate},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "traffic": None, "kernel": "k_stream",
+                        "kernel_ms": kms, "peak_kind": peak_kind,
+                        "algorithmic_bytes": "16 B x NNZ per system (complex128 values written)"},
+           "cpu_baseline": cpu, "e2e": e2e, "gradient": grad,
+           "gpu_launches": launches_per_step * args.steps, "clocks": clocks}
+    if rank == 0:
+        print(json.dumps(out))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,587 @@
+// C ABI of libfem25gpu (include/fem25gpu.h): argument checks, device
+// memory, context life cycle and the orchestration of the kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+
+#include "ctx.cuh"
+
+using namespace fem25;
+
+struct fem25_graph {
+  HostGraph g;
+};
+struct fem25_ctx {
+  Ctx c;
+};
+
+namespace {
+
+int fail(Ctx *c, int code, const std::string &msg) {
+  if (c) c->err = msg;
+  std::fprintf(stderr, "fem25gpu: %s\n", msg.c_str());
+  return code;
+}
+
+int cuda_fail(Ctx *c, cudaError_t e, const char *where) {
+  return fail(c, FEM25_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call, where)                              \
+  do {                                               \
+    cudaError_t _e = (call);                         \
+    if (_e != cudaSuccess) return cuda_fail(c, _e, where); \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc_copy(T **d, const T *h, size_t n) {
+  cudaError_t e = cudaMalloc((void **)d, sizeof(T) * (n ? n : 1));
+  if (e) return e;
+  if (n) e = cudaMemcpy(*d, h, sizeof(T) * n, cudaMemcpyHostToDevice);
+  return e;
+}
+
+int check_mesh(const fem25_mesh *m, std::string *msg) {
+  if (!m || !m->ieng || !m->cdomain || !m->cnnpg || !m->xlocs || !m->zlocs || !m->xd || !m->zd ||
+      !m->ecoeff || !m->dens) {
+    *msg = "mesh: null array";
+    return FEM25_ERR_ARG;
+  }
+  if (m->nelem <= 0 || m->nnpg <= 0) {
+    *msg = "mesh: empty";
+    return FEM25_ERR_ARG;
+  }
+  if (m->nord != kNord) {
+    *msg = "mesh: only NORD = 4 (5x5 GLL nodes) is built";
+    return FEM25_ERR_UNSUPPORTED;
+  }
+  if (m->ldisp) {
+    *msg = "mesh: dispersive media (KMDAMP/CMDAMP) are not supported";
+    return FEM25_ERR_UNSUPPORTED;
+  }
+  for (int e = 0; e < m->nelem; e++) {
+    for (int a = 0; a < 4; a++) {
+      int p = m->ieng[4 * (size_t)e + a];
+      if (p < 1 || p > m->nnpg) {
+        *msg = "mesh: IENG entry out of range";
+        return FEM25_ERR_ARG;
+      }
+    }
+    char d = m->cdomain[e];
+    if (d != 'I' && d != 'E' && d != 'A') {
+      *msg = "mesh: CDOMAIN must be 'I', 'E' or 'A'";
+      return FEM25_ERR_ARG;
+    }
+  }
+  return FEM25_OK;
+}
+
+void free_ctx(Ctx *c) {
+  void *ptrs[] = {c->dt.xigll, c->dt.wts, c->dt.shl, c->dt.sf, c->dt.dsf, c->d_ieng, c->d_cdomain,
+                  c->d_x, c->d_z, c->d_xd, c->d_zd, c->d_lam, c->d_mu, c->d_rho, c->d_lm,
+                  c->d_irptr, c->d_jcptr, c->d_cnp, c->d_elemmat, c->d_gptr, c->d_glist, c->d_err,
+                  c->d_brptr, c->d_brow, c->d_basis, c->d_ebasis, c->d_bgptr, c->d_bglist,
+                  c->d_pml_elems, c->d_pml_idx, c->d_pgptr, c->d_pglist, c->d_pml_emat,
+                  c->d_pml_delta, c->d_sys, c->d_jcsc, c->d_icsc, c->d_rg_anchor, c->d_mconn,
+                  c->d_elem_wts, c->d_fmat, c->d_pairs, c->d_nonpml, c->d_cdist};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (c->h_sys_pinned) cudaFreeHost(c->h_sys_pinned);
+  for (auto &e : c->ev)
+    if (e) cudaEventDestroy(e);
+}
+
+int read_err_word(Ctx *c, cudaStream_t st) {
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "error word");
+  CK(cudaStreamSynchronize(st), "synchronize");
+  if (h > 0) {
+    char buf[128];
+    std::snprintf(buf, sizeof buf, "element %d: Jacobian undefined or negative", h);
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), st);
+    return fail(c, FEM25_ERR_JACOBIAN, buf);
+  }
+  if (h < 0) {
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), st);
+    return fail(c, FEM25_ERR_PATTERN, "element entry without a CSR / CSC slot");
+  }
+  return FEM25_OK;
+}
+
+int upload_model(Ctx *c, const double *ecoeff, const double *dens) {
+  const size_t n = c->nnpg;
+  for (size_t p = 0; p < n; p++)
+    if (!(dens[p] > 0.0) || !(ecoeff[n + p] >= 0.0) || !(ecoeff[p] + 2.0 * ecoeff[n + p] > 0.0))
+      return fail(c, FEM25_ERR_ARG, "model: density must be > 0, mu >= 0, lambda + 2 mu > 0");
+  CK(cudaMemcpy(c->d_lam, ecoeff, sizeof(double) * n, cudaMemcpyHostToDevice), "model upload");
+  CK(cudaMemcpy(c->d_mu, ecoeff + n, sizeof(double) * n, cudaMemcpyHostToDevice), "model upload");
+  CK(cudaMemcpy(c->d_rho, dens, sizeof(double) * n, cudaMemcpyHostToDevice), "model upload");
+  c->basis_valid = false;
+  return FEM25_OK;
+}
+
+int ensure_plain(Ctx *c, cudaStream_t st) {
+  if (c->d_gptr) return FEM25_OK;
+  CK(cudaMalloc(&c->d_elemmat, sizeof(double2) * 9 * (size_t)c->nelem * kNab), "element matrices");
+  CK(build_gather_map(c, st), "gather map");
+  return read_err_word(c, st);
+}
+
+int ensure_batch(Ctx *c, cudaStream_t st) {
+  if (!c->d_bgptr) {
+    CK(build_batch_structures(c, st), "batch structures");
+    int r = read_err_word(c, st);
+    if (r) return r;
+  }
+  if (!c->basis_valid) {
+    CK(build_basis(c, st), "basis");
+    int r = read_err_word(c, st);
+    if (r) return r;
+    c->basis_valid = true;
+  }
+  return FEM25_OK;
+}
+
+int ensure_refgrad(Ctx *c) {
+  if (c->refgrad_ready) return FEM25_OK;
+  fem25_mesh m = c->mesh_scalars;
+  m.ieng = c->h_ieng.data();
+  m.cdomain = c->h_cdomain.data();
+  m.cnnpg = c->h_cnnpg.data();
+  m.xlocs = c->h_x.data();
+  m.zlocs = c->h_z.data();
+  std::string msg;
+  int r = build_ref_grad(&m, c->h_lm.data(), &c->rg, &msg);
+  if (r) return fail(c, r, msg);
+  CK(dalloc_copy(&c->d_jcsc, c->rg.jcsc.data(), c->rg.jcsc.size()), "ref grad");
+  CK(dalloc_copy(&c->d_icsc, c->rg.icsc.data(), c->rg.icsc.size()), "ref grad");
+  CK(dalloc_copy(&c->d_rg_anchor, c->rg.anchor_of_col.data(), c->rg.anchor_of_col.size()), "ref grad");
+  CK(dalloc_copy(&c->d_mconn, c->rg.mconn.data(), c->rg.mconn.size()), "ref grad");
+  CK(dalloc_copy(&c->d_elem_wts, c->rg.elem_wts.data(), c->rg.elem_wts.size()), "ref grad");
+  CK(cudaMalloc(&c->d_fmat, sizeof(float2) * (c->rg.nz ? c->rg.nz : 1)), "ref grad");
+  c->refgrad_ready = true;
+  return FEM25_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fem25_graph_build(const fem25_mesh *m, fem25_graph **out) {
+  std::string msg;
+  if (!out) return FEM25_ERR_ARG;
+  int r = check_mesh(m, &msg);
+  if (r) return fail(nullptr, r, msg);
+  fem25_graph *g = new fem25_graph();
+  r = build_graph(m, &g->g, &msg);
+  if (r) {
+    delete g;
+    return fail(nullptr, r, msg);
+  }
+  *out = g;
+  return FEM25_OK;
+}
+
+int fem25_graph_info(const fem25_graph *g, int *nnp, int *ndof, long long *nzero) {
+  if (!g) return FEM25_ERR_ARG;
+  if (nnp) *nnp = g->g.nnp;
+  if (ndof) *ndof = g->g.ndof;
+  if (nzero) *nzero = g->g.nzero;
+  return FEM25_OK;
+}
+
+int fem25_graph_copy(const fem25_graph *g, int *ien, int *lm, int *irptr, int *jcptr, char *cnp) {
+  if (!g) return FEM25_ERR_ARG;
+  const HostGraph &h = g->g;
+  if (ien) std::memcpy(ien, h.ien.data(), sizeof(int) * h.ien.size());
+  if (lm) std::memcpy(lm, h.lm.data(), sizeof(int) * h.lm.size());
+  if (irptr) std::memcpy(irptr, h.irptr.data(), sizeof(int) * h.irptr.size());
+  if (jcptr) std::memcpy(jcptr, h.jcptr.data(), sizeof(int) * h.jcptr.size());
+  if (cnp) std::memcpy(cnp, h.cnp.data(), h.cnp.size());
+  return FEM25_OK;
+}
+
+void fem25_graph_free(fem25_graph *g) { delete g; }
+
+int fem25_create(const fem25_mesh *m, int ndof, long long nzero, const int *lm, const int *irptr,
+                 const int *jcptr, const char *cnp, int device, fem25_ctx **out) {
+  std::string msg;
+  if (!out) return FEM25_ERR_ARG;
+  *out = nullptr;
+  int r = check_mesh(m, &msg);
+  if (r) return fail(nullptr, r, msg);
+  if (!lm || !irptr || !jcptr || !cnp || ndof <= 0 || nzero <= 0)
+    return fail(nullptr, FEM25_ERR_ARG, "create: graph arrays missing");
+  if (nzero > 2147483647LL) return fail(nullptr, FEM25_ERR_ARG, "create: NZERO exceeds int32");
+  if (irptr[0] != 1 || irptr[ndof] - 1 != nzero)
+    return fail(nullptr, FEM25_ERR_ARG, "create: IRPTR inconsistent with NZERO");
+  for (size_t k = 0; k < (size_t)3 * kNen * m->nelem; k++)
+    if (lm[k] < 0 || lm[k] > ndof) return fail(nullptr, FEM25_ERR_ARG, "create: LM out of range");
+  int ndev = 0;
+  cudaError_t ce = cudaGetDeviceCount(&ndev);
+  if (ce != cudaSuccess || device < 0 || device >= ndev)
+    return fail(nullptr, FEM25_ERR_CUDA, "create: no such CUDA device");
+  fem25_ctx *h = new fem25_ctx();
+  Ctx *c = &h->c;
+  c->device = device;
+  if ((ce = cudaSetDevice(device))) {
+    delete h;
+    return fail(nullptr, FEM25_ERR_CUDA, cudaGetErrorString(ce));
+  }
+  c->mesh_scalars = *m;
+  c->mesh_scalars.ieng = nullptr;
+  c->mesh_scalars.cdomain = nullptr;
+  c->mesh_scalars.cnnpg = nullptr;
+  c->mesh_scalars.xlocs = c->mesh_scalars.zlocs = c->mesh_scalars.xd = c->mesh_scalars.zd = nullptr;
+  c->mesh_scalars.ecoeff = c->mesh_scalars.dens = nullptr;
+  c->nelem = m->nelem;
+  c->nnpg = m->nnpg;
+  c->ndof = ndof;
+  c->nzero = nzero;
+  c->h_cdomain.assign(m->cdomain, m->cdomain + m->nelem);
+  c->h_cnnpg.assign(m->cnnpg, m->cnnpg + 2 * (size_t)m->nnpg);
+  c->h_x.assign(m->xlocs, m->xlocs + m->nnpg);
+  c->h_z.assign(m->zlocs, m->zlocs + m->nnpg);
+  c->h_ieng.assign(m->ieng, m->ieng + 4 * (size_t)m->nelem);
+  c->h_lm.assign(lm, lm + 3 * (size_t)kNen * m->nelem);
+  c->h_irptr.assign(irptr, irptr + ndof + 1);
+  r = build_block_csr(ndof, nzero, irptr, jcptr, &c->bcsr, &msg);
+  if (r) {
+    fail(c, r, msg);
+    free_ctx(c);
+    delete h;
+    return r;
+  }
+  build_tables(&c->tab);
+  auto setup = [&]() -> int {
+    CK(dalloc_copy(&c->dt.xigll, c->tab.xigll, kNint), "tables");
+    CK(dalloc_copy(&c->dt.wts, c->tab.wts, kNint), "tables");
+    CK(dalloc_copy(&c->dt.shl, c->tab.shl, 3 * kNen * kNq), "tables");
+    CK(dalloc_copy(&c->dt.sf, &c->tab.sf[0][0], 4 * kNq), "tables");
+    CK(dalloc_copy(&c->dt.dsf, &c->tab.dsf[0][0][0], 8 * kNq), "tables");
+    CK(dalloc_copy(&c->d_ieng, reinterpret_cast<const int4 *>(m->ieng), m->nelem), "mesh");
+    CK(dalloc_copy(&c->d_cdomain, m->cdomain, m->nelem), "mesh");
+    CK(dalloc_copy(&c->d_x, m->xlocs, m->nnpg), "mesh");
+    CK(dalloc_copy(&c->d_z, m->zlocs, m->nnpg), "mesh");
+    CK(dalloc_copy(&c->d_xd, m->xd, m->nnpg), "mesh");
+    CK(dalloc_copy(&c->d_zd, m->zd, m->nnpg), "mesh");
+    CK(cudaMalloc(&c->d_lam, sizeof(double) * m->nnpg), "mesh");
+    CK(cudaMalloc(&c->d_mu, sizeof(double) * m->nnpg), "mesh");
+    CK(cudaMalloc(&c->d_rho, sizeof(double) * m->nnpg), "mesh");
+    int rr = upload_model(c, m->ecoeff, m->dens);
+    if (rr) return rr;
+    CK(dalloc_copy(&c->d_lm, lm, 3 * (size_t)kNen * m->nelem), "graph");
+    CK(dalloc_copy(&c->d_irptr, irptr, (size_t)ndof + 1), "graph");
+    CK(dalloc_copy(&c->d_jcptr, jcptr, (size_t)nzero), "graph");
+    CK(dalloc_copy(&c->d_cnp, cnp, (size_t)ndof), "graph");
+    CK(cudaMalloc(&c->d_err, sizeof(int)), "error word");
+    CK(cudaMemset(c->d_err, 0, sizeof(int)), "error word");
+    std::vector<int> nonpml;
+    for (int e = 0; e < m->nelem; e++)
+      if (m->cdomain[e] != 'A') nonpml.push_back(e);
+    c->n_nonpml = (int)nonpml.size();
+    CK(dalloc_copy(&c->d_nonpml, nonpml.data(), nonpml.size()), "element lists");
+    c->mv.nelem = m->nelem;
+    c->mv.nnpg = m->nnpg;
+    c->mv.ieng = c->d_ieng;
+    c->mv.cdomain = c->d_cdomain;
+    c->mv.x = c->d_x;
+    c->mv.z = c->d_z;
+    c->mv.xd = c->d_xd;
+    c->mv.zd = c->d_zd;
+    c->mv.lam = c->d_lam;
+    c->mv.mu = c->d_mu;
+    c->mv.rho = c->d_rho;
+    CK(check_jacobians(c, 0), "jacobian check");
+    return read_err_word(c, 0);
+  };
+  r = setup();
+  if (r) {
+    free_ctx(c);
+    delete h;
+    return r;
+  }
+  *out = h;
+  return FEM25_OK;
+}
+
+void fem25_destroy(fem25_ctx *h) {
+  if (!h) return;
+  cudaSetDevice(h->c.device);
+  cudaDeviceSynchronize();
+  free_ctx(&h->c);
+  delete h;
+}
+
+int fem25_last_error(const fem25_ctx *h, char *buf, int n) {
+  if (!h || !buf || n <= 0) return FEM25_ERR_ARG;
+  std::snprintf(buf, n, "%s", h->c.err.c_str());
+  return FEM25_OK;
+}
+
+int fem25_sizes(const fem25_ctx *h, int *ndof, long long *nzero, long long *nblocks) {
+  if (!h) return FEM25_ERR_ARG;
+  if (ndof) *ndof = h->c.ndof;
+  if (nzero) *nzero = h->c.nzero;
+  if (nblocks) *nblocks = h->c.bcsr.nblocks;
+  return FEM25_OK;
+}
+
+int fem25_update_model(fem25_ctx *h, const double *ecoeff, const double *dens) {
+  if (!h || !ecoeff || !dens) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  CK(cudaSetDevice(c->device), "set device");
+  return upload_model(c, ecoeff, dens);
+}
+
+int fem25_assemble_dev(fem25_ctx *h, char cftype, double freq, double py, double *csr128,
+                       float *csr64, void *stream) {
+  if (!h) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  if (cftype != 'S' && cftype != 'B') return fail(c, FEM25_ERR_ARG, "assemble: CFTYPE must be 'S' or 'B'");
+  if (!(freq > 0.0)) return fail(c, FEM25_ERR_ARG, "assemble: FREQ must be > 0");
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaSetDevice(c->device), "set device");
+  int r = ensure_plain(c, st);
+  if (r) return r;
+  if (c->prof) CK(cudaEventRecord(c->ev[2], st), "event");
+  CK(launch_elem_plain(c, cftype, freq, py, st), "element kernel");
+  CK(launch_gather_plain(c, csr128, csr64, st), "gather kernel");
+  if (c->prof) CK(cudaEventRecord(c->ev[3], st), "event");
+  return FEM25_OK;
+}
+
+int fem25_asmble_driver(fem25_ctx *h, int nzloc, char cftype, double freq, double py,
+                        float *cdist) {
+  if (!h || !cdist) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  if ((long long)nzloc != c->nzero) return fail(c, FEM25_ERR_ARG, "asmble_driver: NZLOC != NZERO");
+  CK(cudaSetDevice(c->device), "set device");
+  if (!c->d_cdist) CK(cudaMalloc(&c->d_cdist, sizeof(float2) * (size_t)nzloc), "cdist buffer");
+  int r = fem25_assemble_dev(h, cftype, freq, py, nullptr, (float *)c->d_cdist, nullptr);
+  if (!r) {
+    cudaError_t e =
+        cudaMemcpy(cdist, c->d_cdist, sizeof(float2) * (size_t)nzloc, cudaMemcpyDeviceToHost);
+    if (e) r = cuda_fail(c, e, "cdist copy");
+  }
+  if (!r) r = read_err_word(c, 0);
+  return r;
+}
+
+int fem25_assemble_batch_dev(fem25_ctx *h, int n, const char *cftype, const double *freq,
+                             const double *py, double *ring_base, long long slot_stride,
+                             int nslots, void *stream) {
+  if (!h || !cftype || !freq || !py || !ring_base || n <= 0 || nslots <= 0) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  if (slot_stride < 2 * c->nzero || (slot_stride & 1))
+    return fail(c, FEM25_ERR_ARG, "batch: slot stride must be even and >= 2*NZERO");
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaSetDevice(c->device), "set device");
+  int r = ensure_batch(c, st);
+  if (r) return r;
+  // distinct (omega, cftype) -> PML delta slots
+  std::map<std::pair<double, char>, int> slots;
+  std::vector<std::pair<double, char>> order;
+  for (int k = 0; k < n; k++) {
+    if (cftype[k] != 'S' && cftype[k] != 'B')
+      return fail(c, FEM25_ERR_ARG, "batch: CFTYPE must be 'S' or 'B'");
+    if (!(freq[k] > 0.0)) return fail(c, FEM25_ERR_ARG, "batch: FREQ must be > 0");
+    auto key = std::make_pair(freq[k], cftype[k]);
+    if (!slots.count(key)) {
+      slots[key] = (int)order.size();
+      order.push_back(key);
+    }
+  }
+  const int nps = (int)order.size();
+  if (c->npml_blocks > 0 && nps > c->pml_delta_cap) {
+    if (c->d_pml_delta) cudaFree(c->d_pml_delta);
+    CK(cudaMalloc(&c->d_pml_delta, sizeof(double2) * 9 * (size_t)c->npml_blocks * nps), "pml delta");
+    c->pml_delta_cap = nps;
+  }
+  for (int k = 0; k < nps; k++) {
+    PmlParams pp = pml_params(c, order[k].second, order[k].first);
+    CK(build_pml_delta(c, pp, k, st), "pml delta");
+  }
+  if (n > c->sys_cap) {
+    CK(cudaStreamSynchronize(st), "synchronize");
+    if (c->d_sys) cudaFree(c->d_sys);
+    if (c->h_sys_pinned) cudaFreeHost(c->h_sys_pinned);
+    CK(cudaMalloc(&c->d_sys, sizeof(SysParam) * n), "system table");
+    CK(cudaMallocHost(&c->h_sys_pinned, sizeof(SysParam) * n), "system table");
+    c->sys_cap = n;
+  }
+  CK(cudaStreamSynchronize(st), "synchronize");  // the pinned table may still be in flight
+  for (int k = 0; k < n; k++) {
+    double omega = 6.2831853071795862 * freq[k];
+    c->h_sys_pinned[k].w2 = omega * omega;
+    c->h_sys_pinned[k].wpy = omega * py[k];
+    c->h_sys_pinned[k].pml_slot = slots[std::make_pair(freq[k], cftype[k])];
+    c->h_sys_pinned[k].pad = 0;
+  }
+  CK(cudaMemcpyAsync(c->d_sys, c->h_sys_pinned, sizeof(SysParam) * n, cudaMemcpyHostToDevice, st),
+     "system table");
+  if (c->prof) CK(cudaEventRecord(c->ev[0], st), "event");
+  CK(launch_stream_batch(c, n, ring_base, slot_stride, nslots, st), "stream kernel");
+  if (c->prof) CK(cudaEventRecord(c->ev[1], st), "event");
+  return FEM25_OK;
+}
+
+int fem25_profile_enable(fem25_ctx *h, int enable) {
+  if (!h) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  CK(cudaSetDevice(c->device), "set device");
+  for (auto &e : c->ev)
+    if (!e) CK(cudaEventCreate(&e), "event");
+  c->prof = enable != 0;
+  return FEM25_OK;
+}
+
+int fem25_profile_ms(fem25_ctx *h, int which, double *ms) {
+  if (!h || !ms || which < 0 || which > 1) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  if (!c->ev[2 * which]) return fail(c, FEM25_ERR_ARG, "profiling not enabled");
+  CK(cudaEventSynchronize(c->ev[2 * which + 1]), "event");
+  float t = 0.f;
+  CK(cudaEventElapsedTime(&t, c->ev[2 * which], c->ev[2 * which + 1]), "event");
+  *ms = t;
+  return FEM25_OK;
+}
+
+int fem25_peff_dev(fem25_ctx *h, int nsrc, const float *a_loc, const float *ue, float *peff,
+                   void *stream) {
+  if (!h || !a_loc || !ue || !peff || nsrc <= 0) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  CK(cudaSetDevice(c->device), "set device");
+  CK(launch_peff(c, nsrc, a_loc, ue, peff, (cudaStream_t)stream), "peff");
+  return FEM25_OK;
+}
+
+int fem25_gradient_dev(fem25_ctx *h, int npairs, const double *freq, const double *py, int nsrc,
+                       const double *u, const double *lam, int prec, double *grad, void *stream) {
+  if (!h || !freq || !py || !u || !lam || !grad || npairs <= 0 || nsrc <= 0) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaSetDevice(c->device), "set device");
+  if (npairs > c->pairs_cap) {
+    CK(cudaStreamSynchronize(st), "synchronize");
+    if (c->d_pairs) cudaFree(c->d_pairs);
+    CK(cudaMalloc(&c->d_pairs, sizeof(double2) * npairs), "pairs");
+    c->pairs_cap = npairs;
+  }
+  std::vector<double2> hp(npairs);
+  for (int k = 0; k < npairs; k++) {
+    double omega = 6.2831853071795862 * freq[k];
+    hp[k] = make_double2(omega, omega * py[k]);
+  }
+  CK(cudaStreamSynchronize(st), "synchronize");
+  CK(cudaMemcpy(c->d_pairs, hp.data(), sizeof(double2) * npairs, cudaMemcpyHostToDevice), "pairs");
+  if (prec == FEM25_PREC_FP64) {
+    CK(launch_grad_plain(c, npairs, nsrc, u, lam, grad, st), "gradient");
+  } else if (prec == FEM25_PREC_TF32X3) {
+    cudaError_t e = launch_grad_tc(c, npairs, nsrc, u, lam, grad, st);
+    if (e == cudaErrorNotSupported)
+      return fail(c, FEM25_ERR_UNSUPPORTED, "gradient: split-precision path not available");
+    CK(e, "gradient (tf32x3)");
+  } else {
+    return fail(c, FEM25_ERR_ARG, "gradient: unknown precision");
+  }
+  return FEM25_OK;
+}
+
+int fem25_ref_gradient_info(fem25_ctx *h, int *nnpinv, long long *nz_fdist, int *maskg) {
+  if (!h) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  CK(cudaSetDevice(c->device), "set device");
+  int r = ensure_refgrad(c);
+  if (r) return r;
+  if (nnpinv) *nnpinv = c->rg.nnpinv;
+  if (nz_fdist) *nz_fdist = c->rg.nz;
+  if (maskg) std::memcpy(maskg, c->rg.maskg.data(), sizeof(int) * c->nnpg);
+  return FEM25_OK;
+}
+
+int fem25_ref_gradient_dev(fem25_ctx *h, const char *cinvtype, double vpvs, double freq,
+                           double py, const float *wave, const float *adjlam, int accumulate,
+                           float *gradl, void *stream) {
+  if (!h || !cinvtype || !wave || !adjlam || !gradl) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  std::string ct(cinvtype, cinvtype + 2);
+  int lisp;
+  if (ct == "PP" || ct == "pp") lisp = 1;
+  else if (ct == "SS" || ct == "ss") lisp = 0;
+  else if (ct == "PS" || ct == "ps")
+    return fail(c, FEM25_ERR_UNSUPPORTED, "vforce25: Error S and P derivatives not done yet");
+  else return fail(c, FEM25_ERR_UNSUPPORTED, "vforce25: Error anisotropy not programmed!");
+  CK(cudaSetDevice(c->device), "set device");
+  int r = ensure_refgrad(c);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(launch_ref_cfmat(c, lisp, vpvs, 6.2831853071795862 * freq, py, wave, accumulate, st), "cfmat");
+  CK(launch_ref_adjflam(c, adjlam, gradl, st), "adjflam");
+  return FEM25_OK;
+}
+
+int fem25_misfit_dev(fem25_ctx *h, int nsrc, int nrec, const int *mrdof, const double *yrec,
+                     double freq, double py, double azmod, const float *recv, const float *sol,
+                     const float *obs, const float *wghts, float *est, float *rhs, float *misfit,
+                     void *stream) {
+  if (!h || nsrc <= 0 || nrec <= 0 || !mrdof || !yrec || !recv || !sol || !obs || !wghts || !est ||
+      !rhs || !misfit)
+    return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  {
+    std::vector<int> seen;
+    for (int k = 0; k < 3 * nrec; k++) {
+      if (mrdof[k] < 0 || mrdof[k] > c->ndof)
+        return fail(c, FEM25_ERR_ARG, "misfit: MRDOF entry out of range");
+      if (mrdof[k] > 0) seen.push_back(mrdof[k]);
+    }
+    std::sort(seen.begin(), seen.end());
+    if (std::adjacent_find(seen.begin(), seen.end()) != seen.end())
+      return fail(c, FEM25_ERR_ARG, "misfit: two receiver components share a DOF");
+  }
+  CK(cudaSetDevice(c->device), "set device");
+  cudaStream_t st = (cudaStream_t)stream;
+  const double omega = 6.2831853071795862 * freq;
+  std::vector<float> trig(4 * (size_t)nrec);
+  for (int ir = 0; ir < nrec; ir++) {
+    float ph = (float)(omega * py * yrec[ir]);
+    float ph2 = -(float)(omega * py * yrec[ir]);
+    trig[4 * ir + 0] = cosf(ph);
+    trig[4 * ir + 1] = sinf(ph);
+    trig[4 * ir + 2] = cosf(ph2);
+    trig[4 * ir + 3] = sinf(ph2);
+  }
+  int *d_mrdof = nullptr;
+  float *d_trig = nullptr, *d_recv = nullptr, *d_obs = nullptr, *d_w = nullptr, *d_est = nullptr,
+        *d_mis = nullptr;
+  const size_t nr3 = 3 * (size_t)nrec, ns3 = nr3 * nsrc;
+  int r = FEM25_OK;
+  auto run = [&]() -> int {
+    CK(dalloc_copy(&d_mrdof, mrdof, nr3), "misfit");
+    CK(dalloc_copy(&d_trig, trig.data(), trig.size()), "misfit");
+    CK(dalloc_copy(&d_recv, recv, 2 * nr3), "misfit");
+    CK(dalloc_copy(&d_obs, obs, 2 * ns3), "misfit");
+    CK(dalloc_copy(&d_w, wghts, ns3), "misfit");
+    CK(cudaMalloc(&d_est, sizeof(float) * 2 * ns3), "misfit");
+    CK(cudaMalloc(&d_mis, sizeof(float) * nsrc), "misfit");
+    CK(launch_misfit(c, nsrc, nrec, d_mrdof, d_trig, omega, py, azmod, d_recv, sol, d_obs, d_w,
+                     d_est, rhs, d_mis, st),
+       "misfit");
+    CK(cudaMemcpyAsync(est, d_est, sizeof(float) * 2 * ns3, cudaMemcpyDeviceToHost, st), "misfit");
+    CK(cudaMemcpyAsync(misfit, d_mis, sizeof(float) * nsrc, cudaMemcpyDeviceToHost, st), "misfit");
+    CK(cudaStreamSynchronize(st), "misfit");
+    return FEM25_OK;
+  };
+  r = run();
+  for (void *p : {(void *)d_mrdof, (void *)d_trig, (void *)d_recv, (void *)d_obs, (void *)d_w,
+                  (void *)d_est, (void *)d_mis})
+    if (p) cudaFree(p);
+  return r;
+}
+
+}  // extern "C"

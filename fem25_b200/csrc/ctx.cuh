@@ -1,0 +1,133 @@
+// Device context of libfem25gpu and the kernel entry points shared between
+// translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "fem25_internal.h"
+
+namespace fem25 {
+
+// Quadrature tables on the device (built once by build_tables()).
+struct DevTables {
+  double *xigll;  // [13]
+  double *wts;    // [13]
+  double *shl;    // [169][25][3]  SHL(3,NEN,NINT,NINT)
+  double *sf;     // [169][4]
+  double *dsf;    // [169][2][4]
+};
+
+// Per-(omega, cftype) PML parameters resolved on the host (asmble.f90:78-88).
+struct PmlParams {
+  double omega, rcoeff, dmax, kappa, fcent, xwidth, zwidth;
+};
+
+// Arguments of the element kernels that read the mesh.
+struct MeshView {
+  int nelem, nnpg;
+  const int4 *ieng;        // 1-based anchors, one int4 per element
+  const char *cdomain;
+  const double *x, *z, *xd, *zd, *lam, *mu, *rho;
+};
+
+// One (omega, py) system of a batch, pre-digested for the streaming kernel.
+struct SysParam {
+  double w2;     // omega^2
+  double wpy;    // omega * py
+  int pml_slot;  // index of the PML delta of this system's (omega, cftype)
+  int pad;
+};
+
+struct Ctx {
+  int device = 0;
+  std::string err;
+  fem25_mesh mesh_scalars{};   // scalars only (pointers not kept)
+  int nelem = 0, nnpg = 0, ndof = 0;
+  long long nzero = 0;
+  Tables tab;
+  DevTables dt{};
+  MeshView mv{};
+  // device mesh arrays
+  int4 *d_ieng = nullptr;
+  char *d_cdomain = nullptr;
+  double *d_x = nullptr, *d_z = nullptr, *d_xd = nullptr, *d_zd = nullptr;
+  double *d_lam = nullptr, *d_mu = nullptr, *d_rho = nullptr;
+  std::vector<char> h_cdomain, h_cnnpg;
+  std::vector<double> h_x, h_z;
+  std::vector<int> h_ieng, h_lm, h_irptr;
+  // graph
+  int *d_lm = nullptr, *d_irptr = nullptr, *d_jcptr = nullptr;
+  char *d_cnp = nullptr;
+  // plain path: element matrices and the nonzero -> contributions gather map
+  double2 *d_elemmat = nullptr;  // [nelem][625][9]
+  int *d_gptr = nullptr;         // [nzero+1]
+  int *d_glist = nullptr;        // contribution ids, element order per nonzero
+  long long ncontrib = 0;
+  int *d_err = nullptr;          // device error word
+  // batched path
+  BlockCSR bcsr;
+  long long *d_brptr = nullptr;
+  int *d_brow = nullptr;
+  double *d_basis = nullptr;     // [12][nblocks]
+  double *d_ebasis = nullptr;    // [nelem][625][12] scratch
+  int *d_bgptr = nullptr, *d_bglist = nullptr;  // block -> (element node pair) ids
+  bool basis_valid = false;
+  // PML part of the batched path
+  int npml_elem = 0;
+  int *d_pml_elems = nullptr;    // element ids of 'A' elements
+  long long npml_blocks = 0;
+  int *d_pml_idx = nullptr;      // [nblocks] -> PML block index or -1
+  int *d_pgptr = nullptr, *d_pglist = nullptr;  // PML block -> (pml elem, ab) ids
+  double2 *d_pml_emat = nullptr; // [npml_elem][625][9] scratch (one omega)
+  double2 *d_pml_delta = nullptr; // [nslots_pml][npml_blocks][9][2] (CE0, CE1)
+  int pml_delta_cap = 0;
+  SysParam *d_sys = nullptr;     // per-system parameters of the current batch
+  int sys_cap = 0;
+  SysParam *h_sys_pinned = nullptr;
+  // reference-compatible gradient
+  bool refgrad_ready = false;
+  RefGradSetup rg;
+  int *d_jcsc = nullptr, *d_icsc = nullptr, *d_rg_anchor = nullptr, *d_mconn = nullptr;
+  double *d_elem_wts = nullptr;
+  float2 *d_fmat = nullptr;
+  // gradient
+  double2 *d_pairs = nullptr;    // (omega, wpy) per pair
+  int pairs_cap = 0;
+  int *d_nonpml = nullptr;       // ids of the elements outside the PML
+  int n_nonpml = 0;
+  // cached COMPLEX*8 device buffer of fem25_asmble_driver
+  float2 *d_cdist = nullptr;
+  // optional CUDA-event timing of the dominant kernels
+  bool prof = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+// kernels / launchers (defined in the .cu files)
+cudaError_t launch_elem_plain(Ctx *c, char cftype, double freq, double py, cudaStream_t st);
+cudaError_t launch_gather_plain(Ctx *c, double *csr128, float *csr64, cudaStream_t st);
+cudaError_t build_gather_map(Ctx *c, cudaStream_t st);
+cudaError_t check_jacobians(Ctx *c, cudaStream_t st);
+cudaError_t build_batch_structures(Ctx *c, cudaStream_t st);
+cudaError_t build_basis(Ctx *c, cudaStream_t st);
+cudaError_t build_pml_delta(Ctx *c, const PmlParams &pp, int slot, cudaStream_t st);
+cudaError_t launch_stream_batch(Ctx *c, int n, double *ring_base, long long slot_stride,
+                                int nslots, cudaStream_t st);
+cudaError_t launch_peff(Ctx *c, int nsrc, const float *a_loc, const float *ue, float *peff,
+                        cudaStream_t st);
+cudaError_t launch_grad_plain(Ctx *c, int npairs, int nsrc, const double *u, const double *lam,
+                              double *grad, cudaStream_t st);
+cudaError_t launch_grad_tc(Ctx *c, int npairs, int nsrc, const double *u, const double *lam,
+                           double *grad, cudaStream_t st);
+cudaError_t launch_ref_cfmat(Ctx *c, int lisp, double vpvs, double omega, double py,
+                             const float *wave, int accumulate, cudaStream_t st);
+cudaError_t launch_ref_adjflam(Ctx *c, const float *adjlam, float *gradl, cudaStream_t st);
+cudaError_t launch_misfit(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const float *d_trig,
+                          double omega, double py, double azmod, const float *d_recv,
+                          const float *sol, const float *d_obs, const float *d_wghts,
+                          float *d_est, float *rhs, float *d_misfit, cudaStream_t st);
+
+PmlParams pml_params(const Ctx *c, char cftype, double freq);
+
+}  // namespace fem25

@@ -1,0 +1,475 @@
+// Batched assembly of many (omega, py) systems of one mesh.
+//
+// For every non-PML element the KM25ISOQ matrix (estiff25.f:64-154) is affine
+// in (omega^2, omega*py, (omega*py)^2):
+//   A(i,j) = delta_ij (-omega^2 M_rho + (omega py)^2 M_i) + K0_ij + i omega py K1_ij
+// with real K0 on the (1,1),(1,3),(2,2),(3,1),(3,3) component blocks, real K1
+// on (1,2),(2,1),(2,3),(3,2), M_1 = M_3 = int mu N_a N_b, M_2 = int (lambda+2mu)
+// N_a N_b.  The PML elements (CM25ISOQ, estiff25.f:235-332) share the mass
+// part and add CE0(omega) + omega py CE1(omega) with complex coefficients.
+// The basis is summed once per mesh into 3x3 node blocks of the CSR (12 reals
+// per block); the streaming kernel then reads each block's basis once per
+// pass and writes it for B systems: an HBM-write-bound stream.
+#include "ctx.cuh"
+#include "kcommon.cuh"
+
+namespace fem25 {
+
+cudaError_t scan_counts(const int *count, int *ptr, long long n, cudaStream_t st);
+__global__ void k_sort_lists(long long n, const int *__restrict__ ptr, int *__restrict__ list,
+                             int *__restrict__ err);
+
+// basis slots per block
+enum { B_K11 = 0, B_K13, B_K22, B_K31, B_K33, B_K12, B_K21, B_K23, B_K32, B_MRHO, B_MMU, B_ML2M, B_N };
+
+constexpr int kElemThreads = 640;
+
+// Per element node pair: the 12 basis integrals over the 13x13 rule.
+// PML elements contribute their (omega-independent) mass integrals only.
+__global__ void __launch_bounds__(kElemThreads, 1)
+    k_elem_basis(MeshView mv, DevTables dt, double *__restrict__ ebasis, int *__restrict__ err) {
+  extern __shared__ double sm[];
+  double *shx = sm, *shz = sm + kNq * kNen, *shn = sm + 2 * kNq * kNen, *qc = sm + 3 * kNq * kNen;
+  const int e = blockIdx.x, t = threadIdx.x;
+  const int4 ie = mv.ieng[e];
+  const bool pml = mv.cdomain[e] == 'A';
+  if (t < kNq) {
+    const int q = t, intx = q % kNint, intz = q / kNint;
+    QGeo g;
+    if (!quad_geo(mv, dt, ie, q, false, g)) atomicCAS(err, 0, e + 1);
+    double *c = qc + 8 * q;
+    c[0] = g.dxdxi; c[1] = g.dxdeta; c[2] = g.dzdxi; c[3] = g.dzdeta; c[4] = g.rjac;
+    double w = dt.wts[intx] * dt.wts[intz] * g.rjac;
+    c[5] = g.lam * w;
+    c[6] = g.mu * w;
+    c[7] = g.rho * w;
+  }
+  __syncthreads();
+  for (int idx = t; idx < kNq * kNen; idx += kElemThreads) {
+    const int q = idx / kNen;
+    const double *c = qc + 8 * q;
+    const double *sl = dt.shl + 3 * (size_t)idx;
+    shx[idx] = (sl[0] * c[3] - sl[1] * c[2]) / c[4];
+    shz[idx] = -(sl[0] * c[1] - sl[1] * c[0]) / c[4];
+    shn[idx] = sl[2];
+  }
+  __syncthreads();
+  if (t >= kNab) return;
+  const int a = t / kNen, b = t % kNen;
+  double acc[B_N];
+#pragma unroll
+  for (int k = 0; k < B_N; k++) acc[k] = 0.0;
+  for (int q = 0; q < kNq; q++) {
+    const double *c = qc + 8 * q;
+    const double lam = c[5], mu = c[6], rhow = c[7], c11 = lam + 2.0 * mu;
+    const double pa = shn[q * kNen + a], pax = shx[q * kNen + a], paz = shz[q * kNen + a];
+    const double pb = shn[q * kNen + b], pbx = shx[q * kNen + b], pbz = shz[q * kNen + b];
+    const double nn = pa * pb;
+    acc[B_MRHO] += nn * rhow;
+    acc[B_MMU] += nn * mu;
+    acc[B_ML2M] += nn * c11;
+    if (!pml) {
+      acc[B_K11] += pax * c11 * pbx + paz * mu * pbz;
+      acc[B_K13] += pax * lam * pbz + paz * mu * pbx;
+      acc[B_K22] += pax * mu * pbx + paz * mu * pbz;
+      acc[B_K31] += paz * lam * pbx + pax * mu * pbz;
+      acc[B_K33] += paz * c11 * pbz + pax * mu * pbx;
+      acc[B_K12] += -(lam * pax * pb - mu * pa * pbx);
+      acc[B_K21] += (lam * pa * pbx - mu * pax * pb);
+      acc[B_K23] += (lam * pa * pbz - mu * paz * pb);
+      acc[B_K32] += -(lam * paz * pb - mu * pa * pbz);
+    }
+  }
+  double *o = ebasis + ((size_t)e * kNab + t) * B_N;
+#pragma unroll
+  for (int k = 0; k < B_N; k++) o[k] = acc[k];
+}
+
+// Per PML element node pair at one omega: the 9 complex CE coefficients
+// (CE0 on the (1,1),(1,3),(2,2),(3,1),(3,3) blocks, CE1 -- the coefficient of
+// omega*py -- on the others), entry k = 3i+j.
+__global__ void __launch_bounds__(kElemThreads, 1)
+    k_elem_pml(MeshView mv, DevTables dt, const int *__restrict__ pml_elems, PmlParams pp,
+               double logr, double2 *__restrict__ pemat, int *__restrict__ err) {
+  extern __shared__ double sm[];
+  double *shx = sm, *shz = sm + kNq * kNen, *qc = sm + 2 * kNq * kNen;
+  const int pe = blockIdx.x, e = pml_elems[pe], t = threadIdx.x;
+  const int4 ie = mv.ieng[e];
+  if (t < kNq) {
+    const int q = t, intx = q % kNint, intz = q / kNint;
+    QGeo g;
+    if (!quad_geo(mv, dt, ie, q, true, g)) atomicCAS(err, 0, e + 1);
+    dcx ex = dcx{1.0, 0.0}, ez = dcx{1.0, 0.0};
+    if (g.xdep > 2.22e-16)
+      ex = zdampfn(g.xdep, g.vel, pp.xwidth, pp.dmax, logr, pp.kappa, pp.fcent, pp.omega);
+    if (g.zdep > 2.22e-16)
+      ez = zdampfn(g.zdep, g.vel, pp.zwidth, pp.dmax, logr, pp.kappa, pp.fcent, pp.omega);
+    double *c = qc + 11 * q;
+    c[0] = g.dxdxi; c[1] = g.dxdeta; c[2] = g.dzdxi; c[3] = g.dzdeta; c[4] = g.rjac;
+    double w = dt.wts[intx] * dt.wts[intz] * g.rjac;
+    c[5] = g.lam * w;
+    c[6] = g.mu * w;
+    c[7] = ex.re; c[8] = ex.im; c[9] = ez.re; c[10] = ez.im;
+  }
+  __syncthreads();
+  for (int idx = t; idx < kNq * kNen; idx += kElemThreads) {
+    const int q = idx / kNen;
+    const double *c = qc + 11 * q;
+    const double *sl = dt.shl + 3 * (size_t)idx;
+    shx[idx] = (sl[0] * c[3] - sl[1] * c[2]) / c[4];
+    shz[idx] = -(sl[0] * c[1] - sl[1] * c[0]) / c[4];
+  }
+  __syncthreads();
+  if (t >= kNab) return;
+  const int a = t / kNen, b = t % kNen;
+  dcx acc[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) acc[k] = dcx{0.0, 0.0};
+  for (int q = 0; q < kNq; q++) {
+    const double *c = qc + 11 * q;
+    const double lam = c[5], mu = c[6], c11 = lam + 2.0 * mu;
+    const dcx ex = dcx{c[7], c[8]}, ez = dcx{c[9], c[10]};
+    const double pa = dt.shl[3 * (q * kNen + a) + 2], pb = dt.shl[3 * (q * kNen + b) + 2];
+    const dcx pax = dcx{shx[q * kNen + a] * ex.re, shx[q * kNen + a] * ex.im};
+    const dcx paz = dcx{shz[q * kNen + a] * ez.re, shz[q * kNen + a] * ez.im};
+    const dcx pbx = dcx{shx[q * kNen + b] * ex.re, shx[q * kNen + b] * ex.im};
+    const dcx pbz = dcx{shz[q * kNen + b] * ez.re, shz[q * kNen + b] * ez.im};
+    // CE0 blocks
+    dcx xx = zmul(pax, pbx), zz = zmul(paz, pbz), xz = zmul(pax, pbz), zx = zmul(paz, pbx);
+    acc[0] = zadd(acc[0], dcx{c11 * xx.re + mu * zz.re, c11 * xx.im + mu * zz.im});
+    acc[2] = zadd(acc[2], dcx{lam * xz.re + mu * zx.re, lam * xz.im + mu * zx.im});
+    acc[4] = zadd(acc[4], dcx{mu * xx.re + mu * zz.re, mu * xx.im + mu * zz.im});
+    acc[6] = zadd(acc[6], dcx{lam * zx.re + mu * xz.re, lam * zx.im + mu * xz.im});
+    acc[8] = zadd(acc[8], dcx{c11 * zz.re + mu * xx.re, c11 * zz.im + mu * xx.im});
+    // CE1 blocks: i * (...)
+    dcx t12 = dcx{-(lam * pax.re * pb - mu * pa * pbx.re), -(lam * pax.im * pb - mu * pa * pbx.im)};
+    dcx t21 = dcx{lam * pa * pbx.re - mu * pax.re * pb, lam * pa * pbx.im - mu * pax.im * pb};
+    dcx t23 = dcx{lam * pa * pbz.re - mu * paz.re * pb, lam * pa * pbz.im - mu * paz.im * pb};
+    dcx t32 = dcx{-(lam * paz.re * pb - mu * pa * pbz.re), -(lam * paz.im * pb - mu * pa * pbz.im)};
+    acc[1] = zadd(acc[1], dcx{-t12.im, t12.re});
+    acc[3] = zadd(acc[3], dcx{-t21.im, t21.re});
+    acc[5] = zadd(acc[5], dcx{-t23.im, t23.re});
+    acc[7] = zadd(acc[7], dcx{-t32.im, t32.re});
+  }
+  double2 *o = pemat + ((size_t)pe * kNab + t) * 9;
+#pragma unroll
+  for (int k = 0; k < 9; k++) o[k] = make_double2(acc[k].re, acc[k].im);
+}
+
+// block id of element node pair (a,b): position of node B in block row A
+__device__ __forceinline__ long long find_block(const long long *brptr, const int *bcol, int A,
+                                                int B) {
+  long long lo = brptr[A], hi = brptr[A + 1] - 1;
+  while (lo <= hi) {
+    long long mid = (lo + hi) >> 1;
+    int v = bcol[mid];
+    if (v == B) return mid;
+    if (v < B) lo = mid + 1;
+    else hi = mid - 1;
+  }
+  return -1;
+}
+
+__global__ void k_map_blocks(int nelem, const int *__restrict__ lm, const long long *__restrict__ brptr,
+                             const int *__restrict__ bcol, int *__restrict__ count,
+                             const int *__restrict__ ptr, int *__restrict__ cursor,
+                             int *__restrict__ list, int pass, int *__restrict__ err) {
+  long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (long long)nelem * kNab) return;
+  int e = (int)(gid / kNab), ab = (int)(gid % kNab);
+  int a = ab / kNen, b = ab % kNen;
+  int ra = lm[(size_t)e * kNee + 3 * a], rb = lm[(size_t)e * kNee + 3 * b];
+  if (ra <= 0 || rb <= 0) return;
+  long long blk = find_block(brptr, bcol, (ra - 1) / 3, (rb - 1) / 3);
+  if (blk < 0) {
+    atomicCAS(err, 0, e + 1);
+    return;
+  }
+  if (pass == 0) {
+    atomicAdd(&count[blk], 1);
+  } else {
+    int slot = atomicAdd(&cursor[blk], 1);
+    list[ptr[blk] + slot] = (int)gid;
+  }
+}
+
+__global__ void k_gather_basis(long long nblocks, const int *__restrict__ ptr,
+                               const int *__restrict__ list, const double *__restrict__ ebasis,
+                               double *__restrict__ basis) {
+  long long blk = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (blk >= nblocks) return;
+  double acc[B_N];
+#pragma unroll
+  for (int k = 0; k < B_N; k++) acc[k] = 0.0;
+  for (int i = ptr[blk]; i < ptr[blk + 1]; i++) {
+    const double *s = ebasis + (size_t)list[i] * B_N;
+#pragma unroll
+    for (int k = 0; k < B_N; k++) acc[k] += s[k];
+  }
+#pragma unroll
+  for (int k = 0; k < B_N; k++) basis[(size_t)k * nblocks + blk] = acc[k];
+}
+
+// PML structure: count the PML contributors of every block
+__global__ void k_pml_count(long long nblocks, const int *__restrict__ ptr,
+                            const int *__restrict__ list, const char *__restrict__ cdomain,
+                            int *__restrict__ pcount, int *__restrict__ isp) {
+  long long blk = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (blk >= nblocks) return;
+  int n = 0;
+  for (int i = ptr[blk]; i < ptr[blk + 1]; i++)
+    if (cdomain[list[i] / kNab] == 'A') n++;
+  pcount[blk] = n;
+  isp[blk] = n > 0 ? 1 : 0;
+}
+
+__global__ void k_pml_fill(long long nblocks, const int *__restrict__ ptr,
+                           const int *__restrict__ list, const char *__restrict__ cdomain,
+                           const int *__restrict__ isp_scan, const int *__restrict__ pml_local,
+                           const int *__restrict__ pcount_scan_by_pblk, int *__restrict__ pml_idx,
+                           int *__restrict__ plist) {
+  long long blk = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (blk >= nblocks) return;
+  bool has = false;
+  for (int i = ptr[blk]; i < ptr[blk + 1]; i++)
+    if (cdomain[list[i] / kNab] == 'A') has = true;
+  if (!has) {
+    pml_idx[blk] = -1;
+    return;
+  }
+  int pb = isp_scan[blk];
+  pml_idx[blk] = pb;
+  int o = pcount_scan_by_pblk[pb];
+  for (int i = ptr[blk]; i < ptr[blk + 1]; i++) {
+    int id = list[i], e = id / kNab;
+    if (cdomain[e] == 'A') plist[o++] = pml_local[e] * kNab + id % kNab;
+  }
+}
+
+__global__ void k_compact_counts(long long nblocks, const int *__restrict__ pcount,
+                                 const int *__restrict__ isp_scan, int *__restrict__ pcount_c) {
+  long long blk = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (blk >= nblocks) return;
+  if (pcount[blk] > 0) pcount_c[isp_scan[blk]] = pcount[blk];
+}
+
+__global__ void k_gather_pml(long long npblk, const int *__restrict__ pptr,
+                             const int *__restrict__ plist, const double2 *__restrict__ pemat,
+                             double2 *__restrict__ delta) {
+  long long pb = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (pb >= npblk) return;
+  double2 acc[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) acc[k] = make_double2(0.0, 0.0);
+  for (int i = pptr[pb]; i < pptr[pb + 1]; i++) {
+    const double2 *s = pemat + (size_t)plist[i] * 9;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      acc[k].x += s[k].x;
+      acc[k].y += s[k].y;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 9; k++) delta[pb * 9 + k] = acc[k];
+}
+
+// ---------------------------------------------------------------------------
+// the streaming kernel
+// ---------------------------------------------------------------------------
+constexpr int kStreamThreads = 256;
+constexpr int kMaxPass = 16;
+
+__device__ __forceinline__ void st_cs(double2 *p, double2 v) {
+  asm volatile("st.global.cs.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(v.x), "d"(v.y) : "memory");
+}
+
+// One launch writes systems [s0, s1) (at most kMaxPass, each to its own ring
+// slot): every thread reads the basis of one 3x3 block once and writes that
+// block of all the launch's systems.  Launches that reuse ring slots are
+// ordered by the stream.
+__global__ void __launch_bounds__(kStreamThreads)
+    k_stream(long long nblocks, const long long *__restrict__ brptr, const int *__restrict__ brow,
+             const double *__restrict__ basis, const int *__restrict__ pml_idx,
+             const double2 *__restrict__ pml_delta, long long npblk, const SysParam *__restrict__ sys,
+             int s0, int s1, double *__restrict__ ring, long long stride, int nslots) {
+  const long long nchunk = (nblocks + kStreamThreads - 1) / kStreamThreads;
+  for (long long w = blockIdx.x; w < nchunk; w += gridDim.x) {
+    const long long blk = w * kStreamThreads + threadIdx.x;
+    if (blk >= nblocks) continue;
+    double bs[B_N];
+#pragma unroll
+    for (int k = 0; k < B_N; k++) bs[k] = __ldcs(basis + (size_t)k * nblocks + blk);
+    const int A = brow[blk];
+    const long long b0 = brptr[A], deg = brptr[A + 1] - b0;
+    const long long base = 9 * b0 + 3 * (blk - b0), rs = 3 * deg;
+    const int pidx = pml_idx[blk];
+    for (int s = s0; s < s1; s++) {
+      const SysParam sp = sys[s];
+      const double w2 = sp.w2, wpy = sp.wpy, wpy2 = wpy * wpy;
+      double2 v[9];
+      v[0] = make_double2(bs[B_K11] - w2 * bs[B_MRHO] + wpy2 * bs[B_MMU], 0.0);
+      v[1] = make_double2(0.0, wpy * bs[B_K12]);
+      v[2] = make_double2(bs[B_K13], 0.0);
+      v[3] = make_double2(0.0, wpy * bs[B_K21]);
+      v[4] = make_double2(bs[B_K22] - w2 * bs[B_MRHO] + wpy2 * bs[B_ML2M], 0.0);
+      v[5] = make_double2(0.0, wpy * bs[B_K23]);
+      v[6] = make_double2(bs[B_K31], 0.0);
+      v[7] = make_double2(0.0, wpy * bs[B_K32]);
+      v[8] = make_double2(bs[B_K33] - w2 * bs[B_MRHO] + wpy2 * bs[B_MMU], 0.0);
+      if (pidx >= 0) {
+        const double2 *d = pml_delta + ((size_t)sp.pml_slot * npblk + pidx) * 9;
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+          const double2 dv = d[k];
+          const double f = (k & 1) ? wpy : 1.0;  // entries 1,3,5,7 carry omega*py
+          v[k].x += f * dv.x;
+          v[k].y += f * dv.y;
+        }
+      }
+      double2 *out = reinterpret_cast<double2 *>(ring + (size_t)(s % nslots) * stride) + base;
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) st_cs(out + i * rs + j, v[3 * i + j]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static size_t basis_smem() { return sizeof(double) * (3 * kNq * kNen + 8 * kNq); }
+static size_t pml_smem() { return sizeof(double) * (2 * kNq * kNen + 11 * kNq); }
+
+cudaError_t build_batch_structures(Ctx *c, cudaStream_t st) {
+  cudaError_t e;
+  const long long nb = c->bcsr.nblocks;
+  int *d_bcol = nullptr, *d_count = nullptr, *d_cursor = nullptr;
+  if ((e = cudaMalloc(&c->d_brptr, sizeof(long long) * (c->bcsr.nbrow + 1)))) return e;
+  if ((e = cudaMalloc(&c->d_brow, sizeof(int) * nb))) return e;
+  if ((e = cudaMallocAsync(&d_bcol, sizeof(int) * nb, st))) return e;
+  cudaMemcpyAsync(c->d_brptr, c->bcsr.brptr.data(), sizeof(long long) * (c->bcsr.nbrow + 1),
+                  cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(c->d_brow, c->bcsr.brow.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_bcol, c->bcsr.bcol.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, st);
+  if ((e = cudaMallocAsync(&d_count, sizeof(int) * (nb + 1), st))) return e;
+  if ((e = cudaMallocAsync(&d_cursor, sizeof(int) * (nb + 1), st))) return e;
+  cudaMemsetAsync(d_count, 0, sizeof(int) * (nb + 1), st);
+  cudaMemsetAsync(d_cursor, 0, sizeof(int) * (nb + 1), st);
+  if ((e = cudaMalloc(&c->d_bgptr, sizeof(int) * (nb + 1)))) return e;
+  long long tot = (long long)c->nelem * kNab;
+  unsigned g = (unsigned)((tot + 255) / 256);
+  k_map_blocks<<<g, 256, 0, st>>>(c->nelem, c->d_lm, c->d_brptr, d_bcol, d_count, nullptr, nullptr,
+                                  nullptr, 0, c->d_err);
+  if ((e = scan_counts(d_count, c->d_bgptr, nb, st))) return e;
+  int total = 0;
+  cudaMemcpyAsync(&total, c->d_bgptr + nb, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if ((e = cudaStreamSynchronize(st))) return e;
+  if ((e = cudaMalloc(&c->d_bglist, sizeof(int) * (size_t)(total > 0 ? total : 1)))) return e;
+  k_map_blocks<<<g, 256, 0, st>>>(c->nelem, c->d_lm, c->d_brptr, d_bcol, nullptr, c->d_bgptr,
+                                  d_cursor, c->d_bglist, 1, c->d_err);
+  unsigned gb = (unsigned)((nb + 255) / 256);
+  k_sort_lists<<<gb, 256, 0, st>>>(nb, c->d_bgptr, c->d_bglist, c->d_err);
+  // PML elements and blocks
+  std::vector<int> pml_elems, pml_local(c->nelem, -1);
+  for (int i = 0; i < c->nelem; i++)
+    if (c->h_cdomain[i] == 'A') {
+      pml_local[i] = (int)pml_elems.size();
+      pml_elems.push_back(i);
+    }
+  c->npml_elem = (int)pml_elems.size();
+  if ((e = cudaMalloc(&c->d_pml_idx, sizeof(int) * nb))) return e;
+  if (c->npml_elem > 0) {
+    int *d_pml_local = nullptr, *d_isp = nullptr, *d_isp_scan = nullptr, *d_pcount_c = nullptr;
+    if ((e = cudaMalloc(&c->d_pml_elems, sizeof(int) * c->npml_elem))) return e;
+    cudaMemcpyAsync(c->d_pml_elems, pml_elems.data(), sizeof(int) * c->npml_elem,
+                    cudaMemcpyHostToDevice, st);
+    if ((e = cudaMallocAsync(&d_pml_local, sizeof(int) * c->nelem, st))) return e;
+    cudaMemcpyAsync(d_pml_local, pml_local.data(), sizeof(int) * c->nelem, cudaMemcpyHostToDevice,
+                    st);
+    if ((e = cudaMallocAsync(&d_isp, sizeof(int) * (nb + 1), st))) return e;
+    if ((e = cudaMallocAsync(&d_isp_scan, sizeof(int) * (nb + 1), st))) return e;
+    cudaMemsetAsync(d_count, 0, sizeof(int) * (nb + 1), st);
+    cudaMemsetAsync(d_isp, 0, sizeof(int) * (nb + 1), st);
+    k_pml_count<<<gb, 256, 0, st>>>(nb, c->d_bgptr, c->d_bglist, c->d_cdomain, d_count, d_isp);
+    if ((e = scan_counts(d_isp, d_isp_scan, nb, st))) return e;
+    int npb = 0;
+    cudaMemcpyAsync(&npb, d_isp_scan + nb, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st))) return e;
+    c->npml_blocks = npb;
+    if ((e = cudaMallocAsync(&d_pcount_c, sizeof(int) * (npb + 1), st))) return e;
+    cudaMemsetAsync(d_pcount_c, 0, sizeof(int) * (npb + 1), st);
+    k_compact_counts<<<gb, 256, 0, st>>>(nb, d_count, d_isp_scan, d_pcount_c);
+    if ((e = cudaMalloc(&c->d_pgptr, sizeof(int) * (npb + 1)))) return e;
+    if ((e = scan_counts(d_pcount_c, c->d_pgptr, npb, st))) return e;
+    int ptot = 0;
+    cudaMemcpyAsync(&ptot, c->d_pgptr + npb, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st))) return e;
+    if ((e = cudaMalloc(&c->d_pglist, sizeof(int) * (size_t)(ptot > 0 ? ptot : 1)))) return e;
+    k_pml_fill<<<gb, 256, 0, st>>>(nb, c->d_bgptr, c->d_bglist, c->d_cdomain, d_isp_scan,
+                                   d_pml_local, c->d_pgptr, c->d_pml_idx, c->d_pglist);
+    if ((e = cudaMalloc(&c->d_pml_emat, sizeof(double2) * 9 * (size_t)c->npml_elem * kNab))) return e;
+    cudaFreeAsync(d_pml_local, st);
+    cudaFreeAsync(d_isp, st);
+    cudaFreeAsync(d_isp_scan, st);
+    cudaFreeAsync(d_pcount_c, st);
+  } else {
+    cudaMemsetAsync(c->d_pml_idx, 0xff, sizeof(int) * nb, st);
+  }
+  cudaFreeAsync(d_count, st);
+  cudaFreeAsync(d_cursor, st);
+  cudaFreeAsync(d_bcol, st);
+  if ((e = cudaFuncSetAttribute(k_elem_basis, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)basis_smem())))
+    return e;
+  if ((e = cudaFuncSetAttribute(k_elem_pml, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)pml_smem())))
+    return e;
+  return cudaGetLastError();
+}
+
+cudaError_t build_basis(Ctx *c, cudaStream_t st) {
+  cudaError_t e;
+  const long long nb = c->bcsr.nblocks;
+  if (!c->d_basis)
+    if ((e = cudaMalloc(&c->d_basis, sizeof(double) * B_N * nb))) return e;
+  double *d_eb = nullptr;
+  if ((e = cudaMallocAsync(&d_eb, sizeof(double) * B_N * (size_t)c->nelem * kNab, st))) return e;
+  k_elem_basis<<<c->nelem, kElemThreads, basis_smem(), st>>>(c->mv, c->dt, d_eb, c->d_err);
+  k_gather_basis<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(nb, c->d_bgptr, c->d_bglist, d_eb,
+                                                               c->d_basis);
+  cudaFreeAsync(d_eb, st);
+  return cudaGetLastError();
+}
+
+cudaError_t build_pml_delta(Ctx *c, const PmlParams &pp, int slot, cudaStream_t st) {
+  if (c->npml_elem == 0 || c->npml_blocks == 0) return cudaSuccess;
+  double logr = std::log(pp.rcoeff);
+  k_elem_pml<<<c->npml_elem, kElemThreads, pml_smem(), st>>>(c->mv, c->dt, c->d_pml_elems, pp, logr,
+                                                            c->d_pml_emat, c->d_err);
+  long long npb = c->npml_blocks;
+  k_gather_pml<<<(unsigned)((npb + 255) / 256), 256, 0, st>>>(
+      npb, c->d_pgptr, c->d_pglist, c->d_pml_emat, c->d_pml_delta + (size_t)slot * npb * 9);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stream_batch(Ctx *c, int n, double *ring_base, long long slot_stride,
+                                int nslots, cudaStream_t st) {
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stream, kStreamThreads, 0);
+  if (occ < 1) occ = 1;
+  const long long nchunk = (c->bcsr.nblocks + kStreamThreads - 1) / kStreamThreads;
+  const unsigned grid = (unsigned)std::min<long long>((long long)nsm * occ, nchunk);
+  const int per = std::min(kMaxPass, nslots);
+  for (int s0 = 0; s0 < n; s0 += per) {
+    const int s1 = std::min(n, s0 + per);
+    k_stream<<<grid, kStreamThreads, 0, st>>>(c->bcsr.nblocks, c->d_brptr, c->d_brow, c->d_basis,
+                                              c->d_pml_idx, c->d_pml_delta, c->npml_blocks,
+                                              c->d_sys, s0, s1, ring_base, slot_stride, nslots);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace fem25

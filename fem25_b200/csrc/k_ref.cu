@@ -1,0 +1,384 @@
+// Kernels that reproduce the reference's single-precision bookkeeping around
+// the operator: the Bielak effective force ASMB_PEFF (asmble.f90:318-377),
+// the forward misfit / adjoint source (EXRESP25D, CRESID, BPRESID4, COBJ4,
+// RESID_DRHS) and the reference-compatible virtual-force gradient
+// (CFMAT_DIST / VFORCE25 / DJACAB / DKM_VPVS, ADJFLAM_DIST).
+//
+// Compiled with -fmad=false so every COMPLEX*8 / REAL*8 operation is rounded
+// on its own, as the reference writes it.
+#include "ctx.cuh"
+#include "kcommon.cuh"
+
+namespace fem25 {
+
+// ---------------------------------------------------------------------------
+// ASMB_PEFF: PEFF(i) -= S_ij ue_j for (B,E) pairs, += for (E,B) pairs
+// ---------------------------------------------------------------------------
+__global__ void k_peff(int ndof, int nsrc, const int *__restrict__ irptr, const int *__restrict__ jcptr,
+                       const char *__restrict__ cnp, const float2 *__restrict__ a,
+                       const float2 *__restrict__ ue, float2 *__restrict__ peff) {
+  long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (long long)ndof * nsrc) return;
+  const int s = (int)(gid / ndof), row = (int)(gid % ndof);  // row 0-based
+  const float2 *u = ue + (size_t)s * ndof;
+  float br = 0.0f, bi = 0.0f;
+  const char c1 = cnp[row];
+  if (c1 == 'B' || c1 == 'E') {
+    for (int j = irptr[row] - 1; j < irptr[row + 1] - 1; j++) {
+      const int col = jcptr[j] - 1;
+      const char c2 = cnp[col];
+      const float2 av = a[j], uv = u[col];
+      const float pr = av.x * uv.x - av.y * uv.y, pi = av.x * uv.y + av.y * uv.x;
+      if (c1 == 'B' && c2 == 'E') {
+        br = br - pr;
+        bi = bi - pi;
+      } else if (c1 == 'E' && c2 == 'B') {
+        br = br + pr;
+        bi = bi + pi;
+      }
+    }
+  }
+  peff[gid] = make_float2(br, bi);
+}
+
+cudaError_t launch_peff(Ctx *c, int nsrc, const float *a_loc, const float *ue, float *peff,
+                        cudaStream_t st) {
+  long long n = (long long)c->ndof * nsrc;
+  k_peff<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(c->ndof, nsrc, c->d_irptr, c->d_jcptr,
+                                                      c->d_cnp, (const float2 *)a_loc,
+                                                      (const float2 *)ue, (float2 *)peff);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// misfit + adjoint source, one thread per (source, receiver)
+//   trig[ir] = (cos, sin) of omega*py*yrec in single precision; rot = (cos th,
+//   sin th, cos -th, sin -th) of the model azimuth (computed on the host).
+// ---------------------------------------------------------------------------
+struct cfl {
+  float re, im;
+};
+__device__ __forceinline__ cfl cmulf(cfl a, cfl b) {
+  return cfl{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+
+__global__ void k_misfit(int nsrc, int nrec, int ndof, const int *__restrict__ mrdof,
+                         const float4 *__restrict__ trig, float4 rot, const float2 *__restrict__ recv,
+                         const float2 *__restrict__ sol, const float2 *__restrict__ obs,
+                         const float *__restrict__ wghts, float2 *__restrict__ est,
+                         float2 *__restrict__ rhs, float *__restrict__ part) {
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nsrc * nrec) return;
+  const int s = gid / nrec, ir = gid % nrec;
+  const float4 tg = trig[ir];
+  const cfl cf = cfl{tg.x, tg.y}, cf2 = cfl{tg.z, tg.w};
+  cfl e3[3], o3[3];
+  for (int i = 0; i < 3; i++) {
+    int d = mrdof[3 * ir + i];
+    if (d != 0) {
+      float2 rv = recv[3 * ir + i], sv = sol[(size_t)s * ndof + d - 1];
+      e3[i] = cmulf(cmulf(cfl{rv.x, rv.y}, cfl{sv.x, sv.y}), cf);
+    } else {
+      e3[i] = cfl{0.0f, 0.0f};
+    }
+    est[((size_t)s * nrec + ir) * 3 + i] = make_float2(e3[i].re, e3[i].im);
+    float2 ov = obs[((size_t)s * nrec + ir) * 3 + i];
+    o3[i] = cfl{ov.x, ov.y};
+  }
+  const float ct = rot.x, st = rot.y;
+  cfl er[3];
+  er[0] = cfl{e3[0].re * ct - e3[1].re * st, e3[0].im * ct - e3[1].im * st};
+  er[1] = cfl{e3[0].re * st + e3[1].re * ct, e3[0].im * st + e3[1].im * ct};
+  er[2] = e3[2];
+  cfl res[3];
+  for (int i = 0; i < 3; i++) {
+    res[i] = cfl{0.0f, 0.0f};
+    part[(size_t)gid * 3 + i] = 0.0f;
+    if (o3[i].re == 0.0f && o3[i].im == 0.0f) continue;
+    cfl ob = cmulf(o3[i], cf2), es = cmulf(er[i], cf2);
+    cfl dif = cfl{ob.re - es.re, ob.im - es.im};
+    float wv = fabsf(wghts[((size_t)s * nrec + ir) * 3 + i]);
+    float w2 = wv * wv;
+    res[i] = cfl{w2 * dif.re, w2 * dif.im};
+    cfl dif0 = cfl{o3[i].re - er[i].re, o3[i].im - er[i].im};
+    part[(size_t)gid * 3 + i] = w2 * (dif0.re * dif0.re + dif0.im * dif0.im);
+  }
+  const float ct2 = rot.z, st2 = rot.w;
+  cfl rr[3];
+  rr[0] = cfl{res[0].re * ct2 - res[1].re * st2, res[0].im * ct2 - res[1].im * st2};
+  rr[1] = cfl{res[0].re * st2 + res[1].re * ct2, res[0].im * st2 + res[1].im * ct2};
+  rr[2] = res[2];
+  for (int i = 0; i < 3; i++) {
+    int d = mrdof[3 * ir + i];
+    if (d <= 0 || d > ndof) continue;
+    // receivers map to distinct DOFs (checked by the host); conjugate for
+    // the transpose solve (adjgrad.f90:519-521)
+    rhs[(size_t)s * ndof + d - 1] = make_float2(0.0f + rr[i].re, -(0.0f + rr[i].im));
+  }
+}
+
+// RESID_DRHS conjugates the whole right-hand side (adjgrad.f90:519-521): the
+// untouched entries become (0, -0)
+__global__ void k_fill_conj_zero(long long n, float2 *__restrict__ rhs) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) rhs[i] = make_float2(0.0f, -0.0f);
+}
+
+// per-source sum of the receiver partials in receiver order (COBJ4 order)
+__global__ void k_misfit_sum(int nsrc, int nrec, const float *__restrict__ part,
+                             float *__restrict__ out) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsrc) return;
+  // COBJ4 order: receivers, then components, skipping absent observations
+  float acc = 0.0f;
+  for (int k = 0; k < 3 * nrec; k++) {
+    float v = part[(size_t)s * nrec * 3 + k];
+    if (v != 0.0f) acc = acc + v;
+  }
+  out[s] = acc;
+}
+
+cudaError_t launch_misfit(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const float *d_trig,
+                          double omega, double py, double azmod, const float *d_recv,
+                          const float *sol, const float *d_obs, const float *d_wghts,
+                          float *d_est, float *rhs, float *d_misfit, cudaStream_t st) {
+  (void)omega;
+  (void)py;
+  float th = (float)azmod * 0.017453292519943295f;
+  float4 rot = make_float4(cosf(th), sinf(th), cosf(-th), sinf(-th));
+  float *d_part = nullptr;
+  cudaError_t e = cudaMallocAsync(&d_part, sizeof(float) * 3 * (size_t)nsrc * nrec, st);
+  if (e) return e;
+  const long long nrhs = (long long)nsrc * c->ndof;
+  k_fill_conj_zero<<<(unsigned)((nrhs + 255) / 256), 256, 0, st>>>(nrhs, (float2 *)rhs);
+  int n = nsrc * nrec;
+  k_misfit<<<(n + 127) / 128, 128, 0, st>>>(nsrc, nrec, c->ndof, d_mrdof, (const float4 *)d_trig,
+                                            rot, (const float2 *)d_recv, (const float2 *)sol,
+                                            (const float2 *)d_obs, d_wghts, (float2 *)d_est,
+                                            (float2 *)rhs, d_part);
+  k_misfit_sum<<<(nsrc + 127) / 128, 128, 0, st>>>(nsrc, nrec, d_part, d_misfit);
+  cudaFreeAsync(d_part, st);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// reference-compatible virtual forces: one CTA per CSC column (inversion
+// anchor), elements of MCONN in order.  DKM_VPVS (dstiff25.f:498-662) is
+// evaluated by 625 threads (node pairs) into shared memory as COMPLEX*8
+// CARG = CMPLX(DCMPLX(DME) + DKE) (vforce25.f:311-312), then 75 threads form
+// FORCEV(row) += CARG * WAVE * CWGHT in IQE order (vforce25.f:326-330).
+// ---------------------------------------------------------------------------
+constexpr int kRefThreads = 640;
+
+struct RefArgs {
+  double omega, py, vpvs2;
+  int lisp, accumulate, ncon, nnpg;
+};
+
+__global__ void __launch_bounds__(kRefThreads, 1)
+    k_ref_cfmat(MeshView mv, DevTables dt, RefArgs ra, const int *__restrict__ lm,
+                const int *__restrict__ anchor_of_col, const int *__restrict__ mconn,
+                const double *__restrict__ elem_wts, const int *__restrict__ jcsc,
+                const int *__restrict__ icsc, const float2 *__restrict__ wave,
+                float2 *__restrict__ fmat, int *__restrict__ err) {
+  extern __shared__ double sm[];
+  double *shx = sm, *shz = sm + kNq * kNen, *shn = sm + 2 * kNq * kNen;
+  double *qc = sm + 3 * kNq * kNen;                       // [kNq][8]
+  float2 *carg = reinterpret_cast<float2 *>(qc + 8 * kNq); // [75][75]
+  const int col = blockIdx.x, t = threadIdx.x;
+  const int p = anchor_of_col[col];  // 0-based anchor (INPG-1)
+  const int i1 = jcsc[col] - 1, i2 = jcsc[col + 1] - 1, nnzrow = i2 - i1;
+  float2 *forcev = fmat + i1;
+  for (int k = t; k < nnzrow; k += kRefThreads) forcev[k] = make_float2(0.0f, 0.0f);
+  // elements of the anchor, in MCONN order; without accumulation only the
+  // last one leaves a trace in FORCEV
+  int elist[8], ne = 0;
+  for (int ic = 0; ic < ra.ncon && ic < 8; ic++) {
+    int e = mconn[p + (size_t)ra.nnpg * ic];
+    if (e <= 0) break;
+    elist[ne++] = e - 1;
+  }
+  const int first = ra.accumulate ? 0 : (ne > 0 ? ne - 1 : 0);
+  const double wpy = ra.omega * ra.py, py2 = ipow2(ra.py), w2 = ipow2(ra.omega);
+  __syncthreads();
+  for (int ie_ = first; ie_ < ne; ie_++) {
+    const int e = elist[ie_];
+    const int4 ie = mv.ieng[e];
+    if (t < kNq) {
+      const int q = t, intx = q % kNint, intz = q / kNint;
+      QGeo g;
+      if (!quad_geo(mv, dt, ie, q, false, g)) atomicCAS(err, 0, e + 1);
+      // DJACAB (djac.f:90-110): DAB = sum_ia 2 alpha_ia SF(ia), alpha nonzero
+      // only at the collocated anchor
+      const int il[4] = {ie.x - 1, ie.y - 1, ie.z - 1, ie.w - 1};
+      double dab1 = 0.0, dab2 = 0.0;
+      for (int ia = 0; ia < 4; ia++) {
+        double alpha = 0.0, beta = 0.0;
+        if (il[ia] == p) {
+          alpha = sqrt((mv.lam[p] + 2.0 * mv.mu[p]) / mv.rho[p]);
+          beta = sqrt(mv.mu[p] / mv.rho[p]);
+        }
+        dab1 = dab1 + 2.0 * alpha * dt.sf[4 * q + ia];
+        dab2 = dab2 + 2.0 * beta * dt.sf[4 * q + ia];
+      }
+      double dvp, dvs;
+      if (ra.lisp) {
+        dvp = dab1;
+        dvs = dab1 / ra.vpvs2;
+      } else {
+        dvp = dab2 * ra.vpvs2;
+        dvs = dab2;
+      }
+      double *c = qc + 8 * q;
+      c[0] = g.dxdxi; c[1] = g.dxdeta; c[2] = g.dzdxi; c[3] = g.dzdeta; c[4] = g.rjac;
+      double weight = dt.wts[intx] * dt.wts[intz] * g.rjac;
+      c[5] = dvp * weight;  // DRVP
+      c[6] = dvs * weight;  // DRVS
+    }
+    __syncthreads();
+    for (int idx = t; idx < kNq * kNen; idx += kRefThreads) {
+      const int q = idx / kNen;
+      const double *c = qc + 8 * q;
+      const double *sl = dt.shl + 3 * (size_t)idx;
+      double drnxi = sl[0], drneta = sl[1];
+      shx[idx] = (drnxi * c[3] - drneta * c[2]) / c[4];
+      shz[idx] = -(drnxi * c[1] - drneta * c[0]) / c[4];
+      shn[idx] = sl[2];
+    }
+    __syncthreads();
+    if (t < kNab) {
+      const int a = t / kNen, b = t % kNen;
+      double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+      double r00 = 0.0, r11 = 0.0, r22 = 0.0, r02 = 0.0, r20 = 0.0;
+      double r01 = 0.0, r10 = 0.0, r12 = 0.0, r21 = 0.0;
+      for (int intx = 0; intx < kNint; intx++)
+        for (int intz = 0; intz < kNint; intz++) {
+          const int q = intx + kNint * intz;
+          const double drvp = qc[8 * q + 5], drvs = qc[8 * q + 6];
+          const double rm1 = w2 * py2 * drvs, rm2 = w2 * py2 * drvp;
+          const double phib = shn[q * kNen + b], phibx = shx[q * kNen + b], phibz = shz[q * kNen + b];
+          const double phia = shn[q * kNen + a], phiax = shx[q * kNen + a], phiaz = shz[q * kNen + a];
+          double rm11t1 = rm1 * phib, rm22t1 = rm2 * phib;
+          double rk11t1 = drvp * phibx, rk11t2 = drvs * phibz;
+          double rk13t1 = drvp * phibz, rk13t2 = drvs * phibx, rk13t3 = -2.0 * drvs * phibz;
+          double rk22t1 = drvs * phibx, rk22t2 = drvs * phibz;
+          double rk31t1 = drvp * phibx, rk31t2 = drvs * phibz, rk31t3 = -2.0 * drvs * phibx;
+          double rk33t1 = drvp * phibz, rk33t2 = drvs * phibx;
+          double rk12t1 = wpy * drvp * phib, rk12t2 = -2.0 * wpy * drvs * phib, rk12t3 = -wpy * drvs * phibx;
+          double rk21t1 = wpy * drvp * phibx, rk21t2 = -2.0 * wpy * drvs * phibx, rk21t3 = -wpy * drvs * phib;
+          double rk23t1 = wpy * drvp * phibz, rk23t2 = -2.0 * wpy * drvs * phibz, rk23t3 = -wpy * drvs * phib;
+          double rk32t1 = wpy * drvp * phib, rk32t2 = -2.0 * wpy * drvs * phib, rk32t3 = -wpy * drvs * phibz;
+          double rme11 = rm11t1 * phia, rme22 = rm22t1 * phia, rme33 = rme11;
+          m0 = m0 + rme11;
+          m1 = m1 + rme22;
+          m2 = m2 + rme33;
+          r00 = r00 + (rk11t1 * phiax + rk11t2 * phiaz);
+          r11 = r11 + (rk22t1 * phiax + rk22t2 * phiaz);
+          r22 = r22 + (rk33t1 * phiaz + rk33t2 * phiax);
+          r02 = r02 + (rk13t1 * phiax + rk13t2 * phiaz + rk13t3 * phiax);
+          r20 = r20 + (rk31t1 * phiaz + rk31t2 * phiax + rk31t3 * phiaz);
+          r01 = r01 - (rk12t1 * phiax + rk12t2 * phiax + rk12t3 * phia);
+          r10 = r10 + (rk21t1 * phia + rk21t2 * phia + rk21t3 * phiax);
+          r12 = r12 + (rk23t1 * phia + rk23t2 * phia + rk23t3 * phiaz);
+          r21 = r21 - (rk32t1 * phiaz + rk32t2 * phiaz + rk32t3 * phia);
+        }
+      // CARG = CMPLX(DCMPLX(DME,0) + DKE): DKE is real in every entry
+      const int ipe = 3 * a, iqe = 3 * b;
+      float2 *row0 = carg + (size_t)ipe * kNee + iqe;
+      row0[0] = make_float2(__double2float_rn(m0 + r00), __double2float_rn(0.0 + 0.0));
+      row0[1] = make_float2(__double2float_rn(0.0 + r01), __double2float_rn(0.0 + 0.0));
+      row0[2] = make_float2(__double2float_rn(0.0 + r02), __double2float_rn(0.0 + 0.0));
+      float2 *row1 = row0 + kNee;
+      row1[0] = make_float2(__double2float_rn(0.0 + r10), __double2float_rn(0.0 + 0.0));
+      row1[1] = make_float2(__double2float_rn(m1 + r11), __double2float_rn(0.0 + 0.0));
+      row1[2] = make_float2(__double2float_rn(0.0 + r12), __double2float_rn(0.0 + 0.0));
+      float2 *row2 = row1 + kNee;
+      row2[0] = make_float2(__double2float_rn(0.0 + r20), __double2float_rn(0.0 + 0.0));
+      row2[1] = make_float2(__double2float_rn(0.0 + r21), __double2float_rn(0.0 + 0.0));
+      row2[2] = make_float2(__double2float_rn(m2 + r22), __double2float_rn(0.0 + 0.0));
+    }
+    __syncthreads();
+    if (!ra.accumulate)
+      for (int k = t; k < nnzrow; k += kRefThreads) forcev[k] = make_float2(0.0f, 0.0f);
+    __syncthreads();
+    if (t < kNee) {
+      const int ipe = t;
+      const int *lme = lm + (size_t)e * kNee;
+      const int idof = lme[ipe];
+      if (idof > 0) {
+        // IBSECT on the CSC column
+        int lo = 0, hi = nnzrow - 1, inz = -1;
+        while (lo <= hi) {
+          int mid = (lo + hi) >> 1, v = icsc[i1 + mid];
+          if (v == idof) { inz = mid; break; }
+          if (v < idof) lo = mid + 1;
+          else hi = mid - 1;
+        }
+        if (inz < 0) {
+          atomicCAS(err, 0, -(col + 1));
+        } else {
+          const float cw = __double2float_rn(elem_wts[e]);
+          float fr = forcev[inz].x, fi = forcev[inz].y;
+          for (int iqe = 0; iqe < kNee; iqe++) {
+            const int jdof = lme[iqe];
+            if (jdof <= 0) continue;
+            const float2 cv = carg[(size_t)ipe * kNee + iqe], wv = wave[jdof - 1];
+            cfl t1 = cmulf(cfl{cv.x, cv.y}, cfl{wv.x, wv.y});
+            cfl t2 = cmulf(t1, cfl{cw, 0.0f});
+            fr = fr + t2.re;
+            fi = fi + t2.im;
+          }
+          forcev[inz] = make_float2(fr, fi);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ADJFLAM_DIST (adjgrad.f90:128-139) + SAXPY(-1) into GRADL (adjgrad.f90:76)
+__global__ void k_ref_adjflam(int ncol, const int *__restrict__ jcsc, const int *__restrict__ icsc,
+                              const float2 *__restrict__ fmat, const float2 *__restrict__ lam,
+                              float *__restrict__ gradl) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ncol) return;
+  float v = 0.0f;
+  for (int i = jcsc[k] - 1; i < jcsc[k + 1] - 1; i++) {
+    const float2 f = fmat[i], l = lam[icsc[i] - 1];
+    const float fr = f.x, fi = -f.y;
+    v = v - (fr * l.x - fi * l.y);
+  }
+  gradl[k] = gradl[k] + (-1.0f) * v;
+}
+
+static size_t ref_smem() {
+  return sizeof(double) * (3 * kNq * kNen + 8 * kNq) + sizeof(float2) * kNee * kNee;
+}
+
+cudaError_t launch_ref_cfmat(Ctx *c, int lisp, double vpvs, double omega, double py,
+                             const float *wave, int accumulate, cudaStream_t st) {
+  RefArgs ra;
+  ra.omega = omega;
+  ra.py = py;
+  ra.vpvs2 = vpvs * vpvs;
+  ra.lisp = lisp;
+  ra.accumulate = accumulate;
+  ra.ncon = c->rg.ncon;
+  ra.nnpg = c->nnpg;
+  cudaError_t e = cudaFuncSetAttribute(k_ref_cfmat, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)ref_smem());
+  if (e) return e;
+  k_ref_cfmat<<<c->rg.nnpinv, kRefThreads, ref_smem(), st>>>(
+      c->mv, c->dt, ra, c->d_lm, c->d_rg_anchor, c->d_mconn, c->d_elem_wts, c->d_jcsc, c->d_icsc,
+      (const float2 *)wave, c->d_fmat, c->d_err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ref_adjflam(Ctx *c, const float *adjlam, float *gradl, cudaStream_t st) {
+  int n = c->rg.nnpinv;
+  k_ref_adjflam<<<(n + 255) / 256, 256, 0, st>>>(n, c->d_jcsc, c->d_icsc, c->d_fmat,
+                                                 (const float2 *)adjlam, gradl);
+  return cudaGetLastError();
+}
+
+}  // namespace fem25

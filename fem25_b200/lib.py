@@ -1,0 +1,267 @@
+"""ctypes binding of libfem25gpu.so and the host-side context object."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfem25gpu.so")
+
+FEM25_OK = 0
+FEM25_PREC_FP64 = 0
+FEM25_PREC_TF32X3 = 1
+_CODES = {1: "ERR_ARG", 2: "ERR_JACOBIAN", 3: "ERR_PATTERN", 4: "ERR_CUDA", 5: "ERR_ALLOC",
+          6: "ERR_GRAPH", 7: "ERR_UNSUPPORTED", 8: "ERR_NOMESH"}
+
+
+class Fem25Error(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"fem25 {_CODES.get(code, code)} ({code}): {msg}")
+        self.code = code
+
+
+class Mesh(C.Structure):
+    _fields_ = [("nelem", C.c_int), ("nnpg", C.c_int), ("nord", C.c_int), ("ldisp", C.c_int),
+                ("ieng", C.c_void_p), ("cdomain", C.c_void_p), ("cnnpg", C.c_void_p),
+                ("xlocs", C.c_void_p), ("zlocs", C.c_void_p), ("xd", C.c_void_p),
+                ("zd", C.c_void_p), ("ecoeff", C.c_void_p), ("dens", C.c_void_p),
+                ("xwidth", C.c_double), ("zwidth", C.c_double),
+                ("rcoeff_srf", C.c_double), ("dmax_srf", C.c_double), ("kappa_srf", C.c_double),
+                ("fcent_srf", C.c_double), ("rcoeff_bdy", C.c_double), ("dmax_bdy", C.c_double),
+                ("kappa_bdy", C.c_double), ("fcent_bdy", C.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libfem25gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m fem25_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        vp, i, d, ll = C.c_void_p, C.c_int, C.c_double, C.c_longlong
+        L.fem25_graph_build.argtypes = [vp, C.POINTER(vp)]
+        L.fem25_graph_info.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(ll)]
+        L.fem25_graph_copy.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.fem25_graph_free.argtypes = [vp]
+        L.fem25_graph_free.restype = None
+        L.fem25_create.argtypes = [vp, i, ll, vp, vp, vp, vp, i, C.POINTER(vp)]
+        L.fem25_destroy.argtypes = [vp]
+        L.fem25_destroy.restype = None
+        L.fem25_last_error.argtypes = [vp, C.c_char_p, i]
+        L.fem25_sizes.argtypes = [vp, C.POINTER(i), C.POINTER(ll), C.POINTER(ll)]
+        L.fem25_update_model.argtypes = [vp, vp, vp]
+        L.fem25_asmble_driver.argtypes = [vp, i, C.c_char, d, d, vp]
+        L.fem25_assemble_dev.argtypes = [vp, C.c_char, d, d, vp, vp, vp]
+        L.fem25_assemble_batch_dev.argtypes = [vp, i, vp, vp, vp, vp, ll, i, vp]
+        L.fem25_peff_dev.argtypes = [vp, i, vp, vp, vp, vp]
+        L.fem25_gradient_dev.argtypes = [vp, i, vp, vp, i, vp, vp, i, vp, vp]
+        L.fem25_ref_gradient_dev.argtypes = [vp, C.c_char_p, d, d, d, vp, vp, i, vp, vp]
+        L.fem25_ref_gradient_info.argtypes = [vp, C.POINTER(i), C.POINTER(ll), vp]
+        L.fem25_misfit_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.fem25_profile_enable.argtypes = [vp, i]
+        L.fem25_profile_ms.argtypes = [vp, i, C.POINTER(d)]
+        _lib = L
+    return _lib
+
+
+def _np(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _ptr(t):
+    """Device pointer of a torch tensor (or an int address)."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return C.c_void_p(t)
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(s):
+    if s is None:
+        return None
+    if isinstance(s, int):
+        return C.c_void_p(s)
+    return C.c_void_p(s.cuda_stream)
+
+
+class _MeshKeep:
+    """Contiguous numpy copies of the mesh arrays + the C struct pointing at them."""
+
+    def __init__(self, mesh):
+        self.a = dict(ieng=np.ascontiguousarray(mesh.ieng, np.int32),
+                      cdomain=np.ascontiguousarray(mesh.cdomain, np.uint8),
+                      cnnpg=np.ascontiguousarray(mesh.cnnpg, np.uint8),
+                      xlocs=np.ascontiguousarray(mesh.xlocs, np.float64),
+                      zlocs=np.ascontiguousarray(mesh.zlocs, np.float64),
+                      xd=np.ascontiguousarray(mesh.xd, np.float64),
+                      zd=np.ascontiguousarray(mesh.zd, np.float64),
+                      ecoeff=np.ascontiguousarray(mesh.ecoeff, np.float64),
+                      dens=np.ascontiguousarray(mesh.dens, np.float64))
+        s = Mesh()
+        s.nelem, s.nnpg, s.nord, s.ldisp = mesh.nelem, mesh.nnpg, mesh.nord, 0
+        for k, v in self.a.items():
+            setattr(s, k, _np(v))
+        s.xwidth, s.zwidth = mesh.xwidth, mesh.zwidth
+        s.rcoeff_srf, s.rcoeff_bdy = mesh.rcoeff
+        s.dmax_srf, s.dmax_bdy = mesh.dmax
+        s.kappa_srf, s.kappa_bdy = mesh.kappa
+        s.fcent_srf, s.fcent_bdy = mesh.fcent
+        self.s = s
+        self.ptr = C.cast(C.pointer(s), C.c_void_p)
+
+
+def mesh_struct(mesh):
+    return _MeshKeep(mesh)
+
+
+class Graph:
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+
+def graph_build(mesh):
+    """GEN_GRAPH25: IEN, LM, IRPTR, JCPTR (1-based) and CNP of a mesh."""
+    L = lib()
+    mk = _MeshKeep(mesh)
+    h = C.c_void_p()
+    r = L.fem25_graph_build(mk.ptr, C.byref(h))
+    if r:
+        raise Fem25Error(r, "graph build failed")
+    nnp, ndof, nz = C.c_int(), C.c_int(), C.c_longlong()
+    L.fem25_graph_info(h, C.byref(nnp), C.byref(ndof), C.byref(nz))
+    nen = (mesh.nord + 1) ** 2
+    ien = np.empty((mesh.nelem, nen), np.int32)
+    lm = np.empty((mesh.nelem, nen, 3), np.int32)
+    irptr = np.empty(ndof.value + 1, np.int32)
+    jcptr = np.empty(nz.value, np.int32)
+    cnp = np.empty(ndof.value, np.uint8)
+    L.fem25_graph_copy(h, _np(ien), _np(lm), _np(irptr), _np(jcptr), _np(cnp))
+    L.fem25_graph_free(h)
+    return Graph(nnp=nnp.value, ndof=ndof.value, nzero=nz.value, ien=ien, lm=lm, irptr=irptr,
+                 jcptr=jcptr, cnp=cnp)
+
+
+class Context:
+    """Device context for one mesh (fem25_create)."""
+
+    def __init__(self, mesh, graph=None, device=0):
+        L = lib()
+        self.mesh = mesh
+        self.g = graph_build(mesh) if graph is None else graph
+        self._mk = _MeshKeep(mesh)
+        h = C.c_void_p()
+        g = self.g
+        self._lm = np.ascontiguousarray(g.lm, np.int32)
+        self._irptr = np.ascontiguousarray(g.irptr, np.int32)
+        self._jcptr = np.ascontiguousarray(g.jcptr, np.int32)
+        self._cnp = np.ascontiguousarray(g.cnp, np.uint8)
+        r = L.fem25_create(self._mk.ptr, g.ndof, g.nzero, _np(self._lm), _np(self._irptr),
+                           _np(self._jcptr), _np(self._cnp), device, C.byref(h))
+        if r:
+            raise Fem25Error(r, "fem25_create failed (see stderr)")
+        self.h = h
+        self.device = device
+        self.ndof = g.ndof
+        self.nzero = g.nzero
+        nb = C.c_longlong()
+        L.fem25_sizes(h, None, None, C.byref(nb))
+        self.nblocks = nb.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fem25_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, r):
+        if r:
+            buf = C.create_string_buffer(512)
+            lib().fem25_last_error(self.h, buf, 512)
+            raise Fem25Error(r, buf.value.decode(errors="replace"))
+
+    # ---- profiling
+    def profile(self, enable=True):
+        self._check(lib().fem25_profile_enable(self.h, 1 if enable else 0))
+
+    def profile_ms(self, which):
+        v = C.c_double()
+        self._check(lib().fem25_profile_ms(self.h, which, C.byref(v)))
+        return v.value
+
+    # ---- model
+    def update_model(self, ecoeff, dens):
+        e = np.ascontiguousarray(ecoeff, np.float64)
+        d = np.ascontiguousarray(dens, np.float64)
+        self._check(lib().fem25_update_model(self.h, _np(e), _np(d)))
+
+    # ---- assembly
+    def asmble_driver(self, cftype, freq, py, out=None):
+        """ASMBLE_DRIVER: host COMPLEX*8 CDIST(NZLOC) (mid%A_LOC order)."""
+        if out is None:
+            out = np.empty(self.nzero, np.complex64)
+        ptr = C.c_void_p(out.data_ptr()) if hasattr(out, "data_ptr") else _np(out)
+        self._check(lib().fem25_asmble_driver(self.h, self.nzero, cftype.encode(), freq, py, ptr))
+        return out
+
+    def assemble(self, cftype, freq, py, out128=None, out64=None, stream=None):
+        self._check(lib().fem25_assemble_dev(self.h, cftype.encode(), freq, py, _ptr(out128),
+                                             _ptr(out64), _stream(stream)))
+
+    def assemble_batch(self, cftypes, freqs, pys, ring, slot_stride, nslots, stream=None):
+        """Systems k -> ring + (k % nslots) * slot_stride doubles (complex128)."""
+        n = len(freqs)
+        ct = np.frombuffer("".join(cftypes).encode(), np.uint8).copy() if isinstance(
+            cftypes, (list, tuple)) else np.full(n, ord(cftypes), np.uint8)
+        f = np.ascontiguousarray(freqs, np.float64)
+        p = np.ascontiguousarray(pys, np.float64)
+        self._check(lib().fem25_assemble_batch_dev(self.h, n, _np(ct), _np(f), _np(p), _ptr(ring),
+                                                   slot_stride, nslots, _stream(stream)))
+
+    # ---- Bielak effective force
+    def asmb_peff(self, nsrc, a_loc, ue, peff, stream=None):
+        self._check(lib().fem25_peff_dev(self.h, nsrc, _ptr(a_loc), _ptr(ue), _ptr(peff),
+                                         _stream(stream)))
+
+    # ---- gradients
+    def gradient(self, freqs, pys, nsrc, u, lam, grad, prec=FEM25_PREC_FP64, stream=None):
+        f = np.ascontiguousarray(freqs, np.float64)
+        p = np.ascontiguousarray(pys, np.float64)
+        self._check(lib().fem25_gradient_dev(self.h, len(f), _np(f), _np(p), nsrc, _ptr(u),
+                                             _ptr(lam), prec, _ptr(grad), _stream(stream)))
+
+    def ref_gradient_info(self):
+        n, nz = C.c_int(), C.c_longlong()
+        maskg = np.zeros(self.mesh.nnpg, np.int32)
+        self._check(lib().fem25_ref_gradient_info(self.h, C.byref(n), C.byref(nz), _np(maskg)))
+        return n.value, nz.value, maskg
+
+    def cfmat_adjgrad(self, cinvtype, vpvs, freq, py, wave, adjlam, gradl, accumulate=False,
+                      stream=None):
+        self._check(lib().fem25_ref_gradient_dev(self.h, cinvtype.encode(), vpvs, freq, py,
+                                                 _ptr(wave), _ptr(adjlam), 1 if accumulate else 0,
+                                                 _ptr(gradl), _stream(stream)))
+
+    # ---- misfit
+    def misfit(self, nsrc, mrdof, yrec, freq, py, azmod, recv, sol, obs, wghts, rhs, stream=None):
+        nrec = mrdof.shape[0]
+        est = np.zeros((nsrc, nrec, 3), np.complex64)
+        mis = np.zeros(nsrc, np.float32)
+        self._check(lib().fem25_misfit_dev(
+            self.h, nsrc, nrec, _np(np.ascontiguousarray(mrdof, np.int32)),
+            _np(np.ascontiguousarray(yrec, np.float64)), freq, py, azmod,
+            _np(np.ascontiguousarray(recv, np.complex64)), _ptr(sol),
+            _np(np.ascontiguousarray(obs, np.complex64)),
+            _np(np.ascontiguousarray(wghts, np.float32)), _np(est), _ptr(rhs), _np(mis),
+            _stream(stream)))
+        return est, mis

@@ -1,0 +1,163 @@
+/*
+ * fem25gpu.h -- C ABI of the B200 (sm_100a) library for the fem25 hot path:
+ * 2.5D spectral-element operator assembly into CSR per (omega, py), the
+ * Bielak effective force, the forward misfit / adjoint source and the adjoint
+ * gradient.
+ *
+ * Conventions kept from the reference Fortran (bakerb845/fem25) so that its
+ * drivers can bind these entry points through ISO_C_BINDING unchanged:
+ *   - every entry point returns an int status, 0 = OK (the reference's IERR);
+ *     nothing aborts or exits; the last error text is kept per context;
+ *   - index arrays hold Fortran 1-based values (IENG, LM, IRPTR, JCPTR ...)
+ *     and two-dimensional arrays keep their Fortran column-major layout;
+ *   - buffers belong to the caller; complex values are interleaved (re, im).
+ * A context is not re-entrant; several contexts may run on separate streams.
+ * `stream` arguments are cudaStream_t values passed as void* (NULL = default).
+ */
+#ifndef FEM25GPU_H
+#define FEM25GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FEM25_OK 0
+#define FEM25_ERR_ARG 1          /* bad argument or size mismatch            */
+#define FEM25_ERR_JACOBIAN 2     /* undefined/negative Jacobian, cjac.f:115-125 */
+#define FEM25_ERR_PATTERN 3      /* (row,col) not in CSR, asmble.f90:296-300  */
+#define FEM25_ERR_CUDA 4         /* CUDA runtime error                         */
+#define FEM25_ERR_ALLOC 5        /* device or host allocation failed           */
+#define FEM25_ERR_GRAPH 6        /* mesh graph construction failed            */
+#define FEM25_ERR_UNSUPPORTED 7  /* anisotropy, dispersion, CINVTYPE 'PS' ...  */
+#define FEM25_ERR_NOMESH 8       /* context lacks a table the call needs      */
+
+/* Mesh as read by RDMESHBK (mesh_utils.f:982-1165), fields of MESH_INFO
+ * (fwd_struc.h:10-141).  Isotropic (INPTYP 1/2), NGNOD = 4 anchors. */
+typedef struct fem25_mesh {
+    int nelem;               /* NELEM                                        */
+    int nnpg;                /* NNPG, anchor nodes                           */
+    int nord;                /* NORD, polynomial order (NLXI = NORD+1)       */
+    int ldisp;               /* dispersive media flag (must be 0)            */
+    const int *ieng;         /* IENG(4,NELEM), 1-based                        */
+    const char *cdomain;     /* CDOMAIN(NELEM): 'I','E','A'                   */
+    const char *cnnpg;       /* CNNPG(NNPG): CHARACTER(2), 2 bytes per anchor */
+    const double *xlocs, *zlocs;  /* anchor coordinates (m)                   */
+    const double *xd, *zd;   /* anchor depth into the PML (m)                 */
+    const double *ecoeff;    /* ECOEFF(NNPG,2): lambda then mu (Pa)           */
+    const double *dens;      /* DENS(NNPG) (kg/m^3)                           */
+    double xwidth, zwidth;   /* PML widths (max XD, max ZD)                   */
+    double rcoeff_srf, dmax_srf, kappa_srf, fcent_srf;  /* CFTYPE 'S'         */
+    double rcoeff_bdy, dmax_bdy, kappa_bdy, fcent_bdy;  /* CFTYPE 'B'         */
+} fem25_mesh;
+
+typedef struct fem25_graph fem25_graph;  /* host graph (opaque)            */
+typedef struct fem25_ctx fem25_ctx;      /* device context (opaque)        */
+
+/* ---- mesh graph: replaces GEN_GRAPH25 (graph25_driver.f90:2-72) ----------
+ * GENIEN -> GENID -> GENLM -> CONNECT -> GENCRS_QUICK -> CNMESH with the
+ * reference's node de-duplication tolerance (1e-8), Dirichlet rules on 'A'
+ * elements, element-order DOF numbering and sorted, de-duplicated columns. */
+int fem25_graph_build(const fem25_mesh *m, fem25_graph **out);
+int fem25_graph_info(const fem25_graph *g, int *nnp, int *ndof, long long *nzero);
+/* any pointer may be NULL; sizes: ien[NEN*NELEM], lm[3*NEN*NELEM],
+ * irptr[NDOF+1], jcptr[NZERO], cnp[NDOF] */
+int fem25_graph_copy(const fem25_graph *g, int *ien, int *lm, int *irptr, int *jcptr, char *cnp);
+void fem25_graph_free(fem25_graph *g);
+
+/* ---- context --------------------------------------------------------------
+ * Copies mesh, model and graph (LM, IRPTR, JCPTR, CNP as GEN_GRAPH25 leaves
+ * them in MESH_INFO) to `device` and builds the element-to-nonzero map.
+ * Returns FEM25_ERR_JACOBIAN if an element has a non-positive Jacobian and
+ * FEM25_ERR_PATTERN if an element entry has no CSR slot. */
+int fem25_create(const fem25_mesh *m, int ndof, long long nzero, const int *lm,
+                 const int *irptr, const int *jcptr, const char *cnp, int device,
+                 fem25_ctx **out);
+void fem25_destroy(fem25_ctx *ctx);
+int fem25_last_error(const fem25_ctx *ctx, char *buf, int n);
+int fem25_sizes(const fem25_ctx *ctx, int *ndof, long long *nzero, long long *nblocks);
+
+/* New model per outer iteration (UPDMOD, gengmask.f90:657): ECOEFF(NNPG,2)
+ * and DENS(NNPG), host pointers.  Invalidates the batched-assembly basis. */
+int fem25_update_model(fem25_ctx *ctx, const double *ecoeff, const double *dens);
+
+/* ---- assembly -------------------------------------------------------------
+ * Drop-in for ASMBLE_DRIVER(NZLOC,CFTYPE,FREQ,PY,MSH,CDIST,IERR)
+ * (asmble.f90:1-2): fills the host COMPLEX*8 CDIST(NZLOC) (mid%A_LOC order)
+ * with the reference's own arithmetic (FP64 element matrices, FP32
+ * accumulation in element order).  Single process: NZLOC = NZERO. */
+int fem25_asmble_driver(fem25_ctx *ctx, int nzloc, char cftype, double freq, double py,
+                        float *cdist);
+
+/* Plain per-(omega,py) FP64 assembly on device buffers.  csr128: complex128
+ * values summed in FP64 in element order (NZERO x 2 doubles); csr64: the
+ * reference's COMPLEX*8 accumulation.  Either may be NULL. */
+int fem25_assemble_dev(fem25_ctx *ctx, char cftype, double freq, double py, double *csr128,
+                       float *csr64, void *stream);
+
+/* Batched assembly of n systems (cftype[k], freq[k], py[k]) into complex128
+ * device slots: system k goes to ring_base + (k % nslots) * slot_stride
+ * doubles (slot_stride >= 2*NZERO).  Uses the per-mesh affine basis (built
+ * on first use) and one persistent streaming launch. */
+int fem25_assemble_batch_dev(fem25_ctx *ctx, int n, const char *cftype, const double *freq,
+                             const double *py, double *ring_base, long long slot_stride,
+                             int nslots, void *stream);
+
+/* ---- Bielak effective force ------------------------------------------------
+ * Drop-in for ASMB_PEFF (asmble.f90:318-377) for nsrc background fields at
+ * once: ue, peff are COMPLEX*8 [nsrc][NDOF]; a_loc is the COMPLEX*8 CSR.
+ * Device pointers. */
+int fem25_peff_dev(fem25_ctx *ctx, int nsrc, const float *a_loc, const float *ue, float *peff,
+                   void *stream);
+
+/* ---- adjoint gradient -------------------------------------------------------
+ * Exact gradient of the misfit with respect to the anchor-node lambda, mu and
+ * rho:  grad[m*NNPG + p] += sum_s Re( lam_s^H (dA/dm_p) u_s )
+ * for m = lambda, mu, rho, summed over the n (omega, py) pairs; fields are
+ * complex128 device arrays [pair][src][NDOF]; grad is FP64 on the device.
+ * Elements of domain 'A' (PML) do not contribute.
+ * prec: FEM25_PREC_FP64 (plain FP64 kernels) or FEM25_PREC_TF32X3
+ * (split-precision tensor-core contraction, FP64 cross-pair reduction). */
+#define FEM25_PREC_FP64 0
+#define FEM25_PREC_TF32X3 1
+int fem25_gradient_dev(fem25_ctx *ctx, int npairs, const double *freq, const double *py,
+                       int nsrc, const double *u, const double *lam, int prec, double *grad,
+                       void *stream);
+
+/* Reference-compatible gradient (CFMAT_DIST hessloc.f90:1-133 + ADJFLAM_DIST
+ * adjgrad.f90:88-145 + SAXPY adjgrad.f90:76): derivative in Vp ('PP') or Vs
+ * ('SS') at the inversion anchors of GENGMASK, density-normalised element
+ * operator DKM_VPVS, ELEM_WTS weighting, COMPLEX*8 virtual forces.  wave and
+ * adjlam are COMPLEX*8 [NDOF] device arrays, gradl REAL*4 [NNPINV] device
+ * array updated in place.  accumulate = 0 keeps the reference's behaviour of
+ * keeping only the last connected element's force (vforce25.f:274-280). */
+int fem25_ref_gradient_dev(fem25_ctx *ctx, const char *cinvtype, double vpvs, double freq,
+                           double py, const float *wave, const float *adjlam, int accumulate,
+                           float *gradl, void *stream);
+int fem25_ref_gradient_info(fem25_ctx *ctx, int *nnpinv, long long *nz_fdist,
+                            int *maskg /* [NNPG], nullable */);
+
+/* ---- forward misfit + adjoint source ---------------------------------------
+ * EXRESP25D (locrec2d.f:867-925) + rotation + CRESID/BPRESID4 L2 + COBJ4 +
+ * RESID_DRHS (adjgrad.f90:448-523) for nsrc solutions at once.
+ * sol: COMPLEX*8 [nsrc][NDOF] device; mrdof: MRDOF(3,NREC) host;
+ * yrec[NREC], recv COMPLEX*8 (3,NREC), obs COMPLEX*8 [nsrc](3,NREC),
+ * wghts REAL*4 [nsrc](3,NREC) host; outputs: est COMPLEX*8 [nsrc](3,NREC)
+ * host, rhs COMPLEX*8 [nsrc][NDOF] device (conjugated, ready for the
+ * transpose solve), misfit[nsrc] host (sum |w|^2 |obs-est|^2, not halved). */
+int fem25_misfit_dev(fem25_ctx *ctx, int nsrc, int nrec, const int *mrdof, const double *yrec,
+                     double freq, double py, double azmod, const float *recv, const float *sol,
+                     const float *obs, const float *wghts, float *est, float *rhs, float *misfit,
+                     void *stream);
+
+/* ---- profiling ----------------------------------------------------------------
+ * With profiling enabled the library records CUDA events on the launching
+ * stream around its dominant kernels; fem25_profile_ms returns the duration
+ * of the last launch: which = 0 the batched streaming kernel, which = 1 the
+ * plain element + gather kernels of fem25_assemble_dev. */
+int fem25_profile_enable(fem25_ctx *ctx, int enable);
+int fem25_profile_ms(fem25_ctx *ctx, int which, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FEM25GPU_H */

@@ -1,0 +1,250 @@
+"""GPU parity of libfem25gpu (through its C ABI) against the CPU oracle.
+
+Tolerances (CSR values are compared per row against the row's largest
+magnitude, the definition used for every CSR error in this repository):
+  * plain FP64 assembly vs oracle FP64:            <= 1e-12 (expected bit-exact)
+  * COMPLEX*8 CDIST (reference FP32 accumulation): bit-exact
+  * batched affine assembly vs oracle FP64:        <= 1e-12
+  * exact gradient FP64 vs oracle:                 <= 1e-10 relative (2-norm)
+  * reference-compatible gradient, P_eff, misfit:  bit-exact
+"""
+import numpy as np
+import pytest
+
+import oracle
+from fem25_b200 import FEM25_PREC_FP64, Context, Fem25Error, synth
+from tests import helpers
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def _dev():
+    return torch.device("cuda:0")
+
+
+@pytest.fixture(scope="module")
+def case0():
+    mesh, pairs, _ = synth.make_config(0)
+    g = oracle.graph_build(mesh)
+    ctx = Context(mesh, g)
+    yield mesh, pairs, g, ctx
+    ctx.close()
+
+
+def test_plain_assembly_matches_oracle(case0):
+    mesh, pairs, g, ctx = case0
+    for (f, py) in (pairs[0], pairs[7], pairs[15]):
+        ref128, ref64 = oracle.asmble(mesh, g, "B", f, py)
+        o128 = torch.zeros(g.nzero, dtype=torch.complex128, device=_dev())
+        o64 = torch.zeros(g.nzero, dtype=torch.complex64, device=_dev())
+        ctx.assemble("B", f, py, o128, o64)
+        torch.cuda.synchronize()
+        a128 = o128.cpu().numpy()
+        a64 = o64.cpu().numpy()
+        err = helpers.row_norm_err(a128, ref128, g.irptr)
+        assert err <= 1e-12, err
+        exact = np.mean(a128 == ref128)
+        assert exact == 1.0, f"bit-identical fraction {exact}"
+        assert np.array_equal(a64.view(np.uint32), ref64.view(np.uint32))
+
+
+def test_asmble_driver_host_buffer(case0):
+    mesh, pairs, g, ctx = case0
+    f, py = pairs[4]
+    _, ref64 = oracle.asmble(mesh, g, "S", f, py)
+    out = ctx.asmble_driver("S", f, py)
+    assert np.array_equal(out.view(np.uint32), ref64.view(np.uint32))
+
+
+def test_batched_matches_oracle(case0):
+    mesh, pairs, g, ctx = case0
+    sel = [pairs[0], pairs[5], pairs[11], pairs[15], (0.8, 2.0e-4), (0.3, 0.0)]
+    n = len(sel)
+    stride = 2 * g.nzero
+    ring = torch.zeros(n * stride, dtype=torch.float64, device=_dev())
+    ctx.assemble_batch(["B"] * n, [p[0] for p in sel], [p[1] for p in sel], ring, stride, n)
+    torch.cuda.synchronize()
+    r = ring.view(n, g.nzero, 2).cpu().numpy()
+    for k, (f, py) in enumerate(sel):
+        ref128, _ = oracle.asmble(mesh, g, "B", f, py, want64=False)
+        got = r[k, :, 0] + 1j * r[k, :, 1]
+        err = helpers.row_norm_err(got, ref128, g.irptr)
+        assert err <= 1e-12, (k, err)
+
+
+def test_batched_ring_wraps(case0):
+    mesh, pairs, g, ctx = case0
+    sel = pairs[:7]
+    stride = 2 * g.nzero + 2  # padded slots
+    ring = torch.zeros(3 * stride, dtype=torch.float64, device=_dev())
+    ctx.assemble_batch("S", [p[0] for p in sel], [p[1] for p in sel], ring, stride, 3)
+    torch.cuda.synchronize()
+    r = ring.view(3, stride).cpu().numpy()
+    # system 6 lands in slot 0, system 4 in slot 1, system 5 in slot 2
+    for k in (4, 5, 6):
+        ref128, _ = oracle.asmble(mesh, g, "S", *sel[k], want64=False)
+        got = r[k % 3, :2 * g.nzero:2] + 1j * r[k % 3, 1:2 * g.nzero:2]
+        assert helpers.row_norm_err(got, ref128, g.irptr) <= 1e-12
+
+
+def test_peff_matches_oracle(case0):
+    mesh, pairs, g, ctx = case0
+    _, a64 = oracle.asmble(mesh, g, "B", *pairs[3])
+    rng = np.random.default_rng(3)
+    nsrc = 3
+    ue = (rng.standard_normal((nsrc, g.ndof)) + 1j * rng.standard_normal((nsrc, g.ndof))).astype(np.complex64)
+    d_a = torch.from_numpy(a64).to(_dev())
+    d_u = torch.from_numpy(ue).to(_dev())
+    d_p = torch.zeros((nsrc, g.ndof), dtype=torch.complex64, device=_dev())
+    ctx.asmb_peff(nsrc, d_a, d_u, d_p)
+    got = d_p.cpu().numpy()
+    for s in range(nsrc):
+        ref = oracle.peff(g, a64, ue[s])
+        assert np.array_equal(got[s].view(np.uint32), ref.view(np.uint32))
+
+
+def test_gradient_fp64_matches_oracle():
+    mesh, pairs, _ = synth.make_config(0, nx=10, nz=6)
+    g = oracle.graph_build(mesh)
+    ctx = Context(mesh, g)
+    rng = np.random.default_rng(11)
+    use = [pairs[1], pairs[6], pairs[13]]
+    nsrc = 3
+    u = rng.standard_normal((len(use), nsrc, g.ndof)) + 1j * rng.standard_normal((len(use), nsrc, g.ndof))
+    lam = rng.standard_normal((len(use), nsrc, g.ndof)) + 1j * rng.standard_normal((len(use), nsrc, g.ndof))
+    ref = np.zeros((3, mesh.nnpg))
+    for p, (f, py) in enumerate(use):
+        oracle.grad_exact(mesh, g, f, py, u[p], lam[p], out=ref)
+    d_u = torch.from_numpy(u).to(_dev())
+    d_l = torch.from_numpy(lam).to(_dev())
+    d_g = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=_dev())
+    ctx.gradient([p[0] for p in use], [p[1] for p in use], nsrc, d_u, d_l, d_g, FEM25_PREC_FP64)
+    got = d_g.cpu().numpy()
+    for m in range(3):
+        rel = np.linalg.norm(got[m] - ref[m]) / np.linalg.norm(ref[m])
+        assert rel <= 1e-10, (m, rel)
+    ctx.close()
+
+
+def test_gradient_finite_difference_gpu_pipeline():
+    """GPU assembly + host direct solve + GPU misfit + GPU gradient vs central
+    finite differences (h = 1e-4 relative, Richardson-extrapolated)."""
+    mesh, pairs, _ = synth.make_config(0, nx=12, nz=6)
+    g = oracle.graph_build(mesh)
+    ctx = Context(mesh, g)
+    mrdof = helpers.surface_receivers(mesh, g, 8)
+    fwi = helpers.DirectFWI(g, mrdof)
+    use = [pairs[3], pairs[10]]
+    rng = np.random.default_rng(8)
+    f_src = helpers.point_force_rhs(g, mrdof[len(mrdof) // 2])
+    obs = [(rng.standard_normal(len(fwi.rdofs)) + 1j * rng.standard_normal(len(fwi.rdofs))) * 1e-9
+           for _ in use]
+
+    def chi_grad(want):
+        chi, grad = 0.0, torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=_dev())
+        for (f, py), ob in zip(use, obs):
+            o128 = torch.zeros(g.nzero, dtype=torch.complex128, device=_dev())
+            ctx.assemble("B", f, py, o128)
+            c, u, lam = fwi.misfit_and_fields(o128.cpu().numpy(), f_src, ob)
+            chi += c
+            if want:
+                ctx.gradient([f], [py], 1, torch.from_numpy(u[None, None]).to(_dev()),
+                             torch.from_numpy(lam[None, None]).to(_dev()), grad)
+        return chi, grad.cpu().numpy()
+
+    _, grad = chi_grad(True)
+    touch = np.zeros(mesh.nnpg, bool)
+    for e in range(mesh.nelem):
+        if chr(mesh.cdomain[e]) == "A":
+            touch[mesh.ieng[e] - 1] = True
+    base = np.stack([mesh.ecoeff[0], mesh.ecoeff[1], mesh.dens])
+
+    def chi_at(m3):
+        ctx.update_model(m3[:2], m3[2])
+        return chi_grad(False)[0]
+
+    h = 1e-4
+    for trial in range(3):
+        dm = rng.standard_normal((3, mesh.nnpg)) * ~touch * base
+        an = float(np.sum(grad * dm))
+        fd1 = (chi_at(base + h * dm) - chi_at(base - h * dm)) / (2 * h)
+        fd2 = (chi_at(base + h / 2 * dm) - chi_at(base - h / 2 * dm)) / h
+        fd = (4 * fd2 - fd1) / 3
+        assert abs(fd - an) <= 1e-6 * abs(an), (trial, fd, an)
+    ctx.update_model(base[:2], base[2])
+    ctx.close()
+
+
+@pytest.mark.parametrize("cinv,accumulate", [("PP", False), ("SS", False), ("PP", True)])
+def test_reference_gradient_matches_oracle(case0, cinv, accumulate):
+    mesh, pairs, g, ctx = case0
+    rg = oracle.RefGrad(mesh, g)
+    nnpinv, nz, maskg = ctx.ref_gradient_info()
+    assert nnpinv == rg.nnpinv and nz == rg.nz and np.array_equal(maskg, rg.maskg)
+    rng = np.random.default_rng(4)
+    wave = (rng.standard_normal(g.ndof) + 1j * rng.standard_normal(g.ndof)).astype(np.complex64)
+    lam = (rng.standard_normal(g.ndof) + 1j * rng.standard_normal(g.ndof)).astype(np.complex64)
+    f, py = pairs[5]
+    fm = rg.cfmat(f, py, wave, lisp=(cinv == "PP"), accumulate=accumulate)
+    ref = rg.adjflam(fm, lam)
+    d_g = torch.zeros(nnpinv, dtype=torch.float32, device=_dev())
+    ctx.cfmat_adjgrad(cinv, 1.7320508075688772, f, py, torch.from_numpy(wave).to(_dev()),
+                      torch.from_numpy(lam).to(_dev()), d_g, accumulate=accumulate)
+    got = d_g.cpu().numpy()
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+def test_reference_gradient_rejects_ps(case0):
+    mesh, pairs, g, ctx = case0
+    d = torch.zeros(g.ndof, dtype=torch.complex64, device=_dev())
+    gl = torch.zeros(16, dtype=torch.float32, device=_dev())
+    with pytest.raises(Fem25Error) as ei:
+        ctx.cfmat_adjgrad("PS", 1.7, 0.5, 0.0, d, d, gl)
+    assert ei.value.code == 7
+
+
+def test_misfit_matches_oracle(case0):
+    mesh, pairs, g, ctx = case0
+    mrdof = helpers.surface_receivers(mesh, g, 20)
+    nrec = len(mrdof)
+    rng = np.random.default_rng(9)
+    nsrc = 2
+    f, py = pairs[6]
+    yrec = rng.uniform(-500, 500, nrec)
+    recv = (1 + 0.1j * rng.standard_normal((nrec, 3))).astype(np.complex64)
+    sol = (rng.standard_normal((nsrc, g.ndof)) + 1j * rng.standard_normal((nsrc, g.ndof))).astype(np.complex64)
+    obs = (rng.standard_normal((nsrc, nrec, 3)) + 1j * rng.standard_normal((nsrc, nrec, 3))).astype(np.complex64)
+    obs[0, 3, 1] = 0  # an absent observation
+    w = rng.uniform(0.5, 1.5, (nsrc, nrec, 3)).astype(np.float32)
+    d_sol = torch.from_numpy(sol).to(_dev())
+    d_rhs = torch.zeros((nsrc, g.ndof), dtype=torch.complex64, device=_dev())
+    est, mis = ctx.misfit(nsrc, mrdof, yrec, f, py, 12.5, recv, d_sol, obs, w, d_rhs)
+    rhs = d_rhs.cpu().numpy()
+    for s in range(nsrc):
+        e_ref, r_ref, m_ref = oracle.misfit(g.ndof, mrdof, yrec, f, py, 12.5, recv, sol[s], obs[s], w[s])
+        assert np.array_equal(est[s].view(np.uint32), e_ref.view(np.uint32))
+        assert np.array_equal(rhs[s].view(np.uint32), r_ref.view(np.uint32))
+        assert np.float32(m_ref) == mis[s]
+
+
+def test_jacobian_error_is_reported():
+    mesh, _, _ = synth.make_config(0, nx=6, nz=4)
+    g = oracle.graph_build(mesh)
+    # fold one interior element: swap two anchors
+    bad = mesh.ieng.copy()
+    e = [k for k in range(mesh.nelem) if chr(mesh.cdomain[k]) == "I"][0]
+    bad[e, [1, 3]] = bad[e, [3, 1]]
+    mesh.ieng = bad
+    with pytest.raises(Fem25Error) as ei:
+        Context(mesh, g)
+    assert ei.value.code == 2
+
+
+def test_nzloc_mismatch_is_rejected(case0):
+    mesh, pairs, g, ctx = case0
+    from fem25_b200.lib import lib as L
+    import ctypes
+    buf = np.zeros(4, np.complex64)
+    r = L().fem25_asmble_driver(ctx.h, 4, b"B", 0.5, 0.0, buf.ctypes.data_as(ctypes.c_void_p))
+    assert r == 1

@@ -1,0 +1,176 @@
+"""CPU checks of the oracle (the CPU restatement of the reference hot path).
+
+The reference ships no golden vectors for this path, so the oracle is pinned
+by closed-form properties of its tables, element invariants, its own
+committed fixtures (tests/golden) and a finite-difference check of the
+gradient through a full assemble + direct solve."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from fem25_b200 import synth
+from tests import helpers
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_lobatto_rule_closed_form():
+    for n in (5, 13):
+        x, w = oracle.lobatto(n)
+        # interior nodes are the roots of P'_{n-1}
+        P = np.polynomial.legendre.Legendre.basis(n - 1)
+        roots = np.sort(P.deriv().roots().real)
+        assert np.allclose(x[1:-1], roots, atol=1e-14)
+        assert x[0] == -1.0 and x[-1] == 1.0
+        assert abs(w.sum() - 2.0) < 1e-14
+        # exact for polynomials up to degree 2n-3
+        for k in range(0, 2 * n - 2):
+            exact = 0.0 if k % 2 else 2.0 / (k + 1)
+            assert abs(np.sum(w * x ** k) - exact) < 1e-13
+
+
+def test_shape_function_tables():
+    xw, shl = oracle.tables(4)
+    xi = xw[0]
+    assert xi[6] == 0.0  # midpoint forced to zero (dshl.f:145)
+    gll, _ = oracle.lobatto(5)
+    gll[2] = 0.0
+    # N_a = l_i(xi) l_j(eta), a = j*5 + i  (dshl.f:41-62)
+    def lag(k, t, deriv=False):
+        others = [gll[m] for m in range(5) if m != k]
+        p = np.poly1d(np.poly(others)) / np.prod([gll[k] - o for o in others])
+        return (p.deriv() if deriv else p)(t)
+    for iz in (0, 3, 12):
+        for ix in (0, 5, 6):
+            for a in (0, 7, 24):
+                i, j = a % 5, a // 5
+                ref_n = lag(i, xi[ix]) * lag(j, xi[iz])
+                ref_dx = lag(i, xi[ix], True) * lag(j, xi[iz])
+                ref_dz = lag(i, xi[ix]) * lag(j, xi[iz], True)
+                got = shl[iz, ix, a]
+                assert abs(got[2] - ref_n) < 1e-13
+                assert abs(got[0] - ref_dx) < 1e-12
+                assert abs(got[1] - ref_dz) < 1e-12
+    # partition of unity and zero-sum derivatives at every quadrature point
+    assert np.allclose(shl[..., 2].sum(-1), 1.0, atol=1e-13)
+    assert np.allclose(shl[..., 0].sum(-1), 0.0, atol=1e-12)
+    assert np.allclose(shl[..., 1].sum(-1), 0.0, atol=1e-12)
+
+
+def test_element_matrix_invariants(small_case):
+    mesh, _ = small_case
+    ie = [e for e in range(mesh.nelem) if chr(mesh.cdomain[e]) == "I"][0]
+    f, py = 0.5, 1.3e-4
+    me, ce = oracle.element_matrix(mesh, ie, "B", f, py)
+    A = me + ce
+    # KM25ISOQ is Hermitian for real media (estiff25.f:142-150)
+    assert np.abs(A - A.conj().T).max() < 1e-9 * np.abs(A).max()
+    # static (omega = 0): rigid translations in x, y, z are in the null space
+    me0, ce0 = oracle.element_matrix(mesh, ie, "B", 1e-12, 0.0)
+    K0 = me0 + ce0
+    for comp in range(3):
+        t = np.zeros(75)
+        t[comp::3] = 1.0
+        assert np.abs(K0 @ t).max() < 1e-9 * np.abs(K0).max()
+    # mass: -omega^2 sum_ab M_ab over one component = -omega^2 int rho dA
+    me1, _ = oracle.element_matrix(mesh, ie, "B", 1.0, 0.0)
+    mass = -me1[0::3, 0::3].sum() / (2 * np.pi) ** 2
+    ia = mesh.ieng[ie] - 1
+    x, z = mesh.xlocs[ia], mesh.zlocs[ia]
+    area = 0.5 * abs(np.dot(x, np.roll(z, -1)) - np.dot(z, np.roll(x, -1)))
+    rho_mean = mesh.dens[ia].mean()
+    assert abs(mass / (area * rho_mean) - 1.0) < 1e-12
+
+
+def test_oracle_c64_is_fp32_of_c128(small_case):
+    mesh, pairs = small_case
+    g = oracle.graph_build(mesh)
+    c128, c64 = oracle.asmble(mesh, g, "B", *pairs[3])
+    err = helpers.row_norm_err(c64.astype(np.complex128), c128, g.irptr)
+    assert err < 5e-7
+
+
+def test_graph_structure(small_case):
+    mesh, _ = small_case
+    g = oracle.graph_build(mesh)
+    assert g.irptr[0] == 1 and g.irptr[-1] - 1 == g.nzero
+    rows = np.repeat(np.arange(g.ndof), np.diff(g.irptr))
+    cols = g.jcptr - 1
+    # sorted, distinct columns per row and a symmetric pattern
+    assert np.all((np.diff(cols) > 0) | (np.diff(rows) > 0))
+    s = set(zip(rows.tolist(), cols.tolist()))
+    assert all((c, r) in s for r, c in list(s)[:2000])
+    # every DOF classified A/E/I/B
+    assert set(bytes(g.cnp)) <= set(b"AEIB")
+
+
+def test_golden_fixtures():
+    path = os.path.join(GOLDEN, "oracle_small.npz")
+    if not os.path.exists(path):
+        pytest.skip("golden fixtures not generated")
+    ref = np.load(path)
+    from tests.golden.make_golden import compute
+    got = compute()
+    for k in ref.files:
+        a, b = ref[k], got[k]
+        if np.issubdtype(a.dtype, np.integer) or a.dtype == np.uint8:
+            assert np.array_equal(a, b), k
+        else:
+            assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), k
+
+
+def test_oracle_gradient_finite_difference(small_case):
+    """Exact lambda/mu/rho adjoint of the oracle vs central differences of the
+    L2 misfit through assemble + direct solve (h = 1e-4 relative)."""
+    mesh, pairs = small_case
+    g = oracle.graph_build(mesh)
+    mrdof = helpers.surface_receivers(mesh, g, 6)
+    fwi = helpers.DirectFWI(g, mrdof)
+    use = [pairs[2], pairs[9]]
+    rng = np.random.default_rng(5)
+    f_src = helpers.point_force_rhs(g, mrdof[len(mrdof) // 2])
+    obs = [rng.standard_normal(len(fwi.rdofs)) * 1e-9 + 1j * rng.standard_normal(len(fwi.rdofs)) * 1e-9
+           for _ in use]
+
+    def chi_grad(m, want_grad):
+        chi = 0.0
+        grad = np.zeros((3, mesh.nnpg))
+        for (f, py), ob in zip(use, obs):
+            c128, _ = oracle.asmble(m, g, "B", f, py, want64=False)
+            c, u, lam = fwi.misfit_and_fields(c128, f_src, ob)
+            chi += c
+            if want_grad:
+                oracle.grad_exact(m, g, f, py, u[None], lam[None], out=grad)
+        return chi, grad
+
+    chi0, grad = chi_grad(mesh, True)
+    # perturb anchors that touch no PML element
+    touch = np.zeros(mesh.nnpg, bool)
+    for e in range(mesh.nelem):
+        if chr(mesh.cdomain[e]) == "A":
+            touch[mesh.ieng[e] - 1] = True
+    base = np.stack([mesh.ecoeff[0], mesh.ecoeff[1], mesh.dens])
+    h = 1e-4
+
+    def cfd(dm, hh):
+        mp, mm = _perturbed(mesh, base + hh * dm), _perturbed(mesh, base - hh * dm)
+        return (chi_grad(mp, False)[0] - chi_grad(mm, False)[0]) / (2 * hh)
+
+    for trial in range(3):
+        d = rng.standard_normal((3, mesh.nnpg)) * ~touch
+        dm = d * base
+        an = float(np.sum(grad * dm))
+        # central differences at h and h/2, Richardson-extrapolated to remove
+        # the O(h^2) truncation term
+        fd = (4.0 * cfd(dm, h / 2) - cfd(dm, h)) / 3.0
+        assert abs(fd - an) <= 1e-6 * abs(an), (trial, fd, an)
+
+
+def _perturbed(mesh, m3):
+    import copy
+    m = copy.copy(mesh)
+    m.ecoeff = np.ascontiguousarray(m3[:2])
+    m.dens = np.ascontiguousarray(m3[2])
+    return m
