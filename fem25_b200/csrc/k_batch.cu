@@ -10,6 +10,8 @@
 // The basis is summed once per mesh into 3x3 node blocks of the CSR (12 reals
 // per block); the streaming kernel then reads each block's basis once per
 // pass and writes it for B systems: an HBM-write-bound stream.
+#include <cstdlib>
+
 #include "ctx.cuh"
 #include "kcommon.cuh"
 
@@ -283,56 +285,274 @@ __device__ __forceinline__ void st_cs(double2 *p, double2 v) {
   asm volatile("st.global.cs.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(v.x), "d"(v.y) : "memory");
 }
 
-// One launch writes systems [s0, s1) (at most kMaxPass, each to its own ring
-// slot): every thread reads the basis of one 3x3 block once and writes that
-// block of all the launch's systems.  Launches that reuse ring slots are
-// ordered by the stream.
-__global__ void __launch_bounds__(kStreamThreads)
-    k_stream(long long nblocks, const long long *__restrict__ brptr, const int *__restrict__ brow,
-             const double *__restrict__ basis, const int *__restrict__ pml_idx,
-             const double2 *__restrict__ pml_delta, long long npblk, const SysParam *__restrict__ sys,
-             int s0, int s1, double *__restrict__ ring, long long stride, int nslots) {
-  const long long nchunk = (nblocks + kStreamThreads - 1) / kStreamThreads;
-  for (long long w = blockIdx.x; w < nchunk; w += gridDim.x) {
-    const long long blk = w * kStreamThreads + threadIdx.x;
-    if (blk >= nblocks) continue;
-    double bs[B_N];
-#pragma unroll
-    for (int k = 0; k < B_N; k++) bs[k] = __ldcs(basis + (size_t)k * nblocks + blk);
-    const int A = brow[blk];
-    const long long b0 = brptr[A], deg = brptr[A + 1] - b0;
-    const long long base = 9 * b0 + 3 * (blk - b0), rs = 3 * deg;
-    const int pidx = pml_idx[blk];
-    for (int s = s0; s < s1; s++) {
-      const SysParam sp = sys[s];
-      const double w2 = sp.w2, wpy = sp.wpy, wpy2 = wpy * wpy;
-      double2 v[9];
-      v[0] = make_double2(bs[B_K11] - w2 * bs[B_MRHO] + wpy2 * bs[B_MMU], 0.0);
-      v[1] = make_double2(0.0, wpy * bs[B_K12]);
-      v[2] = make_double2(bs[B_K13], 0.0);
-      v[3] = make_double2(0.0, wpy * bs[B_K21]);
-      v[4] = make_double2(bs[B_K22] - w2 * bs[B_MRHO] + wpy2 * bs[B_ML2M], 0.0);
-      v[5] = make_double2(0.0, wpy * bs[B_K23]);
-      v[6] = make_double2(bs[B_K31], 0.0);
-      v[7] = make_double2(0.0, wpy * bs[B_K32]);
-      v[8] = make_double2(bs[B_K33] - w2 * bs[B_MRHO] + wpy2 * bs[B_MMU], 0.0);
-      if (pidx >= 0) {
-        const double2 *d = pml_delta + ((size_t)sp.pml_slot * npblk + pidx) * 9;
-#pragma unroll
-        for (int k = 0; k < 9; k++) {
-          const double2 dv = d[k];
-          const double f = (k & 1) ? wpy : 1.0;  // entries 1,3,5,7 carry omega*py
-          v[k].x += f * dv.x;
-          v[k].y += f * dv.y;
-        }
-      }
-      double2 *out = reinterpret_cast<double2 *>(ring + (size_t)(s % nslots) * stride) + base;
-#pragma unroll
-      for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) st_cs(out + i * rs + j, v[3 * i + j]);
+// basis slot of CSR entry (i, j) of a 3x3 block
+__device__ __constant__ int kEntrySlot[9] = {B_K11, B_K12, B_K13, B_K21, B_K22,
+                                             B_K23, B_K31, B_K32, B_K33};
+
+// Per-entry "primary" basis value in CSR order (K0_ij on the real entries,
+// K1_ij on the entries that carry i*omega*py) and a packed descriptor
+// desc = block << 4 | i << 2 | j.  One warp per block row: the three CSR rows
+// of a node are contiguous ([9 b0, 9 b1)), row i holds 3 deg entries, entry r
+// of a row is block b0 + r/3, component r%3.
+__global__ void k_build_prim(int nbrow, const long long *__restrict__ brptr,
+                             const double *__restrict__ basis, long long nblocks,
+                             double *__restrict__ prim, unsigned *__restrict__ desc) {
+  const int lane = threadIdx.x & 31;
+  const long long nwarp = (long long)gridDim.x * blockDim.x / 32;
+  for (long long A = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32; A < nbrow; A += nwarp) {
+    const long long b0 = brptr[A];
+    const int deg = (int)(brptr[A + 1] - b0), rl = 3 * deg;
+    for (int nl = lane; nl < 9 * deg; nl += 32) {
+      const int i = (nl >= rl) + (nl >= 2 * rl);
+      const int r = nl - i * rl, t = r / 3, j = r - 3 * t;
+      prim[9 * b0 + nl] = basis[(size_t)kEntrySlot[3 * i + j] * nblocks + b0 + t];
+      desc[9 * b0 + nl] = ((unsigned)(b0 + t) << 4) | (unsigned)(i << 2) | (unsigned)j;
     }
   }
+}
+
+// One launch writes systems [s0, s1) (at most kMaxPass, each to its own ring
+// slot).  Grid-stride over the CSR entries: each thread takes UNR entries
+// (n, n + G, ...), issues all their loads (primary value and descriptor,
+// then the block's mass terms and PML index) before any store, and writes
+// each entry for every system of the launch.  Consecutive threads hold
+// consecutive entries, so each warp store writes 512 contiguous bytes.
+// Launches that reuse ring slots are ordered by the stream.
+template <int UNR>
+__global__ void __launch_bounds__(kStreamThreads)
+    k_stream(long long nzero, const double *__restrict__ prim, const unsigned *__restrict__ desc,
+             const double *__restrict__ basis, long long nblocks, const int *__restrict__ pml_idx,
+             const double2 *__restrict__ pml_delta, long long npblk, const SysParam *__restrict__ sys,
+             int s0, int s1, double *__restrict__ ring, long long stride, int nslots) {
+  __shared__ SysParam sp[kMaxPass];
+  __shared__ double2 *outp[kMaxPass];
+  const int ns = s1 - s0;
+  if (threadIdx.x < ns) {
+    sp[threadIdx.x] = sys[s0 + threadIdx.x];
+    outp[threadIdx.x] =
+        reinterpret_cast<double2 *>(ring + (size_t)((s0 + threadIdx.x) % nslots) * stride);
+  }
+  __syncthreads();
+  const long long G = (long long)gridDim.x * blockDim.x;
+  const double *mrho = basis + (size_t)B_MRHO * nblocks;
+  const double *mmu = basis + (size_t)B_MMU * nblocks;
+  const double *ml2m = basis + (size_t)B_ML2M * nblocks;
+  for (long long n0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; n0 < nzero; n0 += UNR * G) {
+    double p[UNR], mr[UNR], mc[UNR];
+    unsigned d[UNR];
+    int pidx[UNR];
+#pragma unroll
+    for (int u = 0; u < UNR; u++) {
+      const long long n = n0 + u * G;
+      d[u] = 0u;
+      p[u] = 0.0;
+      if (n < nzero) {
+        p[u] = __ldcs(prim + n);
+        d[u] = __ldcs(desc + n);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < UNR; u++) {
+      const unsigned blk = d[u] >> 4, i = (d[u] >> 2) & 3u, j = d[u] & 3u;
+      mr[u] = 0.0;
+      mc[u] = 0.0;
+      if (i == j) {
+        mr[u] = mrho[blk];
+        mc[u] = (i == 1u) ? ml2m[blk] : mmu[blk];
+      }
+      pidx[u] = pml_idx[blk];
+    }
+    for (int k = 0; k < ns; k++) {
+      const double w2 = sp[k].w2, wpy = sp[k].wpy, wpy2 = wpy * wpy;
+      const int slot = sp[k].pml_slot;
+      double2 *o = outp[k];
+#pragma unroll
+      for (int u = 0; u < UNR; u++) {
+        const long long n = n0 + u * G;
+        if (n >= nzero) continue;
+        const unsigned i = (d[u] >> 2) & 3u, j = d[u] & 3u;
+        const bool odd = (i + j) & 1u;
+        double2 v;
+        if (odd) v = make_double2(0.0, wpy * p[u]);
+        else v = make_double2(p[u] - w2 * mr[u] + wpy2 * mc[u], 0.0);  // mr = mc = 0 off the diagonal
+        if (pidx[u] >= 0) {
+          const double2 dv = pml_delta[((size_t)slot * npblk + pidx[u]) * 9 + 3 * i + j];
+          const double f = odd ? wpy : 1.0;
+          v.x += f * dv.x;
+          v.y += f * dv.y;
+        }
+        st_cs(o + n, v);
+      }
+    }
+  }
+}
+
+// Same as k_stream<1>, software-pipelined over the grid-stride loop: while
+// the stores of entry n are issued, the descriptor/primary loads of n+2G and
+// the block loads (mass terms, PML index) of n+G are already in flight.
+struct EntryIn {
+  double p, mr, mc;
+  unsigned d;
+  int pidx;
+};
+
+__global__ void __launch_bounds__(kStreamThreads)
+    k_stream_pipe(long long nzero, const double *__restrict__ prim, const unsigned *__restrict__ desc,
+                  const double *__restrict__ basis, long long nblocks, const int *__restrict__ pml_idx,
+                  const double2 *__restrict__ pml_delta, long long npblk,
+                  const SysParam *__restrict__ sys, int s0, int s1, double *__restrict__ ring,
+                  long long stride, int nslots) {
+  __shared__ SysParam sp[kMaxPass];
+  __shared__ double2 *outp[kMaxPass];
+  const int ns = s1 - s0;
+  if (threadIdx.x < ns) {
+    sp[threadIdx.x] = sys[s0 + threadIdx.x];
+    outp[threadIdx.x] =
+        reinterpret_cast<double2 *>(ring + (size_t)((s0 + threadIdx.x) % nslots) * stride);
+  }
+  __syncthreads();
+  const long long G = (long long)gridDim.x * blockDim.x;
+  const double *mrho = basis + (size_t)B_MRHO * nblocks;
+  const double *mmu = basis + (size_t)B_MMU * nblocks;
+  const double *ml2m = basis + (size_t)B_ML2M * nblocks;
+  auto ld1 = [&](long long n, double &p, unsigned &d) {
+    p = 0.0;
+    d = 0u;
+    if (n < nzero) {
+      p = __ldcs(prim + n);
+      d = __ldcs(desc + n);
+    }
+  };
+  auto ld2 = [&](unsigned d, double &mr, double &mc, int &pidx) {
+    const unsigned blk = d >> 4, i = (d >> 2) & 3u, j = d & 3u;
+    mr = 0.0;
+    mc = 0.0;
+    if (i == j) {
+      mr = mrho[blk];
+      mc = (i == 1u) ? ml2m[blk] : mmu[blk];
+    }
+    pidx = pml_idx[blk];
+  };
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double pa, pb, mra, mca;
+  unsigned da, db;
+  int pia;
+  ld1(n, pa, da);
+  ld1(n + G, pb, db);
+  ld2(da, mra, mca, pia);
+  for (; n < nzero; n += G) {
+    double pc;
+    unsigned dc;
+    ld1(n + 2 * G, pc, dc);        // two ahead
+    double mrb, mcb;
+    int pib;
+    ld2(db, mrb, mcb, pib);         // one ahead
+    const unsigned i = (da >> 2) & 3u, j = da & 3u;
+    const bool odd = (i + j) & 1u;
+    for (int k = 0; k < ns; k++) {
+      const double w2 = sp[k].w2, wpy = sp[k].wpy;
+      double2 v;
+      if (odd) v = make_double2(0.0, wpy * pa);
+      else v = make_double2(pa - w2 * mra + (wpy * wpy) * mca, 0.0);
+      if (pia >= 0) {
+        const double2 dv = pml_delta[((size_t)sp[k].pml_slot * npblk + pia) * 9 + 3 * i + j];
+        const double f = odd ? wpy : 1.0;
+        v.x += f * dv.x;
+        v.y += f * dv.y;
+      }
+      st_cs(outp[k] + n, v);
+    }
+    pa = pb; da = db; mra = mrb; mca = mcb; pia = pib;
+    pb = pc; db = dc;
+  }
+}
+
+// TMA variant: each CTA computes a chunk of T consecutive entries for all
+// systems of the launch into a shared-memory staging buffer (one contiguous
+// T*16-byte run per system), then one thread hands every run to the TMA unit
+// with cp.async.bulk.global.shared::cta (untiled bulk store: 16-byte aligned
+// addresses, sizes a multiple of 16).  Two staging buffers alternate, so the
+// bulk stores of chunk c drain while chunk c+1 is computed.
+__device__ __forceinline__ void bulk_store(void *gdst, const void *ssrc, unsigned bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(ssrc);
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(s),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read1() {
+  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+template <int T>
+__global__ void __launch_bounds__(T)
+    k_stream_tma(long long nzero, const double *__restrict__ prim, const unsigned *__restrict__ desc,
+                 const double *__restrict__ basis, long long nblocks, const int *__restrict__ pml_idx,
+                 const double2 *__restrict__ pml_delta, long long npblk,
+                 const SysParam *__restrict__ sys, int s0, int s1, double *__restrict__ ring,
+                 long long stride, int nslots) {
+  extern __shared__ __align__(128) double2 stage[];  // [2][kMaxPass][T]
+  __shared__ SysParam sp[kMaxPass];
+  __shared__ double2 *outp[kMaxPass];
+  const int ns = s1 - s0;
+  if (threadIdx.x < ns) {
+    sp[threadIdx.x] = sys[s0 + threadIdx.x];
+    outp[threadIdx.x] =
+        reinterpret_cast<double2 *>(ring + (size_t)((s0 + threadIdx.x) % nslots) * stride);
+  }
+  __syncthreads();
+  const double *mrho = basis + (size_t)B_MRHO * nblocks;
+  const double *mmu = basis + (size_t)B_MMU * nblocks;
+  const double *ml2m = basis + (size_t)B_ML2M * nblocks;
+  const long long nchunk = (nzero + T - 1) / T;
+  int it = 0;
+  for (long long c = blockIdx.x; c < nchunk; c += gridDim.x, it++) {
+    double2 *buf = stage + (size_t)(it & 1) * kMaxPass * T;
+    if (it >= 2) {
+      // the bulk stores issued from this buffer two chunks ago must have
+      // finished reading it
+      if (threadIdx.x == 0) bulk_wait_read1();
+      __syncthreads();
+    }
+    const long long n0 = c * T, n = n0 + threadIdx.x;
+    if (n < nzero) {
+      const double p = __ldcs(prim + n);
+      const unsigned d = __ldcs(desc + n);
+      const unsigned blk = d >> 4, i = (d >> 2) & 3u, j = d & 3u;
+      double mr = 0.0, mc = 0.0;
+      if (i == j) {
+        mr = mrho[blk];
+        mc = (i == 1u) ? ml2m[blk] : mmu[blk];
+      }
+      const int pidx = pml_idx[blk];
+      const bool odd = (i + j) & 1u;
+      for (int k = 0; k < ns; k++) {
+        const double w2 = sp[k].w2, wpy = sp[k].wpy;
+        double2 v;
+        if (odd) v = make_double2(0.0, wpy * p);
+        else v = make_double2(p - w2 * mr + (wpy * wpy) * mc, 0.0);
+        if (pidx >= 0) {
+          const double2 dv = pml_delta[((size_t)sp[k].pml_slot * npblk + pidx) * 9 + 3 * i + j];
+          const double f = odd ? wpy : 1.0;
+          v.x += f * dv.x;
+          v.y += f * dv.y;
+        }
+        buf[k * T + threadIdx.x] = v;
+      }
+    }
+    fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const long long cnt = min((long long)T, nzero - n0);
+      for (int k = 0; k < ns; k++) bulk_store(outp[k] + n0, buf + k * T, (unsigned)(cnt * 16));
+      bulk_commit();
+    }
+  }
+  if (threadIdx.x == 0) bulk_wait_all();
 }
 
 // ---------------------------------------------------------------------------
@@ -439,6 +659,13 @@ cudaError_t build_basis(Ctx *c, cudaStream_t st) {
   k_gather_basis<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(nb, c->d_bgptr, c->d_bglist, d_eb,
                                                                c->d_basis);
   cudaFreeAsync(d_eb, st);
+  if (!c->d_prim) {
+    if ((e = cudaMalloc(&c->d_prim, sizeof(double) * (size_t)c->nzero))) return e;
+    if ((e = cudaMalloc(&c->d_desc, sizeof(unsigned) * (size_t)c->nzero))) return e;
+  }
+  const long long g = ((long long)c->bcsr.nbrow * 32 + 255) / 256;
+  k_build_prim<<<(unsigned)std::min<long long>(g, 1 << 20), 256, 0, st>>>(
+      c->bcsr.nbrow, c->d_brptr, c->d_basis, nb, c->d_prim, c->d_desc);
   return cudaGetLastError();
 }
 
@@ -453,23 +680,111 @@ cudaError_t build_pml_delta(Ctx *c, const PmlParams &pp, int slot, cudaStream_t 
   return cudaGetLastError();
 }
 
+template <int UNR>
+static cudaError_t stream_range(Ctx *c, int s0, int s1, double *ring_base, long long slot_stride,
+                                int nslots, cudaStream_t st) {
+  int nsm = 0, occ = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stream<UNR>, kStreamThreads, 0);
+  if (occ < 1) occ = 1;
+  const long long grid_need = (c->nzero + kStreamThreads - 1) / kStreamThreads;
+  const unsigned grid = (unsigned)std::min<long long>((long long)nsm * occ, grid_need);
+  k_stream<UNR><<<grid, kStreamThreads, 0, st>>>(c->nzero, c->d_prim, c->d_desc, c->d_basis,
+                                                 c->bcsr.nblocks, c->d_pml_idx, c->d_pml_delta,
+                                                 c->npml_blocks, c->d_sys, s0, s1, ring_base,
+                                                 slot_stride, nslots);
+  return cudaGetLastError();
+}
+
+static cudaError_t stream_pipe(Ctx *c, int s0, int s1, double *ring_base, long long slot_stride,
+                               int nslots, cudaStream_t st) {
+  int nsm = 0, occ = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stream_pipe, kStreamThreads, 0);
+  if (occ < 1) occ = 1;
+  const long long grid_need = (c->nzero + kStreamThreads - 1) / kStreamThreads;
+  const unsigned grid = (unsigned)std::min<long long>((long long)nsm * occ, grid_need);
+  k_stream_pipe<<<grid, kStreamThreads, 0, st>>>(c->nzero, c->d_prim, c->d_desc, c->d_basis,
+                                                 c->bcsr.nblocks, c->d_pml_idx, c->d_pml_delta,
+                                                 c->npml_blocks, c->d_sys, s0, s1, ring_base,
+                                                 slot_stride, nslots);
+  return cudaGetLastError();
+}
+
+template <int T>
+static cudaError_t stream_tma(Ctx *c, int s0, int s1, double *ring_base, long long slot_stride,
+                              int nslots, cudaStream_t st) {
+  const size_t smem = sizeof(double2) * 2 * kMaxPass * T;
+  cudaError_t e = cudaFuncSetAttribute(k_stream_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e) return e;
+  int nsm = 0, occ = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stream_tma<T>, T, smem);
+  if (occ < 1) occ = 1;
+  const long long nchunk = (c->nzero + T - 1) / T;
+  const unsigned grid = (unsigned)std::min<long long>((long long)nsm * occ, nchunk);
+  k_stream_tma<T><<<grid, T, smem, st>>>(c->nzero, c->d_prim, c->d_desc, c->d_basis,
+                                         c->bcsr.nblocks, c->d_pml_idx, c->d_pml_delta,
+                                         c->npml_blocks, c->d_sys, s0, s1, ring_base, slot_stride,
+                                         nslots);
+  return cudaGetLastError();
+}
+
+constexpr int kNumStreamVariants = 6;
+static cudaError_t stream_variant(Ctx *c, int v, int s0, int s1, double *ring_base,
+                                  long long slot_stride, int nslots, cudaStream_t st) {
+  switch (v) {
+    case 0: return stream_range<1>(c, s0, s1, ring_base, slot_stride, nslots, st);
+    case 1: return stream_range<2>(c, s0, s1, ring_base, slot_stride, nslots, st);
+    case 2: return stream_range<4>(c, s0, s1, ring_base, slot_stride, nslots, st);
+    case 3: return stream_pipe(c, s0, s1, ring_base, slot_stride, nslots, st);
+    case 4: return stream_tma<64>(c, s0, s1, ring_base, slot_stride, nslots, st);
+    default: return stream_tma<128>(c, s0, s1, ring_base, slot_stride, nslots, st);
+  }
+}
+
+// The first batch of a context times the streaming variants (1, 2 or 4
+// entries per thread, software-pipelined, TMA bulk stores) on its first launch -- each writes the same values -- and keeps the
+// fastest for the life of the context.
 cudaError_t launch_stream_batch(Ctx *c, int n, double *ring_base, long long slot_stride,
                                 int nslots, cudaStream_t st) {
-  int nsm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-  int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stream, kStreamThreads, 0);
-  if (occ < 1) occ = 1;
-  const long long nchunk = (c->bcsr.nblocks + kStreamThreads - 1) / kStreamThreads;
-  const unsigned grid = (unsigned)std::min<long long>((long long)nsm * occ, nchunk);
   const int per = std::min(kMaxPass, nslots);
-  for (int s0 = 0; s0 < n; s0 += per) {
-    const int s1 = std::min(n, s0 + per);
-    k_stream<<<grid, kStreamThreads, 0, st>>>(c->bcsr.nblocks, c->d_brptr, c->d_brow, c->d_basis,
-                                              c->d_pml_idx, c->d_pml_delta, c->npml_blocks,
-                                              c->d_sys, s0, s1, ring_base, slot_stride, nslots);
+  cudaError_t e;
+  int s0 = 0;
+  if (c->stream_variant < 0) {
+    const char *env = std::getenv("FEM25_STREAM_VARIANT");
+    if (env) {
+      c->stream_variant = std::min(kNumStreamVariants - 1, std::max(0, std::atoi(env)));
+    } else {
+      cudaEvent_t ev[kNumStreamVariants + 1];
+      for (auto &x : ev) cudaEventCreate(&x);
+      const int s1 = std::min(n, per);
+      cudaEventRecord(ev[0], st);
+      for (int v = 0; v < kNumStreamVariants; v++) {
+        if ((e = stream_variant(c, v, 0, s1, ring_base, slot_stride, nslots, st))) return e;
+        cudaEventRecord(ev[v + 1], st);
+      }
+      cudaEventSynchronize(ev[kNumStreamVariants]);
+      float best = 1e30f;
+      for (int v = 0; v < kNumStreamVariants; v++) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev[v], ev[v + 1]);
+        if (t < best) {
+          best = t;
+          c->stream_variant = v;
+        }
+      }
+      for (auto &x : ev) cudaEventDestroy(x);
+      s0 = s1;
+    }
   }
-  return cudaGetLastError();
+  for (; s0 < n; s0 += per) {
+    const int s1 = std::min(n, s0 + per);
+    if ((e = stream_variant(c, c->stream_variant, s0, s1, ring_base, slot_stride, nslots, st)))
+      return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace fem25
