@@ -1,0 +1,87 @@
+"""Multi-process host logic on CPU (gloo, world size 2): LPT pair sharding,
+the gradient all-reduce, and failure detection through the store (a rank
+that raises makes every rank raise; nobody waits in the collective)."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from fem25_b200.parallel import pair_costs, shard_lpt
+
+
+def test_lpt_balances_and_covers():
+    freqs = [0.1 * (i + 1) for i in range(24) for _ in range(int(np.ceil(16 * (i + 1))))]
+    costs = pair_costs(freqs, nsrc=64)
+    for world in (1, 2, 4, 8):
+        parts = shard_lpt(costs, world)
+        allk = sorted(k for p in parts for k in p)
+        assert allk == list(range(len(freqs)))
+        loads = [sum(costs[k] for k in p) for p in parts]
+        assert max(loads) - min(loads) <= max(costs)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, mode, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=30))
+    import oracle
+    from fem25_b200 import synth
+    from fem25_b200.parallel import RankFailure, distributed_gradient
+    mesh, pairs, _ = synth.make_config(0, nx=6, nz=4)
+    g = oracle.graph_build(mesh)
+    sel = pairs[:6]
+    rng = np.random.default_rng(7)
+    u = rng.standard_normal((len(sel), 1, g.ndof)) + 1j * rng.standard_normal((len(sel), 1, g.ndof))
+    lam = rng.standard_normal((len(sel), 1, g.ndof)) + 1j * rng.standard_normal((len(sel), 1, g.ndof))
+
+    def partial(idx):
+        if mode == "fail" and rank == 1:
+            raise ValueError("injected host failure")
+        out_g = np.zeros((3, mesh.nnpg))
+        for k in idx:
+            oracle.grad_exact(mesh, g, sel[k][0], sel[k][1], u[k], lam[k], out=out_g)
+        return torch.from_numpy(out_g)
+
+    try:
+        res = distributed_gradient(sel, partial, mesh.nnpg, step=0)
+        if rank == 0:
+            ref = np.zeros((3, mesh.nnpg))
+            for k in range(len(sel)):
+                oracle.grad_exact(mesh, g, sel[k][0], sel[k][1], u[k], lam[k], out=ref)
+            out.put(("ok", float(np.abs(res.numpy() - ref).max() / np.abs(ref).max())))
+    except RankFailure as e:
+        out.put(("failure", rank, str(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("mode", ["ok", "fail"])
+def test_two_rank_gradient(mode):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, mode, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    msgs = [q.get(timeout=5) for _ in range(1 if mode == "ok" else 2)]
+    if mode == "ok":
+        assert msgs[0][0] == "ok" and msgs[0][1] < 1e-12
+    else:
+        assert sorted(m[1] for m in msgs) == [0, 1]
+        assert all("injected host failure" in m[2] for m in msgs)
