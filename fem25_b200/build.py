@@ -27,6 +27,7 @@ UNITS = [
     ("k_ref.cu", ["-fmad=false"]),
     ("k_batch.cu", []),
     ("k_grad.cu", []),
+    ("k_grad_tc.cu", []),
     ("api.cu", []),
 ]
 HOST = [("host_setup.cpp", ["-O2", "-ffp-contract=off", "-fPIC", "-fopenmp", "-std=c++17"])]

@@ -87,7 +87,8 @@ void free_ctx(Ctx *c) {
                   c->d_brptr, c->d_brow, c->d_basis, c->d_ebasis, c->d_bgptr, c->d_bglist,
                   c->d_pml_elems, c->d_pml_idx, c->d_pgptr, c->d_pglist, c->d_pml_emat,
                   c->d_pml_delta, c->d_sys, c->d_jcsc, c->d_icsc, c->d_rg_anchor, c->d_mconn,
-                  c->d_elem_wts, c->d_fmat, c->d_pairs, c->d_nonpml, c->d_cdist, c->d_prim, c->d_desc};
+                  c->d_elem_wts, c->d_fmat, c->d_pairs, c->d_nonpml, c->d_cdist, c->d_prim, c->d_desc,
+                  c->d_tc_tab};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->h_sys_pinned) cudaFreeHost(c->h_sys_pinned);

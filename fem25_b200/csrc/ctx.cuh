@@ -100,6 +100,7 @@ struct Ctx {
   int pairs_cap = 0;
   int *d_nonpml = nullptr;       // ids of the elements outside the PML
   int n_nonpml = 0;
+  unsigned char *d_tc_tab = nullptr;  // SHL tables of the tensor-core gradient (tf32 hi/lo)
   // cached COMPLEX*8 device buffer of fem25_asmble_driver
   float2 *d_cdist = nullptr;
   // optional CUDA-event timing of the dominant kernels

@@ -188,14 +188,3 @@ cudaError_t launch_grad_plain(Ctx *c, int npairs, int nsrc, const double *u, con
 }
 
 }  // namespace fem25
-
-namespace fem25 {
-// The split-precision tensor-core contraction lives in k_grad_tc.cu when
-// built; without it the entry point reports that the path is absent.
-#ifndef FEM25_HAVE_TC
-cudaError_t launch_grad_tc(Ctx *, int, int, const double *, const double *, double *,
-                           cudaStream_t) {
-  return cudaErrorNotSupported;
-}
-#endif
-}  // namespace fem25

@@ -6,13 +6,14 @@ magnitude, the definition used for every CSR error in this repository):
   * COMPLEX*8 CDIST (reference FP32 accumulation): bit-exact
   * batched affine assembly vs oracle FP64:        <= 1e-12
   * exact gradient FP64 vs oracle:                 <= 1e-10 relative (2-norm)
+  * exact gradient 3xTF32 tensor cores vs oracle:  <= 2e-5 relative (2-norm)
   * reference-compatible gradient, P_eff, misfit:  bit-exact
 """
 import numpy as np
 import pytest
 
 import oracle
-from fem25_b200 import FEM25_PREC_FP64, Context, Fem25Error, synth
+from fem25_b200 import FEM25_PREC_FP64, FEM25_PREC_TF32X3, Context, Fem25Error, synth
 from tests import helpers
 
 torch = pytest.importorskip("torch")
@@ -124,6 +125,34 @@ def test_gradient_fp64_matches_oracle():
     for m in range(3):
         rel = np.linalg.norm(got[m] - ref[m]) / np.linalg.norm(ref[m])
         assert rel <= 1e-10, (m, rel)
+    ctx.close()
+
+
+@pytest.mark.parametrize("nsrc", [1, 7])
+def test_gradient_tf32x3_matches_oracle(nsrc):
+    """Split-precision tensor-core gradient; 3 pairs x 7 sources = 21 combos
+    exercises two full batches of 10 and a ragged one, nsrc=1 a batch of 3."""
+    mesh, pairs, _ = synth.make_config(0, nx=10, nz=6)
+    g = oracle.graph_build(mesh)
+    ctx = Context(mesh, g)
+    rng = np.random.default_rng(12 + nsrc)
+    use = [pairs[2], pairs[9], pairs[14]]
+    shape = (len(use), nsrc, g.ndof)
+    u = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    lam = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    ref = np.zeros((3, mesh.nnpg))
+    for p, (f, py) in enumerate(use):
+        oracle.grad_exact(mesh, g, f, py, u[p], lam[p], out=ref)
+    d_u = torch.from_numpy(u).to(_dev())
+    d_l = torch.from_numpy(lam).to(_dev())
+    for rep in range(2):
+        d_g = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=_dev())
+        ctx.gradient([p[0] for p in use], [p[1] for p in use], nsrc, d_u, d_l, d_g,
+                     FEM25_PREC_TF32X3)
+        got = d_g.cpu().numpy()
+        for m in range(3):
+            rel = np.linalg.norm(got[m] - ref[m]) / np.linalg.norm(ref[m])
+            assert rel <= 2e-5, (rep, m, rel)
     ctx.close()
 
 
