@@ -29,6 +29,7 @@ UNITS = [
     ("k_grad.cu", []),
     ("k_grad_tc.cu", []),
     ("api.cu", []),
+    ("misfit_noalloc.cu", ["-fmad=false"]),
 ]
 HOST = [("host_setup.cpp", ["-O2", "-ffp-contract=off", "-fPIC", "-fopenmp", "-std=c++17"])]
 

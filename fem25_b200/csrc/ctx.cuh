@@ -132,6 +132,11 @@ cudaError_t launch_misfit(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const 
                           const float *sol, const float *d_obs, const float *d_wghts,
                           float *d_est, float *rhs, float *d_misfit, cudaStream_t st);
 
+cudaError_t launch_misfit_part(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const float *d_trig,
+                               double azmod, const float *d_recv, const float *sol,
+                               const float *d_obs, const float *d_wghts, float *d_est, float *rhs,
+                               float *d_part, float *d_misfit, cudaStream_t st);
+
 PmlParams pml_params(const Ctx *c, char cftype, double freq);
 
 }  // namespace fem25

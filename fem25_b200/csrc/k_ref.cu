@@ -161,6 +161,26 @@ cudaError_t launch_misfit(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const 
   return cudaGetLastError();
 }
 
+// The same three launches with the per-(source, receiver) partials in a
+// caller-provided device buffer of 3 * nsrc * nrec floats (every entry is
+// written by k_misfit before k_misfit_sum reads it).
+cudaError_t launch_misfit_part(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const float *d_trig,
+                               double azmod, const float *d_recv, const float *sol,
+                               const float *d_obs, const float *d_wghts, float *d_est, float *rhs,
+                               float *d_part, float *d_misfit, cudaStream_t st) {
+  float th = (float)azmod * 0.017453292519943295f;
+  float4 rot = make_float4(cosf(th), sinf(th), cosf(-th), sinf(-th));
+  const long long nrhs = (long long)nsrc * c->ndof;
+  k_fill_conj_zero<<<(unsigned)((nrhs + 255) / 256), 256, 0, st>>>(nrhs, (float2 *)rhs);
+  int n = nsrc * nrec;
+  k_misfit<<<(n + 127) / 128, 128, 0, st>>>(nsrc, nrec, c->ndof, d_mrdof, (const float4 *)d_trig,
+                                            rot, (const float2 *)d_recv, (const float2 *)sol,
+                                            (const float2 *)d_obs, d_wghts, (float2 *)d_est,
+                                            (float2 *)rhs, d_part);
+  k_misfit_sum<<<(nsrc + 127) / 128, 128, 0, st>>>(nsrc, nrec, d_part, d_misfit);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // reference-compatible virtual forces: one CTA per CSC column (inversion
 // anchor), elements of MCONN in order.  DKM_VPVS (dstiff25.f:498-662) is

@@ -63,6 +63,8 @@ def lib():
         L.fem25_ref_gradient_dev.argtypes = [vp, C.c_char_p, d, d, d, vp, vp, i, vp, vp]
         L.fem25_ref_gradient_info.argtypes = [vp, C.POINTER(i), C.POINTER(ll), vp]
         L.fem25_misfit_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.fem25_misfit_noalloc_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp,
+                                               vp]
         L.fem25_profile_enable.argtypes = [vp, i]
         L.fem25_profile_ms.argtypes = [vp, i, C.POINTER(d)]
         _lib = L
@@ -265,3 +267,14 @@ class Context:
             _np(np.ascontiguousarray(wghts, np.float32)), _np(est), _ptr(rhs), _np(mis),
             _stream(stream)))
         return est, mis
+
+    def misfit_noalloc(self, nsrc, mrdof, yrec, freq, py, azmod, recv, sol, obs, wghts, est, rhs,
+                       misfit, stream=None):
+        """fem25_misfit_noalloc_dev: obs, wghts, est, misfit are device tensors;
+        mrdof, yrec, recv host arrays.  Allocates no device memory."""
+        nrec = mrdof.shape[0]
+        self._check(lib().fem25_misfit_noalloc_dev(
+            self.h, nsrc, nrec, _np(np.ascontiguousarray(mrdof, np.int32)),
+            _np(np.ascontiguousarray(yrec, np.float64)), freq, py, azmod,
+            _np(np.ascontiguousarray(recv, np.complex64)), _ptr(sol), _ptr(obs), _ptr(wghts),
+            _ptr(est), _ptr(rhs), _ptr(misfit), _stream(stream)))

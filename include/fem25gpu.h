@@ -149,6 +149,32 @@ int fem25_misfit_dev(fem25_ctx *ctx, int nsrc, int nrec, const int *mrdof, const
                      const float *obs, const float *wghts, float *est, float *rhs, float *misfit,
                      void *stream);
 
+/* The same misfit and adjoint source without any device allocation, for
+ * callers that must not allocate device memory while they run: an inversion
+ * loop that has given the rest of HBM to a sparse direct solver's factors, or
+ * one that cannot take the device-wide synchronisation that cudaMalloc and
+ * cudaFree imply between frequencies.  No counterpart in the reference (it
+ * has no device memory); it computes what fem25_misfit_dev computes, with
+ * bit-identical outputs.
+ * Differences from fem25_misfit_dev: obs, wghts, est and misfit are DEVICE
+ * arrays here (same layouts); mrdof, yrec and recv stay host arrays and are
+ * copied into a fixed device scratch before the call returns.
+ * Limits: nrec <= FEM25_NOALLOC_MAX_REC and nsrc * nrec <=
+ * FEM25_NOALLOC_MAX_SRC_REC; larger calls return FEM25_ERR_ARG with a message.
+ * The scratch (about 3.1 MB) is one static array per device, shared by every
+ * context on that device: calls that overlap in time on one device (two
+ * threads, or two streams with no ordering between them) race on it and give
+ * wrong results.  The first call on each device sets the scratch up (looks up
+ * its address, which may load the library's device code); make that first
+ * call before any stream capture begins. */
+#define FEM25_NOALLOC_MAX_REC 2048
+#define FEM25_NOALLOC_MAX_SRC_REC 262144
+int fem25_misfit_noalloc_dev(fem25_ctx *ctx, int nsrc, int nrec, const int *mrdof,
+                             const double *yrec, double freq, double py, double azmod,
+                             const float *recv, const float *sol, const float *obs,
+                             const float *wghts, float *est, float *rhs, float *misfit,
+                             void *stream);
+
 /* ---- profiling ----------------------------------------------------------------
  * With profiling enabled the library records CUDA events on the launching
  * stream around its dominant kernels; fem25_profile_ms returns the duration
