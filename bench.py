@@ -11,7 +11,11 @@ Also reported on the same line:
   * plain_fp64: the per-(omega, py) FP64 element + gather kernels (systems/s)
   * e2e: ASMBLE_DRIVER through the C ABI with host buffers (model upload from
     pinned memory, COMPLEX*8 CDIST read back to pinned memory) -- systems/s
-  * gradient: exact adjoint gradient, elem.rhs/s, config-1 mesh, 32 sources
+  * gradient: exact adjoint gradient, elem.rhs/s, 400x120 layered mesh, 32 sources
+  * pipeline: the uneven-batch workload (600x200 jittered mesh with
+    topography, 24 frequencies 0.1-2.4 Hz x ceil(16 f / 0.1) ky = 4800 systems,
+    64 sources): batched assembly + split-precision gradient against the plain
+    per-(omega, py) FP64 assembly + FP64 gradient
   * roofline of the streaming kernel and the CPU baseline (the oracle).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -145,12 +149,113 @@ def run_reference(args, rank):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 512 / v * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded layered model, 400x120 mesh)",
-           "config": {"workload": "configs[1]: batched assembly, 400x120 deg-4 mesh, 8 f x 64 ky "
+           "config": {"workload": "batched assembly, 400x120 deg-4 layered-model mesh, 8 f x 64 ky "
                                   "= 512 complex128 CSR systems",
                       "systems_per_step": 512, "nelem": 48000},
            "cpu_baseline": base,
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
+
+
+def pipeline_uneven(local, dev):
+    """Batched split-precision path against the plain per-(omega, py) FP64 path
+    on the uneven-batch workload (600x200 jittered mesh with +-200 m
+    topography, Bielak strip 4, 24 frequencies 0.1-2.4 Hz, nky = ceil(16 f /
+    0.1), 4800 systems, 64 sources).  The batched assembly runs all 4800
+    systems; the plain assembly runs one system per frequency and each
+    gradient one (omega, py) pair with all 64 sources, scaled to the 4800 pairs
+    (per-system and per-pair costs do not depend on the pair).  Parity at full
+    size: the last batched system against the plain FP64 CSR, the
+    split-precision gradient against the FP64 one."""
+    import torch
+    from fem25_b200 import FEM25_PREC_FP64, FEM25_PREC_TF32X3, Context, synth
+    mesh, pairs, cfg = synth.make_config(4)
+    nsrc = cfg["nsrc"]
+    t0 = time.perf_counter()
+    ctx = Context(mesh, device=local)
+    setup_s = time.perf_counter() - t0
+    nz, ndof, npairs = ctx.nzero, ctx.ndof, len(pairs)
+    stream = torch.cuda.current_stream(dev)
+    freqs = [p[0] for p in pairs]
+    pys = [p[1] for p in pairs]
+
+    def timed(fn, reps=1):
+        best = None
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        return best / 1e3
+
+    # batched assembly: every system, ring of 8 complex128 slots
+    nslots = 8
+    ring = torch.empty(nslots * 2 * nz, dtype=torch.float64, device=dev)
+    ctx.assemble_batch("B", freqs[:nslots], pys[:nslots], ring, 2 * nz, nslots, stream=stream)
+    torch.cuda.synchronize()
+    t_basm = timed(lambda: ctx.assemble_batch("B", freqs, pys, ring, 2 * nz, nslots, stream=stream))
+    k = npairs - 1
+    slot = ring[(k % nslots) * 2 * nz:(k % nslots + 1) * 2 * nz].clone()
+    del ring
+    torch.cuda.empty_cache()
+    plain = torch.empty(2 * nz, dtype=torch.float64, device=dev)
+    ctx.assemble("B", freqs[k], pys[k], plain, None, stream=stream)
+    torch.cuda.synchronize()
+    csr_rel = float((slot - plain).abs().max() / plain.abs().max())
+    del slot
+    # plain assembly: the middle ky of every frequency
+    sel = []
+    for f in cfg["freqs"]:
+        idx = [i for i, p in enumerate(pairs) if p[0] == f]
+        sel.append(idx[len(idx) // 2])
+    ctx.assemble("B", freqs[sel[0]], pys[sel[0]], plain, None, stream=stream)
+    torch.cuda.synchronize()
+    t_pasm = timed(lambda: [ctx.assemble("B", freqs[i], pys[i], plain, None, stream=stream)
+                            for i in sel]) / len(sel)
+    del plain
+    # gradient: one pair, all sources, both precisions
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(2031)
+    u = torch.randn((1, nsrc, ndof), dtype=torch.complex128, device=dev, generator=gen)
+    lam = torch.randn((1, nsrc, ndof), dtype=torch.complex128, device=dev, generator=gen)
+    gp = pairs[npairs // 2]
+    g64 = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=dev)
+    g32 = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=dev)
+    ctx.gradient([gp[0]], [gp[1]], nsrc, u, lam, g32, FEM25_PREC_TF32X3, stream=stream)
+    torch.cuda.synchronize()
+
+    def run_grad(out, prec):
+        out.zero_()
+        ctx.gradient([gp[0]], [gp[1]], nsrc, u, lam, out, prec, stream=stream)
+    t_g64 = timed(lambda: run_grad(g64, FEM25_PREC_FP64))
+    t_g32 = timed(lambda: run_grad(g32, FEM25_PREC_TF32X3), reps=3)
+    grel = max(float(torch.linalg.norm(g32[m] - g64[m]) / torch.linalg.norm(g64[m]))
+               for m in range(3))
+    del u, lam, g64, g32
+    ctx.close()
+    torch.cuda.empty_cache()
+    plain_total = (t_pasm + t_g64) * npairs
+    batched_total = t_basm + t_g32 * npairs
+    units = mesh.nelem * nsrc
+    return {"workload": f"uneven batch: 600x200 jittered deg-4 mesh with topography, strip 4 "
+                        f"({mesh.nelem} elements, NDOF {ndof}, NNZ {nz}), "
+                        f"24 f x ceil(16 f/0.1) ky = {npairs} systems, {nsrc} sources",
+            "batched_tf32x3_s": batched_total, "plain_fp64_s": plain_total,
+            "speedup": plain_total / batched_total,
+            "batched_assembly_s": t_basm, "batched_assemblies_per_s": npairs / t_basm,
+            "plain_assembly_s_per_system": t_pasm,
+            "gradient_tf32x3_s_per_pair": t_g32, "gradient_fp64_s_per_pair": t_g64,
+            "gradient_tf32x3_elem_rhs_per_s": units / t_g32,
+            "gradient_fp64_elem_rhs_per_s": units / t_g64,
+            "gradient_rel_err_vs_fp64": grel, "csr_rel_err_batched_vs_plain": csr_rel,
+            "sample": f"batched assembly: all {npairs} systems; plain assembly: 1 system per "
+                      f"frequency ({len(sel)}); gradients: 1 pair x {nsrc} sources; totals scaled "
+                      f"to {npairs} pairs",
+            "setup_s": round(setup_s, 1)}
 
 
 def main():
@@ -163,6 +268,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-grad", action="store_true")
     ap.add_argument("--small", action="store_true", help="small mesh (profiling captures)")
+    ap.add_argument("--no-pipeline", action="store_true",
+                    help="skip the uneven-batch pipeline comparison")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -203,6 +310,7 @@ def main():
         mesh, pairs, cfg = synth.make_config(1)
     ctx = Context(mesh, device=local)
     nz = ctx.nzero
+    ndof_main = ctx.ndof
     nsys = len(pairs)
     freqs = [p[0] for p in pairs]
     pys = [p[1] for p in pairs]
@@ -287,7 +395,7 @@ def main():
     step()
     torch.cuda.synchronize()
 
-    # ---------------- gradient (exact lambda/mu/rho, FP64), config-2 shape
+    # ---------------- gradient (exact lambda/mu/rho), 400x120 mesh, 32 sources x 2 pairs
     grad = None
     if not args.no_grad:
         nsrc = 32
@@ -331,6 +439,14 @@ def main():
                 "algorithmic_tflops_fp64": units * 547200 / (gms / 1e3) / 1e12}
         del u, lam
 
+    pipe = None
+    if world == 1 and not args.no_pipeline and not args.small:
+        del ring
+        ctx.close()
+        torch.cuda.empty_cache()
+        ctx = None
+        pipe = pipeline_uneven(local, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_assembly_sample(1, seconds_target=12.0)
@@ -339,8 +455,8 @@ def main():
            "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded layered model; no public dataset exists for this path)",
-           "config": {"workload": "configs[1]: batched assembly, 400x120 deg-4 mesh "
-                                  f"({mesh.nelem} elements, NDOF {ctx.ndof}, NNZ {nz}), "
+           "config": {"workload": "batched assembly, 400x120 deg-4 layered-model mesh "
+                                  f"({mesh.nelem} elements, NDOF {ndof_main}, NNZ {nz}), "
                                   f"8 f x 64 ky = {nsys} complex128 CSR systems per step",
                       "systems_per_step": nsys, "nslots": nslots, "parallelism": f"replicas x{world}",
                       "l2": "inputs (basis 2.6 GB) and outputs (4 GB/system) larger than L2",
@@ -350,11 +466,12 @@ def main():
                         "frac": achieved / peak, "traffic": None, "kernel": "k_stream",
                         "kernel_ms": kms, "peak_kind": peak_kind,
                         "algorithmic_bytes": "16 B x NNZ per system (complex128 values written)"},
-           "cpu_baseline": cpu, "e2e": e2e, "gradient": grad,
+           "cpu_baseline": cpu, "e2e": e2e, "gradient": grad, "pipeline": pipe,
            "gpu_launches": launches_per_step * args.steps, "clocks": clocks}
     if rank == 0:
         print(json.dumps(out))
-    ctx.close()
+    if ctx is not None:
+        ctx.close()
     if world > 1:
         dist.destroy_process_group()
 

@@ -240,7 +240,7 @@ CONFIGS = {
     # batched assembly: 400x120, 8 f over 0.2-1.6 Hz x 64 ky
     1: dict(nx=400, nz=120, lx=200000.0, lz=60000.0, strip=2, model="layered",
             freqs=list(np.linspace(0.2, 1.6, 8)), nky=[64] * 8, nsrc=0, jitter=0.0, topo=0.0),
-    # adjoint gradient: config-1 mesh, 32 sources, 8 f x 64 ky
+    # adjoint gradient: the 400x120 layered mesh, 32 sources, 8 f x 64 ky
     2: dict(nx=400, nz=120, lx=200000.0, lz=60000.0, strip=2, model="layered",
             freqs=list(np.linspace(0.2, 1.6, 8)), nky=[64] * 8, nsrc=32, jitter=0.0, topo=0.0),
     # split-precision contraction: 300x150 jittered, 128 src x 96 ky x 12 f

@@ -14,7 +14,7 @@ def pytest_configure(config):
 
 @pytest.fixture(scope="session")
 def small_case():
-    """6x4-element mesh of the configs[0] layout (strip 2) and two (f, py) pairs."""
+    """6x4-element mesh of the small half-space layout (strip 2) and two (f, py) pairs."""
     from fem25_b200 import synth
     mesh, pairs, _ = synth.make_config(0, nx=8, nz=5)
     return mesh, pairs
