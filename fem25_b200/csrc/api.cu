@@ -59,9 +59,9 @@ int check_mesh(const fem25_mesh *m, std::string *msg) {
     *msg = "mesh: only NORD = 4 (5x5 GLL nodes) is built";
     return FEM25_ERR_UNSUPPORTED;
   }
-  if (m->ldisp) {
-    *msg = "mesh: dispersive media (KMDAMP/CMDAMP) are not supported";
-    return FEM25_ERR_UNSUPPORTED;
+  if (m->ldisp && (!m->qp || !m->qs)) {
+    *msg = "mesh: dispersive media (ldisp = 1) need QP and QS";
+    return FEM25_ERR_ARG;
   }
   for (int e = 0; e < m->nelem; e++) {
     for (int a = 0; a < 4; a++) {
@@ -88,7 +88,7 @@ void free_ctx(Ctx *c) {
                   c->d_pml_elems, c->d_pml_idx, c->d_pgptr, c->d_pglist, c->d_pml_emat,
                   c->d_pml_delta, c->d_sys, c->d_jcsc, c->d_icsc, c->d_rg_anchor, c->d_mconn,
                   c->d_elem_wts, c->d_fmat, c->d_pairs, c->d_nonpml, c->d_cdist, c->d_prim, c->d_desc,
-                  c->d_tc_tab};
+                  c->d_tc_tab, c->d_qp, c->d_qs};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->h_sys_pinned) cudaFreeHost(c->h_sys_pinned);
@@ -133,6 +133,10 @@ int ensure_plain(Ctx *c, cudaStream_t st) {
 }
 
 int ensure_batch(Ctx *c, cudaStream_t st) {
+  if (c->mesh_scalars.ldisp)
+    return fail(c, FEM25_ERR_UNSUPPORTED,
+                "batch: dispersive media have frequency-dependent complex velocities "
+                "(no per-mesh affine basis); use fem25_assemble_dev");
   if (c->bcsr.nblocks >= (1LL << 28))
     return fail(c, FEM25_ERR_UNSUPPORTED, "batch: more than 2^28 node blocks");
   if (!c->d_bgptr) {
@@ -151,6 +155,8 @@ int ensure_batch(Ctx *c, cudaStream_t st) {
 
 int ensure_refgrad(Ctx *c) {
   if (c->refgrad_ready) return FEM25_OK;
+  if (c->mesh_scalars.ldisp)
+    return fail(c, FEM25_ERR_UNSUPPORTED, "gradient: dispersive media are not supported");
   fem25_mesh m = c->mesh_scalars;
   m.ieng = c->h_ieng.data();
   m.cdomain = c->h_cdomain.data();
@@ -241,6 +247,7 @@ int fem25_create(const fem25_mesh *m, int ndof, long long nzero, const int *lm, 
   c->mesh_scalars.cnnpg = nullptr;
   c->mesh_scalars.xlocs = c->mesh_scalars.zlocs = c->mesh_scalars.xd = c->mesh_scalars.zd = nullptr;
   c->mesh_scalars.ecoeff = c->mesh_scalars.dens = nullptr;
+  c->mesh_scalars.qp = c->mesh_scalars.qs = nullptr;
   c->nelem = m->nelem;
   c->nnpg = m->nnpg;
   c->ndof = ndof;
@@ -277,6 +284,10 @@ int fem25_create(const fem25_mesh *m, int ndof, long long nzero, const int *lm, 
     CK(cudaMalloc(&c->d_rho, sizeof(double) * m->nnpg), "mesh");
     int rr = upload_model(c, m->ecoeff, m->dens);
     if (rr) return rr;
+    if (m->ldisp) {
+      CK(dalloc_copy(&c->d_qp, m->qp, m->nnpg), "mesh");
+      CK(dalloc_copy(&c->d_qs, m->qs, m->nnpg), "mesh");
+    }
     CK(dalloc_copy(&c->d_lm, lm, 3 * (size_t)kNen * m->nelem), "graph");
     CK(dalloc_copy(&c->d_irptr, irptr, (size_t)ndof + 1), "graph");
     CK(dalloc_copy(&c->d_jcptr, jcptr, (size_t)nzero), "graph");
@@ -299,6 +310,8 @@ int fem25_create(const fem25_mesh *m, int ndof, long long nzero, const int *lm, 
     c->mv.lam = c->d_lam;
     c->mv.mu = c->d_mu;
     c->mv.rho = c->d_rho;
+    c->mv.qp = c->d_qp;
+    c->mv.qs = c->d_qs;
     CK(check_jacobians(c, 0), "jacobian check");
     return read_err_word(c, 0);
   };
@@ -467,6 +480,8 @@ int fem25_gradient_dev(fem25_ctx *h, int npairs, const double *freq, const doubl
                        const double *u, const double *lam, int prec, double *grad, void *stream) {
   if (!h || !freq || !py || !u || !lam || !grad || npairs <= 0 || nsrc <= 0) return FEM25_ERR_ARG;
   Ctx *c = &h->c;
+  if (c->mesh_scalars.ldisp)
+    return fail(c, FEM25_ERR_UNSUPPORTED, "gradient: dispersive media are not supported");
   cudaStream_t st = (cudaStream_t)stream;
   CK(cudaSetDevice(c->device), "set device");
   if (npairs > c->pairs_cap) {

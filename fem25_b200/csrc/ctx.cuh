@@ -30,6 +30,7 @@ struct MeshView {
   const int4 *ieng;        // 1-based anchors, one int4 per element
   const char *cdomain;
   const double *x, *z, *xd, *zd, *lam, *mu, *rho;
+  const double *qp, *qs;   // quality factors (dispersive media only, else null)
 };
 
 // One (omega, py) system of a batch, pre-digested for the streaming kernel.
@@ -54,6 +55,7 @@ struct Ctx {
   char *d_cdomain = nullptr;
   double *d_x = nullptr, *d_z = nullptr, *d_xd = nullptr, *d_zd = nullptr;
   double *d_lam = nullptr, *d_mu = nullptr, *d_rho = nullptr;
+  double *d_qp = nullptr, *d_qs = nullptr;  // dispersive media
   std::vector<char> h_cdomain, h_cnnpg;
   std::vector<double> h_x, h_z;
   std::vector<int> h_ieng, h_lm, h_irptr;

@@ -30,7 +30,8 @@ class Mesh(C.Structure):
                 ("xwidth", C.c_double), ("zwidth", C.c_double),
                 ("rcoeff_srf", C.c_double), ("dmax_srf", C.c_double), ("kappa_srf", C.c_double),
                 ("fcent_srf", C.c_double), ("rcoeff_bdy", C.c_double), ("dmax_bdy", C.c_double),
-                ("kappa_bdy", C.c_double), ("fcent_bdy", C.c_double)]
+                ("kappa_bdy", C.c_double), ("fcent_bdy", C.c_double),
+                ("qp", C.c_void_p), ("qs", C.c_void_p), ("freq0", C.c_double)]
 
 
 _lib = None
@@ -105,8 +106,13 @@ class _MeshKeep:
                       zd=np.ascontiguousarray(mesh.zd, np.float64),
                       ecoeff=np.ascontiguousarray(mesh.ecoeff, np.float64),
                       dens=np.ascontiguousarray(mesh.dens, np.float64))
+        ldisp = bool(getattr(mesh, "ldisp", False))
+        if ldisp:
+            self.a["qp"] = np.ascontiguousarray(mesh.qp, np.float64)
+            self.a["qs"] = np.ascontiguousarray(mesh.qs, np.float64)
         s = Mesh()
-        s.nelem, s.nnpg, s.nord, s.ldisp = mesh.nelem, mesh.nnpg, mesh.nord, 0
+        s.nelem, s.nnpg, s.nord, s.ldisp = mesh.nelem, mesh.nnpg, mesh.nord, int(ldisp)
+        s.freq0 = float(getattr(mesh, "freq0", 0.0)) if ldisp else 0.0
         for k, v in self.a.items():
             setattr(s, k, _np(v))
         s.xwidth, s.zwidth = mesh.xwidth, mesh.zwidth

@@ -47,6 +47,12 @@ class Mesh:
     fcent: tuple = (0.0, 0.0)
     nx: int = 0
     nz: int = 0
+    # dispersive media (RDMESHBK IDISP > 0, mesh_utils.f:1082-1133): quality
+    # factors at the anchors and the reference frequency; 9999 = no damping
+    ldisp: bool = False
+    qp: np.ndarray | None = None
+    qs: np.ndarray | None = None
+    freq0: float = 0.0
 
 
 def dmfrho(vp: np.ndarray) -> np.ndarray:
@@ -252,6 +258,21 @@ CONFIGS = {
             nky=[int(math.ceil(16 * 0.1 * (i + 1) / 0.1 - 1e-9)) for i in range(24)],
             nsrc=64, jitter=0.2, topo=200.0),
 }
+
+
+def make_dispersive(mesh: Mesh, seed: int, freq0: float = 1.0, qs_mean: float = 40.0) -> Mesh:
+    """Turn ``mesh`` into a dispersive medium: Qs around ``qs_mean`` with a
+    seeded +-25 % variation, Qp = 2.25 Qs (the common Qp/Qs ratio for a
+    Poisson solid), reference frequency ``freq0``; a few anchors keep the
+    reference's "no damping" value 9999."""
+    rng = np.random.default_rng(seed)
+    qs = qs_mean * (1.0 + 0.25 * rng.uniform(-1.0, 1.0, mesh.nnpg))
+    qp = 2.25 * qs
+    off = rng.random(mesh.nnpg) < 0.05
+    qs[off] = 9999.0
+    qp[off] = 9999.0
+    mesh.qp, mesh.qs, mesh.freq0, mesh.ldisp = qp, qs, float(freq0), True
+    return mesh
 
 
 def make_config(idx, nx=None, nz=None):

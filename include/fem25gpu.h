@@ -37,7 +37,7 @@ typedef struct fem25_mesh {
     int nelem;               /* NELEM                                        */
     int nnpg;                /* NNPG, anchor nodes                           */
     int nord;                /* NORD, polynomial order (NLXI = NORD+1)       */
-    int ldisp;               /* dispersive media flag (must be 0)            */
+    int ldisp;               /* LDISP: 1 = dispersive media (qp, qs, freq0)   */
     const int *ieng;         /* IENG(4,NELEM), 1-based                        */
     const char *cdomain;     /* CDOMAIN(NELEM): 'I','E','A'                   */
     const char *cnnpg;       /* CNNPG(NNPG): CHARACTER(2), 2 bytes per anchor */
@@ -48,6 +48,11 @@ typedef struct fem25_mesh {
     double xwidth, zwidth;   /* PML widths (max XD, max ZD)                   */
     double rcoeff_srf, dmax_srf, kappa_srf, fcent_srf;  /* CFTYPE 'S'         */
     double rcoeff_bdy, dmax_bdy, kappa_bdy, fcent_bdy;  /* CFTYPE 'B'         */
+    /* dispersive media (read only when ldisp = 1; RDMESHBK IDISP > 0,
+     * mesh_utils.f:1082-1133): the assembly uses the complex velocities of
+     * VCMPLX (haskattn.f:602-646) in KMDAMP / CMDAMP (estiff25.f:511-961) */
+    const double *qp, *qs;   /* QP(NNPG), QS(NNPG) quality factors; 9999 = none */
+    double freq0;            /* FREQ0 reference frequency (Hz); 0 = none      */
 } fem25_mesh;
 
 typedef struct fem25_graph fem25_graph;  /* host graph (opaque)            */

@@ -39,7 +39,9 @@ class OrcMesh(C.Structure):
                 ("zd", C.c_void_p), ("ecoeff", C.c_void_p), ("dens", C.c_void_p),
                 ("xwidth", C.c_double), ("zwidth", C.c_double),
                 ("rcoeff", C.c_double * 2), ("dmax", C.c_double * 2),
-                ("kappa", C.c_double * 2), ("fcent", C.c_double * 2)]
+                ("kappa", C.c_double * 2), ("fcent", C.c_double * 2),
+                ("ldisp", C.c_int), ("qp", C.c_void_p), ("qs", C.c_void_p),
+                ("freq0", C.c_double)]
 
 
 def _p(a):
@@ -91,6 +93,9 @@ class OracleMesh:
             zd=np.ascontiguousarray(mesh.zd, np.float64),
             ecoeff=np.ascontiguousarray(mesh.ecoeff, np.float64),
             dens=np.ascontiguousarray(mesh.dens, np.float64))
+        q9 = np.full(mesh.nnpg, 9999.0)
+        self.keep["qp"] = np.ascontiguousarray(q9 if mesh.qp is None else mesh.qp, np.float64)
+        self.keep["qs"] = np.ascontiguousarray(q9 if mesh.qs is None else mesh.qs, np.float64)
         k = self.keep
         s = OrcMesh()
         s.nelem, s.nnpg, s.nord = mesh.nelem, mesh.nnpg, mesh.nord
@@ -99,6 +104,9 @@ class OracleMesh:
         s.xwidth, s.zwidth = mesh.xwidth, mesh.zwidth
         for f in ("rcoeff", "dmax", "kappa", "fcent"):
             getattr(s, f)[0], getattr(s, f)[1] = getattr(mesh, f)
+        s.ldisp = 1 if mesh.ldisp else 0
+        s.qp, s.qs = _p(k["qp"]), _p(k["qs"])
+        s.freq0 = mesh.freq0
         self.s = s
         self.mesh = mesh
         self.ptr = C.cast(C.pointer(s), C.c_void_p)

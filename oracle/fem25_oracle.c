@@ -43,6 +43,9 @@ typedef struct {
     const double *dens;
     double xwidth, zwidth;
     double rcoeff[2], dmax[2], kappa[2], fcent[2]; /* [0]='S' [1]='B'        */
+    int ldisp;              /* LDISP: dispersive media (QP, QS, FREQ0 used)  */
+    const double *qp, *qs;  /* QP(NNPG), QS(NNPG) quality factors           */
+    double freq0;           /* FREQ0 reference frequency (Hz)               */
 } orc_mesh;
 
 typedef struct {
@@ -540,11 +543,274 @@ static void cm25isoq(int nen, int nint, double omega, double py, const double *w
 }
 
 /* ------------------------------------------------------------------------ */
+/* dispersive media (LDISP)                                                   */
+/* ------------------------------------------------------------------------ */
+/* VCMPLX (haskattn.f:602-646): complex velocity of Aki & Richards 5.94,
+ * v (1 + ln(f/f0) / (pi Q)) - i v / (2 Q); Q = 9999 or f0 = 0 means none */
+static zc vcmplx(double freq, double freq0, double v, double q)
+{
+    const double PI = 3.1415926535897932384626434;
+    if (freq0 == 0.0 || fabs(q - 9999.0) < 1.0e-5) return zmk(v, 0.0);
+    if (q == 0.0) return zmk(v, 0.0);
+    double fac1 = log(freq / freq0);
+    double fact = 1.0 + 1.0 / (PI * q) * fac1;
+    if (fact < 0.1) fact = 0.1;
+    return zmk(v * fact, -v / (2.0 * q));
+}
+
+/* Fortran Z**2 of a COMPLEX*16: Z*Z */
+static inline zc zsq(zc z) { return zmul(z, z); }
+
+/* CJKM_QUAL (cjac.f:142-278) and, for PML elements, CJCM_QUAL
+ * (cjac.f:585-755): Jacobian, interpolated Vp, Vs (interpolated velocities,
+ * not moduli), QP, QS and the PML stretching factors at the points */
+static int cj_qual(const orc_mesh *m, int ielem, int nen, int nint, const double *xigll,
+                   const double *shl, int pml, double omega, double rcoeff, double dmax_in,
+                   double rkappa, double fcent, double *det, double *vp, double *vs,
+                   double *qpp, double *qss, double *shg, zc *dampx, zc *dampz)
+{
+    const double EPS = 2.22e-16;
+    const int *ieng = m->ieng + 4 * ielem;
+    int nnpg = m->nnpg;
+    for (int intx = 0; intx < nint; intx++) {
+        double xi = xigll[intx];
+        for (int intz = 0; intz < nint; intz++) {
+            double eta = xigll[intz];
+            double sf[4], dsf[8];
+            if (csf2d(xi, eta, sf, dsf)) return 1;
+            double x = 0.0, z = 0.0, xdep = 0.0, zdep = 0.0;
+            double vpq = 0.0, vsq = 0.0, qpq = 0.0, qsq = 0.0;
+            double dxdxi = 0.0, dxdeta = 0.0, dzdxi = 0.0, dzdeta = 0.0;
+            for (int ia = 0; ia < 4; ia++) {
+                int iloc = ieng[ia] - 1;
+                x = x + sf[ia] * m->xlocs[iloc];
+                z = z + sf[ia] * m->zlocs[iloc];
+                double rlam = m->ecoeff[iloc], rmu = m->ecoeff[iloc + nnpg];
+                double vpp = sqrt((rlam + 2.0 * rmu) / m->dens[iloc]);
+                double vss = sqrt(rmu / m->dens[iloc]);
+                vpq = vpq + sf[ia] * vpp;
+                vsq = vsq + sf[ia] * vss;
+                qpq = qpq + sf[ia] * m->qp[iloc];
+                qsq = qsq + sf[ia] * m->qs[iloc];
+                if (pml) {
+                    xdep = xdep + sf[ia] * m->xd[iloc];
+                    zdep = zdep + sf[ia] * m->zd[iloc];
+                }
+                dxdxi = dxdxi + dsf[0 + 2 * ia] * m->xlocs[iloc];
+                dxdeta = dxdeta + dsf[1 + 2 * ia] * m->xlocs[iloc];
+                dzdxi = dzdxi + dsf[0 + 2 * ia] * m->zlocs[iloc];
+                dzdeta = dzdeta + dsf[1 + 2 * ia] * m->zlocs[iloc];
+            }
+            int q = intx + nint * intz;
+            vp[q] = vpq; vs[q] = vsq; qpp[q] = qpq; qss[q] = qsq;
+            double rjac = dxdxi * dzdeta - dxdeta * dzdxi;
+            det[q] = rjac;
+            if (fabs(rjac) <= EPS || rjac < 0.0) return 1;
+            if (pml) {
+                double vel = vpq;
+                if (xdep > EPS)
+                    dampx[q] = zdampfn(xdep, vel, m->xwidth, dmax_in, rcoeff, rkappa, fcent, omega);
+                else
+                    dampx[q] = zmk(1.0, 0.0);
+                if (zdep > EPS)
+                    dampz[q] = zdampfn(zdep, vel, m->zwidth, dmax_in, rcoeff, rkappa, fcent, omega);
+                else
+                    dampz[q] = zmk(1.0, 0.0);
+            }
+            fill_shg(nen, nint, intx, intz, shl, dxdxi, dxdeta, dzdxi, dzdeta, rjac, shg);
+        }
+    }
+    return 0;
+}
+
+/* KMDAMP (estiff25.f:511-752): density-normalised element operator with
+ * complex velocities; ME real, the imaginary mass part goes into KE */
+static void kmdamp(int nen, int nint, double freq, double freq0, double py, const double *wts,
+                   const double *vp, const double *vs, const double *qpp, const double *qss,
+                   const double *det, const double *shg, double *me, zc *ke)
+{
+    const double TWOPI = 6.2831853071795862;
+    int nee = nen * NDIM;
+    for (int i = 0; i < nee * nee; i++) { me[i] = 0.0; ke[i] = zmk(0.0, 0.0); }
+    double omega = TWOPI * freq, wpy = omega * py, py2 = ipow(py, 2), w2 = ipow(omega, 2);
+    for (int intx = 0; intx < nint; intx++) {
+        for (int intz = 0; intz < nint; intz++) {
+            int q = intx + nint * intz;
+            double weight = wts[intx] * wts[intz] * det[q];
+            zc zvp2 = zsq(vcmplx(freq, freq0, vp[q], qpp[q]));
+            zc zvs2 = zsq(vcmplx(freq, freq0, vs[q], qss[q]));
+            double rvp2 = zvp2.re * weight, qvp2 = zvp2.im * weight;
+            double rvs2 = zvs2.re * weight, qvs2 = zvs2.im * weight;
+            double rm1 = -(w2 * weight) + w2 * py2 * rvs2, qm1 = w2 * py2 * qvs2;
+            double rm2 = -(w2 * weight) + w2 * py2 * rvp2, qm2 = w2 * py2 * qvp2;
+            for (int ibe = 0; ibe < nen; ibe++) {
+                size_t bb = 3 * ((size_t)ibe + (size_t)nen * q);
+                double phib = shg[bb + 2], phibx = shg[bb + 0], phibz = shg[bb + 1];
+                double rm11t1 = rm1 * phib, qm11t1 = qm1 * phib;
+                double rm22t1 = rm2 * phib, qm22t1 = qm2 * phib;
+                double rk11t1 = rvp2 * phibx, qk11t1 = qvp2 * phibx;
+                double rk11t2 = rvs2 * phibz, qk11t2 = qvs2 * phibz;
+                double rk13t1 = rvp2 * phibz, qk13t1 = qvp2 * phibz;
+                double rk13t2 = rvs2 * phibx, qk13t2 = qvs2 * phibx;
+                double rk13t3 = -(2.0 * rvs2 * phibz), qk13t3 = -(2.0 * qvs2 * phibz);
+                double rk22t1 = rvs2 * phibx, qk22t1 = qvs2 * phibx;
+                double rk22t2 = rvs2 * phibz, qk22t2 = qvs2 * phibz;
+                double rk31t1 = rvp2 * phibx, qk31t1 = qvp2 * phibx;
+                double rk31t2 = rvs2 * phibz, qk31t2 = qvs2 * phibz;
+                double rk31t3 = -(2.0 * rvs2 * phibx), qk31t3 = -(2.0 * qvs2 * phibx);
+                double rk33t1 = rvp2 * phibz, qk33t1 = qvp2 * phibz;
+                double rk33t2 = rvs2 * phibx, qk33t2 = qvs2 * phibx;
+                double rk12t1 = wpy * rvp2 * phib, qk12t1 = wpy * qvp2 * phib;
+                double rk12t2 = -(2.0 * wpy * rvs2 * phib), qk12t2 = -(2.0 * wpy * qvs2 * phib);
+                double rk12t3 = -(wpy * rvs2 * phibx), qk12t3 = -(wpy * qvs2 * phibx);
+                double rk21t1 = wpy * rvp2 * phibx, qk21t1 = wpy * qvp2 * phibx;
+                double rk21t2 = -(2.0 * wpy * rvs2 * phibx), qk21t2 = -(2.0 * wpy * qvs2 * phibx);
+                double rk21t3 = -(wpy * rvs2 * phib), qk21t3 = -(wpy * qvs2 * phib);
+                double rk23t1 = wpy * rvp2 * phibz, qk23t1 = wpy * qvp2 * phibz;
+                double rk23t2 = -(2.0 * wpy * rvs2 * phibz), qk23t2 = -(2.0 * wpy * qvs2 * phibz);
+                double rk23t3 = -(wpy * rvs2 * phib), qk23t3 = -(wpy * qvs2 * phib);
+                double rk32t1 = wpy * rvp2 * phib, qk32t1 = wpy * qvp2 * phib;
+                double rk32t2 = -(2.0 * wpy * rvs2 * phib), qk32t2 = -(2.0 * wpy * qvs2 * phib);
+                double rk32t3 = -(wpy * rvs2 * phibz), qk32t3 = -(wpy * qvs2 * phibz);
+                for (int iae = 0; iae < nen; iae++) {
+                    size_t ab = 3 * ((size_t)iae + (size_t)nen * q);
+                    double phia = shg[ab + 2], phiax = shg[ab + 0], phiaz = shg[ab + 1];
+                    int ipe = NDIM * iae, iqe = NDIM * ibe;
+                    double rme11 = rm11t1 * phia, qme11 = qm11t1 * phia;
+                    double rme22 = rm22t1 * phia, qme22 = qm22t1 * phia;
+                    double rme33 = rme11, qme33 = qme11;
+                    double rke11 = rk11t1 * phiax + rk11t2 * phiaz;
+                    double qke11 = qk11t1 * phiax + qk11t2 * phiaz;
+                    double rke13 = rk13t1 * phiax + rk13t2 * phiaz + rk13t3 * phiax;
+                    double qke13 = qk13t1 * phiax + qk13t2 * phiaz + qk13t3 * phiax;
+                    double rke22 = rk22t1 * phiax + rk22t2 * phiaz;
+                    double qke22 = qk22t1 * phiax + qk22t2 * phiaz;
+                    double rke31 = rk31t1 * phiaz + rk31t2 * phiax + rk31t3 * phiaz;
+                    double qke31 = qk31t1 * phiaz + qk31t2 * phiax + qk31t3 * phiaz;
+                    double rke33 = rk33t1 * phiaz + rk33t2 * phiax;
+                    double qke33 = qk33t1 * phiaz + qk33t2 * phiax;
+                    double rke12 = rk12t1 * phiax + rk12t2 * phiax + rk12t3 * phia;
+                    double qke12 = qk12t1 * phiax + qk12t2 * phiax + qk12t3 * phia;
+                    double rke21 = rk21t1 * phia + rk21t2 * phia + rk21t3 * phiax;
+                    double qke21 = qk21t1 * phia + qk21t2 * phia + qk21t3 * phiax;
+                    double rke23 = rk23t1 * phia + rk23t2 * phia + rk23t3 * phiaz;
+                    double qke23 = qk23t1 * phia + qk23t2 * phia + qk23t3 * phiaz;
+                    double rke32 = rk32t1 * phiaz + rk32t2 * phiaz + rk32t3 * phia;
+                    double qke32 = qk32t1 * phiaz + qk32t2 * phiaz + qk32t3 * phia;
+                    ME(ipe, iqe) = ME(ipe, iqe) + rme11;
+                    ME(ipe + 1, iqe + 1) = ME(ipe + 1, iqe + 1) + rme22;
+                    ME(ipe + 2, iqe + 2) = ME(ipe + 2, iqe + 2) + rme33;
+                    KE(ipe, iqe) = zadd(KE(ipe, iqe), zmk(rke11, qke11 + qme11));
+                    KE(ipe + 1, iqe + 1) = zadd(KE(ipe + 1, iqe + 1), zmk(rke22, qke22 + qme22));
+                    KE(ipe + 2, iqe + 2) = zadd(KE(ipe + 2, iqe + 2), zmk(rke33, qke33 + qme33));
+                    KE(ipe, iqe + 2) = zadd(KE(ipe, iqe + 2), zmk(rke13, qke13));
+                    KE(ipe + 2, iqe) = zadd(KE(ipe + 2, iqe), zmk(rke31, qke31));
+                    KE(ipe, iqe + 1) = zsub(KE(ipe, iqe + 1), zmk(-qke12, rke12));
+                    KE(ipe + 1, iqe) = zadd(KE(ipe + 1, iqe), zmk(-qke21, rke21));
+                    KE(ipe + 1, iqe + 2) = zadd(KE(ipe + 1, iqe + 2), zmk(-qke23, rke23));
+                    KE(ipe + 2, iqe + 1) = zsub(KE(ipe + 2, iqe + 1), zmk(-qke32, rke32));
+                }
+            }
+        }
+    }
+}
+
+static inline zc zneg(zc a) { return zmk(-a.re, -a.im); }
+
+/* CMDAMP (estiff25.f:756-961): PML version of KMDAMP with the stretched
+ * derivatives d/dx EX, d/dz EZ and complex arithmetic throughout */
+static void cmdamp(int nen, int nint, double freq, double freq0, double py, const double *wts,
+                   const double *vp, const double *vs, const double *qpp, const double *qss,
+                   const double *det, const double *shg, const zc *dampx, const zc *dampz,
+                   double *me, zc *ce)
+{
+    const double TWOPI = 6.2831853071795862;
+    int nee = nen * NDIM;
+    for (int i = 0; i < nee * nee; i++) { me[i] = 0.0; ce[i] = zmk(0.0, 0.0); }
+    double omega = TWOPI * freq, wpy = omega * py;
+    zc cwpy = zmk(0.0, wpy), ztwo = zmk(2.0, 0.0);
+    double py2 = ipow(py, 2), w2 = ipow(omega, 2);
+    for (int intx = 0; intx < nint; intx++) {
+        for (int intz = 0; intz < nint; intz++) {
+            int q = intx + nint * intz;
+            double weight = wts[intx] * wts[intz] * det[q];
+            zc ex = dampx[q], ez = dampz[q];
+            zc zvp2 = zmul(zsq(vcmplx(freq, freq0, vp[q], qpp[q])), zmk(weight, 0.0));
+            zc zvs2 = zmul(zsq(vcmplx(freq, freq0, vs[q], qss[q])), zmk(weight, 0.0));
+            double rvp2 = zvp2.re, qvp2 = zvp2.im, rvs2 = zvs2.re, qvs2 = zvs2.im;
+            double rm1 = -(w2 * weight) + w2 * py2 * rvs2, qm1 = w2 * py2 * qvs2;
+            double rm2 = -(w2 * weight) + w2 * py2 * rvp2, qm2 = w2 * py2 * qvp2;
+            for (int ibe = 0; ibe < nen; ibe++) {
+                size_t bb = 3 * ((size_t)ibe + (size_t)nen * q);
+                double phib = shg[bb + 2];
+                zc phibx = zmul(zmk(shg[bb + 0], 0.0), ex);
+                zc phibz = zmul(zmk(shg[bb + 1], 0.0), ez);
+                zc cphib = zmk(phib, 0.0);
+                double rm11t1 = rm1 * phib, qm11t1 = qm1 * phib;
+                double rm22t1 = rm2 * phib, qm22t1 = qm2 * phib;
+                zc ce11t1 = zmul(zvp2, phibx), ce11t2 = zmul(zvs2, phibz);
+                zc ce13t1 = zmul(zvp2, phibz), ce13t2 = zmul(zvs2, phibx);
+                zc ce13t3 = zneg(zmul(zmul(ztwo, zvs2), phibz));
+                zc ce22t1 = zmul(zvs2, phibx), ce22t2 = zmul(zvs2, phibz);
+                zc ce31t1 = zmul(zvp2, phibx), ce31t2 = zmul(zvs2, phibz);
+                zc ce31t3 = zneg(zmul(zmul(ztwo, zvs2), phibx));
+                zc ce33t1 = zmul(zvp2, phibz), ce33t2 = zmul(zvs2, phibx);
+                zc ce12t1 = zmul(zmul(cwpy, zvp2), cphib);
+                zc ce12t2 = zneg(zmul(zmul(zmul(ztwo, cwpy), zvs2), cphib));
+                zc ce12t3 = zneg(zmul(zmul(cwpy, zvs2), phibx));
+                zc ce21t1 = zmul(zmul(cwpy, zvp2), phibx);
+                zc ce21t2 = zneg(zmul(zmul(zmul(ztwo, cwpy), zvs2), phibx));
+                zc ce21t3 = zneg(zmul(zmul(cwpy, zvs2), cphib));
+                zc ce23t1 = zmul(zmul(cwpy, zvp2), phibz);
+                zc ce23t2 = zneg(zmul(zmul(zmul(ztwo, cwpy), zvs2), phibz));
+                zc ce23t3 = zneg(zmul(zmul(cwpy, zvs2), cphib));
+                zc ce32t1 = zmul(zmul(cwpy, zvp2), cphib);
+                zc ce32t2 = zneg(zmul(zmul(zmul(ztwo, cwpy), zvs2), cphib));
+                zc ce32t3 = zneg(zmul(zmul(cwpy, zvs2), phibz));
+                for (int iae = 0; iae < nen; iae++) {
+                    size_t ab = 3 * ((size_t)iae + (size_t)nen * q);
+                    double phia = shg[ab + 2];
+                    zc phiax = zmul(zmk(shg[ab + 0], 0.0), ex);
+                    zc phiaz = zmul(zmk(shg[ab + 1], 0.0), ez);
+                    zc cphia = zmk(phia, 0.0);
+                    int ipe = NDIM * iae, iqe = NDIM * ibe;
+                    double rme11 = rm11t1 * phia, qme11 = qm11t1 * phia;
+                    double rme22 = rm22t1 * phia, qme22 = qm22t1 * phia;
+                    double rme33 = rme11, qme33 = qme11;
+                    zc ce11 = zadd(zmul(ce11t1, phiax), zmul(ce11t2, phiaz));
+                    zc ce13 = zadd(zadd(zmul(ce13t1, phiax), zmul(ce13t2, phiaz)), zmul(ce13t3, phiax));
+                    zc ce22 = zadd(zmul(ce22t1, phiax), zmul(ce22t2, phiaz));
+                    zc ce31 = zadd(zadd(zmul(ce31t1, phiaz), zmul(ce31t2, phiax)), zmul(ce31t3, phiaz));
+                    zc ce33 = zadd(zmul(ce33t1, phiaz), zmul(ce33t2, phiax));
+                    zc ce12 = zadd(zadd(zmul(ce12t1, phiax), zmul(ce12t2, phiax)), zmul(ce12t3, cphia));
+                    zc ce21 = zadd(zadd(zmul(ce21t1, cphia), zmul(ce21t2, cphia)), zmul(ce21t3, phiax));
+                    zc ce23 = zadd(zadd(zmul(ce23t1, cphia), zmul(ce23t2, cphia)), zmul(ce23t3, phiaz));
+                    zc ce32 = zadd(zadd(zmul(ce32t1, phiaz), zmul(ce32t2, phiaz)), zmul(ce32t3, cphia));
+                    ME(ipe, iqe) = ME(ipe, iqe) + rme11;
+                    ME(ipe + 1, iqe + 1) = ME(ipe + 1, iqe + 1) + rme22;
+                    ME(ipe + 2, iqe + 2) = ME(ipe + 2, iqe + 2) + rme33;
+                    CE(ipe, iqe) = zadd(zadd(CE(ipe, iqe), ce11), zmk(0.0, qme11));
+                    CE(ipe, iqe + 1) = zsub(CE(ipe, iqe + 1), ce12);
+                    CE(ipe, iqe + 2) = zadd(CE(ipe, iqe + 2), ce13);
+                    CE(ipe + 1, iqe) = zadd(CE(ipe + 1, iqe), ce21);
+                    CE(ipe + 1, iqe + 1) = zadd(zadd(CE(ipe + 1, iqe + 1), ce22), zmk(0.0, qme22));
+                    CE(ipe + 1, iqe + 2) = zadd(CE(ipe + 1, iqe + 2), ce23);
+                    CE(ipe + 2, iqe) = zadd(CE(ipe + 2, iqe), ce31);
+                    CE(ipe + 2, iqe + 1) = zsub(CE(ipe + 2, iqe + 1), ce32);
+                    CE(ipe + 2, iqe + 2) = zadd(zadd(CE(ipe + 2, iqe + 2), ce33), zmk(0.0, qme33));
+                }
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
 /* element workspace                                                          */
 /* ------------------------------------------------------------------------ */
 typedef struct {
     int nord, nl, nen, nee, nint, nq;
     double *xigll, *shl, *shg, *det, *rho, *vlam, *vmu, *me;
+    double *vp, *vs, *qpp, *qss;   /* dispersive media */
     zc *ke, *dampx, *dampz;
 } orc_ws;
 
@@ -560,6 +826,10 @@ static void ws_init(orc_ws *w, int nord)
     w->rho = (double *)malloc(sizeof(double) * w->nq);
     w->vlam = (double *)malloc(sizeof(double) * w->nq);
     w->vmu = (double *)malloc(sizeof(double) * w->nq);
+    w->vp = (double *)malloc(sizeof(double) * w->nq);
+    w->vs = (double *)malloc(sizeof(double) * w->nq);
+    w->qpp = (double *)malloc(sizeof(double) * w->nq);
+    w->qss = (double *)malloc(sizeof(double) * w->nq);
     w->me = (double *)malloc(sizeof(double) * w->nee * w->nee);
     w->ke = (zc *)malloc(sizeof(zc) * w->nee * w->nee);
     w->dampx = (zc *)malloc(sizeof(zc) * w->nq);
@@ -571,10 +841,11 @@ static void ws_free(orc_ws *w)
 {
     free(w->xigll); free(w->shl); free(w->shg); free(w->det); free(w->rho);
     free(w->vlam); free(w->vmu); free(w->me); free(w->ke); free(w->dampx); free(w->dampz);
+    free(w->vp); free(w->vs); free(w->qpp); free(w->qss);
 }
 
 /* element matrices of one element as ASMBLE_DRIVER builds them
- * (asmble.f90:140-204), non-dispersive isotropic media */
+ * (asmble.f90:140-204), isotropic media, dispersive when m->ldisp */
 static int element_mats(const orc_mesh *m, orc_ws *w, int ielem, char cftype, double freq,
                         double py)
 {
@@ -582,6 +853,20 @@ static int element_mats(const orc_mesh *m, orc_ws *w, int ielem, char cftype, do
     double omega = TWOPI * freq;
     int k = (cftype == 'S') ? 0 : 1;
     const double *wts = w->xigll + w->nint;
+    if (m->ldisp) {
+        int pml = m->cdomain[ielem] == 'A';
+        if (cj_qual(m, ielem, w->nen, w->nint, w->xigll, w->shl, pml, omega, m->rcoeff[k],
+                    m->dmax[k], m->kappa[k], m->fcent[k], w->det, w->vp, w->vs, w->qpp, w->qss,
+                    w->shg, w->dampx, w->dampz))
+            return 1;
+        if (!pml)
+            kmdamp(w->nen, w->nint, freq, m->freq0, py, wts, w->vp, w->vs, w->qpp, w->qss, w->det,
+                   w->shg, w->me, w->ke);
+        else
+            cmdamp(w->nen, w->nint, freq, m->freq0, py, wts, w->vp, w->vs, w->qpp, w->qss, w->det,
+                   w->shg, w->dampx, w->dampz, w->me, w->ke);
+        return 0;
+    }
     if (m->cdomain[ielem] != 'A') {
         if (cjmk_tvi(m, ielem, w->nen, w->nint, w->xigll, w->shl, w->det, w->rho, w->vlam,
                      w->vmu, w->shg))

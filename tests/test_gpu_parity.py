@@ -277,3 +277,47 @@ def test_nzloc_mismatch_is_rejected(case0):
     buf = np.zeros(4, np.complex64)
     r = L().fem25_asmble_driver(ctx.h, 4, b"B", 0.5, 0.0, buf.ctypes.data_as(ctypes.c_void_p))
     assert r == 1
+
+
+# ---------------------------------------------------------------------------
+# dispersive media (KMDAMP / CMDAMP): plain path only
+# ---------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def case_disp():
+    mesh, pairs, _ = synth.make_config(0, nx=8, nz=5)
+    synth.make_dispersive(mesh, seed=5, freq0=1.0, qs_mean=30.0)
+    g = oracle.graph_build(mesh)
+    ctx = Context(mesh, g)
+    yield mesh, pairs, g, ctx
+    ctx.close()
+
+
+def test_dispersive_plain_assembly_matches_oracle(case_disp):
+    """KMDAMP (interior, Bielak) and CMDAMP (PML) elements: complex128 CSR and
+    the COMPLEX*8 CDIST bit-identical to the oracle, below and above FREQ0."""
+    mesh, pairs, g, ctx = case_disp
+    for (f, py, cft) in ((0.5, pairs[6][1], "B"), (1.7, pairs[11][1], "S")):
+        ref128, ref64 = oracle.asmble(mesh, g, cft, f, py)
+        o128 = torch.zeros(g.nzero, dtype=torch.complex128, device=_dev())
+        o64 = torch.zeros(g.nzero, dtype=torch.complex64, device=_dev())
+        ctx.assemble(cft, f, py, o128, o64)
+        torch.cuda.synchronize()
+        a128 = o128.cpu().numpy()
+        assert np.array_equal(a128.view(np.uint64), ref128.view(np.uint64)), f
+        assert np.array_equal(o64.cpu().numpy().view(np.uint32), ref64.view(np.uint32)), f
+    out = ctx.asmble_driver("B", 0.5, pairs[6][1])
+    _, ref64 = oracle.asmble(mesh, g, "B", 0.5, pairs[6][1])
+    assert np.array_equal(out.view(np.uint32), ref64.view(np.uint32))
+
+
+def test_dispersive_batched_and_gradient_rejected(case_disp):
+    mesh, pairs, g, ctx = case_disp
+    ring = torch.zeros(2 * g.nzero, dtype=torch.float64, device=_dev())
+    with pytest.raises(Fem25Error) as ei:
+        ctx.assemble_batch(["B"], [0.5], [0.0], ring, 2 * g.nzero, 1)
+    assert ei.value.code == 7
+    u = torch.zeros((1, 1, g.ndof), dtype=torch.complex128, device=_dev())
+    d_g = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=_dev())
+    with pytest.raises(Fem25Error) as ei:
+        ctx.gradient([0.5], [0.0], 1, u, u, d_g)
+    assert ei.value.code == 7

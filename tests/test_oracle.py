@@ -172,3 +172,53 @@ def _perturbed(mesh, m3):
     m.ecoeff = np.ascontiguousarray(m3[:2])
     m.dens = np.ascontiguousarray(m3[2])
     return m
+
+
+# ---------------------------------------------------------------------------
+# dispersive media (KMDAMP / CMDAMP with VCMPLX complex velocities)
+# ---------------------------------------------------------------------------
+def _homogeneous(nx=6, nz=4):
+    mesh, pairs, _ = synth.make_config(0, nx=nx, nz=nz)
+    synth.set_model_from_velocities(mesh, np.full(mesh.nnpg, 3000.0), np.full(mesh.nnpg, 1730.0),
+                                    np.full(mesh.nnpg, 2500.0))
+    return mesh, pairs
+
+
+@pytest.mark.parametrize("dom", ["I", "A"])
+def test_dispersive_without_damping_is_density_normalised(dom):
+    """All Q = 9999 (the reference's 'no damping'), homogeneous medium:
+    KMDAMP / CMDAMP interpolate velocities instead of moduli and leave out
+    the density, so A_disp = A_standard / rho up to rounding (all 9 blocks,
+    stiffness, mass and the i omega py terms, PML stretching included)."""
+    mesh, pairs = _homogeneous()
+    e = int(np.flatnonzero(mesh.cdomain == ord(dom))[0])
+    f, py = pairs[9]
+    me, ce = oracle.element_matrix(mesh, e, "B", f, py)
+    ref = (me + ce) / 2500.0
+    mesh.qp = np.full(mesh.nnpg, 9999.0)
+    mesh.qs = np.full(mesh.nnpg, 9999.0)
+    mesh.freq0, mesh.ldisp = 1.0, True
+    me_d, ce_d = oracle.element_matrix(mesh, e, "B", f, py)
+    got = me_d + ce_d
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_dispersive_damping_scales_with_inverse_q():
+    """Finite Q: the operator departs from the undamped one by O(1/Q)
+    (Aki & Richards 5.94: v (1 + ln(f/f0)/(pi Q)) - i v / (2Q)); doubling Q
+    halves the departure to first order, and Q = 9999 gives none."""
+    mesh, pairs = _homogeneous()
+    e = int(np.flatnonzero(mesh.cdomain == ord("I"))[0])
+    f, py = 0.5, pairs[5][1]
+    mesh.freq0, mesh.ldisp = 1.0, True
+
+    def op(qp, qs):
+        mesh.qp = np.full(mesh.nnpg, qp)
+        mesh.qs = np.full(mesh.nnpg, qs)
+        me, ce = oracle.element_matrix(mesh, e, "B", f, py)
+        return me + ce
+
+    a0 = op(9999.0, 9999.0)
+    d1 = np.abs(op(2.25 * 200.0, 200.0) - a0).max()
+    d2 = np.abs(op(2.25 * 400.0, 400.0) - a0).max()
+    assert d1 > 0 and abs(d1 / d2 - 2.0) < 0.05
