@@ -543,6 +543,25 @@ int fem25_ref_gradient_dev(fem25_ctx *h, const char *cinvtype, double vpvs, doub
   return FEM25_OK;
 }
 
+int fem25_ref_vforce2_dev(fem25_ctx *h, const char *cinvtype, double freq, double py,
+                          const float *wave, float *fmat, void *stream) {
+  if (!h || !cinvtype || !wave || !fmat) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  std::string ct(cinvtype, cinvtype + 2);
+  int lisp = 0, liss = 0;
+  if (ct == "PP" || ct == "pp") lisp = 1;
+  else if (ct == "SS" || ct == "ss") liss = 1;
+  else if (ct == "PS" || ct == "ps") lisp = liss = 1;
+  else return fail(c, FEM25_ERR_ARG, "vforce25_2: CINVTYPE must be PP, SS or PS");
+  CK(cudaSetDevice(c->device), "set device");
+  int r = ensure_refgrad(c);
+  if (r) return r;
+  CK(launch_ref_vforce2(c, lisp, liss, 6.2831853071795862 * freq, py, wave, fmat,
+                        (cudaStream_t)stream),
+     "vforce25_2");
+  return FEM25_OK;
+}
+
 int fem25_misfit_dev(fem25_ctx *h, int nsrc, int nrec, const int *mrdof, const double *yrec,
                      double freq, double py, double azmod, const float *recv, const float *sol,
                      const float *obs, const float *wghts, float *est, float *rhs, float *misfit,

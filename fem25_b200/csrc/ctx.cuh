@@ -129,6 +129,8 @@ cudaError_t launch_grad_tc(Ctx *c, int npairs, int nsrc, const double *u, const 
 cudaError_t launch_ref_cfmat(Ctx *c, int lisp, double vpvs, double omega, double py,
                              const float *wave, int accumulate, cudaStream_t st);
 cudaError_t launch_ref_adjflam(Ctx *c, const float *adjlam, float *gradl, cudaStream_t st);
+cudaError_t launch_ref_vforce2(Ctx *c, int lisp, int liss, double omega, double py,
+                               const float *wave, float *fmat, cudaStream_t st);
 cudaError_t launch_misfit(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const float *d_trig,
                           double omega, double py, double azmod, const float *d_recv,
                           const float *sol, const float *d_obs, const float *d_wghts,

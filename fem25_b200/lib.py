@@ -63,6 +63,7 @@ def lib():
         L.fem25_gradient_dev.argtypes = [vp, i, vp, vp, i, vp, vp, i, vp, vp]
         L.fem25_ref_gradient_dev.argtypes = [vp, C.c_char_p, d, d, d, vp, vp, i, vp, vp]
         L.fem25_ref_gradient_info.argtypes = [vp, C.POINTER(i), C.POINTER(ll), vp]
+        L.fem25_ref_vforce2_dev.argtypes = [vp, C.c_char_p, d, d, vp, vp, vp]
         L.fem25_misfit_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp, vp]
         L.fem25_misfit_noalloc_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp,
                                                vp]
@@ -259,6 +260,11 @@ class Context:
         self._check(lib().fem25_ref_gradient_dev(self.h, cinvtype.encode(), vpvs, freq, py,
                                                  _ptr(wave), _ptr(adjlam), 1 if accumulate else 0,
                                                  _ptr(gradl), _stream(stream)))
+
+    def vforce2(self, cinvtype, freq, py, wave, fmat, stream=None):
+        """VFORCE25_2 / DABMKISOB25 virtual forces into fmat (COMPLEX*8 [nvinv][nz])."""
+        self._check(lib().fem25_ref_vforce2_dev(self.h, cinvtype.encode(), freq, py, _ptr(wave),
+                                                _ptr(fmat), _stream(stream)))
 
     # ---- misfit
     def misfit(self, nsrc, mrdof, yrec, freq, py, azmod, recv, sol, obs, wghts, rhs, stream=None):

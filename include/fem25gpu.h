@@ -141,6 +141,17 @@ int fem25_ref_gradient_dev(fem25_ctx *ctx, const char *cinvtype, double vpvs, do
 int fem25_ref_gradient_info(fem25_ctx *ctx, int *nnpinv, long long *nz_fdist,
                             int *maskg /* [NNPG], nullable */);
 
+/* Virtual forces of VFORCE25_2 (vforce25.f:373-607) with the alpha / beta
+ * derivative matrices of DABMKISOB25 (dstiff25.f:1-203), the convention of
+ * the reference's Gauss-Newton / Hessian routines (qpmfree.f90:1119): for
+ * every inversion anchor p, F_p(row) = sum over the connected elements (MCONN
+ * order, no element weights, no reset between elements) of
+ * CMPLX(DCMPLX(DMD,0) + DKD)(row,col) * WAVE(col) in COMPLEX*8.  cinvtype
+ * 'PP', 'SS' or 'PS'; fmat COMPLEX*8 [nvinv][NZ_FDIST] on the device with the
+ * CSC pattern of fem25_ref_gradient_info (alpha first for 'PS'). */
+int fem25_ref_vforce2_dev(fem25_ctx *ctx, const char *cinvtype, double freq, double py,
+                          const float *wave, float *fmat, void *stream);
+
 /* ---- forward misfit + adjoint source ---------------------------------------
  * EXRESP25D (locrec2d.f:867-925) + rotation + CRESID/BPRESID4 L2 + COBJ4 +
  * RESID_DRHS (adjgrad.f90:448-523) for nsrc solutions at once.

@@ -74,6 +74,9 @@ def _setup(L):
     L.orc_cfmat_dist.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, vp, vp, vp, C.c_int,
                                  C.c_double, C.c_double, C.c_double, vp, vp, C.c_int]
     L.orc_adjflam.argtypes = [C.c_int, vp, vp, vp, vp, vp]
+    L.orc_dabm_element.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_double, vp, vp, vp, vp]
+    L.orc_vforce2.argtypes = [vp, vp, vp, vp, C.c_int, vp, vp, C.c_longlong, C.c_int, C.c_int,
+                              C.c_double, C.c_double, vp, vp]
     L.orc_misfit.argtypes = [C.c_int, C.c_int, vp, vp, C.c_double, C.c_double, C.c_double,
                              vp, vp, vp, vp, vp, vp]
     L.orc_misfit.restype = C.c_float
@@ -167,6 +170,19 @@ def element_matrix(mesh, ielem, cftype, freq, py):
     return me, ce
 
 
+def dabm_element(mesh, ielem, inpg, freq, py):
+    """DABMKISOB25 (dM/dalpha, dK/dalpha, dM/dbeta, dK/dbeta) of one element
+    for anchor ``inpg`` (1-based), column-major 75x75."""
+    om = OracleMesh(mesh)
+    nee = 3 * (mesh.nord + 1) ** 2
+    out = [np.empty((nee, nee), order="F"), np.empty((nee, nee), np.complex128, order="F"),
+           np.empty((nee, nee), order="F"), np.empty((nee, nee), np.complex128, order="F")]
+    ierr = lib().orc_dabm_element(om.ptr, ielem, inpg, freq, py, *[_p(a) for a in out])
+    if ierr:
+        raise RuntimeError(f"element {ielem}: Jacobian check failed")
+    return out
+
+
 def asmble(mesh, g, cftype, freq, py, elo=0, ehi=None, want64=True):
     """ASMBLE_DRIVER over elements [elo, ehi): (csr128, csr64)."""
     om = OracleMesh(mesh)
@@ -252,6 +268,19 @@ class RefGrad:
                                     1 if accumulate else 0)
         if ierr:
             raise RuntimeError(f"oracle cfmat ierr={ierr}")
+        return out
+
+    def vforce2(self, freq, py, wave64, cinvtype="PP"):
+        """VFORCE25_2 forces with DABMKISOB25 matrices: COMPLEX*8 [nvinv, nz]."""
+        lisp = cinvtype.upper() in ("PP", "PS")
+        liss = cinvtype.upper() in ("SS", "PS")
+        out = np.zeros((int(lisp) + int(liss), self.nz), np.complex64)
+        ierr = lib().orc_vforce2(self.om.ptr, _p(self.g.lm), _p(self.maskg), _p(self.mconn),
+                                 self.ncon, _p(self.jcsc), _p(self.icsc), self.nz, int(lisp),
+                                 int(liss), freq, py,
+                                 _p(np.ascontiguousarray(wave64, np.complex64)), _p(out))
+        if ierr:
+            raise RuntimeError(f"oracle vforce2 ierr={ierr}")
         return out
 
     def adjflam(self, fmat, adjlam64, gradl=None):

@@ -1741,6 +1741,143 @@ static void dkm_vpvs(int nen, int nint, double omega, double py, const double *w
         }
 }
 
+/* DABMKISOB25 (dstiff25.f:1-203): derivatives of the density-normalised
+ * element operator with respect to the anchor's alpha (LISP) and beta (LISS)
+ * with DAB from DJACAB (2 alpha N_p, 2 beta N_p).  The reference resets
+ * DMDA(IPE,IQE) and DMDA(IPE+2,IQE+2) to zero and copies DMDB(IPE,IQE) into
+ * DMDB(IPE+2,IQE+2) at every point (dstiff25.f:133-143); kept. */
+static void dabmkisob25(int nen, int nint, int lisp, int liss, double omega, double py,
+                        const double *wts, const double *det, const double *dab1,
+                        const double *dab2, const double *shg, double *dmda, double *dmdb,
+                        zc *dkda, zc *dkdb)
+{
+    int nee = nen * NDIM;
+    for (int i = 0; i < nee * nee; i++) {
+        dmda[i] = 0.0; dmdb[i] = 0.0; dkda[i] = zmk(0.0, 0.0); dkdb[i] = zmk(0.0, 0.0);
+    }
+    double wpy = omega * py, wpy2 = ipow(omega * py, 2);
+    for (int intx = 0; intx < nint; intx++)
+        for (int intz = 0; intz < nint; intz++) {
+            int q = intx + nint * intz;
+            double weight = wts[intx] * wts[intz] * det[q];
+            double dalpha = dab1[q] * weight, dbeta = dab2[q] * weight;
+            double dmassda = wpy2 * dalpha, dmassdb = wpy2 * dbeta;
+            for (int ibe = 0; ibe < nen; ibe++) {
+                size_t bb = 3 * ((size_t)ibe + (size_t)nen * q);
+                double phib = shg[bb + 2], phibx = shg[bb + 0], phibz = shg[bb + 1];
+                double dmdat1 = 0.0, dk11da = 0.0, dk13da = 0.0, dk31da = 0.0, dk33da = 0.0;
+                double dk12da = 0.0, dk21da = 0.0, dk23da = 0.0, dk32da = 0.0;
+                double dmdbt1 = 0.0, dk11dbt1 = 0.0, dk13dbt1 = 0.0, dk13dbt2 = 0.0;
+                double dk22dbt1 = 0.0, dk22dbt2 = 0.0, dk31dbt1 = 0.0, dk31dbt2 = 0.0;
+                double dk33dbt1 = 0.0, dk12dbt1 = 0.0, dk12dbt2 = 0.0, dk21dbt1 = 0.0;
+                double dk21dbt2 = 0.0, dk23dbt1 = 0.0, dk23dbt2 = 0.0, dk32dbt1 = 0.0;
+                double dk32dbt2 = 0.0;
+                if (lisp) {
+                    dmdat1 = dmassda * phib;
+                    dk11da = dalpha * phibx;
+                    dk13da = dalpha * phibz;
+                    dk31da = dalpha * phibx;
+                    dk33da = dalpha * phibz;
+                    dk12da = wpy * dalpha * phib;
+                    dk21da = wpy * dalpha * phibx;
+                    dk23da = wpy * dalpha * phibz;
+                    dk32da = wpy * dalpha * phib;
+                }
+                if (liss) {
+                    dmdbt1 = dmassdb * phib;
+                    dk11dbt1 = dbeta * phibz;
+                    dk13dbt1 = dbeta * phibx;
+                    dk13dbt2 = -(2.0 * dbeta * phibz);
+                    dk22dbt1 = dbeta * phibx;
+                    dk22dbt2 = dbeta * phibz;
+                    dk31dbt1 = dbeta * phibz;
+                    dk31dbt2 = -(2.0 * dbeta * phibx);
+                    dk33dbt1 = dbeta * phibx;
+                    dk12dbt1 = 2.0 * wpy * dbeta * phib;
+                    dk12dbt2 = wpy * dbeta * phibx;
+                    dk21dbt1 = 2.0 * wpy * dbeta * phibx;
+                    dk21dbt2 = wpy * dbeta * phib;
+                    dk23dbt1 = 2.0 * wpy * dbeta * phibz;
+                    dk23dbt2 = wpy * dbeta * phib;
+                    dk32dbt1 = 2.0 * wpy * dbeta * phib;
+                    dk32dbt2 = wpy * dbeta * phibz;
+                }
+                for (int iae = 0; iae < nen; iae++) {
+                    size_t ab = 3 * ((size_t)iae + (size_t)nen * q);
+                    double phia = shg[ab + 2], phiax = shg[ab + 0], phiaz = shg[ab + 1];
+                    int ipe = NDIM * iae, iqe = NDIM * ibe;
+#define DMDA(i, j) dmda[(i) + nee * (j)]
+#define DMDB(i, j) dmdb[(i) + nee * (j)]
+#define DKDA(i, j) dkda[(i) + nee * (j)]
+#define DKDB(i, j) dkdb[(i) + nee * (j)]
+                    if (lisp) {
+                        DMDA(ipe, iqe) = 0.0;
+                        DMDA(ipe + 1, iqe + 1) = DMDA(ipe + 1, iqe + 1) + dmdat1 * phia;
+                        DMDA(ipe + 2, iqe + 2) = 0.0;
+                    }
+                    if (liss) {
+                        DMDB(ipe, iqe) = DMDB(ipe, iqe) + dmdbt1 * phia;
+                        DMDB(ipe + 1, iqe + 1) = 0.0;
+                        DMDB(ipe + 2, iqe + 2) = DMDB(ipe, iqe);
+                    }
+                    if (lisp) {
+                        zc dke11 = zmk(phiax * dk11da, 0.0), dke13 = zmk(phiax * dk13da, 0.0);
+                        zc dke22 = zmk(0.0, 0.0);
+                        zc dke31 = zmk(phiaz * dk31da, 0.0), dke33 = zmk(phiaz * dk33da, 0.0);
+                        zc dke12 = zmk(0.0, phiax * dk12da), dke21 = zmk(0.0, phia * dk21da);
+                        zc dke23 = zmk(0.0, phia * dk23da), dke32 = zmk(0.0, phiaz * dk32da);
+                        DKDA(ipe, iqe) = zadd(DKDA(ipe, iqe), dke11);
+                        DKDA(ipe, iqe + 1) = zsub(DKDA(ipe, iqe + 1), dke12);
+                        DKDA(ipe, iqe + 2) = zadd(DKDA(ipe, iqe + 2), dke13);
+                        DKDA(ipe + 1, iqe) = zadd(DKDA(ipe + 1, iqe), dke21);
+                        DKDA(ipe + 1, iqe + 1) = zadd(DKDA(ipe + 1, iqe + 1), dke22);
+                        DKDA(ipe + 1, iqe + 2) = zadd(DKDA(ipe + 1, iqe + 2), dke23);
+                        DKDA(ipe + 2, iqe) = zadd(DKDA(ipe + 2, iqe), dke31);
+                        DKDA(ipe + 2, iqe + 1) = zsub(DKDA(ipe + 2, iqe + 1), dke32);
+                        DKDA(ipe + 2, iqe + 2) = zadd(DKDA(ipe + 2, iqe + 2), dke33);
+                    }
+                    if (liss) {
+                        zc dke11 = zmk(phiaz * dk11dbt1, 0.0);
+                        zc dke13 = zmk(phiaz * dk13dbt1 + phiax * dk13dbt2, 0.0);
+                        zc dke22 = zmk(phiax * dk22dbt1 + phiaz * dk22dbt2, 0.0);
+                        zc dke31 = zmk(phiax * dk31dbt1 + phiaz * dk31dbt2, 0.0);
+                        zc dke33 = zmk(phiax * dk33dbt1, 0.0);
+                        zc dke12 = zmk(0.0, phiax * dk12dbt1 + phia * dk12dbt2);
+                        zc dke21 = zmk(0.0, phia * dk21dbt1 + phiax * dk21dbt2);
+                        zc dke23 = zmk(0.0, phia * dk23dbt1 + phiaz * dk23dbt2);
+                        zc dke32 = zmk(0.0, phiaz * dk32dbt1 + phia * dk32dbt2);
+                        DKDB(ipe, iqe) = zadd(DKDB(ipe, iqe), dke11);
+                        DKDB(ipe, iqe + 1) = zadd(DKDB(ipe, iqe + 1), dke12);
+                        DKDB(ipe, iqe + 2) = zadd(DKDB(ipe, iqe + 2), dke13);
+                        DKDB(ipe + 1, iqe) = zsub(DKDB(ipe + 1, iqe), dke21);
+                        DKDB(ipe + 1, iqe + 1) = zadd(DKDB(ipe + 1, iqe + 1), dke22);
+                        DKDB(ipe + 1, iqe + 2) = zsub(DKDB(ipe + 1, iqe + 2), dke23);
+                        DKDB(ipe + 2, iqe) = zadd(DKDB(ipe + 2, iqe), dke31);
+                        DKDB(ipe + 2, iqe + 1) = zadd(DKDB(ipe + 2, iqe + 1), dke32);
+                        DKDB(ipe + 2, iqe + 2) = zadd(DKDB(ipe + 2, iqe + 2), dke33);
+                    }
+                }
+            }
+        }
+}
+
+/* exported: DABMKISOB25 matrices of element ielem for anchor inpg (1-based) */
+int orc_dabm_element(const orc_mesh *m, int ielem, int inpg, double freq, double py,
+                     double *dmda, double *dkda, double *dmdb, double *dkdb)
+{
+    const double TWOPI = 6.2831853071795862;
+    orc_ws w;
+    ws_init(&w, m->nord);
+    double *dab1 = (double *)malloc(sizeof(double) * w.nq), *dab2 = (double *)malloc(sizeof(double) * w.nq);
+    int ierr = djacab(m, ielem, inpg, w.nen, w.nint, w.xigll, w.shl, w.det, dab1, dab2, w.shg);
+    if (!ierr)
+        dabmkisob25(w.nen, w.nint, 1, 1, TWOPI * freq, py, w.xigll + w.nint, w.det, dab1, dab2,
+                    w.shg, dmda, dmdb, (zc *)dkda, (zc *)dkdb);
+    free(dab1); free(dab2);
+    ws_free(&w);
+    return ierr;
+}
+
 typedef struct { float re, im; } cc;
 static inline cc cmk(float a, float b) { cc z; z.re = a; z.im = b; return z; }
 static inline cc cmulf(cc a, cc b) { return cmk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
@@ -1808,6 +1945,73 @@ int orc_cfmat_dist(const orc_mesh *m, const int *lm, int ndof, const int *maskg,
         }
     }
     free(dab1); free(dab2); free(dvp); free(dvs);
+    ws_free(&w);
+    return ierr;
+}
+
+/*
+ * VFORCE25_2 (vforce25.f:373-607) for every inversion anchor (MASKG order):
+ * F_p(row, ivinv) += CMPLX(DCMPLX(DMD*,0) + DKD*)(row, col) * WAVE(col) over
+ * the connected elements in MCONN order, COMPLEX*8 arithmetic, no element
+ * weights and no reset between elements.  Rows are the CSC pattern of
+ * GRADPTRS.  fmat: COMPLEX*8 [nvinv][nz], variables alpha then beta.
+ */
+int orc_vforce2(const orc_mesh *m, const int *lm, const int *maskg, const int *mconn, int ncon,
+                const int *jcsc, const int *icsc, long long nz, int lisp, int liss, double freq,
+                double py, const float *wave, float *fmat)
+{
+    const double TWOPI = 6.2831853071795862;
+    double omega = TWOPI * freq;
+    orc_ws w;
+    ws_init(&w, m->nord);
+    int nen = w.nen, nee = w.nee, nq = w.nq, nint = w.nint;
+    const double *wts = w.xigll + nint;
+    double *dab1 = (double *)malloc(sizeof(double) * nq), *dab2 = (double *)malloc(sizeof(double) * nq);
+    double *dmdb = (double *)malloc(sizeof(double) * nee * nee);
+    zc *dkdb = (zc *)malloc(sizeof(zc) * nee * nee);
+    int ierr = 0, inpgl = 0;
+    for (int p = 0; p < m->nnpg && !ierr; p++) {
+        if (maskg[p] <= 0) continue;
+        inpgl++;
+        int i1 = jcsc[inpgl - 1], i2 = jcsc[inpgl] - 1, nnzrow = i2 - i1 + 1;
+        for (int v = 0; v < lisp + liss; v++)
+            for (int k = 0; k < 2 * nnzrow; k++) fmat[2 * (size_t)(v * nz + i1 - 1) + k] = 0.0f;
+        for (int ic = 0; ic < ncon; ic++) {
+            int e = mconn[p + (size_t)m->nnpg * ic];
+            if (e <= 0) break;
+            ierr = djacab(m, e - 1, p + 1, nen, nint, w.xigll, w.shl, w.det, dab1, dab2, w.shg);
+            if (ierr) break;
+            dabmkisob25(nen, nint, lisp, liss, omega, py, wts, w.det, dab1, dab2, w.shg, w.me, dmdb,
+                        w.ke, dkdb);
+            const int *lme = lm + (size_t)3 * nen * (e - 1);
+            for (int ipe = 0; ipe < nee; ipe++) {
+                int idof = lme[ipe];
+                if (idof <= 0) continue;
+                int inz = ibsect(nnzrow, idof, icsc + (i1 - 1));
+                if (inz <= 0 || inz > nnzrow) { ierr = 3; break; }
+                for (int iqe = 0; iqe < nee; iqe++) {
+                    int jdof = lme[iqe];
+                    if (jdof <= 0) continue;
+                    cc wv = cmk(wave[2 * (jdof - 1)], wave[2 * (jdof - 1) + 1]);
+                    int v = 0;
+                    for (int var = 0; var < 2; var++) {
+                        if ((var == 0 && !lisp) || (var == 1 && !liss)) continue;
+                        const double *dm = var == 0 ? w.me : dmdb;
+                        const zc *dk = var == 0 ? w.ke : dkdb;
+                        double ar = dm[ipe + nee * iqe] + dk[ipe + nee * iqe].re;
+                        double ai = 0.0 + dk[ipe + nee * iqe].im;
+                        cc t = cmulf(cmk((float)ar, (float)ai), wv);
+                        float *f = fmat + 2 * ((size_t)v * nz + i1 - 1 + inz - 1);
+                        f[0] = f[0] + t.re;
+                        f[1] = f[1] + t.im;
+                        v++;
+                    }
+                }
+            }
+            if (ierr) break;
+        }
+    }
+    free(dab1); free(dab2); free(dmdb); free(dkdb);
     ws_free(&w);
     return ierr;
 }

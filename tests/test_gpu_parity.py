@@ -7,7 +7,7 @@ magnitude, the definition used for every CSR error in this repository):
   * batched affine assembly vs oracle FP64:        <= 1e-12
   * exact gradient FP64 vs oracle:                 <= 1e-10 relative (2-norm)
   * exact gradient 3xTF32 tensor cores vs oracle:  <= 2e-5 relative (2-norm)
-  * reference-compatible gradient, P_eff, misfit:  bit-exact
+  * reference-compatible gradient, VFORCE25_2 forces, P_eff, misfit: bit-exact
 """
 import numpy as np
 import pytest
@@ -221,6 +221,22 @@ def test_reference_gradient_matches_oracle(case0, cinv, accumulate):
     ctx.cfmat_adjgrad(cinv, 1.7320508075688772, f, py, torch.from_numpy(wave).to(_dev()),
                       torch.from_numpy(lam).to(_dev()), d_g, accumulate=accumulate)
     got = d_g.cpu().numpy()
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.parametrize("cinv", ["PP", "SS", "PS"])
+def test_vforce2_matches_oracle(case0, cinv):
+    """VFORCE25_2 virtual forces with the DABMKISOB25 alpha / beta matrices:
+    every COMPLEX*8 value bit-identical to the oracle."""
+    mesh, pairs, g, ctx = case0
+    rg = oracle.RefGrad(mesh, g)
+    rng = np.random.default_rng(8)
+    wave = (rng.standard_normal(g.ndof) + 1j * rng.standard_normal(g.ndof)).astype(np.complex64)
+    f, py = pairs[10]
+    ref = rg.vforce2(f, py, wave, cinv)
+    d_f = torch.full(ref.shape, float("nan"), dtype=torch.complex64, device=_dev())
+    ctx.vforce2(cinv, f, py, torch.from_numpy(wave).to(_dev()), d_f)
+    got = d_f.cpu().numpy()
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
 
 

@@ -222,3 +222,42 @@ def test_dispersive_damping_scales_with_inverse_q():
     d1 = np.abs(op(2.25 * 200.0, 200.0) - a0).max()
     d2 = np.abs(op(2.25 * 400.0, 400.0) - a0).max()
     assert d1 > 0 and abs(d1 / d2 - 2.0) < 0.05
+
+
+# ---------------------------------------------------------------------------
+# DABMKISOB25: alpha / beta derivatives of the density-normalised operator
+# ---------------------------------------------------------------------------
+def test_dabmkisob25_matches_central_difference():
+    """With rho = 1 the KM25ISOQ operator interpolates alpha^2 = lambda + 2 mu
+    and beta^2 = mu, the model DABMKISOB25 differentiates (DAB = 2 alpha N_p,
+    2 beta N_p).  The operator is quadratic in alpha_p and beta_p, so a
+    central difference reproduces dM/dalpha + dK/dalpha and the beta pair up
+    to rounding (all 9 blocks, mass and the i omega py terms)."""
+    mesh, pairs, _ = synth.make_config(0, nx=6, nz=4)
+    rng = np.random.default_rng(4)
+    vp = 3000.0 * (1 + 0.05 * rng.uniform(-1, 1, mesh.nnpg))
+    vs = 1730.0 * (1 + 0.05 * rng.uniform(-1, 1, mesh.nnpg))
+    synth.set_model_from_velocities(mesh, vp, vs, np.ones(mesh.nnpg))
+    e = int(np.flatnonzero(mesh.cdomain == ord("I"))[0])
+    inpg = int(mesh.ieng[e, 2])          # an anchor of the element (1-based)
+    f, py = pairs[7]
+    dmda, dkda, dmdb, dkdb = oracle.dabm_element(mesh, e, inpg, f, py)
+    p = inpg - 1
+    a0, b0 = vp[p], vs[p]
+
+    def op(alpha, beta):
+        m = synth.make_config(0, nx=6, nz=4)[0]
+        a, b = vp.copy(), vs.copy()
+        a[p], b[p] = alpha, beta
+        synth.set_model_from_velocities(m, a, b, np.ones(m.nnpg))
+        me, ce = oracle.element_matrix(m, e, "B", f, py)
+        return me + ce
+
+    h = 1e-3 * a0
+    fd_a = (op(a0 + h, b0) - op(a0 - h, b0)) / (2 * h)
+    got_a = dmda + dkda
+    assert np.abs(got_a - fd_a).max() <= 1e-8 * np.abs(fd_a).max()
+    h = 1e-3 * b0
+    fd_b = (op(a0, b0 + h) - op(a0, b0 - h)) / (2 * h)
+    got_b = dmdb + dkdb
+    assert np.abs(got_b - fd_b).max() <= 1e-8 * np.abs(fd_b).max()
