@@ -198,6 +198,20 @@ def pipeline_uneven(local, dev):
     ctx.assemble_batch("B", freqs[:nslots], pys[:nslots], ring, 2 * nz, nslots, stream=stream)
     torch.cuda.synchronize()
     t_basm = timed(lambda: ctx.assemble_batch("B", freqs, pys, ring, 2 * nz, nslots, stream=stream))
+    # the same batch recorded once into a CUDA graph and replayed: no host
+    # work per launch (system tables are kernel parameters)
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(stream)
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(graph, stream=side):
+            ctx.assemble_batch("B", freqs, pys, ring, 2 * nz, nslots,
+                               stream=torch.cuda.current_stream(dev))
+    stream.wait_stream(side)
+    graph.replay()
+    torch.cuda.synchronize()
+    t_basm_graph = timed(graph.replay, reps=3)
+    del graph
     k = npairs - 1
     slot = ring[(k % nslots) * 2 * nz:(k % nslots + 1) * 2 * nz].clone()
     del ring
@@ -240,13 +254,17 @@ def pipeline_uneven(local, dev):
     torch.cuda.empty_cache()
     plain_total = (t_pasm + t_g64) * npairs
     batched_total = t_basm + t_g32 * npairs
+    batched_graph_total = t_basm_graph + t_g32 * npairs
     units = mesh.nelem * nsrc
     return {"workload": f"uneven batch: 600x200 jittered deg-4 mesh with topography, strip 4 "
                         f"({mesh.nelem} elements, NDOF {ndof}, NNZ {nz}), "
                         f"24 f x ceil(16 f/0.1) ky = {npairs} systems, {nsrc} sources",
             "batched_tf32x3_s": batched_total, "plain_fp64_s": plain_total,
             "speedup": plain_total / batched_total,
+            "batched_tf32x3_graph_s": batched_graph_total,
+            "speedup_graph": plain_total / batched_graph_total,
             "batched_assembly_s": t_basm, "batched_assemblies_per_s": npairs / t_basm,
+            "batched_assembly_graph_s": t_basm_graph,
             "plain_assembly_s_per_system": t_pasm,
             "gradient_tf32x3_s_per_pair": t_g32, "gradient_fp64_s_per_pair": t_g64,
             "gradient_tf32x3_elem_rhs_per_s": units / t_g32,

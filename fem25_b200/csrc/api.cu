@@ -21,6 +21,12 @@ struct fem25_ctx {
 
 namespace {
 
+// true while stream st records into a CUDA graph
+bool capturing(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
 int fail(Ctx *c, int code, const std::string &msg) {
   if (c) c->err = msg;
   std::fprintf(stderr, "fem25gpu: %s\n", msg.c_str());
@@ -86,12 +92,11 @@ void free_ctx(Ctx *c) {
                   c->d_irptr, c->d_jcptr, c->d_cnp, c->d_elemmat, c->d_gptr, c->d_glist, c->d_err,
                   c->d_brptr, c->d_brow, c->d_basis, c->d_ebasis, c->d_bgptr, c->d_bglist,
                   c->d_pml_elems, c->d_pml_idx, c->d_pgptr, c->d_pglist, c->d_pml_emat,
-                  c->d_pml_delta, c->d_sys, c->d_jcsc, c->d_icsc, c->d_rg_anchor, c->d_mconn,
-                  c->d_elem_wts, c->d_fmat, c->d_pairs, c->d_nonpml, c->d_cdist, c->d_prim, c->d_desc,
+                  c->d_pml_delta, c->d_jcsc, c->d_icsc, c->d_rg_anchor, c->d_mconn,
+                  c->d_elem_wts, c->d_fmat, c->d_nonpml, c->d_cdist, c->d_prim, c->d_desc,
                   c->d_tc_tab, c->d_qp, c->d_qs};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  if (c->h_sys_pinned) cudaFreeHost(c->h_sys_pinned);
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
 }
@@ -127,6 +132,10 @@ int upload_model(Ctx *c, const double *ecoeff, const double *dens) {
 
 int ensure_plain(Ctx *c, cudaStream_t st) {
   if (c->d_gptr) return FEM25_OK;
+  if (capturing(st))
+    return fail(c, FEM25_ERR_ARG,
+                "assemble: the gather map is built on the first call (synchronously); make one "
+                "uncaptured call before capturing");
   CK(cudaMalloc(&c->d_elemmat, sizeof(double2) * 9 * (size_t)c->nelem * kNab), "element matrices");
   CK(build_gather_map(c, st), "gather map");
   return read_err_word(c, st);
@@ -139,6 +148,10 @@ int ensure_batch(Ctx *c, cudaStream_t st) {
                 "(no per-mesh affine basis); use fem25_assemble_dev");
   if (c->bcsr.nblocks >= (1LL << 28))
     return fail(c, FEM25_ERR_UNSUPPORTED, "batch: more than 2^28 node blocks");
+  if ((!c->d_bgptr || !c->basis_valid) && capturing(st))
+    return fail(c, FEM25_ERR_ARG,
+                "batch: the affine basis is built on the first call (synchronously); make one "
+                "uncaptured call before capturing");
   if (!c->d_bgptr) {
     CK(build_batch_structures(c, st), "batch structures");
     int r = read_err_word(c, st);
@@ -414,6 +427,11 @@ int fem25_assemble_batch_dev(fem25_ctx *h, int n, const char *cftype, const doub
   }
   const int nps = (int)order.size();
   if (c->npml_blocks > 0 && nps > c->pml_delta_cap) {
+    if (capturing(st))
+      return fail(c, FEM25_ERR_ARG,
+                  "batch: more distinct (FREQ, CFTYPE) pairs than any earlier call; make one "
+                  "uncaptured call of this size before capturing");
+    CK(cudaStreamSynchronize(st), "synchronize");
     if (c->d_pml_delta) cudaFree(c->d_pml_delta);
     CK(cudaMalloc(&c->d_pml_delta, sizeof(double2) * 9 * (size_t)c->npml_blocks * nps), "pml delta");
     c->pml_delta_cap = nps;
@@ -422,26 +440,16 @@ int fem25_assemble_batch_dev(fem25_ctx *h, int n, const char *cftype, const doub
     PmlParams pp = pml_params(c, order[k].second, order[k].first);
     CK(build_pml_delta(c, pp, k, st), "pml delta");
   }
-  if (n > c->sys_cap) {
-    CK(cudaStreamSynchronize(st), "synchronize");
-    if (c->d_sys) cudaFree(c->d_sys);
-    if (c->h_sys_pinned) cudaFreeHost(c->h_sys_pinned);
-    CK(cudaMalloc(&c->d_sys, sizeof(SysParam) * n), "system table");
-    CK(cudaMallocHost(&c->h_sys_pinned, sizeof(SysParam) * n), "system table");
-    c->sys_cap = n;
-  }
-  CK(cudaStreamSynchronize(st), "synchronize");  // the pinned table may still be in flight
+  std::vector<SysParam> sys(n);
   for (int k = 0; k < n; k++) {
     double omega = 6.2831853071795862 * freq[k];
-    c->h_sys_pinned[k].w2 = omega * omega;
-    c->h_sys_pinned[k].wpy = omega * py[k];
-    c->h_sys_pinned[k].pml_slot = slots[std::make_pair(freq[k], cftype[k])];
-    c->h_sys_pinned[k].pad = 0;
+    sys[k].w2 = omega * omega;
+    sys[k].wpy = omega * py[k];
+    sys[k].pml_slot = slots[std::make_pair(freq[k], cftype[k])];
+    sys[k].pad = 0;
   }
-  CK(cudaMemcpyAsync(c->d_sys, c->h_sys_pinned, sizeof(SysParam) * n, cudaMemcpyHostToDevice, st),
-     "system table");
   if (c->prof) CK(cudaEventRecord(c->ev[0], st), "event");
-  CK(launch_stream_batch(c, n, ring_base, slot_stride, nslots, st), "stream kernel");
+  CK(launch_stream_batch(c, n, sys.data(), ring_base, slot_stride, nslots, st), "stream kernel");
   if (c->prof) CK(cudaEventRecord(c->ev[1], st), "event");
   return FEM25_OK;
 }
@@ -482,30 +490,37 @@ int fem25_gradient_dev(fem25_ctx *h, int npairs, const double *freq, const doubl
   Ctx *c = &h->c;
   if (c->mesh_scalars.ldisp)
     return fail(c, FEM25_ERR_UNSUPPORTED, "gradient: dispersive media are not supported");
+  if (prec != FEM25_PREC_FP64 && prec != FEM25_PREC_TF32X3)
+    return fail(c, FEM25_ERR_ARG, "gradient: unknown precision");
+  if ((long long)npairs * nsrc > (1LL << 30))
+    return fail(c, FEM25_ERR_ARG, "gradient: more than 2^30 (pair, source) fields");
   cudaStream_t st = (cudaStream_t)stream;
   CK(cudaSetDevice(c->device), "set device");
-  if (npairs > c->pairs_cap) {
-    CK(cudaStreamSynchronize(st), "synchronize");
-    if (c->d_pairs) cudaFree(c->d_pairs);
-    CK(cudaMalloc(&c->d_pairs, sizeof(double2) * npairs), "pairs");
-    c->pairs_cap = npairs;
-  }
-  std::vector<double2> hp(npairs);
-  for (int k = 0; k < npairs; k++) {
-    double omega = 6.2831853071795862 * freq[k];
-    hp[k] = make_double2(omega, omega * py[k]);
-  }
-  CK(cudaStreamSynchronize(st), "synchronize");
-  CK(cudaMemcpy(c->d_pairs, hp.data(), sizeof(double2) * npairs, cudaMemcpyHostToDevice), "pairs");
-  if (prec == FEM25_PREC_FP64) {
-    CK(launch_grad_plain(c, npairs, nsrc, u, lam, grad, st), "gradient");
-  } else if (prec == FEM25_PREC_TF32X3) {
-    cudaError_t e = launch_grad_tc(c, npairs, nsrc, u, lam, grad, st);
+  if (prec == FEM25_PREC_TF32X3 && !c->d_tc_tab) {
+    if (capturing(st))
+      return fail(c, FEM25_ERR_ARG,
+                  "gradient: make one uncaptured split-precision call before capturing");
+    cudaError_t e = prepare_grad_tc(c);
     if (e == cudaErrorNotSupported)
       return fail(c, FEM25_ERR_UNSUPPORTED, "gradient: split-precision path not available");
-    CK(e, "gradient (tf32x3)");
-  } else {
-    return fail(c, FEM25_ERR_ARG, "gradient: unknown precision");
+    CK(e, "gradient (tf32x3) set-up");
+  }
+  // pairs travel as kernel parameters, kMaxPairs per launch; both kernels
+  // add into grad, so the chunks accumulate
+  const size_t per_pair = (size_t)nsrc * c->ndof * 2;  // doubles of one pair's fields
+  for (int p0 = 0; p0 < npairs; p0 += kMaxPairs) {
+    const int np = std::min(kMaxPairs, npairs - p0);
+    PairTable pt;
+    for (int k = 0; k < kMaxPairs; k++) {
+      const double omega = k < np ? 6.2831853071795862 * freq[p0 + k] : 0.0;
+      pt.p[k] = make_double2(omega, k < np ? omega * py[p0 + k] : 0.0);
+    }
+    const double *uk = u + p0 * per_pair, *lk = lam + p0 * per_pair;
+    if (prec == FEM25_PREC_FP64) {
+      CK(launch_grad_plain(c, pt, np, nsrc, uk, lk, grad, st), "gradient");
+    } else {
+      CK(launch_grad_tc(c, pt, np, nsrc, uk, lk, grad, st), "gradient (tf32x3)");
+    }
   }
   return FEM25_OK;
 }

@@ -41,6 +41,20 @@ struct SysParam {
   int pad;
 };
 
+constexpr int kMaxPass = 16;  // systems per streaming launch
+
+// The systems of one streaming launch, passed by value as a kernel parameter.
+struct SysTable {
+  SysParam s[kMaxPass];
+};
+
+constexpr int kMaxPairs = 64;  // (omega, py) pairs per gradient launch
+
+// (omega, omega * py) of the pairs of one gradient launch, passed by value.
+struct PairTable {
+  double2 p[kMaxPairs];
+};
+
 struct Ctx {
   int device = 0;
   std::string err;
@@ -88,9 +102,6 @@ struct Ctx {
   double2 *d_pml_emat = nullptr; // [npml_elem][625][9] scratch (one omega)
   double2 *d_pml_delta = nullptr; // [nslots_pml][npml_blocks][9][2] (CE0, CE1)
   int pml_delta_cap = 0;
-  SysParam *d_sys = nullptr;     // per-system parameters of the current batch
-  int sys_cap = 0;
-  SysParam *h_sys_pinned = nullptr;
   // reference-compatible gradient
   bool refgrad_ready = false;
   RefGradSetup rg;
@@ -98,8 +109,6 @@ struct Ctx {
   double *d_elem_wts = nullptr;
   float2 *d_fmat = nullptr;
   // gradient
-  double2 *d_pairs = nullptr;    // (omega, wpy) per pair
-  int pairs_cap = 0;
   int *d_nonpml = nullptr;       // ids of the elements outside the PML
   int n_nonpml = 0;
   unsigned char *d_tc_tab = nullptr;  // SHL tables of the tensor-core gradient (tf32 hi/lo)
@@ -118,14 +127,15 @@ cudaError_t check_jacobians(Ctx *c, cudaStream_t st);
 cudaError_t build_batch_structures(Ctx *c, cudaStream_t st);
 cudaError_t build_basis(Ctx *c, cudaStream_t st);
 cudaError_t build_pml_delta(Ctx *c, const PmlParams &pp, int slot, cudaStream_t st);
-cudaError_t launch_stream_batch(Ctx *c, int n, double *ring_base, long long slot_stride,
-                                int nslots, cudaStream_t st);
+cudaError_t launch_stream_batch(Ctx *c, int n, const SysParam *hsys, double *ring_base,
+                                long long slot_stride, int nslots, cudaStream_t st);
 cudaError_t launch_peff(Ctx *c, int nsrc, const float *a_loc, const float *ue, float *peff,
                         cudaStream_t st);
-cudaError_t launch_grad_plain(Ctx *c, int npairs, int nsrc, const double *u, const double *lam,
-                              double *grad, cudaStream_t st);
-cudaError_t launch_grad_tc(Ctx *c, int npairs, int nsrc, const double *u, const double *lam,
-                           double *grad, cudaStream_t st);
+cudaError_t launch_grad_plain(Ctx *c, const PairTable &pt, int npairs, int nsrc, const double *u,
+                              const double *lam, double *grad, cudaStream_t st);
+cudaError_t prepare_grad_tc(Ctx *c);
+cudaError_t launch_grad_tc(Ctx *c, const PairTable &pt, int npairs, int nsrc, const double *u,
+                           const double *lam, double *grad, cudaStream_t st);
 cudaError_t launch_ref_cfmat(Ctx *c, int lisp, double vpvs, double omega, double py,
                              const float *wave, int accumulate, cudaStream_t st);
 cudaError_t launch_ref_adjflam(Ctx *c, const float *adjlam, float *gradl, cudaStream_t st);

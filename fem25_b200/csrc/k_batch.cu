@@ -279,7 +279,6 @@ __global__ void k_gather_pml(long long npblk, const int *__restrict__ pptr,
 // the streaming kernel
 // ---------------------------------------------------------------------------
 constexpr int kStreamThreads = 256;
-constexpr int kMaxPass = 16;
 
 __device__ __forceinline__ void st_cs(double2 *p, double2 v) {
   asm volatile("st.global.cs.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(v.x), "d"(v.y) : "memory");
@@ -322,13 +321,13 @@ template <int UNR>
 __global__ void __launch_bounds__(kStreamThreads)
     k_stream(long long nzero, const double *__restrict__ prim, const unsigned *__restrict__ desc,
              const double *__restrict__ basis, long long nblocks, const int *__restrict__ pml_idx,
-             const double2 *__restrict__ pml_delta, long long npblk, const SysParam *__restrict__ sys,
+             const double2 *__restrict__ pml_delta, long long npblk, SysTable tab,
              int s0, int s1, double *__restrict__ ring, long long stride, int nslots) {
   __shared__ SysParam sp[kMaxPass];
   __shared__ double2 *outp[kMaxPass];
   const int ns = s1 - s0;
   if (threadIdx.x < ns) {
-    sp[threadIdx.x] = sys[s0 + threadIdx.x];
+    sp[threadIdx.x] = tab.s[threadIdx.x];
     outp[threadIdx.x] =
         reinterpret_cast<double2 *>(ring + (size_t)((s0 + threadIdx.x) % nslots) * stride);
   }
@@ -400,13 +399,13 @@ __global__ void __launch_bounds__(kStreamThreads)
     k_stream_pipe(long long nzero, const double *__restrict__ prim, const unsigned *__restrict__ desc,
                   const double *__restrict__ basis, long long nblocks, const int *__restrict__ pml_idx,
                   const double2 *__restrict__ pml_delta, long long npblk,
-                  const SysParam *__restrict__ sys, int s0, int s1, double *__restrict__ ring,
+                  SysTable tab, int s0, int s1, double *__restrict__ ring,
                   long long stride, int nslots) {
   __shared__ SysParam sp[kMaxPass];
   __shared__ double2 *outp[kMaxPass];
   const int ns = s1 - s0;
   if (threadIdx.x < ns) {
-    sp[threadIdx.x] = sys[s0 + threadIdx.x];
+    sp[threadIdx.x] = tab.s[threadIdx.x];
     outp[threadIdx.x] =
         reinterpret_cast<double2 *>(ring + (size_t)((s0 + threadIdx.x) % nslots) * stride);
   }
@@ -493,14 +492,14 @@ __global__ void __launch_bounds__(T)
     k_stream_tma(long long nzero, const double *__restrict__ prim, const unsigned *__restrict__ desc,
                  const double *__restrict__ basis, long long nblocks, const int *__restrict__ pml_idx,
                  const double2 *__restrict__ pml_delta, long long npblk,
-                 const SysParam *__restrict__ sys, int s0, int s1, double *__restrict__ ring,
+                 SysTable tab, int s0, int s1, double *__restrict__ ring,
                  long long stride, int nslots) {
   extern __shared__ __align__(128) double2 stage[];  // [2][kMaxPass][T]
   __shared__ SysParam sp[kMaxPass];
   __shared__ double2 *outp[kMaxPass];
   const int ns = s1 - s0;
   if (threadIdx.x < ns) {
-    sp[threadIdx.x] = sys[s0 + threadIdx.x];
+    sp[threadIdx.x] = tab.s[threadIdx.x];
     outp[threadIdx.x] =
         reinterpret_cast<double2 *>(ring + (size_t)((s0 + threadIdx.x) % nslots) * stride);
   }
@@ -681,8 +680,8 @@ cudaError_t build_pml_delta(Ctx *c, const PmlParams &pp, int slot, cudaStream_t 
 }
 
 template <int UNR>
-static cudaError_t stream_range(Ctx *c, int s0, int s1, double *ring_base, long long slot_stride,
-                                int nslots, cudaStream_t st) {
+static cudaError_t stream_range(Ctx *c, const SysTable &tab, int s0, int s1, double *ring_base,
+                                long long slot_stride, int nslots, cudaStream_t st) {
   int nsm = 0, occ = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stream<UNR>, kStreamThreads, 0);
@@ -691,13 +690,13 @@ static cudaError_t stream_range(Ctx *c, int s0, int s1, double *ring_base, long 
   const unsigned grid = (unsigned)std::min<long long>((long long)nsm * occ, grid_need);
   k_stream<UNR><<<grid, kStreamThreads, 0, st>>>(c->nzero, c->d_prim, c->d_desc, c->d_basis,
                                                  c->bcsr.nblocks, c->d_pml_idx, c->d_pml_delta,
-                                                 c->npml_blocks, c->d_sys, s0, s1, ring_base,
+                                                 c->npml_blocks, tab, s0, s1, ring_base,
                                                  slot_stride, nslots);
   return cudaGetLastError();
 }
 
-static cudaError_t stream_pipe(Ctx *c, int s0, int s1, double *ring_base, long long slot_stride,
-                               int nslots, cudaStream_t st) {
+static cudaError_t stream_pipe(Ctx *c, const SysTable &tab, int s0, int s1, double *ring_base,
+                               long long slot_stride, int nslots, cudaStream_t st) {
   int nsm = 0, occ = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stream_pipe, kStreamThreads, 0);
@@ -706,14 +705,14 @@ static cudaError_t stream_pipe(Ctx *c, int s0, int s1, double *ring_base, long l
   const unsigned grid = (unsigned)std::min<long long>((long long)nsm * occ, grid_need);
   k_stream_pipe<<<grid, kStreamThreads, 0, st>>>(c->nzero, c->d_prim, c->d_desc, c->d_basis,
                                                  c->bcsr.nblocks, c->d_pml_idx, c->d_pml_delta,
-                                                 c->npml_blocks, c->d_sys, s0, s1, ring_base,
+                                                 c->npml_blocks, tab, s0, s1, ring_base,
                                                  slot_stride, nslots);
   return cudaGetLastError();
 }
 
 template <int T>
-static cudaError_t stream_tma(Ctx *c, int s0, int s1, double *ring_base, long long slot_stride,
-                              int nslots, cudaStream_t st) {
+static cudaError_t stream_tma(Ctx *c, const SysTable &tab, int s0, int s1, double *ring_base,
+                              long long slot_stride, int nslots, cudaStream_t st) {
   const size_t smem = sizeof(double2) * 2 * kMaxPass * T;
   cudaError_t e = cudaFuncSetAttribute(k_stream_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
@@ -726,43 +725,54 @@ static cudaError_t stream_tma(Ctx *c, int s0, int s1, double *ring_base, long lo
   const unsigned grid = (unsigned)std::min<long long>((long long)nsm * occ, nchunk);
   k_stream_tma<T><<<grid, T, smem, st>>>(c->nzero, c->d_prim, c->d_desc, c->d_basis,
                                          c->bcsr.nblocks, c->d_pml_idx, c->d_pml_delta,
-                                         c->npml_blocks, c->d_sys, s0, s1, ring_base, slot_stride,
+                                         c->npml_blocks, tab, s0, s1, ring_base, slot_stride,
                                          nslots);
   return cudaGetLastError();
 }
 
 constexpr int kNumStreamVariants = 6;
-static cudaError_t stream_variant(Ctx *c, int v, int s0, int s1, double *ring_base,
-                                  long long slot_stride, int nslots, cudaStream_t st) {
+static cudaError_t stream_variant(Ctx *c, int v, const SysParam *hsys, int s0, int s1,
+                                  double *ring_base, long long slot_stride, int nslots,
+                                  cudaStream_t st) {
+  // the launch's systems travel as a kernel parameter, so a captured graph
+  // keeps the values of its own call
+  SysTable tab;
+  for (int k = 0; k < kMaxPass; k++) tab.s[k] = k < s1 - s0 ? hsys[s0 + k] : SysParam{0.0, 0.0, 0, 0};
   switch (v) {
-    case 0: return stream_range<1>(c, s0, s1, ring_base, slot_stride, nslots, st);
-    case 1: return stream_range<2>(c, s0, s1, ring_base, slot_stride, nslots, st);
-    case 2: return stream_range<4>(c, s0, s1, ring_base, slot_stride, nslots, st);
-    case 3: return stream_pipe(c, s0, s1, ring_base, slot_stride, nslots, st);
-    case 4: return stream_tma<64>(c, s0, s1, ring_base, slot_stride, nslots, st);
-    default: return stream_tma<128>(c, s0, s1, ring_base, slot_stride, nslots, st);
+    case 0: return stream_range<1>(c, tab, s0, s1, ring_base, slot_stride, nslots, st);
+    case 1: return stream_range<2>(c, tab, s0, s1, ring_base, slot_stride, nslots, st);
+    case 2: return stream_range<4>(c, tab, s0, s1, ring_base, slot_stride, nslots, st);
+    case 3: return stream_pipe(c, tab, s0, s1, ring_base, slot_stride, nslots, st);
+    case 4: return stream_tma<64>(c, tab, s0, s1, ring_base, slot_stride, nslots, st);
+    default: return stream_tma<128>(c, tab, s0, s1, ring_base, slot_stride, nslots, st);
   }
 }
 
 // The first batch of a context times the streaming variants (1, 2 or 4
-// entries per thread, software-pipelined, TMA bulk stores) on its first launch -- each writes the same values -- and keeps the
-// fastest for the life of the context.
-cudaError_t launch_stream_batch(Ctx *c, int n, double *ring_base, long long slot_stride,
-                                int nslots, cudaStream_t st) {
+// entries per thread, software-pipelined, TMA bulk stores) on its first
+// launch -- each writes the same values -- and keeps the fastest for the life
+// of the context.  A batch recorded into a CUDA graph before any tuning uses
+// the TMA variant without timing.
+cudaError_t launch_stream_batch(Ctx *c, int n, const SysParam *hsys, double *ring_base,
+                                long long slot_stride, int nslots, cudaStream_t st) {
   const int per = std::min(kMaxPass, nslots);
   cudaError_t e;
   int s0 = 0;
   if (c->stream_variant < 0) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
     const char *env = std::getenv("FEM25_STREAM_VARIANT");
     if (env) {
       c->stream_variant = std::min(kNumStreamVariants - 1, std::max(0, std::atoi(env)));
+    } else if (cs != cudaStreamCaptureStatusNone) {
+      c->stream_variant = 4;
     } else {
       cudaEvent_t ev[kNumStreamVariants + 1];
       for (auto &x : ev) cudaEventCreate(&x);
       const int s1 = std::min(n, per);
       cudaEventRecord(ev[0], st);
       for (int v = 0; v < kNumStreamVariants; v++) {
-        if ((e = stream_variant(c, v, 0, s1, ring_base, slot_stride, nslots, st))) return e;
+        if ((e = stream_variant(c, v, hsys, 0, s1, ring_base, slot_stride, nslots, st))) return e;
         cudaEventRecord(ev[v + 1], st);
       }
       cudaEventSynchronize(ev[kNumStreamVariants]);
@@ -781,7 +791,7 @@ cudaError_t launch_stream_batch(Ctx *c, int n, double *ring_base, long long slot
   }
   for (; s0 < n; s0 += per) {
     const int s1 = std::min(n, s0 + per);
-    if ((e = stream_variant(c, c->stream_variant, s0, s1, ring_base, slot_stride, nslots, st)))
+    if ((e = stream_variant(c, c->stream_variant, hsys, s0, s1, ring_base, slot_stride, nslots, st)))
       return e;
   }
   return cudaSuccess;

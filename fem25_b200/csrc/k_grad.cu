@@ -33,7 +33,7 @@ __device__ __forceinline__ double re_cj(double ar, double ai, double br, double 
 
 __global__ void __launch_bounds__(kGThreads)
     k_grad_plain(MeshView mv, DevTables dt, GradArgs ga, const int *__restrict__ elems,
-                 const int *__restrict__ lm, const double2 *__restrict__ pairs,
+                 const int *__restrict__ lm, PairTable pt,
                  const double2 *__restrict__ u, const double2 *__restrict__ lam,
                  double *__restrict__ grad, int *__restrict__ err) {
   extern __shared__ double sm[];
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(kGThreads)
   }
   double accl = 0.0, accm = 0.0, accr = 0.0;
   for (int p = 0; p < ga.npairs; p++) {
-    const double2 pr = pairs[p];
+    const double2 pr = pt.p[p];
     const double w2 = pr.x * pr.x, wpy = pr.y;
     for (int s0 = 0; s0 < ga.nsrc; s0 += kGSrcTile) {
       const int ns = min(kGSrcTile, ga.nsrc - s0);
@@ -168,8 +168,8 @@ static size_t grad_smem() {
          sizeof(double) * 12 * (kGThreads / 32);
 }
 
-cudaError_t launch_grad_plain(Ctx *c, int npairs, int nsrc, const double *u, const double *lam,
-                              double *grad, cudaStream_t st) {
+cudaError_t launch_grad_plain(Ctx *c, const PairTable &pt, int npairs, int nsrc, const double *u,
+                              const double *lam, double *grad, cudaStream_t st) {
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(k_grad_plain, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)grad_smem())))
@@ -181,7 +181,7 @@ cudaError_t launch_grad_plain(Ctx *c, int npairs, int nsrc, const double *u, con
   ga.nnpg = c->nnpg;
   ga.field_stride = c->ndof;
   if (c->n_nonpml == 0) return cudaSuccess;
-  k_grad_plain<<<c->n_nonpml, kGThreads, grad_smem(), st>>>(c->mv, c->dt, ga, c->d_nonpml, c->d_lm, c->d_pairs,
+  k_grad_plain<<<c->n_nonpml, kGThreads, grad_smem(), st>>>(c->mv, c->dt, ga, c->d_nonpml, c->d_lm, pt,
                                                   (const double2 *)u, (const double2 *)lam, grad,
                                                   c->d_err);
   return cudaGetLastError();

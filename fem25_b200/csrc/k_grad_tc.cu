@@ -285,7 +285,7 @@ __device__ __forceinline__ void point_forms(const PointGeo &pg, float w2, float 
 
 __global__ void __launch_bounds__(tc::kThreads, 1)
     k_grad_tc(MeshView mv, DevTables dt, TcArgs ga, const int *__restrict__ elems,
-              const int *__restrict__ lm, const double2 *__restrict__ pairs,
+              const int *__restrict__ lm, PairTable pt,
               const double2 *__restrict__ u, const double2 *__restrict__ lam,
               const uint8_t *__restrict__ atab, double *__restrict__ grad, int *__restrict__ err) {
   extern __shared__ __align__(1024) uint8_t sm[];
@@ -540,7 +540,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
               asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
               mbar_arrive(smem_u32(&bar_tempty[ts]));
             }
-            const double2 pr = pairs[(c0 + c) / ga.nsrc];
+            const double2 pr = pt.p[(c0 + c) / ga.nsrc];
             point_forms(pg, (float)(pr.x * pr.x), (float)pr.y, val, tl, tm, tr);
           }
         } else {
@@ -591,7 +591,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
               val[1][v] = r1[col + v];
               val[2][v] = r2[col + v];
             }
-            const double2 pr = pairs[(c0 + min(cl, nc - 1)) / ga.nsrc];
+            const double2 pr = pt.p[(c0 + min(cl, nc - 1)) / ga.nsrc];
             float fl = 0.f, fm = 0.f, fr = 0.f;
             point_forms(pg, (float)(pr.x * pr.x), (float)pr.y, val, fl, fm, fr);
             if (act) {
@@ -708,25 +708,38 @@ std::vector<uint8_t> build_tc_tables(const Tables &t) {
   return buf;
 }
 
-cudaError_t launch_grad_tc(Ctx *c, int npairs, int nsrc, const double *u, const double *lam,
-                           double *grad, cudaStream_t st) {
-  cudaError_t e;
-  if (!c->d_tc_tab) {
-    // the gather reads a node's three DOFs as one run: LM(3a+1..3a+3) must be
-    // d, d+1, d+2 or 0, 0, 0 (what GENID produces)
-    for (size_t i = 0; i + 2 < c->h_lm.size(); i += 3) {
-      const int d = c->h_lm[i];
-      const bool ok = d > 0 ? (c->h_lm[i + 1] == d + 1 && c->h_lm[i + 2] == d + 2)
-                            : (c->h_lm[i + 1] == 0 && c->h_lm[i + 2] == 0);
-      if (!ok) return cudaErrorNotSupported;
-    }
-    std::vector<uint8_t> h = build_tc_tables(c->tab);
-    if ((e = cudaMalloc(&c->d_tc_tab, h.size()))) return e;
-    if ((e = cudaMemcpy(c->d_tc_tab, h.data(), h.size(), cudaMemcpyHostToDevice))) return e;
-    if ((e = cudaFuncSetAttribute(k_grad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  tc::kSmemBytes)))
-      return e;
+// One-time set-up of the split-precision gradient: checks the DOF layout and
+// uploads the SHL tables (a synchronous copy, so it runs outside any stream
+// capture).  cudaErrorNotSupported when the layout does not allow the run
+// gather.
+cudaError_t prepare_grad_tc(Ctx *c) {
+  if (c->d_tc_tab) return cudaSuccess;
+  // the gather reads a node's three DOFs as one run: LM(3a+1..3a+3) must be
+  // d, d+1, d+2 or 0, 0, 0 (what GENID produces)
+  for (size_t i = 0; i + 2 < c->h_lm.size(); i += 3) {
+    const int d = c->h_lm[i];
+    const bool ok = d > 0 ? (c->h_lm[i + 1] == d + 1 && c->h_lm[i + 2] == d + 2)
+                          : (c->h_lm[i + 1] == 0 && c->h_lm[i + 2] == 0);
+    if (!ok) return cudaErrorNotSupported;
   }
+  cudaError_t e;
+  std::vector<uint8_t> h = build_tc_tables(c->tab);
+  if ((e = cudaFuncSetAttribute(k_grad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tc::kSmemBytes)))
+    return e;
+  uint8_t *d = nullptr;
+  if ((e = cudaMalloc(&d, h.size()))) return e;
+  if ((e = cudaMemcpy(d, h.data(), h.size(), cudaMemcpyHostToDevice))) {
+    cudaFree(d);
+    return e;
+  }
+  c->d_tc_tab = d;
+  return cudaSuccess;
+}
+
+cudaError_t launch_grad_tc(Ctx *c, const PairTable &pt, int npairs, int nsrc, const double *u,
+                           const double *lam, double *grad, cudaStream_t st) {
+  if (!c->d_tc_tab) return cudaErrorNotReady;
   if (c->n_nonpml == 0) return cudaSuccess;
   if ((long long)npairs * nsrc > (1LL << 30)) return cudaErrorInvalidValue;
   TcArgs ga;
@@ -740,7 +753,7 @@ cudaError_t launch_grad_tc(Ctx *c, int npairs, int nsrc, const double *u, const 
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
   const int grid = std::min(nsm, c->n_nonpml);
   k_grad_tc<<<grid, tc::kThreads, tc::kSmemBytes, st>>>(c->mv, c->dt, ga, c->d_nonpml, c->d_lm,
-                                                         c->d_pairs, (const double2 *)u,
+                                                         pt, (const double2 *)u,
                                                          (const double2 *)lam, c->d_tc_tab, grad,
                                                          c->d_err);
   return cudaGetLastError();
