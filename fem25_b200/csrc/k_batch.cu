@@ -482,6 +482,10 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 __device__ __forceinline__ void bulk_wait_read1() {
   asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
 }
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -550,6 +554,98 @@ __global__ void __launch_bounds__(T)
       for (int k = 0; k < ns; k++) bulk_store(outp[k] + n0, buf + k * T, (unsigned)(cnt * 16));
       bulk_commit();
     }
+  }
+  if (threadIdx.x == 0) bulk_wait_all();
+}
+
+// Staging-ring variant: a CTA of T threads computes a chunk of T consecutive
+// entries and hands it to the TMA unit one system at a time (one T*16-byte
+// bulk store per system) through a ring of NB shared-memory buffers, so the
+// shared memory per CTA stays at NB*T*16 bytes whatever the number of systems
+// and the SM keeps enough resident warps to hide the input loads; the inputs
+// of the CTA's next chunk are loaded before the stores of the current one.
+// Each system's store is its own bulk group: before a buffer is refilled,
+// thread 0 waits until at most NB-1 groups still read shared memory.
+template <int T, int NB>
+__global__ void __launch_bounds__(T)
+    k_stream_ring(long long nzero, const double *__restrict__ prim, const unsigned *__restrict__ desc,
+                  const double *__restrict__ basis, long long nblocks, const int *__restrict__ pml_idx,
+                  const double2 *__restrict__ pml_delta, long long npblk, SysTable tab, int s0,
+                  int s1, double *__restrict__ ring, long long stride, int nslots) {
+  extern __shared__ __align__(128) double2 stage[];  // [NB][T]
+  __shared__ SysParam sp[kMaxPass];
+  __shared__ double2 *outp[kMaxPass];
+  const int ns = s1 - s0;
+  if (threadIdx.x < ns) {
+    sp[threadIdx.x] = tab.s[threadIdx.x];
+    outp[threadIdx.x] =
+        reinterpret_cast<double2 *>(ring + (size_t)((s0 + threadIdx.x) % nslots) * stride);
+  }
+  __syncthreads();
+  const double *mrho = basis + (size_t)B_MRHO * nblocks;
+  const double *mmu = basis + (size_t)B_MMU * nblocks;
+  const double *ml2m = basis + (size_t)B_ML2M * nblocks;
+  auto load = [&](long long n, double &p, unsigned &d, double &mr, double &mc, int &pidx) {
+    p = 0.0;
+    d = 0u;
+    mr = 0.0;
+    mc = 0.0;
+    pidx = -1;
+    if (n >= nzero) return;
+    p = __ldcs(prim + n);
+    d = __ldcs(desc + n);
+    const unsigned blk = d >> 4, i = (d >> 2) & 3u, j = d & 3u;
+    if (i == j) {
+      mr = mrho[blk];
+      mc = (i == 1u) ? ml2m[blk] : mmu[blk];
+    }
+    pidx = pml_idx[blk];
+  };
+  const long long nchunk = (nzero + T - 1) / T;
+  long long c = blockIdx.x;
+  double p, mr, mc;
+  unsigned d;
+  int pidx;
+  load(c * T + threadIdx.x, p, d, mr, mc, pidx);
+  int q = 0;  // running buffer count
+  for (; c < nchunk; c += gridDim.x) {
+    const long long n0 = c * T, n = n0 + threadIdx.x;
+    double p2, mr2, mc2;
+    unsigned d2;
+    int pidx2;
+    load((c + gridDim.x) * T + threadIdx.x, p2, d2, mr2, mc2, pidx2);  // next chunk
+    const unsigned i = (d >> 2) & 3u, j = d & 3u;
+    const bool odd = (i + j) & 1u;
+    const unsigned cnt = (unsigned)min((long long)T, nzero - n0);
+    for (int k = 0; k < ns; k++, q++) {
+      double2 *buf = stage + (size_t)(q % NB) * T;
+      if (q >= NB && threadIdx.x == 0) bulk_wait_read<NB - 1>();
+      __syncthreads();
+      if (n < nzero) {
+        const double w2 = sp[k].w2, wpy = sp[k].wpy;
+        double2 v;
+        if (odd) v = make_double2(0.0, wpy * p);
+        else v = make_double2(p - w2 * mr + (wpy * wpy) * mc, 0.0);
+        if (pidx >= 0) {
+          const double2 dv = pml_delta[((size_t)sp[k].pml_slot * npblk + pidx) * 9 + 3 * i + j];
+          const double f = odd ? wpy : 1.0;
+          v.x += f * dv.x;
+          v.y += f * dv.y;
+        }
+        buf[threadIdx.x] = v;
+      }
+      fence_async_smem();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        bulk_store(outp[k] + n0, buf, cnt * 16u);
+        bulk_commit();
+      }
+    }
+    p = p2;
+    d = d2;
+    mr = mr2;
+    mc = mc2;
+    pidx = pidx2;
   }
   if (threadIdx.x == 0) bulk_wait_all();
 }
@@ -730,7 +826,27 @@ static cudaError_t stream_tma(Ctx *c, const SysTable &tab, int s0, int s1, doubl
   return cudaGetLastError();
 }
 
-constexpr int kNumStreamVariants = 6;
+template <int T, int NB>
+static cudaError_t stream_ring(Ctx *c, const SysTable &tab, int s0, int s1, double *ring_base,
+                               long long slot_stride, int nslots, cudaStream_t st) {
+  const size_t smem = sizeof(double2) * NB * T;
+  cudaError_t e = cudaFuncSetAttribute(k_stream_ring<T, NB>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e) return e;
+  int nsm = 0, occ = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stream_ring<T, NB>, T, smem);
+  if (occ < 1) occ = 1;
+  const long long nchunk = (c->nzero + T - 1) / T;
+  const unsigned grid = (unsigned)std::min<long long>((long long)nsm * occ, nchunk);
+  k_stream_ring<T, NB><<<grid, T, smem, st>>>(c->nzero, c->d_prim, c->d_desc, c->d_basis,
+                                              c->bcsr.nblocks, c->d_pml_idx, c->d_pml_delta,
+                                              c->npml_blocks, tab, s0, s1, ring_base, slot_stride,
+                                              nslots);
+  return cudaGetLastError();
+}
+
+constexpr int kNumStreamVariants = 8;
 static cudaError_t stream_variant(Ctx *c, int v, const SysParam *hsys, int s0, int s1,
                                   double *ring_base, long long slot_stride, int nslots,
                                   cudaStream_t st) {
@@ -744,15 +860,18 @@ static cudaError_t stream_variant(Ctx *c, int v, const SysParam *hsys, int s0, i
     case 2: return stream_range<4>(c, tab, s0, s1, ring_base, slot_stride, nslots, st);
     case 3: return stream_pipe(c, tab, s0, s1, ring_base, slot_stride, nslots, st);
     case 4: return stream_tma<64>(c, tab, s0, s1, ring_base, slot_stride, nslots, st);
-    default: return stream_tma<128>(c, tab, s0, s1, ring_base, slot_stride, nslots, st);
+    case 5: return stream_tma<128>(c, tab, s0, s1, ring_base, slot_stride, nslots, st);
+    case 6: return stream_ring<256, 4>(c, tab, s0, s1, ring_base, slot_stride, nslots, st);
+    default: return stream_ring<512, 4>(c, tab, s0, s1, ring_base, slot_stride, nslots, st);
   }
 }
 
 // The first batch of a context times the streaming variants (1, 2 or 4
-// entries per thread, software-pipelined, TMA bulk stores) on its first
-// launch -- each writes the same values -- and keeps the fastest for the life
-// of the context.  A batch recorded into a CUDA graph before any tuning uses
-// the TMA variant without timing.
+// entries per thread, software-pipelined, TMA bulk stores of all systems of a
+// chunk, TMA staging ring of 256 or 512 entries) on its first launch -- each
+// writes the same values -- and keeps the fastest for the life of the
+// context.  A batch recorded into a CUDA graph before any tuning uses the
+// 512-entry staging ring without timing.
 cudaError_t launch_stream_batch(Ctx *c, int n, const SysParam *hsys, double *ring_base,
                                 long long slot_stride, int nslots, cudaStream_t st) {
   const int per = std::min(kMaxPass, nslots);
@@ -765,7 +884,7 @@ cudaError_t launch_stream_batch(Ctx *c, int n, const SysParam *hsys, double *rin
     if (env) {
       c->stream_variant = std::min(kNumStreamVariants - 1, std::max(0, std::atoi(env)));
     } else if (cs != cudaStreamCaptureStatusNone) {
-      c->stream_variant = 4;
+      c->stream_variant = 7;
     } else {
       cudaEvent_t ev[kNumStreamVariants + 1];
       for (auto &x : ev) cudaEventCreate(&x);

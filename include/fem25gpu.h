@@ -101,8 +101,13 @@ int fem25_assemble_dev(fem25_ctx *ctx, char cftype, double freq, double py, doub
 
 /* Batched assembly of n systems (cftype[k], freq[k], py[k]) into complex128
  * device slots: system k goes to ring_base + (k % nslots) * slot_stride
- * doubles (slot_stride >= 2*NZERO).  Uses the per-mesh affine basis (built
- * on first use) and one persistent streaming launch. */
+ * doubles (slot_stride even and >= 2*NZERO).  Uses the per-mesh affine basis
+ * (built on first use) and streaming launches of up to 16 systems.  Slots
+ * that start on 128-byte boundaries (ring_base 128-byte aligned, slot_stride
+ * a multiple of 16) are written faster.  The first call builds the basis and
+ * times the streaming variants (synchronously); later calls only enqueue
+ * kernels, with the system parameters passed by value, and may be recorded
+ * into a CUDA graph. */
 int fem25_assemble_batch_dev(fem25_ctx *ctx, int n, const char *cftype, const double *freq,
                              const double *py, double *ring_base, long long slot_stride,
                              int nslots, void *stream);
@@ -121,7 +126,10 @@ int fem25_peff_dev(fem25_ctx *ctx, int nsrc, const float *a_loc, const float *ue
  * complex128 device arrays [pair][src][NDOF]; grad is FP64 on the device.
  * Elements of domain 'A' (PML) do not contribute.
  * prec: FEM25_PREC_FP64 (plain FP64 kernels) or FEM25_PREC_TF32X3
- * (split-precision tensor-core contraction, FP64 cross-pair reduction). */
+ * (split-precision tensor-core contraction, FP64 cross-pair reduction).
+ * Pairs are passed to the kernels by value, 64 per launch; the call only
+ * enqueues work and may be recorded into a CUDA graph once the first
+ * TF32X3 call on the context (which uploads its tables) has returned. */
 #define FEM25_PREC_FP64 0
 #define FEM25_PREC_TF32X3 1
 int fem25_gradient_dev(fem25_ctx *ctx, int npairs, const double *freq, const double *py,
