@@ -99,6 +99,9 @@ void free_ctx(Ctx *c) {
     if (p) cudaFree(p);
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
+  for (auto &e : c->drv_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->copy_st) cudaStreamDestroy(c->copy_st);
 }
 
 int read_err_word(Ctx *c, cudaStream_t st) {
@@ -163,6 +166,35 @@ int ensure_batch(Ctx *c, cudaStream_t st) {
     if (r) return r;
     c->basis_valid = true;
   }
+  return FEM25_OK;
+}
+
+// Chunking of fem25_asmble_driver: up to 16 element ranges of at least one
+// wave of CTAs each; the CSR rows are the DOFs, and row r is complete once
+// the last element holding DOF r (GENID numbers DOFs in element order, so
+// rows complete nearly in order) has been computed.
+int ensure_driver_plan(Ctx *c) {
+  if (c->copy_st) return FEM25_OK;
+  const int nch = std::max(1, std::min(16, c->nelem / 148));
+  std::vector<int> last(c->ndof, -1);
+  for (int e = 0; e < c->nelem; e++)
+    for (int k = 0; k < 3 * kNen; k++) {
+      const int d = c->h_lm[(size_t)e * 3 * kNen + k];
+      if (d > 0) last[d - 1] = e;
+    }
+  c->drv_elem.assign(nch + 1, 0);
+  c->drv_row.assign(nch + 1, 0);
+  for (int k = 0; k <= nch; k++) c->drv_elem[k] = (int)((long long)k * c->nelem / nch);
+  int r = 0;
+  for (int k = 1; k <= nch; k++) {
+    while (r < c->ndof && last[r] < c->drv_elem[k]) r++;
+    c->drv_row[k] = r;
+  }
+  if (c->drv_row[nch] != c->ndof)
+    return fail(c, FEM25_ERR_PATTERN, "asmble_driver: DOF outside every element");
+  c->drv_ev.assign(nch, nullptr);
+  for (auto &e : c->drv_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  CK(cudaStreamCreateWithFlags(&c->copy_st, cudaStreamNonBlocking), "copy stream");
   return FEM25_OK;
 }
 
@@ -378,8 +410,8 @@ int fem25_assemble_dev(fem25_ctx *h, char cftype, double freq, double py, double
   int r = ensure_plain(c, st);
   if (r) return r;
   if (c->prof) CK(cudaEventRecord(c->ev[2], st), "event");
-  CK(launch_elem_plain(c, cftype, freq, py, st), "element kernel");
-  CK(launch_gather_plain(c, csr128, csr64, st), "gather kernel");
+  CK(launch_elem_plain(c, cftype, freq, py, 0, c->nelem, st), "element kernel");
+  CK(launch_gather_plain(c, csr128, csr64, 0, c->nzero, st), "gather kernel");
   if (c->prof) CK(cudaEventRecord(c->ev[3], st), "event");
   return FEM25_OK;
 }
@@ -389,16 +421,37 @@ int fem25_asmble_driver(fem25_ctx *h, int nzloc, char cftype, double freq, doubl
   if (!h || !cdist) return FEM25_ERR_ARG;
   Ctx *c = &h->c;
   if ((long long)nzloc != c->nzero) return fail(c, FEM25_ERR_ARG, "asmble_driver: NZLOC != NZERO");
+  if (cftype != 'S' && cftype != 'B')
+    return fail(c, FEM25_ERR_ARG, "asmble_driver: CFTYPE must be 'S' or 'B'");
+  if (!(freq > 0.0)) return fail(c, FEM25_ERR_ARG, "asmble_driver: FREQ must be > 0");
   CK(cudaSetDevice(c->device), "set device");
+  int r = ensure_plain(c, nullptr);
+  if (r) return r;
   if (!c->d_cdist) CK(cudaMalloc(&c->d_cdist, sizeof(float2) * (size_t)nzloc), "cdist buffer");
-  int r = fem25_assemble_dev(h, cftype, freq, py, nullptr, (float *)c->d_cdist, nullptr);
-  if (!r) {
-    cudaError_t e =
-        cudaMemcpy(cdist, c->d_cdist, sizeof(float2) * (size_t)nzloc, cudaMemcpyDeviceToHost);
-    if (e) r = cuda_fail(c, e, "cdist copy");
+  r = ensure_driver_plan(c);
+  if (r) return r;
+  // every chunk's element matrices and gather are enqueued first, then the
+  // host copies follow the chunks as they complete (a pageable destination
+  // makes each copy synchronous for the host, the GPU keeps computing)
+  cudaStream_t st = nullptr;
+  const int nch = (int)c->drv_elem.size() - 1;
+  for (int k = 0; k < nch; k++) {
+    const long long nz0 = c->h_irptr[c->drv_row[k]] - 1, nz1 = c->h_irptr[c->drv_row[k + 1]] - 1;
+    CK(launch_elem_plain(c, cftype, freq, py, c->drv_elem[k], c->drv_elem[k + 1], st),
+       "element kernel");
+    CK(launch_gather_plain(c, nullptr, (float *)c->d_cdist, nz0, nz1, st), "gather kernel");
+    CK(cudaEventRecord(c->drv_ev[k], st), "event");
   }
-  if (!r) r = read_err_word(c, 0);
-  return r;
+  for (int k = 0; k < nch; k++) {
+    const long long nz0 = c->h_irptr[c->drv_row[k]] - 1, nz1 = c->h_irptr[c->drv_row[k + 1]] - 1;
+    if (nz1 <= nz0) continue;
+    CK(cudaStreamWaitEvent(c->copy_st, c->drv_ev[k], 0), "event");
+    CK(cudaMemcpyAsync(cdist + 2 * nz0, c->d_cdist + nz0, sizeof(float2) * (size_t)(nz1 - nz0),
+                       cudaMemcpyDeviceToHost, c->copy_st),
+       "cdist copy");
+  }
+  CK(cudaStreamSynchronize(c->copy_st), "cdist copy");
+  return read_err_word(c, 0);
 }
 
 int fem25_assemble_batch_dev(fem25_ctx *h, int n, const char *cftype, const double *freq,

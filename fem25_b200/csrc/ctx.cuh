@@ -112,16 +112,24 @@ struct Ctx {
   int *d_nonpml = nullptr;       // ids of the elements outside the PML
   int n_nonpml = 0;
   unsigned char *d_tc_tab = nullptr;  // SHL tables of the tensor-core gradient (tf32 hi/lo)
-  // cached COMPLEX*8 device buffer of fem25_asmble_driver
+  // cached COMPLEX*8 device buffer of fem25_asmble_driver, and its pipeline:
+  // element chunk k = [drv_elem[k], drv_elem[k+1]) completes the CSR rows
+  // [drv_row[k], drv_row[k+1]), whose values are gathered and copied to the
+  // host on copy_st while the next chunk computes
   float2 *d_cdist = nullptr;
+  std::vector<int> drv_elem, drv_row;
+  cudaStream_t copy_st = nullptr;
+  std::vector<cudaEvent_t> drv_ev;
   // optional CUDA-event timing of the dominant kernels
   bool prof = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 // kernels / launchers (defined in the .cu files)
-cudaError_t launch_elem_plain(Ctx *c, char cftype, double freq, double py, cudaStream_t st);
-cudaError_t launch_gather_plain(Ctx *c, double *csr128, float *csr64, cudaStream_t st);
+cudaError_t launch_elem_plain(Ctx *c, char cftype, double freq, double py, int e0, int e1,
+                              cudaStream_t st);
+cudaError_t launch_gather_plain(Ctx *c, double *csr128, float *csr64, long long nz0,
+                                long long nz1, cudaStream_t st);
 cudaError_t build_gather_map(Ctx *c, cudaStream_t st);
 cudaError_t check_jacobians(Ctx *c, cudaStream_t st);
 cudaError_t build_batch_structures(Ctx *c, cudaStream_t st);

@@ -21,6 +21,7 @@ struct PlainArgs {
   int ldisp;
   double freq0;
   double fac1;  // log(FREQ / FREQ0) evaluated on the host (VCMPLX, haskattn.f:633)
+  int ebase;    // element of block 0 (launches over an element range)
 };
 
 // VCMPLX (haskattn.f:602-646): complex velocity of Aki & Richards 5.94,
@@ -246,7 +247,7 @@ __global__ void __launch_bounds__(kPlainThreads, 1)
                  int *__restrict__ err) {
   extern __shared__ double sm[];
   double *shx = sm + kSmShx, *shz = sm + kSmShz, *shn = sm + kSmShn, *qc = sm + kSmQ;
-  const int e = blockIdx.x;
+  const int e = pa.ebase + blockIdx.x;
   const int t = threadIdx.x;
   const int4 ie = mv.ieng[e];
   const bool pml = mv.cdomain[e] == 'A';
@@ -471,14 +472,14 @@ __global__ void __launch_bounds__(kPlainThreads, 1)
   }
 }
 
-// Sum of the element contributions of every nonzero in element order:
+// Sum of the element contributions of every nonzero of [nz0, nz1) in element order:
 // FP64 (complex128 output) and the reference's COMPLEX*8 accumulation
 // CDIST = CDIST + CMPLX(CARG) (asmble.f90:302-305).
-__global__ void k_gather_plain(long long nzero, const int *__restrict__ gptr,
+__global__ void k_gather_plain(long long nz0, long long nz1, const int *__restrict__ gptr,
                                const int *__restrict__ glist, const double2 *__restrict__ elemmat,
                                double2 *__restrict__ csr128, float2 *__restrict__ csr64) {
-  long long nz = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (nz >= nzero) return;
+  long long nz = nz0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (nz >= nz1) return;
   double sr = 0.0, si = 0.0;
   float fr = 0.0f, fi = 0.0f;
   for (int k = gptr[nz]; k < gptr[nz + 1]; k++) {
@@ -585,7 +586,9 @@ PmlParams pml_params(const Ctx *c, char cftype, double freq) {
   return p;
 }
 
-cudaError_t launch_elem_plain(Ctx *c, char cftype, double freq, double py, cudaStream_t st) {
+cudaError_t launch_elem_plain(Ctx *c, char cftype, double freq, double py, int e0, int e1,
+                              cudaStream_t st) {
+  if (e1 <= e0) return cudaSuccess;
   PlainArgs pa;
   pa.pml = pml_params(c, cftype, freq);
   pa.omega = pa.pml.omega;
@@ -596,27 +599,30 @@ cudaError_t launch_elem_plain(Ctx *c, char cftype, double freq, double py, cudaS
   pa.ldisp = c->mesh_scalars.ldisp ? 1 : 0;
   pa.freq0 = c->mesh_scalars.freq0;
   pa.fac1 = (pa.ldisp && pa.freq0 != 0.0) ? std::log(freq / pa.freq0) : 0.0;
+  pa.ebase = e0;
   size_t smem = sizeof(double) * kSmTot;
   if (pa.ldisp) {
     cudaError_t e = cudaFuncSetAttribute(k_elem_plain<true>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_elem_plain<true><<<c->nelem, kPlainThreads, smem, st>>>(c->mv, c->dt, pa, c->d_elemmat,
-                                                              c->d_err);
+    k_elem_plain<true><<<e1 - e0, kPlainThreads, smem, st>>>(c->mv, c->dt, pa, c->d_elemmat,
+                                                             c->d_err);
   } else {
     cudaError_t e = cudaFuncSetAttribute(k_elem_plain<false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_elem_plain<false><<<c->nelem, kPlainThreads, smem, st>>>(c->mv, c->dt, pa, c->d_elemmat,
-                                                               c->d_err);
+    k_elem_plain<false><<<e1 - e0, kPlainThreads, smem, st>>>(c->mv, c->dt, pa, c->d_elemmat,
+                                                              c->d_err);
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_gather_plain(Ctx *c, double *csr128, float *csr64, cudaStream_t st) {
+cudaError_t launch_gather_plain(Ctx *c, double *csr128, float *csr64, long long nz0,
+                                long long nz1, cudaStream_t st) {
+  if (nz1 <= nz0) return cudaSuccess;
   int th = 256;
-  long long blocks = (c->nzero + th - 1) / th;
-  k_gather_plain<<<(unsigned)blocks, th, 0, st>>>(c->nzero, c->d_gptr, c->d_glist, c->d_elemmat,
+  long long blocks = (nz1 - nz0 + th - 1) / th;
+  k_gather_plain<<<(unsigned)blocks, th, 0, st>>>(nz0, nz1, c->d_gptr, c->d_glist, c->d_elemmat,
                                                    (double2 *)csr128, (float2 *)csr64);
   return cudaGetLastError();
 }

@@ -58,6 +58,27 @@ def test_asmble_driver_host_buffer(case0):
     assert np.array_equal(out.view(np.uint32), ref64.view(np.uint32))
 
 
+def test_asmble_driver_chunked_pinned_and_pageable():
+    """The driver computes elements in up to 16 chunks and copies each chunk's
+    completed CSR rows while the next computes: the jittered, topographic
+    layout at 48x20 elements (960 elements, 6 chunks) into pinned and
+    pageable host buffers, both bit-exact to the oracle's COMPLEX*8 CDIST,
+    twice in a row."""
+    mesh, pairs, _ = synth.make_config(4, nx=48, nz=20)
+    g = oracle.graph_build(mesh)
+    ctx = Context(mesh, g)
+    f, py = pairs[5]
+    _, ref64 = oracle.asmble(mesh, g, "B", f, py)
+    pinned = torch.empty(g.nzero, dtype=torch.complex64, pin_memory=True)
+    for _ in range(2):
+        pinned.fill_(float("nan"))
+        ctx.asmble_driver("B", f, py, out=pinned)
+        assert np.array_equal(pinned.numpy().view(np.uint32), ref64.view(np.uint32))
+        page = ctx.asmble_driver("B", f, py)
+        assert np.array_equal(page.view(np.uint32), ref64.view(np.uint32))
+    ctx.close()
+
+
 def test_batched_matches_oracle(case0):
     mesh, pairs, g, ctx = case0
     sel = [pairs[0], pairs[5], pairs[11], pairs[15], (0.8, 2.0e-4), (0.3, 0.0)]
