@@ -537,6 +537,14 @@ int fem25_peff_dev(fem25_ctx *h, int nsrc, const float *a_loc, const float *ue, 
   return FEM25_OK;
 }
 
+int fem25_addblk_dev(fem25_ctx *h, int nsrc, const float *ue, float *sol, void *stream) {
+  if (!h || !ue || !sol || nsrc <= 0) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  CK(cudaSetDevice(c->device), "set device");
+  CK(launch_addblk(c, nsrc, ue, sol, (cudaStream_t)stream), "addblk");
+  return FEM25_OK;
+}
+
 int fem25_gradient_dev(fem25_ctx *h, int npairs, const double *freq, const double *py, int nsrc,
                        const double *u, const double *lam, int prec, double *grad, void *stream) {
   if (!h || !freq || !py || !u || !lam || !grad || npairs <= 0 || nsrc <= 0) return FEM25_ERR_ARG;

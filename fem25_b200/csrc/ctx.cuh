@@ -139,6 +139,7 @@ cudaError_t launch_stream_batch(Ctx *c, int n, const SysParam *hsys, double *rin
                                 long long slot_stride, int nslots, cudaStream_t st);
 cudaError_t launch_peff(Ctx *c, int nsrc, const float *a_loc, const float *ue, float *peff,
                         cudaStream_t st);
+cudaError_t launch_addblk(Ctx *c, int nsrc, const float *u0, float *sol, cudaStream_t st);
 cudaError_t launch_grad_plain(Ctx *c, const PairTable &pt, int npairs, int nsrc, const double *u,
                               const double *lam, double *grad, cudaStream_t st);
 cudaError_t prepare_grad_tc(Ctx *c);

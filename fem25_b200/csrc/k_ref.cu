@@ -51,6 +51,26 @@ cudaError_t launch_peff(Ctx *c, int nsrc, const float *a_loc, const float *ue, f
 }
 
 // ---------------------------------------------------------------------------
+// ADDBLK (bielak_utils.f:1116-1125): SOL(i) += U0(i) on the 'E' DOFs, for
+// nsrc solutions at once
+// ---------------------------------------------------------------------------
+__global__ void k_addblk(int ndof, int nsrc, const char *__restrict__ cnp,
+                         const float2 *__restrict__ u0, float2 *__restrict__ sol) {
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (long long)ndof * nsrc) return;
+  if (cnp[gid % ndof] != 'E') return;
+  const float2 a = sol[gid], b = u0[gid];
+  sol[gid] = make_float2(a.x + b.x, a.y + b.y);
+}
+
+cudaError_t launch_addblk(Ctx *c, int nsrc, const float *u0, float *sol, cudaStream_t st) {
+  const long long n = (long long)c->ndof * nsrc;
+  k_addblk<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(c->ndof, nsrc, c->d_cnp,
+                                                        (const float2 *)u0, (float2 *)sol);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // misfit + adjoint source, one thread per (source, receiver)
 //   trig[ir] = (cos, sin) of omega*py*yrec in single precision; rot = (cos th,
 //   sin th, cos -th, sin -th) of the model azimuth (computed on the host).

@@ -60,6 +60,7 @@ def lib():
         L.fem25_assemble_dev.argtypes = [vp, C.c_char, d, d, vp, vp, vp]
         L.fem25_assemble_batch_dev.argtypes = [vp, i, vp, vp, vp, vp, ll, i, vp]
         L.fem25_peff_dev.argtypes = [vp, i, vp, vp, vp, vp]
+        L.fem25_addblk_dev.argtypes = [vp, i, vp, vp, vp]
         L.fem25_gradient_dev.argtypes = [vp, i, vp, vp, i, vp, vp, i, vp, vp]
         L.fem25_ref_gradient_dev.argtypes = [vp, C.c_char_p, d, d, d, vp, vp, i, vp, vp]
         L.fem25_ref_gradient_info.argtypes = [vp, C.POINTER(i), C.POINTER(ll), vp]
@@ -241,6 +242,10 @@ class Context:
     def asmb_peff(self, nsrc, a_loc, ue, peff, stream=None):
         self._check(lib().fem25_peff_dev(self.h, nsrc, _ptr(a_loc), _ptr(ue), _ptr(peff),
                                          _stream(stream)))
+
+    def addblk(self, nsrc, ue, sol, stream=None):
+        """ADDBLK: sol += ue on the 'E' DOFs (COMPLEX*8 [nsrc][NDOF], in place)."""
+        self._check(lib().fem25_addblk_dev(self.h, nsrc, _ptr(ue), _ptr(sol), _stream(stream)))
 
     # ---- gradients
     def gradient(self, freqs, pys, nsrc, u, lam, grad, prec=FEM25_PREC_FP64, stream=None):

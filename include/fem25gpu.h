@@ -119,6 +119,13 @@ int fem25_assemble_batch_dev(fem25_ctx *ctx, int n, const char *cftype, const do
 int fem25_peff_dev(fem25_ctx *ctx, int nsrc, const float *a_loc, const float *ue, float *peff,
                    void *stream);
 
+/* Drop-in for ADDBLK (bielak_utils.f:1116-1125; callers funcgradh.f90:248,
+ * srcrec.f90:694, fgh_window.f90:437, qpmfree.f90:378): after the solve, the
+ * background field is added back on the exterior ('E') DOFs,
+ * sol(i) += ue(i) in COMPLEX*8, for nsrc solutions at once; ue and sol are
+ * COMPLEX*8 [nsrc][NDOF] device arrays, sol updated in place. */
+int fem25_addblk_dev(fem25_ctx *ctx, int nsrc, const float *ue, float *sol, void *stream);
+
 /* ---- adjoint gradient -------------------------------------------------------
  * Exact gradient of the misfit with respect to the anchor-node lambda, mu and
  * rho:  grad[m*NNPG + p] += sum_s Re( lam_s^H (dA/dm_p) u_s )

@@ -65,6 +65,7 @@ def _setup(L):
     L.orc_graph_copy.argtypes = [vp, vp, vp, vp, vp, vp]
     L.orc_graph_free.argtypes = [vp]
     L.orc_peff.argtypes = [C.c_int, vp, vp, vp, vp, vp, vp]
+    L.orc_addblk.argtypes = [C.c_int, vp, vp, vp]
     L.orc_grad_exact.argtypes = [vp, vp, C.c_int, C.c_double, C.c_double, C.c_int, vp, vp, vp]
     L.orc_gengmask.argtypes = [vp, vp, C.c_int, vp, vp, C.POINTER(C.c_int)]
     L.orc_ncon_anchor.argtypes = [vp]
@@ -215,6 +216,13 @@ def peff(g, cdist64, ue64):
     lib().orc_peff(g.ndof, _p(g.irptr), _p(g.jcptr), _p(g.cnp),
                    _p(np.ascontiguousarray(cdist64, np.complex64)),
                    _p(np.ascontiguousarray(ue64, np.complex64)), _p(out))
+    return out
+
+
+def addblk(g, ue64, sol64):
+    """ADDBLK: sol + ue on the 'E' DOFs (COMPLEX*8), returned as a new array."""
+    out = np.array(sol64, np.complex64, copy=True)
+    lib().orc_addblk(g.ndof, _p(g.cnp), _p(np.ascontiguousarray(ue64, np.complex64)), _p(out))
     return out
 
 

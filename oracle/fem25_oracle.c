@@ -1450,6 +1450,19 @@ void orc_peff(int ndof, const int *irptr, const int *jcptr, const char *cnp, con
     }
 }
 
+/* ADDBLK (bielak_utils.f:1116-1125): the Bielak background field is added
+ * back into the total solution on the exterior DOFs, SOL(i) = SOL(i) + U0(i)
+ * for CNP(i) = 'E', in COMPLEX*8 (callers funcgradh.f90:248,
+ * srcrec.f90:694). */
+void orc_addblk(int ndof, const char *cnp, const float *u0, float *sol)
+{
+    for (int idof = 1; idof <= ndof; idof++) {
+        if (cnp[idof - 1] != 'E') continue;
+        sol[2 * (idof - 1)] = sol[2 * (idof - 1)] + u0[2 * (idof - 1)];
+        sol[2 * (idof - 1) + 1] = sol[2 * (idof - 1) + 1] + u0[2 * (idof - 1) + 1];
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* exact adjoint gradient in anchor-node lambda, mu, rho                      */
 /* g[m*nnpg + p] += sum_s Re( lam_s^H (dA/dm_p) u_s ) over non-PML elements.  */

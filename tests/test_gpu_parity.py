@@ -159,6 +159,23 @@ def test_peff_matches_oracle(case0):
         assert np.array_equal(got[s].view(np.uint32), ref.view(np.uint32))
 
 
+def test_addblk_matches_oracle(case0):
+    mesh, pairs, g, ctx = case0
+    rng = np.random.default_rng(4)
+    nsrc = 3
+    shape = (nsrc, g.ndof)
+    ue = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    sol = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    d_u = torch.from_numpy(ue).to(_dev())
+    d_s = torch.from_numpy(sol).to(_dev())
+    ctx.addblk(nsrc, d_u, d_s)
+    got = d_s.cpu().numpy()
+    assert np.count_nonzero(g.cnp == ord("E")) > 0
+    for s in range(nsrc):
+        ref = oracle.addblk(g, ue[s], sol[s])
+        assert np.array_equal(got[s].view(np.uint32), ref.view(np.uint32))
+
+
 def test_gradient_fp64_matches_oracle():
     mesh, pairs, _ = synth.make_config(0, nx=10, nz=6)
     g = oracle.graph_build(mesh)

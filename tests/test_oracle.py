@@ -261,3 +261,17 @@ def test_dabmkisob25_matches_central_difference():
     fd_b = (op(a0, b0 + h) - op(a0, b0 - h)) / (2 * h)
     got_b = dmdb + dkdb
     assert np.abs(got_b - fd_b).max() <= 1e-8 * np.abs(fd_b).max()
+
+
+def test_addblk_touches_only_exterior_dofs(small_case):
+    """ADDBLK adds the background field on the 'E' DOFs only, in COMPLEX*8."""
+    mesh, _ = small_case
+    g = oracle.graph_build(mesh)
+    rng = np.random.default_rng(9)
+    ue = (rng.standard_normal(g.ndof) + 1j * rng.standard_normal(g.ndof)).astype(np.complex64)
+    sol = (rng.standard_normal(g.ndof) + 1j * rng.standard_normal(g.ndof)).astype(np.complex64)
+    out = oracle.addblk(g, ue, sol)
+    ext = g.cnp == ord("E")
+    assert ext.any() and (~ext).any()
+    assert np.array_equal(out[~ext], sol[~ext])
+    assert np.array_equal(out[ext], (sol + ue)[ext])
