@@ -30,6 +30,7 @@ UNITS = [
     ("k_grad_tc.cu", []),
     ("api.cu", []),
     ("misfit_noalloc.cu", ["-fmad=false"]),
+    ("dense_solve.cu", []),
 ]
 HOST = [("host_setup.cpp", ["-O2", "-ffp-contract=off", "-fPIC", "-fopenmp", "-std=c++17"])]
 
@@ -69,7 +70,8 @@ def build(verbose=False, extra=()):
         if _stale(obj, [src, __file__] + headers):
             _run(["g++"] + flags + ["-I", os.path.join(ROOT, "include"), "-I", SRC, "-c", "-o", obj, src])
     if _stale(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-Xcompiler", "-fopenmp", "-lgomp"])
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs +
+             ["-Xcompiler", "-fopenmp", "-lgomp", "-lcusolver"])
     return LIB
 
 

@@ -102,6 +102,7 @@ void free_ctx(Ctx *c) {
   for (auto &e : c->drv_ev)
     if (e) cudaEventDestroy(e);
   if (c->copy_st) cudaStreamDestroy(c->copy_st);
+  free_dense(c);
 }
 
 int read_err_word(Ctx *c, cudaStream_t st) {
@@ -535,6 +536,27 @@ int fem25_peff_dev(fem25_ctx *h, int nsrc, const float *a_loc, const float *ue, 
   CK(cudaSetDevice(c->device), "set device");
   CK(launch_peff(c, nsrc, a_loc, ue, peff, (cudaStream_t)stream), "peff");
   return FEM25_OK;
+}
+
+int fem25_dense_factor_dev(fem25_ctx *h, const double *csr128, void *stream) {
+  if (!h || !csr128) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  if (c->ndof > FEM25_DENSE_MAX_NDOF)
+    return fail(c, FEM25_ERR_UNSUPPORTED,
+                "dense solve: NDOF above FEM25_DENSE_MAX_NDOF (use the sparse host solver)");
+  CK(cudaSetDevice(c->device), "set device");
+  std::string msg;
+  int r = dense_factor(c, csr128, (cudaStream_t)stream, &msg);
+  return r ? fail(c, r, msg) : FEM25_OK;
+}
+
+int fem25_dense_solve_dev(fem25_ctx *h, int nrhs, int trans, double *rhs, void *stream) {
+  if (!h || !rhs || nrhs <= 0 || trans < 0 || trans > 2) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  CK(cudaSetDevice(c->device), "set device");
+  std::string msg;
+  int r = dense_solve(c, nrhs, trans, rhs, (cudaStream_t)stream, &msg);
+  return r ? fail(c, r, msg) : FEM25_OK;
 }
 
 int fem25_addblk_dev(fem25_ctx *h, int nsrc, const float *ue, float *sol, void *stream) {

@@ -55,6 +55,8 @@ struct PairTable {
   double2 p[kMaxPairs];
 };
 
+struct DenseLU;  // dense LU of the small-mesh direct solve (dense_solve.cu)
+
 struct Ctx {
   int device = 0;
   std::string err;
@@ -120,6 +122,7 @@ struct Ctx {
   std::vector<int> drv_elem, drv_row;
   cudaStream_t copy_st = nullptr;
   std::vector<cudaEvent_t> drv_ev;
+  DenseLU *dense = nullptr;
   // optional CUDA-event timing of the dominant kernels
   bool prof = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -140,6 +143,9 @@ cudaError_t launch_stream_batch(Ctx *c, int n, const SysParam *hsys, double *rin
 cudaError_t launch_peff(Ctx *c, int nsrc, const float *a_loc, const float *ue, float *peff,
                         cudaStream_t st);
 cudaError_t launch_addblk(Ctx *c, int nsrc, const float *u0, float *sol, cudaStream_t st);
+int dense_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *msg);
+int dense_solve(Ctx *c, int nrhs, int trans, double *rhs, cudaStream_t st, std::string *msg);
+void free_dense(Ctx *c);
 cudaError_t launch_grad_plain(Ctx *c, const PairTable &pt, int npairs, int nsrc, const double *u,
                               const double *lam, double *grad, cudaStream_t st);
 cudaError_t prepare_grad_tc(Ctx *c);

@@ -61,6 +61,8 @@ def lib():
         L.fem25_assemble_batch_dev.argtypes = [vp, i, vp, vp, vp, vp, ll, i, vp]
         L.fem25_peff_dev.argtypes = [vp, i, vp, vp, vp, vp]
         L.fem25_addblk_dev.argtypes = [vp, i, vp, vp, vp]
+        L.fem25_dense_factor_dev.argtypes = [vp, vp, vp]
+        L.fem25_dense_solve_dev.argtypes = [vp, i, i, vp, vp]
         L.fem25_gradient_dev.argtypes = [vp, i, vp, vp, i, vp, vp, i, vp, vp]
         L.fem25_ref_gradient_dev.argtypes = [vp, C.c_char_p, d, d, d, vp, vp, i, vp, vp]
         L.fem25_ref_gradient_info.argtypes = [vp, C.POINTER(i), C.POINTER(ll), vp]
@@ -242,6 +244,16 @@ class Context:
     def asmb_peff(self, nsrc, a_loc, ue, peff, stream=None):
         self._check(lib().fem25_peff_dev(self.h, nsrc, _ptr(a_loc), _ptr(ue), _ptr(peff),
                                          _stream(stream)))
+
+    def dense_factor(self, csr128, stream=None):
+        """LU of the assembled complex128 CSR (device) for the small-mesh solve."""
+        self._check(lib().fem25_dense_factor_dev(self.h, _ptr(csr128), _stream(stream)))
+
+    def dense_solve(self, rhs, trans=0, stream=None):
+        """op(A) X = B in place; rhs complex128 [nrhs][NDOF] on the device;
+        trans 0: A, 1: A^T, 2: A^H."""
+        nrhs = rhs.numel() // self.ndof if hasattr(rhs, "numel") else rhs.size // self.ndof
+        self._check(lib().fem25_dense_solve_dev(self.h, nrhs, trans, _ptr(rhs), _stream(stream)))
 
     def addblk(self, nsrc, ue, sol, stream=None):
         """ADDBLK: sol += ue on the 'E' DOFs (COMPLEX*8 [nsrc][NDOF], in place)."""

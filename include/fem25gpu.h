@@ -119,6 +119,20 @@ int fem25_assemble_batch_dev(fem25_ctx *ctx, int n, const char *cftype, const do
 int fem25_peff_dev(fem25_ctx *ctx, int nsrc, const float *a_loc, const float *ue, float *peff,
                    void *stream);
 
+/* ---- direct solve on the GPU (small meshes) ---------------------------------
+ * Stands in for the host MUMPS factor / solve hop (forward solve
+ * bielak25.f90:443-446, 545-551; transpose adjoint solve adjgrad.f90:327-341)
+ * when NDOF <= FEM25_DENSE_MAX_NDOF: fem25_dense_factor_dev expands the
+ * complex128 CSR (the output of fem25_assemble_dev / _batch_dev, device) into
+ * a dense matrix (NDOF^2 x 16 bytes of device memory, kept by the context)
+ * and factors it by LU with partial pivoting; it synchronises the stream and
+ * returns FEM25_ERR_ARG for an exactly singular pivot.  fem25_dense_solve_dev
+ * then solves op(A) X = B in place for nrhs complex128 columns [nrhs][NDOF]
+ * on the device; trans = 0: A, 1: A^T (MUMPS ICNTL(9) != 1), 2: A^H. */
+#define FEM25_DENSE_MAX_NDOF 40000
+int fem25_dense_factor_dev(fem25_ctx *ctx, const double *csr128, void *stream);
+int fem25_dense_solve_dev(fem25_ctx *ctx, int nrhs, int trans, double *rhs, void *stream);
+
 /* Drop-in for ADDBLK (bielak_utils.f:1116-1125; callers funcgradh.f90:248,
  * srcrec.f90:694, fgh_window.f90:437, qpmfree.f90:378): after the solve, the
  * background field is added back on the exterior ('E') DOFs,
