@@ -641,6 +641,28 @@ int fem25_ref_gradient_dev(fem25_ctx *h, const char *cinvtype, double vpvs, doub
   return FEM25_OK;
 }
 
+int fem25_ref_met225_dev(fem25_ctx *h, const char *cinvtype, double freq, double py,
+                         const float *adjlam, const float *nu, const float *alpha,
+                         const float *wave, int accumulate, float *p1buf, float *p2buf,
+                         void *stream) {
+  if (!h || !cinvtype || !adjlam || !nu || !alpha || !wave || !p1buf || !p2buf)
+    return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  std::string ct(cinvtype, cinvtype + 2);
+  int lisp = 0, liss = 0;
+  if (ct == "PP" || ct == "pp") lisp = 1;
+  else if (ct == "SS" || ct == "ss") liss = 1;
+  else if (ct == "PS" || ct == "ps") lisp = liss = 1;
+  else return fail(c, FEM25_ERR_UNSUPPORTED, "met225_mod: Error anisotropy not programmed!");
+  CK(cudaSetDevice(c->device), "set device");
+  int r = ensure_refgrad(c);
+  if (r) return r;
+  CK(launch_ref_met225(c, lisp, liss, 6.2831853071795862 * freq, py, adjlam, nu, alpha, wave,
+                       accumulate ? 1 : 0, p1buf, p2buf, (cudaStream_t)stream),
+     "met225");
+  return FEM25_OK;
+}
+
 int fem25_ref_vforce2_dev(fem25_ctx *h, const char *cinvtype, double freq, double py,
                           const float *wave, float *fmat, void *stream) {
   if (!h || !cinvtype || !wave || !fmat) return FEM25_ERR_ARG;

@@ -154,6 +154,10 @@ cudaError_t launch_grad_tc(Ctx *c, const PairTable &pt, int npairs, int nsrc, co
 cudaError_t launch_ref_cfmat(Ctx *c, int lisp, double vpvs, double omega, double py,
                              const float *wave, int accumulate, cudaStream_t st);
 cudaError_t launch_ref_adjflam(Ctx *c, const float *adjlam, float *gradl, cudaStream_t st);
+cudaError_t launch_ref_met225(Ctx *c, int lisp, int liss, double omega, double py,
+                              const float *adjlam, const float *nu, const float *alpha,
+                              const float *wave, int accumulate, float *p1buf, float *p2buf,
+                              cudaStream_t st);
 cudaError_t launch_ref_vforce2(Ctx *c, int lisp, int liss, double omega, double py,
                                const float *wave, float *fmat, cudaStream_t st);
 cudaError_t launch_misfit(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const float *d_trig,

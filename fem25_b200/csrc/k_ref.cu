@@ -6,6 +6,8 @@
 //
 // Compiled with -fmad=false so every COMPLEX*8 / REAL*8 operation is rounded
 // on its own, as the reference writes it.
+#include <algorithm>
+
 #include "ctx.cuh"
 #include "kcommon.cuh"
 
@@ -391,6 +393,139 @@ struct VfArgs {
   long long nz;
 };
 
+// DJACAB (djac.f:1-139) + DABMKISOB25 (dstiff25.f:1-203) of element e for
+// inversion anchor p, into shared memory as COMPLEX*8
+// CARG = CMPLX(DCMPLX(DMD,0) + DKD) [75][75]: carg0 holds the first variable
+// (alpha when lisp), carg1 beta when both.  sm: SHG tables and per-point
+// coefficients.  Every thread of the CTA calls it; it ends with a barrier.
+__device__ __forceinline__ void dabm_carg(const MeshView &mv, const DevTables &dt, int e, int p,
+                                          double wpy, double wpy2, int lisp, int liss, double *sm,
+                                          float2 *carg0, float2 *carg1, int *err) {
+  double *shx = sm, *shz = sm + kNq * kNen, *shn = sm + 2 * kNq * kNen;
+  double *qc = sm + 3 * kNq * kNen;  // [kNq][8]
+  const int t = threadIdx.x;
+  const int4 ie = mv.ieng[e];
+  if (t < kNq) {
+    const int q = t, intx = q % kNint, intz = q / kNint;
+    QGeo g;
+    if (!quad_geo(mv, dt, ie, q, false, g)) atomicCAS(err, 0, e + 1);
+    // DJACAB (djac.f:90-110)
+    const int il[4] = {ie.x - 1, ie.y - 1, ie.z - 1, ie.w - 1};
+    double dab1 = 0.0, dab2 = 0.0;
+    for (int ia = 0; ia < 4; ia++) {
+      double alpha = 0.0, beta = 0.0;
+      if (il[ia] == p) {
+        alpha = sqrt((mv.lam[p] + 2.0 * mv.mu[p]) / mv.rho[p]);
+        beta = sqrt(mv.mu[p] / mv.rho[p]);
+      }
+      dab1 = dab1 + 2.0 * alpha * dt.sf[4 * q + ia];
+      dab2 = dab2 + 2.0 * beta * dt.sf[4 * q + ia];
+    }
+    double *c = qc + 8 * q;
+    c[0] = g.dxdxi; c[1] = g.dxdeta; c[2] = g.dzdxi; c[3] = g.dzdeta; c[4] = g.rjac;
+    double weight = dt.wts[intx] * dt.wts[intz] * g.rjac;
+    c[5] = dab1 * weight;  // DALPHA
+    c[6] = dab2 * weight;  // DBETA
+  }
+  __syncthreads();
+  for (int idx = t; idx < kNq * kNen; idx += kRefThreads) {
+    const int q = idx / kNen;
+    const double *c = qc + 8 * q;
+    const double *sl = dt.shl + 3 * (size_t)idx;
+    double drnxi = sl[0], drneta = sl[1];
+    shx[idx] = (drnxi * c[3] - drneta * c[2]) / c[4];
+    shz[idx] = -(drnxi * c[1] - drneta * c[0]) / c[4];
+    shn[idx] = sl[2];
+  }
+  __syncthreads();
+  if (t < kNab) {
+    const int a = t / kNen, b = t % kNen;
+    // alpha: DMDA(1,1); DKDA real 00 02 20 22, imaginary 01 10 12 21
+    double ma11 = 0.0, ra00 = 0.0, ra02 = 0.0, ra20 = 0.0, ra22 = 0.0;
+    double ia01 = 0.0, ia10 = 0.0, ia12 = 0.0, ia21 = 0.0;
+    // beta: DMDB(0,0) (= DMDB(2,2)); DKDB real 00 02 11 20 22, imaginary 01 10 12 21
+    double mb00 = 0.0, rb00 = 0.0, rb02 = 0.0, rb11 = 0.0, rb20 = 0.0, rb22 = 0.0;
+    double ib01 = 0.0, ib10 = 0.0, ib12 = 0.0, ib21 = 0.0;
+    for (int intx = 0; intx < kNint; intx++)
+      for (int intz = 0; intz < kNint; intz++) {
+        const int q = intx + kNint * intz;
+        const double dalpha = qc[8 * q + 5], dbeta = qc[8 * q + 6];
+        const double phib = shn[q * kNen + b], phibx = shx[q * kNen + b], phibz = shz[q * kNen + b];
+        const double phia = shn[q * kNen + a], phiax = shx[q * kNen + a], phiaz = shz[q * kNen + a];
+        if (lisp) {
+          const double dmassda = wpy2 * dalpha;
+          const double dmdat1 = dmassda * phib;
+          const double dk11da = dalpha * phibx, dk13da = dalpha * phibz;
+          const double dk31da = dalpha * phibx, dk33da = dalpha * phibz;
+          const double dk12da = wpy * dalpha * phib, dk21da = wpy * dalpha * phibx;
+          const double dk23da = wpy * dalpha * phibz, dk32da = wpy * dalpha * phib;
+          ma11 = ma11 + dmdat1 * phia;
+          ra00 = ra00 + phiax * dk11da;
+          ia01 = ia01 - phiax * dk12da;
+          ra02 = ra02 + phiax * dk13da;
+          ia10 = ia10 + phia * dk21da;
+          ia12 = ia12 + phia * dk23da;
+          ra20 = ra20 + phiaz * dk31da;
+          ia21 = ia21 - phiaz * dk32da;
+          ra22 = ra22 + phiaz * dk33da;
+        }
+        if (liss) {
+          const double dmassdb = wpy2 * dbeta;
+          const double dmdbt1 = dmassdb * phib;
+          const double dk11dbt1 = dbeta * phibz;
+          const double dk13dbt1 = dbeta * phibx, dk13dbt2 = -(2.0 * dbeta * phibz);
+          const double dk22dbt1 = dbeta * phibx, dk22dbt2 = dbeta * phibz;
+          const double dk31dbt1 = dbeta * phibz, dk31dbt2 = -(2.0 * dbeta * phibx);
+          const double dk33dbt1 = dbeta * phibx;
+          const double dk12dbt1 = 2.0 * wpy * dbeta * phib, dk12dbt2 = wpy * dbeta * phibx;
+          const double dk21dbt1 = 2.0 * wpy * dbeta * phibx, dk21dbt2 = wpy * dbeta * phib;
+          const double dk23dbt1 = 2.0 * wpy * dbeta * phibz, dk23dbt2 = wpy * dbeta * phib;
+          const double dk32dbt1 = 2.0 * wpy * dbeta * phib, dk32dbt2 = wpy * dbeta * phibz;
+          mb00 = mb00 + dmdbt1 * phia;
+          rb00 = rb00 + phiaz * dk11dbt1;
+          ib01 = ib01 + (phiax * dk12dbt1 + phia * dk12dbt2);
+          rb02 = rb02 + (phiaz * dk13dbt1 + phiax * dk13dbt2);
+          ib10 = ib10 - (phia * dk21dbt1 + phiax * dk21dbt2);
+          rb11 = rb11 + (phiax * dk22dbt1 + phiaz * dk22dbt2);
+          ib12 = ib12 - (phia * dk23dbt1 + phiaz * dk23dbt2);
+          rb20 = rb20 + (phiax * dk31dbt1 + phiaz * dk31dbt2);
+          ib21 = ib21 + (phiaz * dk32dbt1 + phia * dk32dbt2);
+          rb22 = rb22 + phiax * dk33dbt1;
+        }
+      }
+    const int ipe = 3 * a, iqe = 3 * b;
+    auto put = [&](float2 *cg, int i, int j, double re, double im) {
+      cg[(size_t)(ipe + i) * kNee + iqe + j] =
+          make_float2(__double2float_rn(re), __double2float_rn(0.0 + im));
+    };
+    float2 *cb = carg0;
+    if (lisp) {
+      put(cb, 0, 0, 0.0 + ra00, 0.0);
+      put(cb, 0, 1, 0.0 + 0.0, ia01);
+      put(cb, 0, 2, 0.0 + ra02, 0.0);
+      put(cb, 1, 0, 0.0 + 0.0, ia10);
+      put(cb, 1, 1, ma11 + 0.0, 0.0);
+      put(cb, 1, 2, 0.0 + 0.0, ia12);
+      put(cb, 2, 0, 0.0 + ra20, 0.0);
+      put(cb, 2, 1, 0.0 + 0.0, ia21);
+      put(cb, 2, 2, 0.0 + ra22, 0.0);
+      cb = carg1;
+    }
+    if (liss) {
+      put(cb, 0, 0, mb00 + rb00, 0.0);
+      put(cb, 0, 1, 0.0 + 0.0, ib01);
+      put(cb, 0, 2, 0.0 + rb02, 0.0);
+      put(cb, 1, 0, 0.0 + 0.0, ib10);
+      put(cb, 1, 1, 0.0 + rb11, 0.0);
+      put(cb, 1, 2, 0.0 + 0.0, ib12);
+      put(cb, 2, 0, 0.0 + rb20, 0.0);
+      put(cb, 2, 1, 0.0 + 0.0, ib21);
+      put(cb, 2, 2, mb00 + rb22, 0.0);
+    }
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(kRefThreads, 1)
     k_ref_vforce2(MeshView mv, DevTables dt, VfArgs va, const int *__restrict__ lm,
                   const int *__restrict__ anchor_of_col, const int *__restrict__ mconn,
@@ -398,10 +533,8 @@ __global__ void __launch_bounds__(kRefThreads, 1)
                   const float2 *__restrict__ wave, float2 *__restrict__ fmat,
                   int *__restrict__ err) {
   extern __shared__ double sm[];
-  double *shx = sm, *shz = sm + kNq * kNen, *shn = sm + 2 * kNq * kNen;
-  double *qc = sm + 3 * kNq * kNen;                         // [kNq][8]
-  float2 *carg0 = reinterpret_cast<float2 *>(qc + 8 * kNq);  // [75][75] first variable
-  float2 *carg1 = carg0 + kNee * kNee;                       // [75][75] beta when 'PS'
+  float2 *carg0 = reinterpret_cast<float2 *>(sm + 3 * kNq * kNen + 8 * kNq);  // [75][75] first variable
+  float2 *carg1 = carg0 + kNee * kNee;  // [75][75] beta when 'PS'
   const int col = blockIdx.x, t = threadIdx.x;
   const int p = anchor_of_col[col];
   const int i1 = jcsc[col] - 1, i2 = jcsc[col + 1] - 1, nnzrow = i2 - i1;
@@ -414,126 +547,7 @@ __global__ void __launch_bounds__(kRefThreads, 1)
     const int e1 = mconn[p + (size_t)va.nnpg * ic];
     if (e1 <= 0) break;
     const int e = e1 - 1;
-    const int4 ie = mv.ieng[e];
-    if (t < kNq) {
-      const int q = t, intx = q % kNint, intz = q / kNint;
-      QGeo g;
-      if (!quad_geo(mv, dt, ie, q, false, g)) atomicCAS(err, 0, e + 1);
-      // DJACAB (djac.f:90-110)
-      const int il[4] = {ie.x - 1, ie.y - 1, ie.z - 1, ie.w - 1};
-      double dab1 = 0.0, dab2 = 0.0;
-      for (int ia = 0; ia < 4; ia++) {
-        double alpha = 0.0, beta = 0.0;
-        if (il[ia] == p) {
-          alpha = sqrt((mv.lam[p] + 2.0 * mv.mu[p]) / mv.rho[p]);
-          beta = sqrt(mv.mu[p] / mv.rho[p]);
-        }
-        dab1 = dab1 + 2.0 * alpha * dt.sf[4 * q + ia];
-        dab2 = dab2 + 2.0 * beta * dt.sf[4 * q + ia];
-      }
-      double *c = qc + 8 * q;
-      c[0] = g.dxdxi; c[1] = g.dxdeta; c[2] = g.dzdxi; c[3] = g.dzdeta; c[4] = g.rjac;
-      double weight = dt.wts[intx] * dt.wts[intz] * g.rjac;
-      c[5] = dab1 * weight;  // DALPHA
-      c[6] = dab2 * weight;  // DBETA
-    }
-    __syncthreads();
-    for (int idx = t; idx < kNq * kNen; idx += kRefThreads) {
-      const int q = idx / kNen;
-      const double *c = qc + 8 * q;
-      const double *sl = dt.shl + 3 * (size_t)idx;
-      double drnxi = sl[0], drneta = sl[1];
-      shx[idx] = (drnxi * c[3] - drneta * c[2]) / c[4];
-      shz[idx] = -(drnxi * c[1] - drneta * c[0]) / c[4];
-      shn[idx] = sl[2];
-    }
-    __syncthreads();
-    if (t < kNab) {
-      const int a = t / kNen, b = t % kNen;
-      // alpha: DMDA(1,1); DKDA real 00 02 20 22, imaginary 01 10 12 21
-      double ma11 = 0.0, ra00 = 0.0, ra02 = 0.0, ra20 = 0.0, ra22 = 0.0;
-      double ia01 = 0.0, ia10 = 0.0, ia12 = 0.0, ia21 = 0.0;
-      // beta: DMDB(0,0) (= DMDB(2,2)); DKDB real 00 02 11 20 22, imaginary 01 10 12 21
-      double mb00 = 0.0, rb00 = 0.0, rb02 = 0.0, rb11 = 0.0, rb20 = 0.0, rb22 = 0.0;
-      double ib01 = 0.0, ib10 = 0.0, ib12 = 0.0, ib21 = 0.0;
-      for (int intx = 0; intx < kNint; intx++)
-        for (int intz = 0; intz < kNint; intz++) {
-          const int q = intx + kNint * intz;
-          const double dalpha = qc[8 * q + 5], dbeta = qc[8 * q + 6];
-          const double phib = shn[q * kNen + b], phibx = shx[q * kNen + b], phibz = shz[q * kNen + b];
-          const double phia = shn[q * kNen + a], phiax = shx[q * kNen + a], phiaz = shz[q * kNen + a];
-          if (va.lisp) {
-            const double dmassda = wpy2 * dalpha;
-            const double dmdat1 = dmassda * phib;
-            const double dk11da = dalpha * phibx, dk13da = dalpha * phibz;
-            const double dk31da = dalpha * phibx, dk33da = dalpha * phibz;
-            const double dk12da = wpy * dalpha * phib, dk21da = wpy * dalpha * phibx;
-            const double dk23da = wpy * dalpha * phibz, dk32da = wpy * dalpha * phib;
-            ma11 = ma11 + dmdat1 * phia;
-            ra00 = ra00 + phiax * dk11da;
-            ia01 = ia01 - phiax * dk12da;
-            ra02 = ra02 + phiax * dk13da;
-            ia10 = ia10 + phia * dk21da;
-            ia12 = ia12 + phia * dk23da;
-            ra20 = ra20 + phiaz * dk31da;
-            ia21 = ia21 - phiaz * dk32da;
-            ra22 = ra22 + phiaz * dk33da;
-          }
-          if (va.liss) {
-            const double dmassdb = wpy2 * dbeta;
-            const double dmdbt1 = dmassdb * phib;
-            const double dk11dbt1 = dbeta * phibz;
-            const double dk13dbt1 = dbeta * phibx, dk13dbt2 = -(2.0 * dbeta * phibz);
-            const double dk22dbt1 = dbeta * phibx, dk22dbt2 = dbeta * phibz;
-            const double dk31dbt1 = dbeta * phibz, dk31dbt2 = -(2.0 * dbeta * phibx);
-            const double dk33dbt1 = dbeta * phibx;
-            const double dk12dbt1 = 2.0 * wpy * dbeta * phib, dk12dbt2 = wpy * dbeta * phibx;
-            const double dk21dbt1 = 2.0 * wpy * dbeta * phibx, dk21dbt2 = wpy * dbeta * phib;
-            const double dk23dbt1 = 2.0 * wpy * dbeta * phibz, dk23dbt2 = wpy * dbeta * phib;
-            const double dk32dbt1 = 2.0 * wpy * dbeta * phib, dk32dbt2 = wpy * dbeta * phibz;
-            mb00 = mb00 + dmdbt1 * phia;
-            rb00 = rb00 + phiaz * dk11dbt1;
-            ib01 = ib01 + (phiax * dk12dbt1 + phia * dk12dbt2);
-            rb02 = rb02 + (phiaz * dk13dbt1 + phiax * dk13dbt2);
-            ib10 = ib10 - (phia * dk21dbt1 + phiax * dk21dbt2);
-            rb11 = rb11 + (phiax * dk22dbt1 + phiaz * dk22dbt2);
-            ib12 = ib12 - (phia * dk23dbt1 + phiaz * dk23dbt2);
-            rb20 = rb20 + (phiax * dk31dbt1 + phiaz * dk31dbt2);
-            ib21 = ib21 + (phiaz * dk32dbt1 + phia * dk32dbt2);
-            rb22 = rb22 + phiax * dk33dbt1;
-          }
-        }
-      const int ipe = 3 * a, iqe = 3 * b;
-      auto put = [&](float2 *cg, int i, int j, double re, double im) {
-        cg[(size_t)(ipe + i) * kNee + iqe + j] =
-            make_float2(__double2float_rn(re), __double2float_rn(0.0 + im));
-      };
-      float2 *cb = carg0;
-      if (va.lisp) {
-        put(cb, 0, 0, 0.0 + ra00, 0.0);
-        put(cb, 0, 1, 0.0 + 0.0, ia01);
-        put(cb, 0, 2, 0.0 + ra02, 0.0);
-        put(cb, 1, 0, 0.0 + 0.0, ia10);
-        put(cb, 1, 1, ma11 + 0.0, 0.0);
-        put(cb, 1, 2, 0.0 + 0.0, ia12);
-        put(cb, 2, 0, 0.0 + ra20, 0.0);
-        put(cb, 2, 1, 0.0 + 0.0, ia21);
-        put(cb, 2, 2, 0.0 + ra22, 0.0);
-        cb = carg1;
-      }
-      if (va.liss) {
-        put(cb, 0, 0, mb00 + rb00, 0.0);
-        put(cb, 0, 1, 0.0 + 0.0, ib01);
-        put(cb, 0, 2, 0.0 + rb02, 0.0);
-        put(cb, 1, 0, 0.0 + 0.0, ib10);
-        put(cb, 1, 1, 0.0 + rb11, 0.0);
-        put(cb, 1, 2, 0.0 + 0.0, ib12);
-        put(cb, 2, 0, 0.0 + rb20, 0.0);
-        put(cb, 2, 1, 0.0 + 0.0, ib21);
-        put(cb, 2, 2, mb00 + rb22, 0.0);
-      }
-    }
-    __syncthreads();
+    dabm_carg(mv, dt, e, p, wpy, wpy2, va.lisp, va.liss, sm, carg0, carg1, err);
     if (t < kNee) {
       const int ipe = t;
       const int *lme = lm + (size_t)e * kNee;
@@ -567,6 +581,109 @@ __global__ void __launch_bounds__(kRefThreads, 1)
       }
     }
     __syncthreads();
+  }
+}
+
+// MET225_MOD (qpmfree.f90:1000-1250): one CTA per CSC column (inversion
+// anchor).  For each connected element (MCONN order) the DABMKISOB25 blocks
+// are integrated as in VFORCE25_2; 75 threads then add, row by row,
+// (CWGHT * CARG) * WAVE and (CWGHT * CARG) * ALPHA into the shared-memory
+// columns T1, T2 of each variable (nulled inside the element loop, as the
+// reference does, unless accumulate).  Finally one thread per (variable,
+// buffer) forms PBUF1 -= REAL(CONJG(T1) * NU), PBUF2 -= REAL(CONJG(T2) *
+// ADJLAM) over the column's rows in order.  p1buf, p2buf: [ncol * nvar],
+// entry col * nvar + v (alpha before beta).
+struct MetArgs {
+  double omega, py;
+  int lisp, liss, ncon, nnpg, maxrow, accumulate;
+};
+
+__global__ void __launch_bounds__(kRefThreads, 1)
+    k_ref_met225(MeshView mv, DevTables dt, MetArgs ma, const int *__restrict__ lm,
+                 const int *__restrict__ anchor_of_col, const int *__restrict__ mconn,
+                 const double *__restrict__ elem_wts, const int *__restrict__ jcsc,
+                 const int *__restrict__ icsc, const float2 *__restrict__ adjlam,
+                 const float2 *__restrict__ nu, const float2 *__restrict__ alpha,
+                 const float2 *__restrict__ wave, float *__restrict__ p1buf,
+                 float *__restrict__ p2buf, int *__restrict__ err) {
+  extern __shared__ double sm[];
+  float2 *carg0 = reinterpret_cast<float2 *>(sm + 3 * kNq * kNen + 8 * kNq);
+  float2 *carg1 = carg0 + kNee * kNee;
+  float2 *t1 = carg1 + kNee * kNee;  // [2][maxrow]
+  float2 *t2 = t1 + 2 * ma.maxrow;   // [2][maxrow]
+  const int col = blockIdx.x, t = threadIdx.x;
+  const int p = anchor_of_col[col];
+  const int i1 = jcsc[col] - 1, i2 = jcsc[col + 1] - 1, nnzrow = i2 - i1;
+  const int nvar = ma.lisp + ma.liss;
+  const double wpy = ma.omega * ma.py, wpy2 = ipow2(ma.omega * ma.py);
+  for (int k = t; k < 2 * ma.maxrow; k += kRefThreads) {
+    t1[k] = make_float2(0.0f, 0.0f);
+    t2[k] = make_float2(0.0f, 0.0f);
+  }
+  __syncthreads();
+  for (int ic = 0; ic < ma.ncon; ic++) {
+    const int e1 = mconn[p + (size_t)ma.nnpg * ic];
+    if (e1 <= 0) break;
+    const int e = e1 - 1;
+    dabm_carg(mv, dt, e, p, wpy, wpy2, ma.lisp, ma.liss, sm, carg0, carg1, err);
+    if (!ma.accumulate) {
+      for (int k = t; k < 2 * ma.maxrow; k += kRefThreads) {
+        t1[k] = make_float2(0.0f, 0.0f);
+        t2[k] = make_float2(0.0f, 0.0f);
+      }
+      __syncthreads();
+    }
+    if (t < kNee) {
+      const int ipe = t;
+      const int *lme = lm + (size_t)e * kNee;
+      const int idof = lme[ipe];
+      if (idof > 0) {
+        int lo = 0, hi = nnzrow - 1, inz = -1;
+        while (lo <= hi) {
+          int mid = (lo + hi) >> 1, v = icsc[i1 + mid];
+          if (v == idof) { inz = mid; break; }
+          if (v < idof) lo = mid + 1;
+          else hi = mid - 1;
+        }
+        if (inz < 0) {
+          atomicCAS(err, 0, -(col + 1));
+        } else {
+          const cfl cwght{__double2float_rn(elem_wts[e]), 0.0f};
+          for (int v = 0; v < nvar; v++) {
+            const float2 *cg = v == 0 ? carg0 : carg1;
+            float2 *r1 = t1 + v * ma.maxrow + inz, *r2 = t2 + v * ma.maxrow + inz;
+            float ar = r1->x, ai = r1->y, br = r2->x, bi = r2->y;
+            for (int iqe = 0; iqe < kNee; iqe++) {
+              const int jdof = lme[iqe];
+              if (jdof <= 0) continue;
+              const float2 cv = cg[(size_t)ipe * kNee + iqe];
+              const cfl cw = cmulf(cwght, cfl{cv.x, cv.y});
+              const float2 wv = wave[jdof - 1], av = alpha[jdof - 1];
+              const cfl a1 = cmulf(cw, cfl{wv.x, wv.y}), a2 = cmulf(cw, cfl{av.x, av.y});
+              ar = ar + a1.re;
+              ai = ai + a1.im;
+              br = br + a2.re;
+              bi = bi + a2.im;
+            }
+            *r1 = make_float2(ar, ai);
+            *r2 = make_float2(br, bi);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (t < 2 * nvar) {
+    const int v = t >> 1, which = t & 1;
+    const float2 *tv = (which ? t2 : t1) + v * ma.maxrow;
+    const float2 *x = which ? adjlam : nu;
+    float acc = 0.0f;
+    for (int k = 0; k < nnzrow; k++) {
+      const float2 a = tv[k], b = x[icsc[i1 + k] - 1];
+      const float ar = a.x, ai = -a.y;  // CONJG
+      acc = acc - (ar * b.x - ai * b.y);
+    }
+    (which ? p2buf : p1buf)[(size_t)col * nvar + v] = acc;
   }
 }
 
@@ -628,6 +745,32 @@ cudaError_t launch_ref_vforce2(Ctx *c, int lisp, int liss, double omega, double 
   k_ref_vforce2<<<c->rg.nnpinv, kRefThreads, vforce2_smem(), st>>>(
       c->mv, c->dt, va, c->d_lm, c->d_rg_anchor, c->d_mconn, c->d_jcsc, c->d_icsc,
       (const float2 *)wave, (float2 *)fmat, c->d_err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ref_met225(Ctx *c, int lisp, int liss, double omega, double py,
+                              const float *adjlam, const float *nu, const float *alpha,
+                              const float *wave, int accumulate, float *p1buf, float *p2buf,
+                              cudaStream_t st) {
+  MetArgs ma;
+  ma.omega = omega;
+  ma.py = py;
+  ma.lisp = lisp;
+  ma.liss = liss;
+  ma.ncon = c->rg.ncon;
+  ma.nnpg = c->nnpg;
+  ma.accumulate = accumulate;
+  ma.maxrow = 1;
+  for (int k = 0; k < c->rg.nnpinv; k++)
+    ma.maxrow = std::max(ma.maxrow, c->rg.jcsc[k + 1] - c->rg.jcsc[k]);
+  const size_t smem = vforce2_smem() + sizeof(float2) * 4 * (size_t)ma.maxrow;
+  cudaError_t e = cudaFuncSetAttribute(k_ref_met225, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e) return e;
+  k_ref_met225<<<c->rg.nnpinv, kRefThreads, smem, st>>>(
+      c->mv, c->dt, ma, c->d_lm, c->d_rg_anchor, c->d_mconn, c->d_elem_wts, c->d_jcsc, c->d_icsc,
+      (const float2 *)adjlam, (const float2 *)nu, (const float2 *)alpha, (const float2 *)wave,
+      p1buf, p2buf, c->d_err);
   return cudaGetLastError();
 }
 

@@ -67,6 +67,8 @@ def lib():
         L.fem25_ref_gradient_dev.argtypes = [vp, C.c_char_p, d, d, d, vp, vp, i, vp, vp]
         L.fem25_ref_gradient_info.argtypes = [vp, C.POINTER(i), C.POINTER(ll), vp]
         L.fem25_ref_vforce2_dev.argtypes = [vp, C.c_char_p, d, d, vp, vp, vp]
+        L.fem25_ref_met225_dev.argtypes = [vp, C.c_char_p, C.c_double, C.c_double, vp, vp, vp, vp,
+                                           i, vp, vp, vp]
         L.fem25_misfit_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp, vp]
         L.fem25_misfit_noalloc_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp,
                                                vp]
@@ -277,6 +279,14 @@ class Context:
         self._check(lib().fem25_ref_gradient_dev(self.h, cinvtype.encode(), vpvs, freq, py,
                                                  _ptr(wave), _ptr(adjlam), 1 if accumulate else 0,
                                                  _ptr(gradl), _stream(stream)))
+
+    def met225(self, cinvtype, freq, py, adjlam, nu, alpha, wave, p1buf, p2buf,
+               accumulate=False, stream=None):
+        """MET225_MOD Hessian-vector buffers (REAL*4 [nnpinv * nvinv] each)."""
+        self._check(lib().fem25_ref_met225_dev(self.h, cinvtype.encode(), freq, py, _ptr(adjlam),
+                                               _ptr(nu), _ptr(alpha), _ptr(wave),
+                                               1 if accumulate else 0, _ptr(p1buf), _ptr(p2buf),
+                                               _stream(stream)))
 
     def vforce2(self, cinvtype, freq, py, wave, fmat, stream=None):
         """VFORCE25_2 / DABMKISOB25 virtual forces into fmat (COMPLEX*8 [nvinv][nz])."""

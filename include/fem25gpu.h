@@ -181,6 +181,22 @@ int fem25_ref_gradient_info(fem25_ctx *ctx, int *nnpinv, long long *nz_fdist,
 int fem25_ref_vforce2_dev(fem25_ctx *ctx, const char *cinvtype, double freq, double py,
                           const float *wave, float *fmat, void *stream);
 
+/* Drop-in for MET225_MOD (qpmfree.f90:1000-1250), the Hessian-vector terms
+ * of the reference's truncated-Newton inner loop (QPMFREE): for every
+ * inversion anchor, with the DABMKISOB25 alpha / beta derivative matrices of
+ * its connected elements weighted by ELEM_WTS,
+ *   P1BUF(ia) = -sum_rows REAL(CONJG(T1) * NU),  T1 = sum_e w_e dS_e WAVE
+ *   P2BUF(ia) = -sum_rows REAL(CONJG(T2) * ADJLAM), T2 = sum_e w_e dS_e ALPHA
+ * in COMPLEX*8 / REAL*4, ia = (inpinv - 1) * nvinv + ivinv (alpha first for
+ * 'PS').  As in the reference the T columns are nulled inside the element
+ * loop, so only the last connected element contributes (accumulate = 0);
+ * accumulate = 1 sums every element.  adjlam, nu, alpha, wave: COMPLEX*8
+ * [NDOF]; p1buf, p2buf: REAL*4 [nnpinv * nvinv] (overwritten); device. */
+int fem25_ref_met225_dev(fem25_ctx *ctx, const char *cinvtype, double freq, double py,
+                         const float *adjlam, const float *nu, const float *alpha,
+                         const float *wave, int accumulate, float *p1buf, float *p2buf,
+                         void *stream);
+
 /* ---- forward misfit + adjoint source ---------------------------------------
  * EXRESP25D (locrec2d.f:867-925) + rotation + CRESID/BPRESID4 L2 + COBJ4 +
  * RESID_DRHS (adjgrad.f90:448-523) for nsrc solutions at once.

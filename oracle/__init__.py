@@ -78,6 +78,8 @@ def _setup(L):
     L.orc_dabm_element.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_double, vp, vp, vp, vp]
     L.orc_vforce2.argtypes = [vp, vp, vp, vp, C.c_int, vp, vp, C.c_longlong, C.c_int, C.c_int,
                               C.c_double, C.c_double, vp, vp]
+    L.orc_met225.argtypes = [vp, vp, vp, vp, C.c_int, vp, vp, vp, C.c_int, C.c_int, C.c_double,
+                             C.c_double, vp, vp, vp, vp, C.c_int, vp, vp]
     L.orc_misfit.argtypes = [C.c_int, C.c_int, vp, vp, C.c_double, C.c_double, C.c_double,
                              vp, vp, vp, vp, vp, vp]
     L.orc_misfit.restype = C.c_float
@@ -290,6 +292,23 @@ class RefGrad:
         if ierr:
             raise RuntimeError(f"oracle vforce2 ierr={ierr}")
         return out
+
+    def met225(self, freq, py, adjlam64, nu64, alpha64, wave64, cinvtype="PP",
+               accumulate=False):
+        """MET225_MOD: (P1BUF, P2BUF) REAL*4 [nnpinv * nvinv] (alpha before beta)."""
+        lisp = cinvtype.upper() in ("PP", "PS")
+        liss = cinvtype.upper() in ("SS", "PS")
+        nv = int(lisp) + int(liss)
+        p1 = np.zeros(self.nnpinv * nv, np.float32)
+        p2 = np.zeros(self.nnpinv * nv, np.float32)
+        c64 = lambda x: _p(np.ascontiguousarray(x, np.complex64))
+        ierr = lib().orc_met225(self.om.ptr, _p(self.g.lm), _p(self.maskg), _p(self.mconn),
+                                self.ncon, _p(self.elem_wts), _p(self.jcsc), _p(self.icsc),
+                                int(lisp), int(liss), freq, py, c64(adjlam64), c64(nu64),
+                                c64(alpha64), c64(wave64), 1 if accumulate else 0, _p(p1), _p(p2))
+        if ierr:
+            raise RuntimeError(f"oracle met225 ierr={ierr}")
+        return p1, p2
 
     def adjflam(self, fmat, adjlam64, gradl=None):
         if gradl is None:

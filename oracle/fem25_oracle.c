@@ -2029,6 +2029,111 @@ int orc_vforce2(const orc_mesh *m, const int *lm, const int *maskg, const int *m
     return ierr;
 }
 
+/*
+ * MET225_MOD (qpmfree.f90:1000-1250), one process: the Hessian-vector terms
+ * of the Gauss-Newton / second-order adjoint inner loop.  For every
+ * inversion anchor (MASKG order) and its connected elements (MCONN order),
+ * with the DJACAB + DABMKISOB25 matrices C_v = CMPLX(DCMPLX(DMD_v,0) + DKD_v)
+ * and CWGHT = CMPLX(SNGL(ELEM_WTS(e)), 0):
+ *     T1_v(row) += (CWGHT * C_v(row, col)) * WAVE(col)
+ *     T2_v(row) += (CWGHT * C_v(row, col)) * ALPHA(col)
+ * in COMPLEX*8.  T1, T2 are nulled inside the element loop
+ * (qpmfree.f90:1149-1156), so only the last connected element survives;
+ * accumulate = 1 keeps every element.  Then, over the anchor's CSC rows in
+ * order, PBUF1(ia35) -= REAL(CONJG(T1_v) * NU), PBUF2(ia35) -=
+ * REAL(CONJG(T2_v) * ADJLAM) (qpmfree.f90:1223-1226), ia35 =
+ * (inpinv - 1) * nvinv + ivinv, alpha before beta.  The MPI_REDUCE of the
+ * buffers is a copy here.  p1buf, p2buf: REAL*4 [nnpinv * nvinv],
+ * overwritten.  Vectors: COMPLEX*8 [ndof].
+ */
+int orc_met225(const orc_mesh *m, const int *lm, const int *maskg, const int *mconn, int ncon,
+               const double *elem_wts, const int *jcsc, const int *icsc, int lisp, int liss,
+               double freq, double py, const float *adjlam, const float *nu, const float *alpha,
+               const float *wave, int accumulate, float *p1buf, float *p2buf)
+{
+    const double TWOPI = 6.2831853071795862;
+    double omega = TWOPI * freq;
+    orc_ws w;
+    ws_init(&w, m->nord);
+    int nen = w.nen, nee = w.nee, nq = w.nq, nint = w.nint, nvinv = lisp + liss;
+    const double *wts = w.xigll + nint;
+    double *dab1 = (double *)malloc(sizeof(double) * nq), *dab2 = (double *)malloc(sizeof(double) * nq);
+    double *dmdb = (double *)malloc(sizeof(double) * nee * nee);
+    zc *dkdb = (zc *)malloc(sizeof(zc) * nee * nee);
+    int maxrow = 0, nnpinv = 0;
+    for (int p = 0; p < m->nnpg; p++)
+        if (maskg[p] > 0) nnpinv++;
+    for (int k = 0; k < nnpinv; k++)
+        if (jcsc[k + 1] - jcsc[k] > maxrow) maxrow = jcsc[k + 1] - jcsc[k];
+    cc *t1 = (cc *)malloc(sizeof(cc) * 2 * (maxrow + 1)), *t2 = (cc *)malloc(sizeof(cc) * 2 * (maxrow + 1));
+    for (int k = 0; k < nnpinv * nvinv; k++) p1buf[k] = p2buf[k] = 0.0f;
+    int ierr = 0, inpgl = 0;
+    for (int p = 0; p < m->nnpg && !ierr; p++) {
+        if (maskg[p] <= 0) continue;
+        inpgl++;
+        const int inpinv = maskg[p];
+        int i1 = jcsc[inpgl - 1], i2 = jcsc[inpgl] - 1, nnzrow = i2 - i1 + 1;
+        for (int k = 0; k < 2 * maxrow; k++) t1[k] = t2[k] = cmk(0.0f, 0.0f);
+        for (int ic = 0; ic < ncon; ic++) {
+            int e = mconn[p + (size_t)m->nnpg * ic];
+            if (e <= 0) break;
+            ierr = djacab(m, e - 1, p + 1, nen, nint, w.xigll, w.shl, w.det, dab1, dab2, w.shg);
+            if (ierr) break;
+            dabmkisob25(nen, nint, lisp, liss, omega, py, wts, w.det, dab1, dab2, w.shg, w.me, dmdb,
+                        w.ke, dkdb);
+            if (!accumulate)
+                for (int k = 0; k < 2 * maxrow; k++) t1[k] = t2[k] = cmk(0.0f, 0.0f);
+            cc cwght = cmk((float)elem_wts[e - 1], 0.0f);
+            const int *lme = lm + (size_t)3 * nen * (e - 1);
+            for (int ipe = 0; ipe < nee; ipe++) {
+                int idof = lme[ipe];
+                if (idof <= 0) continue;
+                int inz = ibsect(nnzrow, idof, icsc + (i1 - 1));
+                if (inz <= 0 || inz > nnzrow) { ierr = 3; break; }
+                for (int iqe = 0; iqe < nee; iqe++) {
+                    int jdof = lme[iqe];
+                    if (jdof <= 0) continue;
+                    cc wv = cmk(wave[2 * (jdof - 1)], wave[2 * (jdof - 1) + 1]);
+                    cc av = cmk(alpha[2 * (jdof - 1)], alpha[2 * (jdof - 1) + 1]);
+                    int v = 0;
+                    for (int var = 0; var < 2; var++) {
+                        if ((var == 0 && !lisp) || (var == 1 && !liss)) continue;
+                        const double *dm = var == 0 ? w.me : dmdb;
+                        const zc *dk = var == 0 ? w.ke : dkdb;
+                        double ar = dm[ipe + nee * iqe] + dk[ipe + nee * iqe].re;
+                        double ai = 0.0 + dk[ipe + nee * iqe].im;
+                        cc cw = cmulf(cwght, cmk((float)ar, (float)ai));
+                        cc a1 = cmulf(cw, wv), a2 = cmulf(cw, av);
+                        cc *r1 = &t1[v * maxrow + inz - 1], *r2 = &t2[v * maxrow + inz - 1];
+                        r1->re = r1->re + a1.re;
+                        r1->im = r1->im + a1.im;
+                        r2->re = r2->re + a2.re;
+                        r2->im = r2->im + a2.im;
+                        v++;
+                    }
+                }
+            }
+            if (ierr) break;
+        }
+        if (ierr) break;
+        for (int v = 0; v < nvinv; v++) {
+            const int ia35 = (inpinv - 1) * nvinv + v;
+            for (int k = 0; k < nnzrow; k++) {
+                const int idof = icsc[i1 - 1 + k];
+                const cc a = t1[v * maxrow + k], b = t2[v * maxrow + k];
+                const float nr = nu[2 * (idof - 1)], ni = nu[2 * (idof - 1) + 1];
+                const float lr = adjlam[2 * (idof - 1)], li = adjlam[2 * (idof - 1) + 1];
+                const float ar = a.re, ai = -a.im, br = b.re, bi = -b.im; /* CONJG */
+                p1buf[ia35] = p1buf[ia35] - (ar * nr - ai * ni);
+                p2buf[ia35] = p2buf[ia35] - (br * lr - bi * li);
+            }
+        }
+    }
+    free(dab1); free(dab2); free(dmdb); free(dkdb); free(t1); free(t2);
+    ws_free(&w);
+    return ierr;
+}
+
 /* ADJFLAM_DIST (adjgrad.f90:88-145) followed by GRADL = GRADL - GPROD
  * (adjgrad.f90:76); REAL*4 arithmetic. gradl: [nnpinv], adjlam: COMPLEX*8 */
 void orc_adjflam(int nnpinv, const int *jcsc, const int *icsc, const float *fmat,

@@ -311,6 +311,27 @@ def test_vforce2_matches_oracle(case0, cinv):
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
 
 
+@pytest.mark.parametrize("cinv,accumulate", [("PP", False), ("SS", False), ("PS", False),
+                                             ("PS", True)])
+def test_met225_matches_oracle(case0, cinv, accumulate):
+    """MET225_MOD Hessian-vector buffers: every REAL*4 value bit-identical to
+    the oracle, twice in a row (the buffers are overwritten, not added to)."""
+    mesh, pairs, g, ctx = case0
+    rg = oracle.RefGrad(mesh, g)
+    rng = np.random.default_rng(23)
+    vec = [(rng.standard_normal(g.ndof) + 1j * rng.standard_normal(g.ndof)).astype(np.complex64)
+           for _ in range(4)]
+    f, py = pairs[6]
+    r1, r2 = rg.met225(f, py, *vec, cinvtype=cinv, accumulate=accumulate)
+    d = [torch.from_numpy(v).to(_dev()) for v in vec]
+    p1 = torch.full(r1.shape, float("nan"), dtype=torch.float32, device=_dev())
+    p2 = torch.full(r2.shape, float("nan"), dtype=torch.float32, device=_dev())
+    for _ in range(2):
+        ctx.met225(cinv, f, py, *d, p1, p2, accumulate=accumulate)
+        assert np.array_equal(p1.cpu().numpy().view(np.uint32), r1.view(np.uint32))
+        assert np.array_equal(p2.cpu().numpy().view(np.uint32), r2.view(np.uint32))
+
+
 def test_reference_gradient_rejects_ps(case0):
     mesh, pairs, g, ctx = case0
     d = torch.zeros(g.ndof, dtype=torch.complex64, device=_dev())

@@ -275,3 +275,55 @@ def test_addblk_touches_only_exterior_dofs(small_case):
     assert ext.any() and (~ext).any()
     assert np.array_equal(out[~ext], sol[~ext])
     assert np.array_equal(out[ext], (sol + ue)[ext])
+
+
+@pytest.mark.parametrize("accumulate", [False, True])
+def test_met225_matches_numpy_restatement(small_case, accumulate):
+    """MET225_MOD's FP32 Hessian-vector buffers against an FP64 numpy
+    evaluation of the same sums built from the oracle's DABMKISOB25 element
+    matrices (weights ELEM_WTS, CONJG dot products, only the last connected
+    element unless accumulate)."""
+    mesh, pairs = small_case
+    g = oracle.graph_build(mesh)
+    rg = oracle.RefGrad(mesh, g)
+    f, py = pairs[1]
+    rng = np.random.default_rng(21)
+    vec = [(rng.standard_normal(g.ndof) + 1j * rng.standard_normal(g.ndof)).astype(np.complex64)
+           for _ in range(4)]
+    adjlam, nu, alpha, wave = vec
+    p1, p2 = rg.met225(f, py, adjlam, nu, alpha, wave, cinvtype="PS", accumulate=accumulate)
+    lm = g.lm.reshape(mesh.nelem, -1)
+    r1 = np.zeros_like(p1, dtype=np.float64)
+    r2 = np.zeros_like(r1)
+    col = 0
+    for p in range(mesh.nnpg):
+        if rg.maskg[p] <= 0:
+            continue
+        rows = rg.icsc[rg.jcsc[col] - 1:rg.jcsc[col + 1] - 1]
+        pos = {int(d): k for k, d in enumerate(rows)}
+        t1 = np.zeros((2, len(rows)), np.complex128)
+        t2 = np.zeros_like(t1)
+        for ic in range(rg.ncon):
+            e = rg.mconn[ic, p]
+            if e <= 0:
+                break
+            if not accumulate:
+                t1[:] = 0
+                t2[:] = 0
+            dmda, dkda, dmdb, dkdb = oracle.dabm_element(mesh, e - 1, p + 1, f, py)
+            dofs = lm[e - 1]
+            ok = dofs > 0
+            w = float(np.float32(rg.elem_wts[e - 1]))
+            for v, cm in enumerate((dmda + dkda, dmdb + dkdb)):
+                sub = cm[np.ix_(ok, ok)]
+                idx = [pos[int(d)] for d in dofs[ok]]
+                t1[v, idx] += w * sub @ wave.astype(np.complex128)[dofs[ok] - 1]
+                t2[v, idx] += w * sub @ alpha.astype(np.complex128)[dofs[ok] - 1]
+        for v in range(2):
+            ia = (rg.maskg[p] - 1) * 2 + v
+            r1[ia] = -np.real(np.sum(np.conj(t1[v]) * nu[rows - 1]))
+            r2[ia] = -np.real(np.sum(np.conj(t2[v]) * adjlam[rows - 1]))
+        col += 1
+    assert col == rg.nnpinv
+    for got, ref in ((p1, r1), (p2, r2)):
+        assert np.max(np.abs(got - ref)) <= 2e-4 * np.max(np.abs(ref))
