@@ -93,7 +93,8 @@ void free_ctx(Ctx *c) {
                   c->d_brptr, c->d_brow, c->d_basis, c->d_ebasis, c->d_bgptr, c->d_bglist,
                   c->d_pml_elems, c->d_pml_idx, c->d_pgptr, c->d_pglist, c->d_pml_emat,
                   c->d_pml_delta, c->d_jcsc, c->d_icsc, c->d_rg_anchor, c->d_mconn,
-                  c->d_elem_wts, c->d_fmat, c->d_nonpml, c->d_cdist, c->d_prim, c->d_desc,
+                  c->d_elem_wts, c->d_fmat, c->d_cadj_col0, c->d_cadj_pair_col, c->d_cadj_pair_elem,
+                  c->d_cadj_dptr, c->d_cadj_dent, c->d_cadj_w, c->d_nonpml, c->d_cdist, c->d_prim, c->d_desc,
                   c->d_tc_tab, c->d_qp, c->d_qs};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -660,6 +661,30 @@ int fem25_ref_met225_dev(fem25_ctx *h, const char *cinvtype, double freq, double
   CK(launch_ref_met225(c, lisp, liss, 6.2831853071795862 * freq, py, adjlam, nu, alpha, wave,
                        accumulate ? 1 : 0, p1buf, p2buf, (cudaStream_t)stream),
      "met225");
+  return FEM25_OK;
+}
+
+int fem25_ref_cadj_nu_alpha_dev(fem25_ctx *h, const char *cinvtype, double freq, double py,
+                                const float *v, const float *adjlam, const float *wave,
+                                int accumulate, float *rhsbnu, float *rhsalp, float *p3,
+                                void *stream) {
+  if (!h || !cinvtype || !v || !adjlam || !wave || !rhsbnu || !rhsalp || !p3)
+    return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  std::string ct(cinvtype, cinvtype + 2);
+  int lisp = 0, liss = 0;
+  if (ct == "PP" || ct == "pp") lisp = 1;
+  else if (ct == "SS" || ct == "ss") liss = 1;
+  else if (ct == "PS" || ct == "ps") lisp = liss = 1;
+  else return fail(c, FEM25_ERR_UNSUPPORTED, "cadj_nu_alpha2: Error anisotropy not programmed!");
+  CK(cudaSetDevice(c->device), "set device");
+  int r = ensure_refgrad(c);
+  if (r) return r;
+  std::string msg;
+  if ((r = prepare_cadj(c, &msg))) return fail(c, r, msg);
+  CK(launch_ref_cadj(c, lisp, liss, 6.2831853071795862 * freq, py, v, adjlam, wave,
+                     accumulate ? 1 : 0, rhsbnu, rhsalp, p3, (cudaStream_t)stream),
+     "cadj_nu_alpha");
   return FEM25_OK;
 }
 

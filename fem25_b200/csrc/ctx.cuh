@@ -110,6 +110,14 @@ struct Ctx {
   int *d_jcsc = nullptr, *d_icsc = nullptr, *d_rg_anchor = nullptr, *d_mconn = nullptr;
   double *d_elem_wts = nullptr;
   float2 *d_fmat = nullptr;
+  // CADJ_NU_ALPHA: (anchor column, connected element) pairs in the reference's
+  // loop order, each DOF's (pair, local DOF) list, and the weighted blocks
+  int cadj_npairs = -1;
+  int *d_cadj_col0 = nullptr;  // [nnpinv + 1] first pair of each column
+  int *d_cadj_pair_col = nullptr, *d_cadj_pair_elem = nullptr;
+  int *d_cadj_dptr = nullptr, *d_cadj_dent = nullptr;
+  float2 *d_cadj_w = nullptr;
+  size_t cadj_w_cap = 0;
   // gradient
   int *d_nonpml = nullptr;       // ids of the elements outside the PML
   int n_nonpml = 0;
@@ -154,6 +162,10 @@ cudaError_t launch_grad_tc(Ctx *c, const PairTable &pt, int npairs, int nsrc, co
 cudaError_t launch_ref_cfmat(Ctx *c, int lisp, double vpvs, double omega, double py,
                              const float *wave, int accumulate, cudaStream_t st);
 cudaError_t launch_ref_adjflam(Ctx *c, const float *adjlam, float *gradl, cudaStream_t st);
+int prepare_cadj(Ctx *c, std::string *msg);
+cudaError_t launch_ref_cadj(Ctx *c, int lisp, int liss, double omega, double py, const float *v,
+                            const float *adjlam, const float *wave, int accumulate, float *rhsbnu,
+                            float *rhsalp, float *p3, cudaStream_t st);
 cudaError_t launch_ref_met225(Ctx *c, int lisp, int liss, double omega, double py,
                               const float *adjlam, const float *nu, const float *alpha,
                               const float *wave, int accumulate, float *p1buf, float *p2buf,

@@ -687,6 +687,152 @@ __global__ void __launch_bounds__(kRefThreads, 1)
   }
 }
 
+// CADJ_NU_ALPHA (qpmfree.f90:622-996) without its solves, in three passes so
+// that every FP32 sum runs in the reference's order:
+//  1. one CTA per (anchor column, connected element) pair: the DABMKISOB25
+//     blocks (the first-derivative blocks of DABM2KISOB25 are the same
+//     arithmetic) times CWGHT = CMPLX(SNGL(ELEM_WTS) * V(ia35), 0), stored as
+//     W[pair][v][75][75];
+//  2. one thread per DOF d walks d's (pair, local index l) list in pair order:
+//     RHSALP(d) += W_v(l, iqe) * WAVE(JDOF) over iqe, v, and
+//     RHSBNU(d) += ADJLAM(IDOF) * CONJG(W_v(ipe, l)) over ipe, v;
+//  3. one CTA per column: TEMP_v(row) += W_v(ipe, iqe) * WAVE(JDOF) over the
+//     column's elements (nulled per element unless accumulate), then
+//     P3(ia35) -= REAL(CONJG(TEMP_v) * ADJLAM) over the column's rows.
+struct CadjArgs {
+  double omega, py;
+  int lisp, liss, nnpg, maxrow, accumulate, ndof;
+};
+
+__global__ void __launch_bounds__(kRefThreads, 1)
+    k_ref_cadj_w(MeshView mv, DevTables dt, CadjArgs ca, const int *__restrict__ anchor_of_col,
+                 const int *__restrict__ pair_col, const int *__restrict__ pair_elem,
+                 const double *__restrict__ elem_wts, const float *__restrict__ v,
+                 float2 *__restrict__ wout, int *__restrict__ err) {
+  extern __shared__ double sm[];
+  float2 *carg0 = reinterpret_cast<float2 *>(sm + 3 * kNq * kNen + 8 * kNq);
+  float2 *carg1 = carg0 + kNee * kNee;
+  const int k = blockIdx.x, col = pair_col[k], e = pair_elem[k];
+  const int p = anchor_of_col[col];
+  const int nvar = ca.lisp + ca.liss;
+  const double wpy = ca.omega * ca.py, wpy2 = ipow2(ca.omega * ca.py);
+  dabm_carg(mv, dt, e, p, wpy, wpy2, ca.lisp, ca.liss, sm, carg0, carg1, err);
+  const float swt = __double2float_rn(elem_wts[e]);
+  for (int var = 0; var < nvar; var++) {
+    const cfl cwght{swt * v[(size_t)col * nvar + var], 0.0f};
+    const float2 *cg = var == 0 ? carg0 : carg1;
+    float2 *wo = wout + ((size_t)k * nvar + var) * kNee * kNee;
+    for (int i = threadIdx.x; i < kNee * kNee; i += kRefThreads) {
+      const cfl w = cmulf(cwght, cfl{cg[i].x, cg[i].y});
+      wo[i] = make_float2(w.re, w.im);
+    }
+  }
+}
+
+__global__ void k_ref_cadj_rhs(CadjArgs ca, const int *__restrict__ lm,
+                               const int *__restrict__ pair_elem, const int *__restrict__ dptr,
+                               const int *__restrict__ dent, const float2 *__restrict__ w,
+                               const float2 *__restrict__ adjlam, const float2 *__restrict__ wave,
+                               float2 *__restrict__ rhsbnu, float2 *__restrict__ rhsalp) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= ca.ndof) return;
+  const int nvar = ca.lisp + ca.liss;
+  float br = 0.0f, bi = 0.0f, ar = 0.0f, ai = 0.0f;
+  for (int j = dptr[d]; j < dptr[d + 1]; j++) {
+    const int k = dent[j] >> 7, l = dent[j] & 127;
+    const int *lme = lm + (size_t)pair_elem[k] * kNee;
+    const float2 *wk = w + (size_t)k * nvar * kNee * kNee;
+    // RHSALP(d): row l of each variable's block
+    for (int iqe = 0; iqe < kNee; iqe++) {
+      const int jdof = lme[iqe];
+      if (jdof <= 0) continue;
+      const float2 x = wave[jdof - 1];
+      for (int var = 0; var < nvar; var++) {
+        const float2 c = wk[(size_t)var * kNee * kNee + l * kNee + iqe];
+        const cfl t = cmulf(cfl{c.x, c.y}, cfl{x.x, x.y});
+        ar = ar + t.re;
+        ai = ai + t.im;
+      }
+    }
+    // RHSBNU(d): column l of each variable's block
+    for (int ipe = 0; ipe < kNee; ipe++) {
+      const int idof = lme[ipe];
+      if (idof <= 0) continue;
+      const float2 x = adjlam[idof - 1];
+      for (int var = 0; var < nvar; var++) {
+        const float2 c = wk[(size_t)var * kNee * kNee + ipe * kNee + l];
+        const cfl t = cmulf(cfl{x.x, x.y}, cfl{c.x, -c.y});
+        br = br + t.re;
+        bi = bi + t.im;
+      }
+    }
+  }
+  rhsalp[d] = make_float2(ar, ai);
+  rhsbnu[d] = make_float2(br, bi);
+}
+
+__global__ void __launch_bounds__(128)
+    k_ref_cadj_p3(CadjArgs ca, const int *__restrict__ lm, const int *__restrict__ col_pair0,
+                  const int *__restrict__ pair_elem, const int *__restrict__ jcsc,
+                  const int *__restrict__ icsc, const float2 *__restrict__ w,
+                  const float2 *__restrict__ adjlam, const float2 *__restrict__ wave,
+                  float *__restrict__ p3, int *__restrict__ err) {
+  extern __shared__ float2 temp[];  // [2][maxrow]
+  const int col = blockIdx.x, t = threadIdx.x;
+  const int i1 = jcsc[col] - 1, i2 = jcsc[col + 1] - 1, nnzrow = i2 - i1;
+  const int nvar = ca.lisp + ca.liss;
+  for (int k = t; k < 2 * ca.maxrow; k += blockDim.x) temp[k] = make_float2(0.0f, 0.0f);
+  __syncthreads();
+  for (int k = col_pair0[col]; k < col_pair0[col + 1]; k++) {
+    if (!ca.accumulate) {
+      for (int i = t; i < 2 * ca.maxrow; i += blockDim.x) temp[i] = make_float2(0.0f, 0.0f);
+      __syncthreads();
+    }
+    const int *lme = lm + (size_t)pair_elem[k] * kNee;
+    if (t < kNee) {
+      const int idof = lme[t];
+      if (idof > 0) {
+        int lo = 0, hi = nnzrow - 1, inz = -1;
+        while (lo <= hi) {
+          int mid = (lo + hi) >> 1, v = icsc[i1 + mid];
+          if (v == idof) { inz = mid; break; }
+          if (v < idof) lo = mid + 1;
+          else hi = mid - 1;
+        }
+        if (inz < 0) {
+          atomicCAS(err, 0, -(col + 1));
+        } else {
+          for (int var = 0; var < nvar; var++) {
+            const float2 *wr = w + ((size_t)k * nvar + var) * kNee * kNee + (size_t)t * kNee;
+            float2 *r = temp + var * ca.maxrow + inz;
+            float xr = r->x, xi = r->y;
+            for (int iqe = 0; iqe < kNee; iqe++) {
+              const int jdof = lme[iqe];
+              if (jdof <= 0) continue;
+              const float2 c = wr[iqe], x = wave[jdof - 1];
+              const cfl s = cmulf(cfl{c.x, c.y}, cfl{x.x, x.y});
+              xr = xr + s.re;
+              xi = xi + s.im;
+            }
+            *r = make_float2(xr, xi);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (t < nvar) {
+    const float2 *tv = temp + t * ca.maxrow;
+    float acc = 0.0f;
+    for (int k = 0; k < nnzrow; k++) {
+      const float2 a = tv[k], b = adjlam[icsc[i1 + k] - 1];
+      const float xr = a.x, xi = -a.y;  // CONJG
+      acc = acc - (xr * b.x - xi * b.y);
+    }
+    p3[(size_t)col * nvar + t] = acc;
+  }
+}
+
 // ADJFLAM_DIST (adjgrad.f90:128-139) + SAXPY(-1) into GRADL (adjgrad.f90:76)
 __global__ void k_ref_adjflam(int ncol, const int *__restrict__ jcsc, const int *__restrict__ icsc,
                               const float2 *__restrict__ fmat, const float2 *__restrict__ lam,
@@ -771,6 +917,99 @@ cudaError_t launch_ref_met225(Ctx *c, int lisp, int liss, double omega, double p
       c->mv, c->dt, ma, c->d_lm, c->d_rg_anchor, c->d_mconn, c->d_elem_wts, c->d_jcsc, c->d_icsc,
       (const float2 *)adjlam, (const float2 *)nu, (const float2 *)alpha, (const float2 *)wave,
       p1buf, p2buf, c->d_err);
+  return cudaGetLastError();
+}
+
+// Pair list and per-DOF contribution lists of CADJ_NU_ALPHA (host, once).
+int prepare_cadj(Ctx *c, std::string *msg) {
+  if (c->cadj_npairs >= 0) return 0;
+  const RefGradSetup &rg = c->rg;
+  std::vector<int> pcol, pelem, col0(rg.nnpinv + 1, 0);
+  for (int col = 0; col < rg.nnpinv; col++) {
+    col0[col] = (int)pcol.size();
+    const int p = rg.anchor_of_col[col];
+    for (int ic = 0; ic < rg.ncon; ic++) {
+      const int e1 = rg.mconn[p + (size_t)c->nnpg * ic];
+      if (e1 <= 0) break;
+      pcol.push_back(col);
+      pelem.push_back(e1 - 1);
+    }
+  }
+  const int np = (int)pcol.size();
+  col0[rg.nnpinv] = np;
+  if ((long long)np >= (1LL << 24)) {
+    *msg = "cadj_nu_alpha: more than 2^24 (anchor, element) pairs";
+    return FEM25_ERR_UNSUPPORTED;
+  }
+  std::vector<int> cnt(c->ndof + 1, 0);
+  for (int k = 0; k < np; k++)
+    for (int l = 0; l < kNee; l++) {
+      const int d = c->h_lm[(size_t)pelem[k] * kNee + l];
+      if (d > 0) cnt[d - 1 + 1]++;
+    }
+  for (int d = 0; d < c->ndof; d++) cnt[d + 1] += cnt[d];
+  std::vector<int> ent(cnt[c->ndof]), cur(cnt.begin(), cnt.end() - 1);
+  for (int k = 0; k < np; k++)
+    for (int l = 0; l < kNee; l++) {
+      const int d = c->h_lm[(size_t)pelem[k] * kNee + l];
+      if (d > 0) ent[cur[d - 1]++] = (k << 7) | l;
+    }
+  cudaError_t e = cudaSuccess;
+  auto up = [&](int **dst, const std::vector<int> &src) {
+    if ((e = cudaMalloc(dst, sizeof(int) * std::max<size_t>(1, src.size())))) return false;
+    if (!src.empty() &&
+        (e = cudaMemcpy(*dst, src.data(), sizeof(int) * src.size(), cudaMemcpyHostToDevice)))
+      return false;
+    return true;
+  };
+  if (!up(&c->d_cadj_col0, col0) || !up(&c->d_cadj_pair_col, pcol) ||
+      !up(&c->d_cadj_pair_elem, pelem) || !up(&c->d_cadj_dptr, cnt) ||
+      !up(&c->d_cadj_dent, ent)) {
+    *msg = std::string("cadj_nu_alpha: ") + cudaGetErrorString(e);
+    return FEM25_ERR_ALLOC;
+  }
+  c->cadj_npairs = np;
+  return 0;
+}
+
+cudaError_t launch_ref_cadj(Ctx *c, int lisp, int liss, double omega, double py, const float *v,
+                            const float *adjlam, const float *wave, int accumulate, float *rhsbnu,
+                            float *rhsalp, float *p3, cudaStream_t st) {
+  CadjArgs ca;
+  ca.omega = omega;
+  ca.py = py;
+  ca.lisp = lisp;
+  ca.liss = liss;
+  ca.nnpg = c->nnpg;
+  ca.accumulate = accumulate;
+  ca.ndof = c->ndof;
+  ca.maxrow = 1;
+  for (int k = 0; k < c->rg.nnpinv; k++)
+    ca.maxrow = std::max(ca.maxrow, c->rg.jcsc[k + 1] - c->rg.jcsc[k]);
+  const int nvar = lisp + liss;
+  const size_t wbytes = sizeof(float2) * (size_t)std::max(1, c->cadj_npairs) * nvar * kNee * kNee;
+  cudaError_t e;
+  if (wbytes > c->cadj_w_cap) {
+    if ((e = cudaStreamSynchronize(st))) return e;
+    if (c->d_cadj_w) cudaFree(c->d_cadj_w);
+    c->d_cadj_w = nullptr;
+    c->cadj_w_cap = 0;
+    if ((e = cudaMalloc(&c->d_cadj_w, wbytes))) return e;
+    c->cadj_w_cap = wbytes;
+  }
+  if ((e = cudaFuncSetAttribute(k_ref_cadj_w, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)vforce2_smem())))
+    return e;
+  if (c->cadj_npairs > 0)
+    k_ref_cadj_w<<<c->cadj_npairs, kRefThreads, vforce2_smem(), st>>>(
+        c->mv, c->dt, ca, c->d_rg_anchor, c->d_cadj_pair_col, c->d_cadj_pair_elem, c->d_elem_wts,
+        v, c->d_cadj_w, c->d_err);
+  k_ref_cadj_rhs<<<(c->ndof + 127) / 128, 128, 0, st>>>(
+      ca, c->d_lm, c->d_cadj_pair_elem, c->d_cadj_dptr, c->d_cadj_dent, c->d_cadj_w,
+      (const float2 *)adjlam, (const float2 *)wave, (float2 *)rhsbnu, (float2 *)rhsalp);
+  k_ref_cadj_p3<<<c->rg.nnpinv, 128, sizeof(float2) * 2 * ca.maxrow, st>>>(
+      ca, c->d_lm, c->d_cadj_col0, c->d_cadj_pair_elem, c->d_jcsc, c->d_icsc, c->d_cadj_w,
+      (const float2 *)adjlam, (const float2 *)wave, p3, c->d_err);
   return cudaGetLastError();
 }
 

@@ -69,6 +69,8 @@ def lib():
         L.fem25_ref_vforce2_dev.argtypes = [vp, C.c_char_p, d, d, vp, vp, vp]
         L.fem25_ref_met225_dev.argtypes = [vp, C.c_char_p, C.c_double, C.c_double, vp, vp, vp, vp,
                                            i, vp, vp, vp]
+        L.fem25_ref_cadj_nu_alpha_dev.argtypes = [vp, C.c_char_p, C.c_double, C.c_double, vp,
+                                                  vp, vp, i, vp, vp, vp, vp]
         L.fem25_misfit_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp, vp]
         L.fem25_misfit_noalloc_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp,
                                                vp]
@@ -287,6 +289,14 @@ class Context:
                                                _ptr(nu), _ptr(alpha), _ptr(wave),
                                                1 if accumulate else 0, _ptr(p1buf), _ptr(p2buf),
                                                _stream(stream)))
+
+    def cadj_nu_alpha(self, cinvtype, freq, py, v, adjlam, wave, rhsbnu, rhsalp, p3,
+                      accumulate=False, stream=None):
+        """CADJ_NU_ALPHA right-hand sides and P3 (see fem25_ref_cadj_nu_alpha_dev)."""
+        self._check(lib().fem25_ref_cadj_nu_alpha_dev(self.h, cinvtype.encode(), freq, py, _ptr(v),
+                                                      _ptr(adjlam), _ptr(wave),
+                                                      1 if accumulate else 0, _ptr(rhsbnu),
+                                                      _ptr(rhsalp), _ptr(p3), _stream(stream)))
 
     def vforce2(self, cinvtype, freq, py, wave, fmat, stream=None):
         """VFORCE25_2 / DABMKISOB25 virtual forces into fmat (COMPLEX*8 [nvinv][nz])."""

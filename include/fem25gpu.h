@@ -197,6 +197,27 @@ int fem25_ref_met225_dev(fem25_ctx *ctx, const char *cinvtype, double freq, doub
                          const float *wave, int accumulate, float *p1buf, float *p2buf,
                          void *stream);
 
+/* Drop-in for the kernels of CADJ_NU_ALPHA (qpmfree.f90:622-996), the
+ * second-order adjoint step of the truncated-Newton inner loop, for a model
+ * perturbation v (REAL*4 [nnpinv * nvinv], device): with the DABMKISOB25
+ * alpha / beta blocks of every (inversion anchor, connected element) pair
+ * weighted by CWGHT = SNGL(ELEM_WTS) * V(ia), in COMPLEX*8 and the
+ * reference's summation order,
+ *   rhsbnu(JDOF) = sum ADJLAM(IDOF) * CONJG(CWGHT * dS(IDOF, JDOF))
+ *   rhsalp(IDOF) = sum CWGHT * dS(IDOF, JDOF) * WAVE(JDOF)
+ *   p3(ia)       = -sum_rows REAL(CONJG(TEMP) * ADJLAM)
+ * (TEMP as rhsalp restricted to the anchor's elements; only the last
+ * connected element survives unless accumulate = 1, as in the reference).
+ * The two MUMPS solves stay with the caller: NU = CONJG(S^-T CONJG(rhsbnu)),
+ * ALPHA = S^-1 rhsalp (fem25_dense_solve_dev on small meshes).  The first
+ * call builds the pair lists and a weighted-block workspace of
+ * pairs x nvinv x 75^2 COMPLEX*8 (about 4 pairs per anchor).  adjlam, wave,
+ * rhsbnu, rhsalp: COMPLEX*8 [NDOF] (outputs overwritten); device. */
+int fem25_ref_cadj_nu_alpha_dev(fem25_ctx *ctx, const char *cinvtype, double freq, double py,
+                                const float *v, const float *adjlam, const float *wave,
+                                int accumulate, float *rhsbnu, float *rhsalp, float *p3,
+                                void *stream);
+
 /* ---- forward misfit + adjoint source ---------------------------------------
  * EXRESP25D (locrec2d.f:867-925) + rotation + CRESID/BPRESID4 L2 + COBJ4 +
  * RESID_DRHS (adjgrad.f90:448-523) for nsrc solutions at once.

@@ -78,6 +78,9 @@ def _setup(L):
     L.orc_dabm_element.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_double, vp, vp, vp, vp]
     L.orc_vforce2.argtypes = [vp, vp, vp, vp, C.c_int, vp, vp, C.c_longlong, C.c_int, C.c_int,
                               C.c_double, C.c_double, vp, vp]
+    L.orc_cadj_nu_alpha.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, vp, vp, vp, C.c_int,
+                                    C.c_int, C.c_double, C.c_double, vp, vp, vp, C.c_int, vp,
+                                    vp, vp]
     L.orc_met225.argtypes = [vp, vp, vp, vp, C.c_int, vp, vp, vp, C.c_int, C.c_int, C.c_double,
                              C.c_double, vp, vp, vp, vp, C.c_int, vp, vp]
     L.orc_misfit.argtypes = [C.c_int, C.c_int, vp, vp, C.c_double, C.c_double, C.c_double,
@@ -309,6 +312,25 @@ class RefGrad:
         if ierr:
             raise RuntimeError(f"oracle met225 ierr={ierr}")
         return p1, p2
+
+    def cadj_nu_alpha(self, freq, py, v, adjlam64, wave64, cinvtype="PP", accumulate=False):
+        """CADJ_NU_ALPHA without its solves: (RHSBNU, RHSALP) COMPLEX*8 [ndof] and
+        P3 REAL*4 [nnpinv * nvinv]; v: REAL*4 [nnpinv * nvinv]."""
+        lisp = cinvtype.upper() in ("PP", "PS")
+        liss = cinvtype.upper() in ("SS", "PS")
+        nv = int(lisp) + int(liss)
+        rb = np.zeros(self.g.ndof, np.complex64)
+        ra = np.zeros(self.g.ndof, np.complex64)
+        p3 = np.zeros(self.nnpinv * nv, np.float32)
+        c64 = lambda x: _p(np.ascontiguousarray(x, np.complex64))
+        ierr = lib().orc_cadj_nu_alpha(self.om.ptr, _p(self.g.lm), self.g.ndof, _p(self.maskg),
+                                       _p(self.mconn), self.ncon, _p(self.elem_wts),
+                                       _p(self.jcsc), _p(self.icsc), int(lisp), int(liss), freq,
+                                       py, _p(np.ascontiguousarray(v, np.float32)), c64(adjlam64),
+                                       c64(wave64), 1 if accumulate else 0, _p(rb), _p(ra), _p(p3))
+        if ierr:
+            raise RuntimeError(f"oracle cadj_nu_alpha ierr={ierr}")
+        return rb, ra, p3
 
     def adjflam(self, fmat, adjlam64, gradl=None):
         if gradl is None:

@@ -2134,6 +2134,119 @@ int orc_met225(const orc_mesh *m, const int *lm, const int *maskg, const int *mc
     return ierr;
 }
 
+/*
+ * CADJ_NU_ALPHA (qpmfree.f90:622-996), one process, without its two MUMPS
+ * solves: the right-hand sides of the second-order adjoint (nu) and of the
+ * model-perturbation field (alpha), and the P3 term, for a model
+ * perturbation V(NA35).  Per inversion anchor (MASKG order), connected
+ * element (MCONN order), row IPE (IDOF > 0), column IQE (JDOF > 0) and
+ * variable (alpha before beta), with C_v the DJACAB2 + DABM2KISOB25
+ * first-derivative blocks (the same arithmetic as DABMKISOB25; the
+ * second-derivative blocks it also forms, CARG2, enter none of the sums) and
+ * CWGHT = CMPLX(SNGL(ELEM_WTS(e)) * V(ia35), 0):
+ *     RHSBNU(JDOF) += ADJLAM(IDOF) * CONJG(CWGHT * C_v(IPE, IQE))
+ *     RHSALP(IDOF) += CWGHT * C_v(IPE, IQE) * WAVE(JDOF)
+ *     TEMP_v(row)  += CWGHT * C_v(IPE, IQE) * WAVE(JDOF)
+ * TEMP is nulled inside the element loop (qpmfree.f90:823-829: only the last
+ * connected element survives; accumulate = 1 keeps every element), then
+ * P3(ia35) -= REAL(CONJG(TEMP_v) * ADJLAM) over the anchor's CSC rows.  The
+ * solves that follow are the caller's: NU = CONJG(S^-T CONJG(RHSBNU)),
+ * ALPHA = S^-1 RHSALP.  Vectors COMPLEX*8 [ndof], v and p3 REAL*4
+ * [nnpinv * nvinv]; outputs overwritten.
+ */
+int orc_cadj_nu_alpha(const orc_mesh *m, const int *lm, int ndof, const int *maskg,
+                      const int *mconn, int ncon, const double *elem_wts, const int *jcsc,
+                      const int *icsc, int lisp, int liss, double freq, double py,
+                      const float *v, const float *adjlam, const float *wave, int accumulate,
+                      float *rhsbnu, float *rhsalp, float *p3)
+{
+    const double TWOPI = 6.2831853071795862;
+    double omega = TWOPI * freq;
+    orc_ws w;
+    ws_init(&w, m->nord);
+    int nen = w.nen, nee = w.nee, nq = w.nq, nint = w.nint, nvinv = lisp + liss;
+    const double *wts = w.xigll + nint;
+    double *dab1 = (double *)malloc(sizeof(double) * nq), *dab2 = (double *)malloc(sizeof(double) * nq);
+    double *dmdb = (double *)malloc(sizeof(double) * nee * nee);
+    zc *dkdb = (zc *)malloc(sizeof(zc) * nee * nee);
+    int maxrow = 0, nnpinv = 0;
+    for (int p = 0; p < m->nnpg; p++)
+        if (maskg[p] > 0) nnpinv++;
+    for (int k = 0; k < nnpinv; k++)
+        if (jcsc[k + 1] - jcsc[k] > maxrow) maxrow = jcsc[k + 1] - jcsc[k];
+    cc *temp = (cc *)malloc(sizeof(cc) * 2 * (maxrow + 1));
+    for (int k = 0; k < 2 * ndof; k++) rhsbnu[k] = rhsalp[k] = 0.0f;
+    for (int k = 0; k < nnpinv * nvinv; k++) p3[k] = 0.0f;
+    int ierr = 0, inpgl = 0;
+    for (int p = 0; p < m->nnpg && !ierr; p++) {
+        if (maskg[p] <= 0) continue;
+        inpgl++;
+        const int inpinv = maskg[p];
+        int i1 = jcsc[inpgl - 1], i2 = jcsc[inpgl] - 1, nnzrow = i2 - i1 + 1;
+        for (int k = 0; k < 2 * maxrow; k++) temp[k] = cmk(0.0f, 0.0f);
+        for (int ic = 0; ic < ncon; ic++) {
+            int e = mconn[p + (size_t)m->nnpg * ic];
+            if (e <= 0) break;
+            ierr = djacab(m, e - 1, p + 1, nen, nint, w.xigll, w.shl, w.det, dab1, dab2, w.shg);
+            if (ierr) break;
+            dabmkisob25(nen, nint, lisp, liss, omega, py, wts, w.det, dab1, dab2, w.shg, w.me, dmdb,
+                        w.ke, dkdb);
+            if (!accumulate)
+                for (int k = 0; k < 2 * maxrow; k++) temp[k] = cmk(0.0f, 0.0f);
+            const float swt = (float)elem_wts[e - 1];
+            const int *lme = lm + (size_t)3 * nen * (e - 1);
+            for (int ipe = 0; ipe < nee; ipe++) {
+                int idof = lme[ipe];
+                if (idof <= 0) continue;
+                int inz = ibsect(nnzrow, idof, icsc + (i1 - 1));
+                if (inz <= 0 || inz > nnzrow) { ierr = 3; break; }
+                cc lam = cmk(adjlam[2 * (idof - 1)], adjlam[2 * (idof - 1) + 1]);
+                for (int iqe = 0; iqe < nee; iqe++) {
+                    int jdof = lme[iqe];
+                    if (jdof <= 0) continue;
+                    cc wv = cmk(wave[2 * (jdof - 1)], wave[2 * (jdof - 1) + 1]);
+                    int vv = 0;
+                    for (int var = 0; var < 2; var++) {
+                        if ((var == 0 && !lisp) || (var == 1 && !liss)) continue;
+                        const double *dm = var == 0 ? w.me : dmdb;
+                        const zc *dk = var == 0 ? w.ke : dkdb;
+                        double ar = dm[ipe + nee * iqe] + dk[ipe + nee * iqe].re;
+                        double ai = 0.0 + dk[ipe + nee * iqe].im;
+                        const int ia35 = (inpinv - 1) * nvinv + vv;
+                        cc cwght = cmk(swt * v[ia35], 0.0f);
+                        cc cw = cmulf(cwght, cmk((float)ar, (float)ai));
+                        cc nb = cmulf(lam, cmk(cw.re, -cw.im));
+                        rhsbnu[2 * (jdof - 1)] = rhsbnu[2 * (jdof - 1)] + nb.re;
+                        rhsbnu[2 * (jdof - 1) + 1] = rhsbnu[2 * (jdof - 1) + 1] + nb.im;
+                        cc al = cmulf(cw, wv);
+                        rhsalp[2 * (idof - 1)] = rhsalp[2 * (idof - 1)] + al.re;
+                        rhsalp[2 * (idof - 1) + 1] = rhsalp[2 * (idof - 1) + 1] + al.im;
+                        cc *t = &temp[vv * maxrow + inz - 1];
+                        t->re = t->re + al.re;
+                        t->im = t->im + al.im;
+                        vv++;
+                    }
+                }
+            }
+            if (ierr) break;
+        }
+        if (ierr) break;
+        for (int vv = 0; vv < nvinv; vv++) {
+            const int ia35 = (inpinv - 1) * nvinv + vv;
+            for (int k = 0; k < nnzrow; k++) {
+                const int idof = icsc[i1 - 1 + k];
+                const cc a = temp[vv * maxrow + k];
+                const float lr = adjlam[2 * (idof - 1)], li = adjlam[2 * (idof - 1) + 1];
+                const float ar = a.re, ai = -a.im; /* CONJG */
+                p3[ia35] = p3[ia35] - (ar * lr - ai * li);
+            }
+        }
+    }
+    free(dab1); free(dab2); free(dmdb); free(dkdb); free(temp);
+    ws_free(&w);
+    return ierr;
+}
+
 /* ADJFLAM_DIST (adjgrad.f90:88-145) followed by GRADL = GRADL - GPROD
  * (adjgrad.f90:76); REAL*4 arithmetic. gradl: [nnpinv], adjlam: COMPLEX*8 */
 void orc_adjflam(int nnpinv, const int *jcsc, const int *icsc, const float *fmat,

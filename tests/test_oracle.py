@@ -327,3 +327,55 @@ def test_met225_matches_numpy_restatement(small_case, accumulate):
     assert col == rg.nnpinv
     for got, ref in ((p1, r1), (p2, r2)):
         assert np.max(np.abs(got - ref)) <= 2e-4 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("accumulate", [False, True])
+def test_cadj_nu_alpha_matches_numpy_restatement(small_case, accumulate):
+    """CADJ_NU_ALPHA's FP32 right-hand sides (nu and alpha fields) and P3
+    buffer against an FP64 numpy evaluation from the oracle's DABMKISOB25
+    element matrices: RHSALP = sum w_e V_p C_e WAVE, RHSBNU = sum conj(w_e V_p
+    C_e)^T ADJLAM, P3 from the last connected element unless accumulate."""
+    mesh, pairs = small_case
+    g = oracle.graph_build(mesh)
+    rg = oracle.RefGrad(mesh, g)
+    f, py = pairs[0]
+    rng = np.random.default_rng(31)
+    adjlam, wave = [(rng.standard_normal(g.ndof) + 1j * rng.standard_normal(g.ndof))
+                    .astype(np.complex64) for _ in range(2)]
+    v = rng.standard_normal(2 * rg.nnpinv).astype(np.float32)
+    rb, ra, p3 = rg.cadj_nu_alpha(f, py, v, adjlam, wave, cinvtype="PS", accumulate=accumulate)
+    lm = g.lm.reshape(mesh.nelem, -1)
+    adj64, wave64 = adjlam.astype(np.complex128), wave.astype(np.complex128)
+    ref_b = np.zeros(g.ndof, np.complex128)
+    ref_a = np.zeros(g.ndof, np.complex128)
+    ref_p3 = np.zeros(p3.shape)
+    col = 0
+    for p in range(mesh.nnpg):
+        if rg.maskg[p] <= 0:
+            continue
+        rows = rg.icsc[rg.jcsc[col] - 1:rg.jcsc[col + 1] - 1]
+        pos = {int(d): k for k, d in enumerate(rows)}
+        temp = np.zeros((2, len(rows)), np.complex128)
+        for ic in range(rg.ncon):
+            e = rg.mconn[ic, p]
+            if e <= 0:
+                break
+            if not accumulate:
+                temp[:] = 0
+            dmda, dkda, dmdb, dkdb = oracle.dabm_element(mesh, e - 1, p + 1, f, py)
+            dofs = lm[e - 1]
+            ok = dofs > 0
+            d = dofs[ok] - 1
+            for var, cm in enumerate((dmda + dkda, dmdb + dkdb)):
+                wv = float(np.float32(rg.elem_wts[e - 1])) * float(v[(rg.maskg[p] - 1) * 2 + var])
+                sub = wv * cm[np.ix_(ok, ok)]
+                y = sub @ wave64[d]
+                ref_a[d] += y
+                ref_b[d] += np.conj(sub).T @ adj64[d]
+                temp[var, [pos[int(x)] for x in dofs[ok]]] += y
+        for var in range(2):
+            ref_p3[(rg.maskg[p] - 1) * 2 + var] = -np.real(np.sum(np.conj(temp[var]) *
+                                                                  adj64[rows - 1]))
+        col += 1
+    for got, ref in ((ra, ref_a), (rb, ref_b), (p3, ref_p3)):
+        assert np.max(np.abs(got - ref)) <= 2e-4 * np.max(np.abs(ref))
