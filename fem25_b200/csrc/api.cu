@@ -688,6 +688,20 @@ int fem25_ref_cadj_nu_alpha_dev(fem25_ctx *h, const char *cinvtype, double freq,
   return FEM25_OK;
 }
 
+int fem25_ref_pchadj_dev(fem25_ctx *h, int nvinv, int nrhs, const float *grns,
+                         const float *fmat, float *hessb, float *jacl, void *stream) {
+  if (!h || !grns || !fmat || !hessb || nrhs <= 0 || nvinv < 1 || nvinv > 2)
+    return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  if ((size_t)nrhs * nvinv * 8 > 200 * 1024)
+    return fail(c, FEM25_ERR_UNSUPPORTED, "pchadj: more than 12 800 / nvinv right-hand sides");
+  CK(cudaSetDevice(c->device), "set device");
+  int r = ensure_refgrad(c);
+  if (r) return r;
+  CK(launch_ref_pchadj(c, nvinv, nrhs, grns, fmat, hessb, jacl, (cudaStream_t)stream), "pchadj");
+  return FEM25_OK;
+}
+
 int fem25_ref_vforce2_dev(fem25_ctx *h, const char *cinvtype, double freq, double py,
                           const float *wave, float *fmat, void *stream) {
   if (!h || !cinvtype || !wave || !fmat) return FEM25_ERR_ARG;

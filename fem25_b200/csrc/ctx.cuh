@@ -162,6 +162,8 @@ cudaError_t launch_grad_tc(Ctx *c, const PairTable &pt, int npairs, int nsrc, co
 cudaError_t launch_ref_cfmat(Ctx *c, int lisp, double vpvs, double omega, double py,
                              const float *wave, int accumulate, cudaStream_t st);
 cudaError_t launch_ref_adjflam(Ctx *c, const float *adjlam, float *gradl, cudaStream_t st);
+cudaError_t launch_ref_pchadj(Ctx *c, int nvinv, int nrhs, const float *grns, const float *fmat,
+                              float *hessb, float *jacl, cudaStream_t st);
 int prepare_cadj(Ctx *c, std::string *msg);
 cudaError_t launch_ref_cadj(Ctx *c, int lisp, int liss, double omega, double py, const float *v,
                             const float *adjlam, const float *wave, int accumulate, float *rhsbnu,

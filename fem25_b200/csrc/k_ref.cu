@@ -833,6 +833,54 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// PCHADJ (pchadj.f90:1-330) after the Green's-function solve: one CTA per
+// inversion anchor column.  Threads over (irhs, v) form
+// JACL(irhs, v) = sum_rows G((irhs-1)*NDOF + JDOF) * FMAT(row, v) in row order
+// (pchadj.f90:241-246) into shared memory (and jacl when given); then one
+// thread per (iv, jv) forms REAL(sum_l CONJG(JACL(l, iv)) * JACL(l, jv)) in
+// the reference BLAS order (CGEMM 'C','N', ALPHA = 1) and adds it to HESSB
+// (pchadj.f90:274-300, 312-323).
+__global__ void __launch_bounds__(256)
+    k_ref_pchadj(int nvinv, long long nz, int ndof, int nrhs, const int *__restrict__ jcsc,
+                 const int *__restrict__ icsc, const float2 *__restrict__ grns,
+                 const float2 *__restrict__ fmat, float *__restrict__ hessb,
+                 float2 *__restrict__ jacl) {
+  extern __shared__ float2 jl[];  // [nrhs][nvinv]
+  const int col = blockIdx.x;
+  const int i1 = jcsc[col] - 1, i2 = jcsc[col + 1] - 1;
+  for (int idx = threadIdx.x; idx < nrhs * nvinv; idx += blockDim.x) {
+    const int irhs = idx / nvinv, v = idx % nvinv;
+    const float2 *gr = grns + (size_t)irhs * ndof;
+    const float2 *fv = fmat + (size_t)v * nz;
+    float ar = 0.0f, ai = 0.0f;
+    for (int i = i1; i < i2; i++) {
+      const int jdof = icsc[i];
+      if (jdof == 0) continue;
+      const float2 g = gr[jdof - 1], f = fv[i];
+      const cfl t = cmulf(cfl{g.x, g.y}, cfl{f.x, f.y});
+      ar = ar + t.re;
+      ai = ai + t.im;
+    }
+    jl[idx] = make_float2(ar, ai);
+    if (jacl) jacl[((size_t)col * nvinv + v) * nrhs + irhs] = make_float2(ar, ai);
+  }
+  __syncthreads();
+  if (threadIdx.x < nvinv * nvinv) {
+    const int iv = threadIdx.x / nvinv, jv = threadIdx.x % nvinv;
+    float tr = 0.0f, ti = 0.0f;
+    for (int l = 0; l < nrhs; l++) {
+      const float2 a = jl[l * nvinv + iv], b = jl[l * nvinv + jv];
+      const cfl t = cmulf(cfl{a.x, -a.y}, cfl{b.x, b.y});
+      tr = tr + t.re;
+      ti = ti + t.im;
+    }
+    const cfl h = cmulf(cfl{1.0f, 0.0f}, cfl{tr, ti});
+    const float hb = 0.0f + h.re;
+    float *y = hessb + ((size_t)col * nvinv + iv) * nvinv + jv;
+    *y = *y + 1.0f * hb;
+  }
+}
+
 // ADJFLAM_DIST (adjgrad.f90:128-139) + SAXPY(-1) into GRADL (adjgrad.f90:76)
 __global__ void k_ref_adjflam(int ncol, const int *__restrict__ jcsc, const int *__restrict__ icsc,
                               const float2 *__restrict__ fmat, const float2 *__restrict__ lam,
@@ -1010,6 +1058,18 @@ cudaError_t launch_ref_cadj(Ctx *c, int lisp, int liss, double omega, double py,
   k_ref_cadj_p3<<<c->rg.nnpinv, 128, sizeof(float2) * 2 * ca.maxrow, st>>>(
       ca, c->d_lm, c->d_cadj_col0, c->d_cadj_pair_elem, c->d_jcsc, c->d_icsc, c->d_cadj_w,
       (const float2 *)adjlam, (const float2 *)wave, p3, c->d_err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ref_pchadj(Ctx *c, int nvinv, int nrhs, const float *grns, const float *fmat,
+                              float *hessb, float *jacl, cudaStream_t st) {
+  const size_t smem = sizeof(float2) * (size_t)nrhs * nvinv;
+  cudaError_t e = cudaFuncSetAttribute(k_ref_pchadj, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e) return e;
+  k_ref_pchadj<<<c->rg.nnpinv, 256, smem, st>>>(nvinv, c->rg.nz, c->ndof, nrhs, c->d_jcsc,
+                                                c->d_icsc, (const float2 *)grns,
+                                                (const float2 *)fmat, hessb, (float2 *)jacl);
   return cudaGetLastError();
 }
 

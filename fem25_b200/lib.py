@@ -71,6 +71,7 @@ def lib():
                                            i, vp, vp, vp]
         L.fem25_ref_cadj_nu_alpha_dev.argtypes = [vp, C.c_char_p, C.c_double, C.c_double, vp,
                                                   vp, vp, i, vp, vp, vp, vp]
+        L.fem25_ref_pchadj_dev.argtypes = [vp, i, i, vp, vp, vp, vp, vp]
         L.fem25_misfit_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp, vp]
         L.fem25_misfit_noalloc_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp,
                                                vp]
@@ -297,6 +298,11 @@ class Context:
                                                       _ptr(adjlam), _ptr(wave),
                                                       1 if accumulate else 0, _ptr(rhsbnu),
                                                       _ptr(rhsalp), _ptr(p3), _stream(stream)))
+
+    def pchadj(self, nvinv, nrhs, grns, fmat, hessb, jacl=None, stream=None):
+        """PCHADJ products: HESSB += REAL(JACL^H JACL) in place, JACL optional."""
+        self._check(lib().fem25_ref_pchadj_dev(self.h, nvinv, nrhs, _ptr(grns), _ptr(fmat),
+                                               _ptr(hessb), _ptr(jacl), _stream(stream)))
 
     def vforce2(self, cinvtype, freq, py, wave, fmat, stream=None):
         """VFORCE25_2 / DABMKISOB25 virtual forces into fmat (COMPLEX*8 [nvinv][nz])."""

@@ -218,6 +218,20 @@ int fem25_ref_cadj_nu_alpha_dev(fem25_ctx *ctx, const char *cinvtype, double fre
                                 int accumulate, float *rhsbnu, float *rhsalp, float *p3,
                                 void *stream);
 
+/* Drop-in for the products of PCHADJ (pchadj.f90:1-330) that follow its
+ * Green's-function solve (G^T = S^-T (-A^T) for the nrhs = NDIM x NREC
+ * receiver components, which the caller's solver provides): per inversion
+ * anchor, the Jacobian block JACL(irhs, v) = sum_rows G(irhs, row) F(row, v)
+ * in COMPLEX*8, and the block-diagonal preconditioner update
+ * HESSB += REAL(JACL^H JACL) (CGEMM order of the reference BLAS, then
+ * SAXPY).  grns: COMPLEX*8 [nrhs][NDOF]; fmat: COMPLEX*8 [nvinv][NZ_FDIST]
+ * (the forces of fem25_ref_gradient_dev / _vforce2_dev); hessb: REAL*4
+ * [nnpinv * nvinv^2] updated in place, block (col, iv, jv) at
+ * (col * nvinv + iv) * nvinv + jv; jacl (nullable, the LGNEWT Jacobian):
+ * COMPLEX*8 [nnpinv * nvinv][nrhs].  nrhs * nvinv <= 25 600.  Device. */
+int fem25_ref_pchadj_dev(fem25_ctx *ctx, int nvinv, int nrhs, const float *grns,
+                         const float *fmat, float *hessb, float *jacl, void *stream);
+
 /* ---- forward misfit + adjoint source ---------------------------------------
  * EXRESP25D (locrec2d.f:867-925) + rotation + CRESID/BPRESID4 L2 + COBJ4 +
  * RESID_DRHS (adjgrad.f90:448-523) for nsrc solutions at once.

@@ -81,6 +81,8 @@ def _setup(L):
     L.orc_cadj_nu_alpha.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, vp, vp, vp, C.c_int,
                                     C.c_int, C.c_double, C.c_double, vp, vp, vp, C.c_int, vp,
                                     vp, vp]
+    L.orc_pchadj.argtypes = [C.c_int, C.c_int, C.c_longlong, C.c_int, C.c_int, vp, vp, vp, vp,
+                             vp, vp]
     L.orc_met225.argtypes = [vp, vp, vp, vp, C.c_int, vp, vp, vp, C.c_int, C.c_int, C.c_double,
                              C.c_double, vp, vp, vp, vp, C.c_int, vp, vp]
     L.orc_misfit.argtypes = [C.c_int, C.c_int, vp, vp, C.c_double, C.c_double, C.c_double,
@@ -331,6 +333,18 @@ class RefGrad:
         if ierr:
             raise RuntimeError(f"oracle cadj_nu_alpha ierr={ierr}")
         return rb, ra, p3
+
+    def pchadj(self, grns64, fmat64, hessb, want_jacl=True):
+        """PCHADJ after the Green's-function solve: HESSB updated in place
+        (REAL*4 [nnpinv * nvinv^2]), returns JACL COMPLEX*8 [nnpinv*nvinv, nrhs]."""
+        fm = np.ascontiguousarray(fmat64, np.complex64).reshape(-1, self.nz)
+        nv = fm.shape[0]
+        gr = np.ascontiguousarray(grns64, np.complex64).reshape(-1, self.g.ndof)
+        jacl = np.zeros((self.nnpinv * nv, gr.shape[0]), np.complex64) if want_jacl else None
+        lib().orc_pchadj(self.nnpinv, nv, self.nz, self.g.ndof, gr.shape[0], _p(self.jcsc),
+                         _p(self.icsc), _p(gr), _p(fm), _p(hessb),
+                         _p(jacl) if jacl is not None else None)
+        return jacl
 
     def adjflam(self, fmat, adjlam64, gradl=None):
         if gradl is None:

@@ -2247,6 +2247,61 @@ int orc_cadj_nu_alpha(const orc_mesh *m, const int *lm, int ndof, const int *mas
     return ierr;
 }
 
+/*
+ * PCHADJ (pchadj.f90:1-330), one process, after its Green's-function solve:
+ * for every inversion anchor column and every receiver right-hand side,
+ *     JACL(irhs, v) = sum_rows GRNSFNS((irhs-1)*NDOF + JDOF) * FMAT(row, v)
+ * in COMPLEX*8 (pchadj.f90:241-246), then the block-diagonal preconditioner
+ * update HESSB += REAL(JACL^H JACL) (CGEMM 'C','N' with ALPHA = 1, BETA = 0,
+ * summed over irhs in order as the reference BLAS does, then SAXPY,
+ * pchadj.f90:274-300, 312-323).  grns: COMPLEX*8 [nrhs][ndof]; fmat:
+ * COMPLEX*8 [nvinv][nz]; hessb: REAL*4 [nnpinv * nvinv^2] updated in place,
+ * block (col, iv, jv) at (col * nvinv + iv) * nvinv + jv; jacl (nullable):
+ * COMPLEX*8 [nnpinv * nvinv][nrhs].
+ */
+void orc_pchadj(int nnpinv, int nvinv, long long nz, int ndof, int nrhs, const int *jcsc,
+                const int *icsc, const float *grns, const float *fmat, float *hessb, float *jacl)
+{
+    cc *jl = (cc *)malloc(sizeof(cc) * (size_t)nrhs * nvinv);
+    for (int col = 0; col < nnpinv; col++) {
+        for (int irhs = 0; irhs < nrhs; irhs++)
+            for (int v = 0; v < nvinv; v++) {
+                cc acc = cmk(0.0f, 0.0f);
+                for (int i = jcsc[col]; i <= jcsc[col + 1] - 1; i++) {
+                    const int jdof = icsc[i - 1];
+                    if (jdof == 0) continue;
+                    const size_t jl0 = (size_t)irhs * ndof + jdof - 1;
+                    cc g = cmk(grns[2 * jl0], grns[2 * jl0 + 1]);
+                    const size_t f0 = (size_t)v * nz + i - 1;
+                    cc f = cmk(fmat[2 * f0], fmat[2 * f0 + 1]);
+                    cc t = cmulf(g, f);
+                    acc.re = acc.re + t.re;
+                    acc.im = acc.im + t.im;
+                }
+                jl[(size_t)irhs * nvinv + v] = acc;
+                if (jacl) {
+                    jacl[2 * (((size_t)col * nvinv + v) * nrhs + irhs)] = acc.re;
+                    jacl[2 * (((size_t)col * nvinv + v) * nrhs + irhs) + 1] = acc.im;
+                }
+            }
+        for (int iv = 0; iv < nvinv; iv++)
+            for (int jv = 0; jv < nvinv; jv++) {
+                cc temp = cmk(0.0f, 0.0f);
+                for (int l = 0; l < nrhs; l++) {
+                    cc a = jl[(size_t)l * nvinv + iv], b = jl[(size_t)l * nvinv + jv];
+                    cc t = cmulf(cmk(a.re, -a.im), b);
+                    temp.re = temp.re + t.re;
+                    temp.im = temp.im + t.im;
+                }
+                cc h = cmulf(cmk(1.0f, 0.0f), temp);
+                float hb = 0.0f + h.re;
+                float *y = &hessb[((size_t)col * nvinv + iv) * nvinv + jv];
+                *y = *y + 1.0f * hb;
+            }
+    }
+    free(jl);
+}
+
 /* ADJFLAM_DIST (adjgrad.f90:88-145) followed by GRADL = GRADL - GPROD
  * (adjgrad.f90:76); REAL*4 arithmetic. gradl: [nnpinv], adjlam: COMPLEX*8 */
 void orc_adjflam(int nnpinv, const int *jcsc, const int *icsc, const float *fmat,

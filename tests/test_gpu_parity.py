@@ -358,6 +358,30 @@ def test_cadj_nu_alpha_matches_oracle(case0, cinv, accumulate):
         assert np.array_equal(d_p.cpu().numpy().view(np.uint32), p3.view(np.uint32))
 
 
+@pytest.mark.parametrize("nvinv", [1, 2])
+def test_pchadj_matches_oracle(case0, nvinv):
+    """PCHADJ Jacobian blocks and preconditioner update: bit-identical to the
+    oracle; HESSB is updated in place, so a second call adds the same block."""
+    mesh, pairs, g, ctx = case0
+    rg = oracle.RefGrad(mesh, g)
+    rng = np.random.default_rng(43)
+    nrhs = 9
+    grns = (rng.standard_normal((nrhs, g.ndof)) + 1j * rng.standard_normal((nrhs, g.ndof))
+            ).astype(np.complex64)
+    fmat = (rng.standard_normal((nvinv, rg.nz)) + 1j * rng.standard_normal((nvinv, rg.nz))
+            ).astype(np.complex64)
+    hess = rng.standard_normal(rg.nnpinv * nvinv * nvinv).astype(np.float32)
+    d_h = torch.from_numpy(hess.copy()).to(_dev())
+    d_j = torch.full((rg.nnpinv * nvinv, nrhs), float("nan"), dtype=torch.complex64,
+                     device=_dev())
+    d_g, d_f = torch.from_numpy(grns).to(_dev()), torch.from_numpy(fmat).to(_dev())
+    for rep in range(2):
+        jacl = rg.pchadj(grns, fmat, hess)
+        ctx.pchadj(nvinv, nrhs, d_g, d_f, d_h, d_j)
+        assert np.array_equal(d_j.cpu().numpy().view(np.uint32), jacl.view(np.uint32)), rep
+        assert np.array_equal(d_h.cpu().numpy().view(np.uint32), hess.view(np.uint32)), rep
+
+
 def test_reference_gradient_rejects_ps(case0):
     mesh, pairs, g, ctx = case0
     d = torch.zeros(g.ndof, dtype=torch.complex64, device=_dev())

@@ -379,3 +379,28 @@ def test_cadj_nu_alpha_matches_numpy_restatement(small_case, accumulate):
         col += 1
     for got, ref in ((ra, ref_a), (rb, ref_b), (p3, ref_p3)):
         assert np.max(np.abs(got - ref)) <= 2e-4 * np.max(np.abs(ref))
+
+
+def test_pchadj_matches_numpy_restatement(small_case):
+    """PCHADJ's Jacobian block JACL = G^T F and the preconditioner update
+    HESSB += REAL(JACL^H JACL) (FP32) against FP64 numpy, 'PS' layout."""
+    mesh, pairs = small_case
+    g = oracle.graph_build(mesh)
+    rg = oracle.RefGrad(mesh, g)
+    rng = np.random.default_rng(41)
+    nrhs = 6
+    grns = (rng.standard_normal((nrhs, g.ndof)) + 1j * rng.standard_normal((nrhs, g.ndof))
+            ).astype(np.complex64)
+    fmat = (rng.standard_normal((2, rg.nz)) + 1j * rng.standard_normal((2, rg.nz))
+            ).astype(np.complex64)
+    hess0 = rng.standard_normal(rg.nnpinv * 4).astype(np.float32)
+    hess = hess0.copy()
+    jacl = rg.pchadj(grns, fmat, hess)
+    ref_h = hess0.astype(np.float64)
+    for col in range(rg.nnpinv):
+        i1, i2 = rg.jcsc[col] - 1, rg.jcsc[col + 1] - 1
+        rows = rg.icsc[i1:i2] - 1
+        j = grns[:, rows].astype(np.complex128) @ fmat[:, i1:i2].T.astype(np.complex128)
+        assert np.allclose(jacl[2 * col:2 * col + 2].T, j, rtol=0, atol=1e-4 * np.abs(j).max())
+        ref_h[4 * col:4 * col + 4] += np.real(j.conj().T @ j).reshape(-1)
+    assert np.max(np.abs(hess - ref_h)) <= 2e-5 * np.max(np.abs(ref_h))
