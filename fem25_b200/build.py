@@ -32,7 +32,8 @@ UNITS = [
     ("misfit_noalloc.cu", ["-fmad=false"]),
     ("dense_solve.cu", []),
 ]
-HOST = [("host_setup.cpp", ["-O2", "-ffp-contract=off", "-fPIC", "-fopenmp", "-std=c++17"])]
+HOST = [("host_setup.cpp", ["-O2", "-ffp-contract=off", "-fPIC", "-fopenmp", "-std=c++17"]),
+        ("mesh_io.cpp", ["-O2", "-ffp-contract=off", "-fPIC", "-std=c++17"])]
 
 
 def _run(cmd):

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <map>
 
@@ -262,6 +263,94 @@ int fem25_graph_copy(const fem25_graph *g, int *ien, int *lm, int *irptr, int *j
 }
 
 void fem25_graph_free(fem25_graph *g) { delete g; }
+// FNV-1a 64 over the mesh arrays the graph depends on
+static uint64_t mesh_fingerprint(const fem25_mesh *m) {
+  uint64_t h = 1469598103934665603ULL;
+  auto mix = [&](const void *p, size_t n) {
+    const unsigned char *b = static_cast<const unsigned char *>(p);
+    for (size_t i = 0; i < n; i++) h = (h ^ b[i]) * 1099511628211ULL;
+  };
+  mix(&m->nelem, sizeof(int));
+  mix(&m->nnpg, sizeof(int));
+  mix(&m->nord, sizeof(int));
+  mix(m->ieng, sizeof(int) * 4 * (size_t)m->nelem);
+  mix(m->cdomain, (size_t)m->nelem);
+  mix(m->cnnpg, 2 * (size_t)m->nnpg);
+  mix(m->xlocs, sizeof(double) * (size_t)m->nnpg);
+  mix(m->zlocs, sizeof(double) * (size_t)m->nnpg);
+  return h;
+}
+
+static const char kGraphMagic[8] = {'F', 'E', 'M', '2', '5', 'G', 'R', '1'};
+
+int fem25_graph_save(const fem25_graph *g, const fem25_mesh *m, const char *path) {
+  if (!g || !m || !path) return FEM25_ERR_ARG;
+  std::string msg;
+  int r = check_mesh(m, &msg);
+  if (r) return fail(nullptr, r, msg);
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return fail(nullptr, FEM25_ERR_ARG, std::string("graph save: cannot open ") + path);
+  const HostGraph &h = g->g;
+  const uint64_t fp = mesh_fingerprint(m);
+  const int hdr[3] = {h.nelem, h.nnp, h.ndof};
+  bool ok = std::fwrite(kGraphMagic, 1, 8, f) == 8 && std::fwrite(&fp, 8, 1, f) == 1 &&
+            std::fwrite(hdr, sizeof(int), 3, f) == 3 && std::fwrite(&h.nzero, 8, 1, f) == 1;
+  auto put = [&](const void *p, size_t sz, size_t n) {
+    ok = ok && (n == 0 || std::fwrite(p, sz, n, f) == n);
+  };
+  put(h.ien.data(), sizeof(int), h.ien.size());
+  put(h.lm.data(), sizeof(int), h.lm.size());
+  put(h.irptr.data(), sizeof(int), h.irptr.size());
+  put(h.jcptr.data(), sizeof(int), h.jcptr.size());
+  put(h.cnp.data(), 1, h.cnp.size());
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? FEM25_OK : fail(nullptr, FEM25_ERR_ARG, "graph save: write failed");
+}
+
+int fem25_graph_load(const fem25_mesh *m, const char *path, fem25_graph **out) {
+  if (!m || !path || !out) return FEM25_ERR_ARG;
+  *out = nullptr;
+  std::string msg;
+  int r = check_mesh(m, &msg);
+  if (r) return fail(nullptr, r, msg);
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return fail(nullptr, FEM25_ERR_ARG, std::string("graph load: cannot open ") + path);
+  char magic[8];
+  uint64_t fp = 0;
+  int hdr[3];
+  long long nz = 0;
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kGraphMagic, 8) == 0 &&
+            std::fread(&fp, 8, 1, f) == 1 && std::fread(hdr, sizeof(int), 3, f) == 3 &&
+            std::fread(&nz, 8, 1, f) == 1;
+  if (!ok || fp != mesh_fingerprint(m) || hdr[0] != m->nelem || hdr[2] <= 0 || nz <= 0) {
+    std::fclose(f);
+    return fail(nullptr, FEM25_ERR_GRAPH, "graph load: file does not belong to this mesh");
+  }
+  fem25_graph *g = new fem25_graph();
+  HostGraph &h = g->g;
+  h.nelem = hdr[0];
+  h.nnp = hdr[1];
+  h.ndof = hdr[2];
+  h.nzero = nz;
+  h.ien.resize((size_t)kNen * h.nelem);
+  h.lm.resize((size_t)3 * kNen * h.nelem);
+  h.irptr.resize((size_t)h.ndof + 1);
+  h.jcptr.resize((size_t)nz);
+  h.cnp.resize((size_t)h.ndof);
+  auto get = [&](void *p, size_t sz, size_t n) { ok = ok && std::fread(p, sz, n, f) == n; };
+  get(h.ien.data(), sizeof(int), h.ien.size());
+  get(h.lm.data(), sizeof(int), h.lm.size());
+  get(h.irptr.data(), sizeof(int), h.irptr.size());
+  get(h.jcptr.data(), sizeof(int), h.jcptr.size());
+  get(h.cnp.data(), 1, h.cnp.size());
+  std::fclose(f);
+  if (!ok || h.irptr[0] != 1 || h.irptr[h.ndof] != nz + 1) {
+    delete g;
+    return fail(nullptr, FEM25_ERR_GRAPH, "graph load: truncated or corrupt file");
+  }
+  *out = g;
+  return FEM25_OK;
+}
 
 int fem25_create(const fem25_mesh *m, int ndof, long long nzero, const int *lm, const int *irptr,
                  const int *jcptr, const char *cnp, int device, fem25_ctx **out) {

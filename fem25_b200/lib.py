@@ -50,6 +50,12 @@ def lib():
         L.fem25_graph_copy.argtypes = [vp, vp, vp, vp, vp, vp]
         L.fem25_graph_free.argtypes = [vp]
         L.fem25_graph_free.restype = None
+        L.fem25_graph_save.argtypes = [vp, vp, C.c_char_p]
+        L.fem25_graph_load.argtypes = [vp, C.c_char_p, C.POINTER(vp)]
+        L.fem25_read_mesh.argtypes = [C.c_char_p, C.POINTER(vp)]
+        L.fem25_mesh_file_get.argtypes = [vp, vp, vp, vp]
+        L.fem25_mesh_file_free.argtypes = [vp]
+        L.fem25_mesh_file_free.restype = None
         L.fem25_create.argtypes = [vp, i, ll, vp, vp, vp, vp, i, C.POINTER(vp)]
         L.fem25_destroy.argtypes = [vp]
         L.fem25_destroy.restype = None
@@ -142,14 +148,26 @@ class Graph:
         self.__dict__.update(kw)
 
 
-def graph_build(mesh):
-    """GEN_GRAPH25: IEN, LM, IRPTR, JCPTR (1-based) and CNP of a mesh."""
+def graph_build(mesh, cache=None):
+    """GEN_GRAPH25: IEN, LM, IRPTR, JCPTR (1-based) and CNP of a mesh.  With
+    ``cache`` (a file path) the graph is read from that file when it was made
+    for this mesh, else built and written there."""
     L = lib()
     mk = _MeshKeep(mesh)
     h = C.c_void_p()
-    r = L.fem25_graph_build(mk.ptr, C.byref(h))
-    if r:
-        raise Fem25Error(r, "graph build failed")
+    if cache is not None and os.path.exists(cache):
+        r = L.fem25_graph_load(mk.ptr, os.fsencode(cache), C.byref(h))
+        if r:
+            h = C.c_void_p()
+    if not h:
+        r = L.fem25_graph_build(mk.ptr, C.byref(h))
+        if r:
+            raise Fem25Error(r, "graph build failed")
+        if cache is not None:
+            r = L.fem25_graph_save(h, mk.ptr, os.fsencode(cache))
+            if r:
+                L.fem25_graph_free(h)
+                raise Fem25Error(r, f"graph save to {cache} failed")
     nnp, ndof, nz = C.c_int(), C.c_int(), C.c_longlong()
     L.fem25_graph_info(h, C.byref(nnp), C.byref(ndof), C.byref(nz))
     nen = (mesh.nord + 1) ** 2
@@ -162,6 +180,45 @@ def graph_build(mesh):
     L.fem25_graph_free(h)
     return Graph(nnp=nnp.value, ndof=ndof.value, nzero=nz.value, ien=ien, lm=lm, irptr=irptr,
                  jcptr=jcptr, cnp=cnp)
+
+
+def read_mesh(projnm):
+    """RDMESHBK: PROJNM.nodes + PROJNM.mesh -> (Mesh, info).  info holds INPTYP,
+    IITYPE, IDISP, NELEME, NABS and the Bielak/absorbing corner latitudes and
+    longitudes; the PML parameters keep the Mesh defaults (they come from the
+    reference's parameter file, not the mesh files)."""
+    from .synth import Mesh as PyMesh
+    L = lib()
+    h = C.c_void_p()
+    r = L.fem25_read_mesh(os.fsencode(projnm), C.byref(h))
+    if r and not h:
+        raise Fem25Error(r, f"reading {projnm}.nodes / .mesh failed (see stderr)")
+    try:
+        m = Mesh()
+        ints = np.zeros(5, np.int32)
+        reals = np.zeros(4)
+        L.fem25_mesh_file_get(h, C.byref(m), _np(ints), _np(reals))
+        if r:
+            raise Fem25Error(r, f"{projnm}: unsupported mesh (INPTYP {ints[0]}, IITYPE {ints[1]})")
+        ne, nn = m.nelem, m.nnpg
+        arr = lambda ptr, n, dt: np.ctypeslib.as_array(C.cast(ptr, C.POINTER(dt)), (n,)).copy()
+        ldisp = bool(m.ldisp)
+        mesh = PyMesh(nelem=ne, nnpg=nn, nord=m.nord,
+                      ieng=arr(m.ieng, 4 * ne, C.c_int32).reshape(ne, 4),
+                      cdomain=arr(m.cdomain, ne, C.c_uint8),
+                      cnnpg=arr(m.cnnpg, 2 * nn, C.c_uint8).reshape(nn, 2),
+                      xlocs=arr(m.xlocs, nn, C.c_double), zlocs=arr(m.zlocs, nn, C.c_double),
+                      xd=arr(m.xd, nn, C.c_double), zd=arr(m.zd, nn, C.c_double),
+                      ecoeff=arr(m.ecoeff, 2 * nn, C.c_double).reshape(2, nn),
+                      dens=arr(m.dens, nn, C.c_double), xwidth=m.xwidth, zwidth=m.zwidth,
+                      ldisp=ldisp, qp=arr(m.qp, nn, C.c_double) if ldisp else None,
+                      qs=arr(m.qs, nn, C.c_double) if ldisp else None)
+        info = dict(inptyp=int(ints[0]), iitype=int(ints[1]), idisp=int(ints[2]),
+                    neleme=int(ints[3]), nabs=int(ints[4]), xlatmin=reals[0], xlonmin=reals[1],
+                    xlatmax=reals[2], xlonmax=reals[3])
+        return mesh, info
+    finally:
+        L.fem25_mesh_file_free(h)
 
 
 class Context:

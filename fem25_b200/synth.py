@@ -275,6 +275,35 @@ def make_dispersive(mesh: Mesh, seed: int, freq0: float = 1.0, qs_mean: float = 
     return mesh
 
 
+def write_mesh(mesh: Mesh, projnm: str, inptyp: int = 2, latlon=(0.0, 0.0, 0.0, 1.0)) -> None:
+    """Writes PROJNM.nodes and PROJNM.mesh in the layout RDMESHBK reads
+    (``mesh_utils.f:982-1165``): element records (CDOMAIN, IENG(1:4)), then a
+    header (NNPG, INPTYP, NORD, IITYPE=1, IDISP), the Bielak/absorbing corner
+    coordinates and anchor records (CNNPG, X, Z, XD, ZD, model, DENS [, QP,
+    QS]).  inptyp 2 writes (lambda, mu) exactly (shortest round-trip decimal);
+    inptyp 1 writes (Vp, Vs)."""
+    with open(projnm + ".nodes", "w") as f:
+        f.write(f"{mesh.nelem}\n")
+        for e in range(mesh.nelem):
+            i = mesh.ieng[e]
+            f.write(f"'{chr(mesh.cdomain[e])}' {i[0]} {i[1]} {i[2]} {i[3]}\n")
+    idisp = 1 if mesh.ldisp else 0
+    with open(projnm + ".mesh", "w") as f:
+        f.write(f"{mesh.nnpg} {inptyp} {mesh.nord} 1 {idisp}\n")
+        f.write(" ".join(repr(float(x)) for x in latlon) + "\n")
+        lam, mu, rho = mesh.ecoeff[0], mesh.ecoeff[1], mesh.dens
+        for p in range(mesh.nnpg):
+            if inptyp == 1:
+                model = (np.sqrt((lam[p] + 2.0 * mu[p]) / rho[p]), np.sqrt(mu[p] / rho[p]))
+            else:
+                model = (lam[p], mu[p])
+            vals = [mesh.xlocs[p], mesh.zlocs[p], mesh.xd[p], mesh.zd[p], *model, rho[p]]
+            if mesh.ldisp:
+                vals += [mesh.qp[p], mesh.qs[p]]
+            cls = bytes(mesh.cnnpg[p]).decode()
+            f.write(f"'{cls}' " + " ".join(repr(float(v)) for v in vals) + "\n")
+
+
 def make_config(idx, nx=None, nz=None):
     """Mesh + model + (freq, py) pairs for benchmark configuration ``idx``.
     ``nx``/``nz`` override the element counts (same physical size), for

@@ -69,6 +69,33 @@ int fem25_graph_info(const fem25_graph *g, int *nnp, int *ndof, long long *nzero
 int fem25_graph_copy(const fem25_graph *g, int *ien, int *lm, int *irptr, int *jcptr, char *cnp);
 void fem25_graph_free(fem25_graph *g);
 
+/* A cache of the graph: fem25_graph_save writes IEN, LM, IRPTR, JCPTR and CNP
+ * with a fingerprint of the mesh (IENG, CDOMAIN, CNNPG, XLOCS, ZLOCS);
+ * fem25_graph_load reads them back for the same mesh, so later runs skip the
+ * graph build, and returns FEM25_ERR_GRAPH for a file made from another
+ * mesh or a truncated one. */
+int fem25_graph_save(const fem25_graph *g, const fem25_mesh *m, const char *path);
+int fem25_graph_load(const fem25_mesh *m, const char *path, fem25_graph **out);
+
+/* ---- mesh files: replaces RDMESHBK (mesh_utils.f:982-1165) ----------------
+ * Reads PROJNM.nodes (NELEM; CDOMAIN, IENG(1:4) per element) and PROJNM.mesh
+ * (NNPG, INPTYP, NORD, IITYPE, IDISP; XLATMIN, XLONMIN, XLATMAX, XLONMAX;
+ * CNNPG, X, Z, XD, ZD, VARS(1:NCOEFF), DENS [, QP, QS] per anchor) with
+ * Fortran list-directed rules.  INPTYP 1 converts (Vp, Vs) to (lambda, mu)
+ * as the reference does; XWIDTH / ZWIDTH are the largest XD / ZD.  Returns
+ * FEM25_ERR_ARG for a missing file or a premature end, and
+ * FEM25_ERR_UNSUPPORTED (with the file still returned) for anisotropic
+ * models (INPTYP > 2) or IITYPE other than 1 (GLL nodes), which this library
+ * does not assemble.  fem25_mesh_file_get points a fem25_mesh at the file's
+ * arrays (valid until fem25_mesh_file_free) and leaves the PML parameters
+ * (RCOEFF, DMAX, KAPPA, FCENT: the reference's parameter file) and FREQ0 at
+ * zero for the caller to set; ints (nullable): INPTYP, IITYPE, IDISP,
+ * NELEME, NABS; reals (nullable): XLATMIN, XLONMIN, XLATMAX, XLONMAX. */
+typedef struct fem25_mesh_file fem25_mesh_file;
+int fem25_read_mesh(const char *projnm, fem25_mesh_file **out);
+int fem25_mesh_file_get(const fem25_mesh_file *f, fem25_mesh *m, int *ints, double *reals);
+void fem25_mesh_file_free(fem25_mesh_file *f);
+
 /* ---- context --------------------------------------------------------------
  * Copies mesh, model and graph (LM, IRPTR, JCPTR, CNP as GEN_GRAPH25 leaves
  * them in MESH_INFO) to `device` and builds the element-to-nonzero map.

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from fem25_b200 import graph_build, lib, synth
+from fem25_b200 import graph_build, lib, read_mesh, synth
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -56,3 +56,68 @@ def test_create_without_gpu_fails_loudly():
     mesh, _, _ = synth.make_config(0, nx=6, nz=4)
     with pytest.raises(Fem25Error):
         Context(mesh)
+
+
+@pytest.mark.parametrize("disp", [False, True])
+def test_mesh_files_round_trip(tmp_path, disp):
+    """synth.write_mesh -> fem25_read_mesh (RDMESHBK) returns the same arrays
+    bit for bit with INPTYP 2, and the graph built from the read mesh equals
+    the original's."""
+    mesh, _, _ = synth.make_config(4, nx=14, nz=6)
+    if disp:
+        mesh = synth.make_dispersive(mesh, 5)
+    proj = str(tmp_path / "model")
+    synth.write_mesh(mesh, proj, latlon=(40.1, -120.5, 40.3, -119.9))
+    got, info = read_mesh(proj)
+    for k in ("ieng", "cdomain", "cnnpg", "xlocs", "zlocs", "xd", "zd", "ecoeff", "dens"):
+        assert np.array_equal(getattr(got, k), getattr(mesh, k)), k
+    assert got.xwidth == mesh.xd.max() and got.zwidth == mesh.zd.max()
+    assert info["neleme"] == int(np.sum(mesh.cdomain == ord("E")))
+    assert info["nabs"] == int(np.sum(mesh.cdomain == ord("A")))
+    assert (info["xlatmin"], info["xlonmax"]) == (40.1, -119.9)
+    assert got.ldisp == disp
+    if disp:
+        assert np.array_equal(got.qp, mesh.qp) and np.array_equal(got.qs, mesh.qs)
+    g0, g1 = graph_build(mesh), graph_build(got)
+    for k in ("ien", "lm", "irptr", "jcptr", "cnp"):
+        assert np.array_equal(getattr(g0, k), getattr(g1, k)), k
+
+
+def test_mesh_files_velocity_input_and_errors(tmp_path):
+    """INPTYP 1 (Vp, Vs) becomes mu = Vs^2 rho, lambda = Vp^2 rho - 2 mu;
+    missing or truncated files are errors, not crashes."""
+    mesh, _, _ = synth.make_config(0, nx=6, nz=4)
+    proj = str(tmp_path / "vel")
+    synth.write_mesh(mesh, proj, inptyp=1)
+    got, info = read_mesh(proj)
+    assert info["inptyp"] == 1
+    assert np.allclose(got.ecoeff, mesh.ecoeff, rtol=1e-12, atol=0)
+    with pytest.raises(Exception):
+        read_mesh(str(tmp_path / "missing"))
+    lines = open(proj + ".mesh").read().splitlines()
+    open(proj + ".mesh", "w").write("\n".join(lines[:-3]) + "\n")
+    with pytest.raises(Exception):
+        read_mesh(proj)
+
+
+def test_graph_cache(tmp_path):
+    """graph_build(cache=...) writes the graph once, reads it back for the same
+    mesh and rebuilds it for another mesh or a corrupt file."""
+    mesh, _, _ = synth.make_config(0, nx=8, nz=5)
+    path = str(tmp_path / "g.bin")
+    g0 = graph_build(mesh, cache=path)
+    assert os.path.exists(path)
+    g1 = graph_build(mesh, cache=path)
+    for k in ("ien", "lm", "irptr", "jcptr", "cnp"):
+        assert np.array_equal(getattr(g0, k), getattr(g1, k)), k
+    other, _, _ = synth.make_config(0, nx=9, nz=5)
+    h = ctypes.c_void_p()
+    from fem25_b200.lib import _MeshKeep
+    mk = _MeshKeep(other)
+    assert lib().fem25_graph_load(mk.ptr, os.fsencode(path), ctypes.byref(h)) != 0
+    g2 = graph_build(other, cache=str(tmp_path / "g2.bin"))
+    assert g2.ndof != g0.ndof
+    data = open(path, "rb").read()
+    open(path, "wb").write(data[:len(data) // 2])
+    mk0 = _MeshKeep(mesh)
+    assert lib().fem25_graph_load(mk0.ptr, os.fsencode(path), ctypes.byref(h)) != 0
