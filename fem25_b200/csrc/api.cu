@@ -598,6 +598,13 @@ int fem25_assemble_batch_dev(fem25_ctx *h, int n, const char *cftype, const doub
   return FEM25_OK;
 }
 
+int fem25_tuning(const fem25_ctx *h, int *stream_variant, int *grad_tile) {
+  if (!h) return FEM25_ERR_ARG;
+  if (stream_variant) *stream_variant = h->c.stream_variant;
+  if (grad_tile) *grad_tile = h->c.grad_tile;
+  return FEM25_OK;
+}
+
 int fem25_profile_enable(fem25_ctx *h, int enable) {
   if (!h) return FEM25_ERR_ARG;
   Ctx *c = &h->c;

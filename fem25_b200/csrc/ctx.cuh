@@ -92,6 +92,7 @@ struct Ctx {
   double *d_prim = nullptr;      // [nzero] K0/K1 basis value of every CSR entry
   unsigned *d_desc = nullptr;    // [nzero] block << 4 | i << 2 | j
   int stream_variant = -1;       // loop order of the streaming kernel (-1: not tuned yet)
+  int grad_tile = -1;            // source tile of the FP64 gradient (-1: not tuned yet)
   double *d_ebasis = nullptr;    // [nelem][625][12] scratch
   int *d_bgptr = nullptr, *d_bglist = nullptr;  // block -> (element node pair) ids
   bool basis_valid = false;

@@ -13,13 +13,14 @@
 // by the bilinear anchor function SF_p (cjac.f:98-108).  Fields are
 // interpolated to the 13x13 points with the SHL table (dshl.f:1-243) and the
 // inverse Jacobian (cjac.f:128-134).
+#include <cstdlib>
+
 #include "ctx.cuh"
 #include "kcommon.cuh"
 
 namespace fem25 {
 
 constexpr int kGThreads = 192;   // >= 169 quadrature points
-constexpr int kGSrcTile = 4;     // sources staged per sync
 constexpr int kShlPad = (3 * kNq * kNen + 1) & ~1;  // shared SHL table, rounded to 16 B
 
 struct GradArgs {
@@ -31,6 +32,9 @@ __device__ __forceinline__ double re_cj(double ar, double ai, double br, double 
   return ar * br + ai * bi;  // Re(conj(a) b)
 }
 
+// TILE sources of both fields are staged in shared memory per sync; the
+// result does not depend on TILE (each point sums the sources in order).
+template <int TILE>
 __global__ void __launch_bounds__(kGThreads)
     k_grad_plain(MeshView mv, DevTables dt, GradArgs ga, const int *__restrict__ elems,
                  const int *__restrict__ lm, PairTable pt,
@@ -40,8 +44,8 @@ __global__ void __launch_bounds__(kGThreads)
   double *shl = sm;                                        // [169][25][3]
   // double2 staging area starts on a 16-byte boundary (12675 doubles -> 12676)
   double2 *fu = reinterpret_cast<double2 *>(sm + kShlPad);  // [tile][75]
-  double2 *fl = fu + kGSrcTile * kNee;
-  double *red = reinterpret_cast<double *>(fl + kGSrcTile * kNee);  // [12][kGThreads/32]
+  double2 *fl = fu + TILE * kNee;
+  double *red = reinterpret_cast<double *>(fl + TILE * kNee);  // [12][kGThreads/32]
   const int t = threadIdx.x;
   for (int i = t; i < 3 * kNq * kNen; i += kGThreads) shl[i] = dt.shl[i];
   const int e = elems[blockIdx.x];
@@ -64,8 +68,8 @@ __global__ void __launch_bounds__(kGThreads)
   for (int p = 0; p < ga.npairs; p++) {
     const double2 pr = pt.p[p];
     const double w2 = pr.x * pr.x, wpy = pr.y;
-    for (int s0 = 0; s0 < ga.nsrc; s0 += kGSrcTile) {
-      const int ns = min(kGSrcTile, ga.nsrc - s0);
+    for (int s0 = 0; s0 < ga.nsrc; s0 += TILE) {
+      const int ns = min(TILE, ga.nsrc - s0);
       __syncthreads();
       for (int i = t; i < ns * kNee; i += kGThreads) {
         const int s = i / kNee, k = i % kNee;
@@ -163,17 +167,44 @@ __global__ void __launch_bounds__(kGThreads)
   }
 }
 
-static size_t grad_smem() {
-  return sizeof(double) * kShlPad + sizeof(double2) * 2 * kGSrcTile * kNee +
+static size_t grad_smem(int tile) {
+  return sizeof(double) * kShlPad + sizeof(double2) * 2 * tile * kNee +
          sizeof(double) * 12 * (kGThreads / 32);
 }
 
+template <int TILE>
+static cudaError_t grad_tile_launch(Ctx *c, const GradArgs &ga, const PairTable &pt,
+                                    const double *u, const double *lam, double *grad,
+                                    cudaStream_t st) {
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_grad_plain<TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)grad_smem(TILE))))
+    return e;
+  k_grad_plain<TILE><<<c->n_nonpml, kGThreads, grad_smem(TILE), st>>>(
+      c->mv, c->dt, ga, c->d_nonpml, c->d_lm, pt, (const double2 *)u, (const double2 *)lam, grad,
+      c->d_err);
+  return cudaGetLastError();
+}
+
+static const int kGradTiles[] = {2, 4, 8};
+
+static cudaError_t grad_variant(Ctx *c, int tile, const GradArgs &ga, const PairTable &pt,
+                                const double *u, const double *lam, double *grad,
+                                cudaStream_t st) {
+  switch (tile) {
+    case 2: return grad_tile_launch<2>(c, ga, pt, u, lam, grad, st);
+    case 8: return grad_tile_launch<8>(c, ga, pt, u, lam, grad, st);
+    default: return grad_tile_launch<4>(c, ga, pt, u, lam, grad, st);
+  }
+}
+
+// The source-tile width (sources of both fields staged per shared-memory
+// pass: 2, 4 or 8, trading shared memory per CTA against syncs per source) is
+// picked on the first call of a context by timing each width once on that
+// call's fields into a scratch gradient, and kept.  FEM25_GRAD_TILE forces a
+// width; a call recorded into a CUDA graph before any tuning uses 4.
 cudaError_t launch_grad_plain(Ctx *c, const PairTable &pt, int npairs, int nsrc, const double *u,
                               const double *lam, double *grad, cudaStream_t st) {
-  cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_grad_plain, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)grad_smem())))
-    return e;
   GradArgs ga;
   ga.npairs = npairs;
   ga.nsrc = nsrc;
@@ -181,10 +212,42 @@ cudaError_t launch_grad_plain(Ctx *c, const PairTable &pt, int npairs, int nsrc,
   ga.nnpg = c->nnpg;
   ga.field_stride = c->ndof;
   if (c->n_nonpml == 0) return cudaSuccess;
-  k_grad_plain<<<c->n_nonpml, kGThreads, grad_smem(), st>>>(c->mv, c->dt, ga, c->d_nonpml, c->d_lm, pt,
-                                                  (const double2 *)u, (const double2 *)lam, grad,
-                                                  c->d_err);
-  return cudaGetLastError();
+  cudaError_t e;
+  if (c->grad_tile < 0) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    const char *env = std::getenv("FEM25_GRAD_TILE");
+    if (env) {
+      const int t = std::atoi(env);
+      c->grad_tile = (t == 2 || t == 8) ? t : 4;
+    } else if (cs != cudaStreamCaptureStatusNone) {
+      c->grad_tile = 4;
+    } else {
+      double *scratch = nullptr;
+      if ((e = cudaMalloc(&scratch, sizeof(double) * 3 * (size_t)c->nnpg))) return e;
+      cudaEvent_t ev[4];
+      for (auto &x : ev) cudaEventCreate(&x);
+      cudaEventRecord(ev[0], st);
+      for (int k = 0; k < 3; k++) {
+        if ((e = grad_variant(c, kGradTiles[k], ga, pt, u, lam, scratch, st))) break;
+        cudaEventRecord(ev[k + 1], st);
+      }
+      if (!e) e = cudaEventSynchronize(ev[3]);
+      float best = 1e30f;
+      for (int k = 0; k < 3 && !e; k++) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+        if (t < best) {
+          best = t;
+          c->grad_tile = kGradTiles[k];
+        }
+      }
+      for (auto &x : ev) cudaEventDestroy(x);
+      cudaFree(scratch);
+      if (e) return e;
+    }
+  }
+  return grad_variant(c, c->grad_tile, ga, pt, u, lam, grad, st);
 }
 
 }  // namespace fem25

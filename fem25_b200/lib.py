@@ -81,6 +81,7 @@ def lib():
         L.fem25_misfit_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp, vp]
         L.fem25_misfit_noalloc_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp,
                                                vp]
+        L.fem25_tuning.argtypes = [vp, C.POINTER(i), C.POINTER(i)]
         L.fem25_profile_enable.argtypes = [vp, i]
         L.fem25_profile_ms.argtypes = [vp, i, C.POINTER(d)]
         _lib = L
@@ -257,6 +258,12 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def tuning(self):
+        """Autotuner choices: {"stream_variant": v, "grad_tile": t} (-1 = not tuned)."""
+        v, t = C.c_int(), C.c_int()
+        lib().fem25_tuning(self.h, C.byref(v), C.byref(t))
+        return {"stream_variant": v.value, "grad_tile": t.value}
 
     def _check(self, r):
         if r:

@@ -303,6 +303,12 @@ int fem25_misfit_noalloc_dev(fem25_ctx *ctx, int nsrc, int nrec, const int *mrdo
  * stream around its dominant kernels; fem25_profile_ms returns the duration
  * of the last launch: which = 0 the batched streaming kernel, which = 1 the
  * plain element + gather kernels of fem25_assemble_dev. */
+/* The choices of the per-context autotuners, -1 before the first call that
+ * tunes them: the streaming-assembly variant (0-2: 1, 2, 4 entries per
+ * thread; 3: software-pipelined; 4, 5: all systems of a 64 / 128-entry chunk
+ * staged for bulk stores; 6, 7: 256 / 512-entry staging ring) and the source
+ * tile of the FP64 gradient (2, 4 or 8 sources per shared-memory pass). */
+int fem25_tuning(const fem25_ctx *ctx, int *stream_variant, int *grad_tile);
 int fem25_profile_enable(fem25_ctx *ctx, int enable);
 int fem25_profile_ms(fem25_ctx *ctx, int which, double *ms);
 

@@ -199,6 +199,43 @@ def test_gradient_fp64_matches_oracle():
     ctx.close()
 
 
+_TILE_OUT = {}
+
+
+@pytest.mark.parametrize("tile", [4, 2, 8])
+def test_gradient_fp64_source_tiles_agree(tile, monkeypatch):
+    """Every source-tile width the FP64 gradient's autotuner can pick gives
+    the same gradient (sources are summed in the same order; only the
+    cross-element atomics differ): 9 sources = 4 full tiles of 2 and a
+    ragged one, a ragged tile of 4, a ragged tile of 8."""
+    monkeypatch.setenv("FEM25_GRAD_TILE", str(tile))
+    mesh, pairs, _ = synth.make_config(0, nx=10, nz=6)
+    g = oracle.graph_build(mesh)
+    ctx = Context(mesh, g)
+    rng = np.random.default_rng(19)
+    use = [pairs[2], pairs[11]]
+    shape = (len(use), 9, g.ndof)
+    u = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    lam = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    d_g = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=_dev())
+    ctx.gradient([p[0] for p in use], [p[1] for p in use], 9, torch.from_numpy(u).to(_dev()),
+                 torch.from_numpy(lam).to(_dev()), d_g, FEM25_PREC_FP64)
+    assert ctx.tuning()["grad_tile"] == tile
+    got = d_g.cpu().numpy()
+    if tile == 4:
+        ref = np.zeros((3, mesh.nnpg))
+        for p, (f, py) in enumerate(use):
+            oracle.grad_exact(mesh, g, f, py, u[p], lam[p], out=ref)
+        for m in range(3):
+            assert np.linalg.norm(got[m] - ref[m]) <= 1e-10 * np.linalg.norm(ref[m])
+        _TILE_OUT[4] = got
+    elif 4 in _TILE_OUT:
+        for m in range(3):
+            ref = _TILE_OUT[4][m]
+            assert np.linalg.norm(got[m] - ref) <= 1e-13 * np.linalg.norm(ref), m
+    ctx.close()
+
+
 @pytest.mark.parametrize("nsrc", [1, 7])
 def test_gradient_tf32x3_matches_oracle(nsrc):
     """Split-precision tensor-core gradient; 3 pairs x 7 sources = 21 combos
