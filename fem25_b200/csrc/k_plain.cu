@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(kPlainThreads, 1)
   __syncthreads();
   // ---- global shape-function derivatives (CJMK_TVI cjac.f:128-134)
   for (int idx = t; idx < kNq * kNen; idx += kPlainThreads) {
-    const int q = idx / kNen, a = idx % kNen;
+    const int q = idx / kNen;
     const double *c = qc + kNqc * q;
     const double *sl = dt.shl + 3 * (size_t)idx;
     double drnxi = sl[0], drneta = sl[1];
