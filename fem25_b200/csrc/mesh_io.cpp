@@ -11,9 +11,9 @@
 // accepted.  INPTYP 1 gives (Vp, Vs), converted as the reference does:
 // MU = VS**2 * DENS, LAMBDA = VP**2 * DENS - 2 MU.
 //
-// fem25_graph_save / fem25_graph_load keep GEN_GRAPH25's output (IEN, LM,
-// IRPTR, JCPTR, CNP) in a binary file so later runs on the same mesh skip the
-// graph build.
+// fem25_fazmod restates FAZMOD / VINCENTY for the model azimuth the misfit
+// needs.  (fem25_graph_save / fem25_graph_load, the graph cache, live with the
+// other graph entry points.)
 #include <cctype>
 #include <cmath>
 #include <cstdint>
@@ -246,5 +246,63 @@ int fem25_mesh_file_get(const fem25_mesh_file *f, fem25_mesh *m, int *ints, doub
 }
 
 void fem25_mesh_file_free(fem25_mesh_file *f) { delete f; }
+
+// FAZMOD (mesh_utils.f:1166-1212) through VINCENTY (distaz.f:141-298): the
+// azimuth from (XLATMIN, XLONMIN) to (XLATMAX, XLONMAX) on the WGS-84
+// ellipsoid by Vincenty's inverse iteration (tolerance 1e-12 rad on lambda,
+// at most 1000 iterations, the reference's pole and equator adjustments), in
+// degrees in [0, 360].  Coincident points give 0.  When the iteration does not
+// converge (nearly antipodal points) the reference falls back to a spherical
+// routine that is not part of its repository; here that is an error.
+int fem25_fazmod(double xlatmin, double xlonmin, double xlatmax, double xlonmax, double *azmod) {
+  if (!azmod) return FEM25_ERR_ARG;
+  const double a = 6378137.0, f = 0.0033528106647474805, pi180 = 0.017453292519943295;
+  const double pi = 3.1415926535897931, hpi = 1.5707963267948966, tol = 1.0e-12, eps = 2.22e-15;
+  *azmod = 0.0;
+  if (std::fabs(xlonmax - xlonmin) < eps && std::fabs(xlatmax - xlatmin) < eps) return FEM25_OK;
+  double phi1 = xlatmin * pi180, phi2 = xlatmax * pi180;
+  // within 1e-10 rad of a pole the reference sets PHI = DSIGN(PHI,1.D0)*(HPI - 1.D-10),
+  // i.e. |PHI| (HPI - 1e-10); kept as written
+  if (std::fabs(hpi - std::fabs(phi1)) < 1.0e-10) phi1 = std::fabs(phi1) * (hpi - 1.0e-10);
+  if (std::fabs(hpi - std::fabs(phi2)) < 1.0e-10) phi2 = std::fabs(phi2) * (hpi - 1.0e-10);
+  const bool on_equator = std::fabs(phi1) < tol && std::fabs(phi2) < tol;
+  const double u1 = std::atan2((1.0 - f) * std::tan(phi1), 1.0);
+  const double u2 = std::atan2((1.0 - f) * std::tan(phi2), 1.0);
+  const double cu1 = std::cos(u1), cu2 = std::cos(u2), su1 = std::sin(u1), su2 = std::sin(u2);
+  const double dl = (xlonmax - xlonmin) * pi180;
+  double lam = dl, lam0 = lam, sinl = 0.0, cosl = 0.0;
+  bool done = false;
+  for (int k = 0; k < 1000 && !done; k++) {
+    sinl = std::sin(lam);
+    cosl = std::cos(lam);
+    const double t1 = cu2 * sinl, t2 = cu1 * su2 - su1 * cu2 * cosl;
+    const double sins = std::sqrt(t1 * t1 + t2 * t2);
+    const double coss = su1 * su2 + cu1 * cu2 * cosl;
+    const double sigma = std::atan2(sins, coss);
+    const double sina = cu1 * cu2 * sinl / sins;
+    const double cos2a = 1.0 - sina * sina;
+    const double cos2s = on_equator ? -1.0 : coss - 2.0 * su1 * su2 / cos2a;
+    const double c = f / 16.0 * cos2a * (4.0 + f * (4.0 - 3.0 * cos2a));
+    lam = dl + (1.0 - c) * f * sina *
+                   (sigma + c * sins * (cos2s + c * coss * (-1.0 + 2.0 * cos2s * cos2s)));
+    if (std::fabs(lam - lam0) < tol) {
+      done = true;
+    } else if (std::fabs(sins) < eps) {
+      lam = pi;  // diametrically opposed
+      done = true;
+    }
+    lam0 = lam;
+  }
+  if (!done) {
+    std::fprintf(stderr, "fem25gpu: fazmod: Vincenty iteration did not converge\n");
+    return FEM25_ERR_ARG;
+  }
+  // the reference takes the azimuth with the last iterate's sin/cos of lambda
+  double az = std::atan2(cu2 * sinl, cu1 * su2 - su1 * cu2 * cosl) / pi180;
+  if (az < 0.0) az += 360.0;
+  if (az > 360.0) az -= 360.0;
+  *azmod = az;
+  return FEM25_OK;
+}
 
 }  // extern "C"

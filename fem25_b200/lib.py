@@ -56,6 +56,7 @@ def lib():
         L.fem25_mesh_file_get.argtypes = [vp, vp, vp, vp]
         L.fem25_mesh_file_free.argtypes = [vp]
         L.fem25_mesh_file_free.restype = None
+        L.fem25_fazmod.argtypes = [d, d, d, d, C.POINTER(d)]
         L.fem25_create.argtypes = [vp, i, ll, vp, vp, vp, vp, i, C.POINTER(vp)]
         L.fem25_destroy.argtypes = [vp]
         L.fem25_destroy.restype = None
@@ -181,6 +182,15 @@ def graph_build(mesh, cache=None):
     L.fem25_graph_free(h)
     return Graph(nnp=nnp.value, ndof=ndof.value, nzero=nz.value, ien=ien, lm=lm, irptr=irptr,
                  jcptr=jcptr, cnp=cnp)
+
+
+def fazmod(xlatmin, xlonmin, xlatmax, xlonmax):
+    """FAZMOD: model azimuth (degrees) of the Bielak/absorbing corners (WGS-84)."""
+    az = C.c_double()
+    r = lib().fem25_fazmod(xlatmin, xlonmin, xlatmax, xlonmax, C.byref(az))
+    if r:
+        raise Fem25Error(r, "fazmod: Vincenty iteration did not converge")
+    return az.value
 
 
 def read_mesh(projnm):

@@ -95,6 +95,12 @@ typedef struct fem25_mesh_file fem25_mesh_file;
 int fem25_read_mesh(const char *projnm, fem25_mesh_file **out);
 int fem25_mesh_file_get(const fem25_mesh_file *f, fem25_mesh *m, int *ints, double *reals);
 void fem25_mesh_file_free(fem25_mesh_file *f);
+/* FAZMOD (mesh_utils.f:1166-1212) with VINCENTY (distaz.f:141-298): model
+ * azimuth in degrees from the Bielak/absorbing corners (XLATMIN, XLONMIN) ->
+ * (XLATMAX, XLONMAX) on WGS-84; the AZMOD that fem25_misfit_dev takes.
+ * FEM25_ERR_ARG when the iteration does not converge (near-antipodal corners,
+ * where the reference falls back to a routine outside its repository). */
+int fem25_fazmod(double xlatmin, double xlonmin, double xlatmax, double xlonmax, double *azmod);
 
 /* ---- context --------------------------------------------------------------
  * Copies mesh, model and graph (LM, IRPTR, JCPTR, CNP as GEN_GRAPH25 leaves

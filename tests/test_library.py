@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from fem25_b200 import graph_build, lib, read_mesh, synth
+from fem25_b200 import fazmod, graph_build, lib, read_mesh, synth
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -121,3 +121,16 @@ def test_graph_cache(tmp_path):
     open(path, "wb").write(data[:len(data) // 2])
     mk0 = _MeshKeep(mesh)
     assert lib().fem25_graph_load(mk0.ptr, os.fsencode(path), ctypes.byref(h)) != 0
+
+
+def test_fazmod_vincenty_published_case():
+    """FAZMOD's Vincenty inverse on the published Flinders Peak -> Buninyong
+    example (WGS-84 forward azimuth 306 deg 52' 05.37"), plus the same-point
+    and due-east / due-north cases."""
+    dms = lambda d, m, s: np.sign(d) * (abs(d) + m / 60.0 + s / 3600.0)
+    az = fazmod(dms(-37, 57, 3.72030), dms(144, 25, 29.52440), dms(-37, 39, 10.15610),
+                dms(143, 55, 35.38390))
+    assert abs(az - dms(306, 52, 5.37)) <= 5e-6, az
+    assert fazmod(10.0, 20.0, 10.0, 20.0) == 0.0
+    assert abs(fazmod(0.0, 0.0, 0.0, 1.0) - 90.0) <= 1e-9
+    assert abs(fazmod(0.0, 0.0, 1.0, 0.0) - 0.0) <= 1e-9
