@@ -287,7 +287,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--nslots", type=int, default=16)
+    ap.add_argument("--nslots", type=int, default=32,
+                    help="ring slots (complex128 systems kept in HBM; 32 x 4 GB at 400x120)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-grad", action="store_true")
     ap.add_argument("--small", action="store_true", help="small mesh (profiling captures)")
@@ -375,7 +376,11 @@ def main():
     kms = statistics.mean(kern_ms)
     peak, peak_kind = peaks()
     achieved = 16.0 * nz * nsys / (kms / 1e3) / 1e9
-    launches_per_step = 2 * len(set(freqs)) + -(-nsys // min(16, nslots))
+    # per step: PML delta (element + gather kernel) per distinct frequency, and
+    # the streaming launches of the tuned variant (16 or, for the large-ring
+    # variants 8 and 9, up to 1024 systems each, never more than the ring)
+    per_launch = min(1024 if ctx.tuning()["stream_variant"] >= 8 else 16, nslots)
+    launches_per_step = 2 * len(set(freqs)) + -(-nsys // per_launch)
 
     # ---------------- plain FP64 per-system path (device buffers)
     o128 = torch.empty(nz, dtype=torch.complex128, device=dev)

@@ -48,6 +48,13 @@ struct SysTable {
   SysParam s[kMaxPass];
 };
 
+constexpr int kMaxBatch = 1024;  // systems per launch of the large-batch streaming kernel
+
+// The systems of one large-batch streaming launch (24 KB kernel parameter).
+struct SysTableBig {
+  SysParam s[kMaxBatch];
+};
+
 constexpr int kMaxPairs = 64;  // (omega, py) pairs per gradient launch
 
 // (omega, omega * py) of the pairs of one gradient launch, passed by value.

@@ -486,6 +486,7 @@ template <int N>
 __device__ __forceinline__ void bulk_wait_read() {
   asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
 }
+
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -638,6 +639,92 @@ __global__ void __launch_bounds__(T)
       __syncthreads();
       if (threadIdx.x == 0) {
         bulk_store(outp[k] + n0, buf, cnt * 16u);
+        bulk_commit();
+      }
+    }
+    p = p2;
+    d = d2;
+    mr = mr2;
+    mc = mc2;
+    pidx = pidx2;
+  }
+  if (threadIdx.x == 0) bulk_wait_all();
+}
+
+// Large-ring staging ring: as k_stream_ring, but one launch takes up to
+// kMaxBatch systems (their parameters a 24 KB __grid_constant__ argument), so
+// with a ring of more than 16 slots each CTA reads its chunk's basis entries
+// once per min(nslots, 1024) systems instead of once per 16.  A launch never
+// holds more systems than the ring has slots: two systems of one launch in the
+// same slot would overwrite each other in L2, and most of them would never
+// reach memory.
+template <int T, int NB>
+__global__ void __launch_bounds__(T)
+    k_stream_big(long long nzero, const double *__restrict__ prim, const unsigned *__restrict__ desc,
+                 const double *__restrict__ basis, long long nblocks, const int *__restrict__ pml_idx,
+                 const double2 *__restrict__ pml_delta, long long npblk,
+                 const __grid_constant__ SysTableBig tab, int s0, int s1,
+                 double *__restrict__ ring, long long stride, int nslots) {
+  extern __shared__ __align__(128) double2 stage[];  // [NB][T]
+  const int ns = s1 - s0;  // <= nslots
+  const double *mrho = basis + (size_t)B_MRHO * nblocks;
+  const double *mmu = basis + (size_t)B_MMU * nblocks;
+  const double *ml2m = basis + (size_t)B_ML2M * nblocks;
+  auto load = [&](long long n, double &p, unsigned &d, double &mr, double &mc, int &pidx) {
+    p = 0.0;
+    d = 0u;
+    mr = 0.0;
+    mc = 0.0;
+    pidx = -1;
+    if (n >= nzero) return;
+    p = __ldcs(prim + n);
+    d = __ldcs(desc + n);
+    const unsigned blk = d >> 4, i = (d >> 2) & 3u, j = d & 3u;
+    if (i == j) {
+      mr = mrho[blk];
+      mc = (i == 1u) ? ml2m[blk] : mmu[blk];
+    }
+    pidx = pml_idx[blk];
+  };
+  const long long nchunk = (nzero + T - 1) / T;
+  long long c = blockIdx.x;
+  double p, mr, mc;
+  unsigned d;
+  int pidx;
+  load(c * T + threadIdx.x, p, d, mr, mc, pidx);
+  int q = 0;  // running buffer count
+  for (; c < nchunk; c += gridDim.x) {
+    const long long n0 = c * T, n = n0 + threadIdx.x;
+    double p2, mr2, mc2;
+    unsigned d2;
+    int pidx2;
+    load((c + gridDim.x) * T + threadIdx.x, p2, d2, mr2, mc2, pidx2);  // next chunk
+    const unsigned i = (d >> 2) & 3u, j = d & 3u;
+    const bool odd = (i + j) & 1u;
+    const unsigned cnt = (unsigned)min((long long)T, nzero - n0);
+    for (int k = 0; k < ns; k++, q++) {
+      double2 *buf = stage + (size_t)(q % NB) * T;
+      if (q >= NB && threadIdx.x == 0) bulk_wait_read<NB - 1>();
+      __syncthreads();
+      if (n < nzero) {
+        const SysParam &sy = tab.s[k];
+        const double w2 = sy.w2, wpy = sy.wpy;
+        double2 v;
+        if (odd) v = make_double2(0.0, wpy * p);
+        else v = make_double2(p - w2 * mr + (wpy * wpy) * mc, 0.0);
+        if (pidx >= 0) {
+          const double2 dv = pml_delta[((size_t)sy.pml_slot * npblk + pidx) * 9 + 3 * i + j];
+          const double f = odd ? wpy : 1.0;
+          v.x += f * dv.x;
+          v.y += f * dv.y;
+        }
+        buf[threadIdx.x] = v;
+      }
+      fence_async_smem();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double2 *o = reinterpret_cast<double2 *>(ring + (size_t)((s0 + k) % nslots) * stride);
+        bulk_store(o + n0, buf, cnt * 16u);
         bulk_commit();
       }
     }
@@ -846,12 +933,43 @@ static cudaError_t stream_ring(Ctx *c, const SysTable &tab, int s0, int s1, doub
   return cudaGetLastError();
 }
 
-constexpr int kNumStreamVariants = 8;
+template <int T, int NB>
+static cudaError_t stream_big(Ctx *c, const SysParam *hsys, int s0, int s1, double *ring_base,
+                              long long slot_stride, int nslots, cudaStream_t st) {
+  SysTableBig tab;  // 24 KB; copied into the launch's parameters
+  for (int k = 0; k < kMaxBatch; k++)
+    tab.s[k] = k < s1 - s0 ? hsys[s0 + k] : SysParam{0.0, 0.0, 0, 0};
+  const size_t smem = sizeof(double2) * NB * T;
+  cudaError_t e = cudaFuncSetAttribute(k_stream_big<T, NB>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e) return e;
+  int nsm = 0, occ = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stream_big<T, NB>, T, smem);
+  if (occ < 1) occ = 1;
+  const long long nchunk = (c->nzero + T - 1) / T;
+  const unsigned grid = (unsigned)std::min<long long>((long long)nsm * occ, nchunk);
+  k_stream_big<T, NB><<<grid, T, smem, st>>>(c->nzero, c->d_prim, c->d_desc, c->d_basis,
+                                             c->bcsr.nblocks, c->d_pml_idx, c->d_pml_delta,
+                                             c->npml_blocks, tab, s0, s1, ring_base, slot_stride,
+                                             nslots);
+  return cudaGetLastError();
+}
+
+constexpr int kNumStreamVariants = 10;
+
+// systems per launch of variant v: never more than the ring's slots, so every
+// system of a launch lands in its own slot
+static int variant_batch(int v, int nslots) {
+  return std::min(v >= 8 ? kMaxBatch : kMaxPass, nslots);
+}
 static cudaError_t stream_variant(Ctx *c, int v, const SysParam *hsys, int s0, int s1,
                                   double *ring_base, long long slot_stride, int nslots,
                                   cudaStream_t st) {
   // the launch's systems travel as a kernel parameter, so a captured graph
   // keeps the values of its own call
+  if (v == 8) return stream_big<512, 4>(c, hsys, s0, s1, ring_base, slot_stride, nslots, st);
+  if (v == 9) return stream_big<256, 4>(c, hsys, s0, s1, ring_base, slot_stride, nslots, st);
   SysTable tab;
   for (int k = 0; k < kMaxPass; k++) tab.s[k] = k < s1 - s0 ? hsys[s0 + k] : SysParam{0.0, 0.0, 0, 0};
   switch (v) {
@@ -868,13 +986,14 @@ static cudaError_t stream_variant(Ctx *c, int v, const SysParam *hsys, int s0, i
 
 // The first batch of a context times the streaming variants (1, 2 or 4
 // entries per thread, software-pipelined, TMA bulk stores of all systems of a
-// chunk, TMA staging ring of 256 or 512 entries) on its first launch -- each
-// writes the same values -- and keeps the fastest for the life of the
+// chunk, TMA staging ring of 256 or 512 entries with up to 16 systems per
+// launch or, for larger rings, up to 1024) on its first launch of each -- each
+// writes the same values
+// -- compares the time per system and keeps the fastest for the life of the
 // context.  A batch recorded into a CUDA graph before any tuning uses the
 // 512-entry staging ring without timing.
 cudaError_t launch_stream_batch(Ctx *c, int n, const SysParam *hsys, double *ring_base,
                                 long long slot_stride, int nslots, cudaStream_t st) {
-  const int per = std::min(kMaxPass, nslots);
   cudaError_t e;
   int s0 = 0;
   if (c->stream_variant < 0) {
@@ -886,11 +1005,13 @@ cudaError_t launch_stream_batch(Ctx *c, int n, const SysParam *hsys, double *rin
     } else if (cs != cudaStreamCaptureStatusNone) {
       c->stream_variant = 7;
     } else {
+      // every variant writes systems [0, its first launch), each in stream
+      // order, so the slots end with the last system written
       cudaEvent_t ev[kNumStreamVariants + 1];
       for (auto &x : ev) cudaEventCreate(&x);
-      const int s1 = std::min(n, per);
       cudaEventRecord(ev[0], st);
       for (int v = 0; v < kNumStreamVariants; v++) {
+        const int s1 = std::min(n, variant_batch(v, nslots));
         if ((e = stream_variant(c, v, hsys, 0, s1, ring_base, slot_stride, nslots, st))) return e;
         cudaEventRecord(ev[v + 1], st);
       }
@@ -899,15 +1020,18 @@ cudaError_t launch_stream_batch(Ctx *c, int n, const SysParam *hsys, double *rin
       for (int v = 0; v < kNumStreamVariants; v++) {
         float t = 0.f;
         cudaEventElapsedTime(&t, ev[v], ev[v + 1]);
+        t /= (float)std::min(n, variant_batch(v, nslots));
         if (t < best) {
           best = t;
           c->stream_variant = v;
         }
       }
       for (auto &x : ev) cudaEventDestroy(x);
-      s0 = s1;
+      // the last tuning launch wrote the largest prefix; continue after it
+      s0 = std::min(n, variant_batch(kNumStreamVariants - 1, nslots));
     }
   }
+  const int per = std::min(n, variant_batch(c->stream_variant, nslots));
   for (; s0 < n; s0 += per) {
     const int s1 = std::min(n, s0 + per);
     if ((e = stream_variant(c, c->stream_variant, hsys, s0, s1, ring_base, slot_stride, nslots, st)))

@@ -135,7 +135,8 @@ int fem25_assemble_dev(fem25_ctx *ctx, char cftype, double freq, double py, doub
 /* Batched assembly of n systems (cftype[k], freq[k], py[k]) into complex128
  * device slots: system k goes to ring_base + (k % nslots) * slot_stride
  * doubles (slot_stride even and >= 2*NZERO).  Uses the per-mesh affine basis
- * (built on first use) and streaming launches of up to 16 systems.  Slots
+ * (built on first use) and streaming launches of up to min(16, nslots)
+ * systems (min(1024, nslots) with the large-ring variants).  Slots
  * that start on 128-byte boundaries (ring_base 128-byte aligned, slot_stride
  * a multiple of 16) are written faster.  The first call builds the basis and
  * times the streaming variants (synchronously); later calls only enqueue
@@ -312,8 +313,11 @@ int fem25_misfit_noalloc_dev(fem25_ctx *ctx, int nsrc, int nrec, const int *mrdo
 /* The choices of the per-context autotuners, -1 before the first call that
  * tunes them: the streaming-assembly variant (0-2: 1, 2, 4 entries per
  * thread; 3: software-pipelined; 4, 5: all systems of a 64 / 128-entry chunk
- * staged for bulk stores; 6, 7: 256 / 512-entry staging ring) and the source
- * tile of the FP64 gradient (2, 4 or 8 sources per shared-memory pass). */
+ * staged for bulk stores; 6, 7: 256 / 512-entry staging ring, 16 systems per
+ * launch; 8, 9: 512 / 256-entry staging ring, up to min(1024, nslots)
+ * systems per launch)
+ * and the source tile of the FP64 gradient (2, 4 or 8 sources per
+ * shared-memory pass). */
 int fem25_tuning(const fem25_ctx *ctx, int *stream_variant, int *grad_tile);
 int fem25_profile_enable(fem25_ctx *ctx, int enable);
 int fem25_profile_ms(fem25_ctx *ctx, int which, double *ms);

@@ -113,7 +113,7 @@ def test_batched_ring_wraps(case0):
 _VARIANT_OUT = {}
 
 
-@pytest.mark.parametrize("variant", range(8))
+@pytest.mark.parametrize("variant", range(10))
 def test_stream_variants_agree(case0, variant, monkeypatch):
     """Every streaming variant the autotuner can pick (forced through
     FEM25_STREAM_VARIANT) writes the same bits: 19 systems = one launch of 16
@@ -141,6 +141,35 @@ def test_stream_variants_agree(case0, variant, monkeypatch):
         assert torch.equal(r, _VARIANT_OUT[0])
     assert torch.count_nonzero(buf[:2]) == 0
     ctx.close()
+
+
+@pytest.mark.parametrize("variant", [8, 9])
+@pytest.mark.parametrize("nslots", [1, 3, 19])
+def test_large_ring_variants_small_rings(case0, variant, nslots, monkeypatch):
+    """The large-ring streaming variants take up to min(1024, nslots) systems
+    per launch: with small rings each slot must still end with its last
+    system, bit-identical to variant 0."""
+    mesh, pairs, g, _ = case0
+    n = 19
+    sel = [(pairs[k % len(pairs)][0] * (1.0 + 0.03 * (k // 4)), pairs[(5 * k) % len(pairs)][1])
+           for k in range(n)]
+    cft = ["S" if k % 4 == 1 else "B" for k in range(n)]
+    stride = 2 * g.nzero
+    out = {}
+    for v in (0, variant):
+        monkeypatch.setenv("FEM25_STREAM_VARIANT", str(v))
+        ctx = Context(mesh, g)
+        ring = torch.full((nslots * stride,), float("nan"), dtype=torch.float64, device=_dev())
+        ctx.assemble_batch(cft, [p[0] for p in sel], [p[1] for p in sel], ring, stride, nslots)
+        torch.cuda.synchronize()
+        assert ctx.tuning()["stream_variant"] == v
+        out[v] = ring.clone()
+        ctx.close()
+    assert torch.equal(out[0], out[variant])
+    k = n - 1
+    ref128, _ = oracle.asmble(mesh, g, cft[k], *sel[k], want64=False)
+    got = out[variant].view(nslots, stride)[k % nslots].cpu().numpy()
+    assert helpers.row_norm_err(got[0::2] + 1j * got[1::2], ref128, g.irptr) <= 1e-12
 
 
 def test_peff_matches_oracle(case0):
