@@ -2,7 +2,8 @@
 
 Headline workload (one step): the batched assembly of 512 complex128 CSR
 systems (8 frequencies 0.2-1.6 Hz x 64 ky) of the 400x120 degree-4 mesh of a
-layered model -- the "CSR assemblies/s" half of the metric.  Each rank does
+layered model into a ring of 32 slots (--nslots) -- the "CSR assemblies/s"
+half of the metric.  Each rank does
 the full 512-system batch (weak scaling, no data-path collective: the
 (omega, py) systems are independent).  Inputs (the per-mesh basis, 2.6 GB)
 and outputs (3.98 GB per system) are larger than L2, so no flush is needed.
