@@ -36,6 +36,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "CSR assemblies/s & gradient elem·rhs/s, batched-TF32x3 vs plain FP64 at 1e-6 rel"
+# streaming-kernel variant index (fem25_tuning) -> kernel
+STREAM_KERNELS = {0: "k_stream<1>", 1: "k_stream<2>", 2: "k_stream<4>", 3: "k_stream_pipe",
+                  4: "k_stream_tma<64>", 5: "k_stream_tma<128>", 6: "k_stream_ring<256, 4>",
+                  7: "k_stream_ring<512, 4>", 8: "k_stream_big<512, 4>", 9: "k_stream_big<256, 4>"}
 UNIT = "assemblies/s"
 
 
@@ -495,7 +499,8 @@ def main():
                       "setup_s": round(setup_s, 2)},
            "plain_fp64": {"value": plain_rate, "unit": UNIT, "speedup_batched": value / world / plain_rate},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "traffic": None, "kernel": "k_stream",
+                        "frac": achieved / peak, "traffic": None,
+                        "kernel": STREAM_KERNELS.get(tuning["stream_variant"], "k_stream"),
                         "kernel_ms": kms, "peak_kind": peak_kind,
                         "algorithmic_bytes": "16 B x NNZ per system (complex128 values written)"},
            "cpu_baseline": cpu, "e2e": e2e, "gradient": grad, "pipeline": pipe,
