@@ -62,7 +62,11 @@ def report_and_check(tag: str, ok: bool, msg: str = "", timeout_s: float = 60.0)
     st = _store()
     st.set(f"fem25/{tag}/{rank}", ("ok" if ok else "fail:" + msg))
     keys = [f"fem25/{tag}/{r}" for r in range(world)]
-    st.wait(keys, timedelta(seconds=timeout_s))
+    try:
+        st.wait(keys, timedelta(seconds=timeout_s))
+    except Exception:  # a rank that died or hangs never reports
+        missing = [r for r, k in enumerate(keys) if not st.check([k])]
+        raise RankFailure(f"rank(s) {missing} did not report within {timeout_s:g} s")
     bad = []
     for r, k in enumerate(keys):
         v = st.get(k).decode()
@@ -73,7 +77,7 @@ def report_and_check(tag: str, ok: bool, msg: str = "", timeout_s: float = 60.0)
 
 
 def distributed_gradient(pairs: Sequence[tuple[float, float]], partial: Callable, nnpg: int,
-                         step: int = 0, device=None):
+                         step: int = 0, device=None, timeout_s: float = 60.0):
     """Sum over ranks of ``partial(my_pair_indices) -> tensor[3, nnpg]``.
 
     ``partial`` computes this rank's gradient over its pairs (on the GPU in
@@ -91,7 +95,7 @@ def distributed_gradient(pairs: Sequence[tuple[float, float]], partial: Callable
     except Exception as e:  # reported to the other ranks below
         err = f"{type(e).__name__}: {e}"
     if world > 1:
-        report_and_check(f"grad{step}", g is not None, err)
+        report_and_check(f"grad{step}", g is not None, err, timeout_s)
     elif g is None:
         raise RankFailure(err)
     if world > 1:

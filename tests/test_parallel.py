@@ -47,6 +47,8 @@ def _worker(rank, world, port, mode, out):
     u = rng.standard_normal((len(sel), 1, g.ndof)) + 1j * rng.standard_normal((len(sel), 1, g.ndof))
     lam = rng.standard_normal((len(sel), 1, g.ndof)) + 1j * rng.standard_normal((len(sel), 1, g.ndof))
 
+    if mode == "exit" and rank == 1:
+        return  # this rank dies before the gradient: it never reports
     def partial(idx):
         if mode == "fail" and rank == 1:
             raise ValueError("injected host failure")
@@ -56,7 +58,8 @@ def _worker(rank, world, port, mode, out):
         return torch.from_numpy(out_g)
 
     try:
-        res = distributed_gradient(sel, partial, mesh.nnpg, step=0)
+        res = distributed_gradient(sel, partial, mesh.nnpg, step=0,
+                                   timeout_s=5.0 if mode == "exit" else 60.0)
         if rank == 0:
             ref = np.zeros((3, mesh.nnpg))
             for k in range(len(sel)):
@@ -68,7 +71,7 @@ def _worker(rank, world, port, mode, out):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("mode", ["ok", "fail"])
+@pytest.mark.parametrize("mode", ["ok", "fail", "exit"])
 def test_two_rank_gradient(mode):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
@@ -79,9 +82,12 @@ def test_two_rank_gradient(mode):
     for p in procs:
         p.join(timeout=120)
         assert p.exitcode == 0
-    msgs = [q.get(timeout=5) for _ in range(1 if mode == "ok" else 2)]
+    msgs = [q.get(timeout=5) for _ in range({"ok": 1, "fail": 2, "exit": 1}[mode])]
     if mode == "ok":
         assert msgs[0][0] == "ok" and msgs[0][1] < 1e-12
+    elif mode == "exit":
+        # the surviving rank learns of the dead one from the store, not a hang
+        assert msgs[0][:2] == ("failure", 0) and "rank(s) [1] did not report" in msgs[0][2]
     else:
         assert sorted(m[1] for m in msgs) == [0, 1]
         assert all("injected host failure" in m[2] for m in msgs)
