@@ -1,7 +1,7 @@
 """ctypes bindings for the CPU oracle (``oracle/fem25_oracle.c``).
 
 TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
-and the CPU-baseline / reference legs of ``bench.py``, as the checker.  The
+and the CPU-baseline / reference legs of ``bench.py``, to compare against.  The
 product library (``fem25_b200``) never imports, links or executes it.
 """
 from __future__ import annotations

@@ -1,8 +1,8 @@
 /*
  * fem25 oracle -- CPU FP64 restatement of the fem25 hot path.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA library in
- * fem25_b200/: only tests/, __graft_entry__.smoke() and the cpu_baseline /
+ * TEST INFRASTRUCTURE ONLY.  The CUDA library in fem25_b200/ is compared
+ * against this file: only tests/, __graft_entry__.smoke() and the cpu_baseline /
  * reference legs of bench.py may load it.  The product path never links it.
  *
  * Every routine restates one reference routine loop for loop (same loop
