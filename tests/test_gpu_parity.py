@@ -59,7 +59,7 @@ def test_asmble_driver_host_buffer(case0):
 
 
 def test_asmble_driver_chunked_pinned_and_pageable():
-    """The driver computes elements in up to 16 chunks and copies each chunk's
+    """fem25_asmble_driver computes elements in up to 16 chunks and copies each chunk's
     completed CSR rows while the next computes: the jittered, topographic
     layout at 48x20 elements (960 elements, 6 chunks) into pinned and
     pageable host buffers, both bit-exact to the oracle's COMPLEX*8 CDIST,
