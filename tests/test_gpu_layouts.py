@@ -6,9 +6,10 @@ Jacobian, the PML depths and the anchor interpolation away from the
 rectangular half-space the other parity tests use.
 
 Tolerances as in test_gpu_parity.py: plain FP64 CSR and the reference's
-COMPLEX*8 CDIST bit-exact; batched CSR <= 1e-12 per row; exact gradient FP64
-<= 1e-10 and 3xTF32 <= 2e-5 relative (2-norm); reference-compatible gradient
-bit-exact.
+COMPLEX*8 CDIST bit-exact (dispersive media included); batched CSR <= 1e-12
+per row; exact gradient FP64 <= 1e-10 and 3xTF32 <= 2e-5 relative (2-norm);
+reference-compatible gradient and the Hessian-path kernels (MET225_MOD,
+CADJ_NU_ALPHA, PCHADJ) bit-exact.
 """
 import numpy as np
 import pytest
@@ -94,3 +95,61 @@ def test_reference_gradient(layout):
         ctx.cfmat_adjgrad(cinv, 1.7320508075688772, f, py, torch.from_numpy(wave).to(_dev()),
                           torch.from_numpy(lam).to(_dev()), d_g)
         assert np.array_equal(d_g.cpu().numpy().view(np.uint32), ref.view(np.uint32)), cinv
+
+
+def test_dispersive_plain_assembly(layout):
+    """KMDAMP / CMDAMP with VCMPLX complex velocities on the distorted layout:
+    FP64 CSR and COMPLEX*8 CDIST bit-exact to the oracle."""
+    mesh, pairs, _, _ = layout
+    dmesh = synth.make_dispersive(mesh, 13)
+    g = oracle.graph_build(dmesh)
+    ctx = Context(dmesh, g)
+    for f, py in (pairs[2], pairs[-3]):
+        ref128, ref64 = oracle.asmble(dmesh, g, "B", f, py)
+        o128 = torch.zeros(g.nzero, dtype=torch.complex128, device=_dev())
+        o64 = torch.zeros(g.nzero, dtype=torch.complex64, device=_dev())
+        ctx.assemble("B", f, py, o128, o64)
+        torch.cuda.synchronize()
+        assert np.array_equal(o128.cpu().numpy(), ref128)
+        assert np.array_equal(o64.cpu().numpy().view(np.uint32), ref64.view(np.uint32))
+    ctx.close()
+
+
+def test_hessian_path_kernels(layout):
+    """MET225_MOD, CADJ_NU_ALPHA and PCHADJ ('PS') on the distorted layout,
+    bit-identical to the oracle."""
+    mesh, pairs, g, ctx = layout
+    rg = oracle.RefGrad(mesh, g)
+    rng = np.random.default_rng(47)
+    vec = [(rng.standard_normal(g.ndof) + 1j * rng.standard_normal(g.ndof)).astype(np.complex64)
+           for _ in range(4)]
+    d = [torch.from_numpy(v).to(_dev()) for v in vec]
+    f, py = pairs[len(pairs) // 2]
+    r1, r2 = rg.met225(f, py, *vec, cinvtype="PS")
+    p1 = torch.zeros(r1.shape, dtype=torch.float32, device=_dev())
+    p2 = torch.zeros(r2.shape, dtype=torch.float32, device=_dev())
+    ctx.met225("PS", f, py, *d, p1, p2)
+    assert np.array_equal(p1.cpu().numpy().view(np.uint32), r1.view(np.uint32))
+    assert np.array_equal(p2.cpu().numpy().view(np.uint32), r2.view(np.uint32))
+    v = rng.standard_normal(2 * rg.nnpinv).astype(np.float32)
+    rb, ra, p3 = rg.cadj_nu_alpha(f, py, v, vec[0], vec[3], cinvtype="PS")
+    d_b = torch.zeros(g.ndof, dtype=torch.complex64, device=_dev())
+    d_a = torch.zeros(g.ndof, dtype=torch.complex64, device=_dev())
+    d_p = torch.zeros(p3.shape, dtype=torch.float32, device=_dev())
+    ctx.cadj_nu_alpha("PS", f, py, torch.from_numpy(v).to(_dev()), d[0], d[3], d_b, d_a, d_p)
+    assert np.array_equal(d_b.cpu().numpy().view(np.uint32), rb.view(np.uint32))
+    assert np.array_equal(d_a.cpu().numpy().view(np.uint32), ra.view(np.uint32))
+    assert np.array_equal(d_p.cpu().numpy().view(np.uint32), p3.view(np.uint32))
+    nrhs = 5
+    grns = (rng.standard_normal((nrhs, g.ndof)) + 1j * rng.standard_normal((nrhs, g.ndof))
+            ).astype(np.complex64)
+    fmat = (rng.standard_normal((2, rg.nz)) + 1j * rng.standard_normal((2, rg.nz))
+            ).astype(np.complex64)
+    hess = np.zeros(rg.nnpinv * 4, np.float32)
+    d_h = torch.zeros(rg.nnpinv * 4, dtype=torch.float32, device=_dev())
+    jacl = rg.pchadj(grns, fmat, hess)
+    d_j = torch.zeros((rg.nnpinv * 2, nrhs), dtype=torch.complex64, device=_dev())
+    ctx.pchadj(2, nrhs, torch.from_numpy(grns).to(_dev()), torch.from_numpy(fmat).to(_dev()),
+               d_h, d_j)
+    assert np.array_equal(d_j.cpu().numpy().view(np.uint32), jacl.view(np.uint32))
+    assert np.array_equal(d_h.cpu().numpy().view(np.uint32), hess.view(np.uint32))
