@@ -488,7 +488,28 @@ def main():
                                    "peak": bpk / 6.0, "unit": "TFLOP/s", "frac": tf / (bpk / 6.0),
                                    "peak_kind": f"{bkind} bf16 burst {bpk:g} / 2 (TF32) / 3 "
                                                 f"(split products)"}
-        del u, lam
+        # the reference-compatible drop-in (CFMAT_DIST + ADJGRAD, COMPLEX*8,
+        # 'PP'): one source's virtual forces and gradient contribution
+        w32 = u[0, 0].to(torch.complex64).contiguous()
+        l32 = lam[0, 0].to(torch.complex64).contiguous()
+        nnpinv, _, _ = ctx.ref_gradient_info()
+        gl = torch.zeros(nnpinv, dtype=torch.float32, device=dev)
+        p0 = pairs[0]
+        ctx.cfmat_adjgrad("PP", 1.73, p0[0], p0[1], w32, l32, gl, stream=stream)
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        nref = 3
+        for _ in range(nref):
+            ctx.cfmat_adjgrad("PP", 1.73, p0[0], p0[1], w32, l32, gl, stream=stream)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        rms = ev[0].elapsed_time(ev[1]) / nref
+        grad["reference_path"] = {
+            "what": "fem25_ref_gradient_dev ('PP'): CFMAT_DIST virtual forces + ADJFLAM_DIST, "
+                    "one source", "ms_per_source": rms,
+            "elem_rhs_per_s": mesh.nelem / (rms / 1e3), "inversion_anchors": nnpinv}
+        del u, lam, w32, l32, gl
     tuning = ctx.tuning()
 
     pipe = None
