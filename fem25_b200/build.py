@@ -28,6 +28,7 @@ UNITS = [
     ("k_batch.cu", []),
     ("k_grad.cu", []),
     ("k_grad_tc.cu", []),
+    ("k_grad_cov.cu", []),
     ("api.cu", []),
     ("misfit_noalloc.cu", ["-fmad=false"]),
     ("dense_solve.cu", []),

@@ -96,7 +96,7 @@ void free_ctx(Ctx *c) {
                   c->d_pml_delta, c->d_jcsc, c->d_icsc, c->d_rg_anchor, c->d_mconn,
                   c->d_elem_wts, c->d_fmat, c->d_cadj_col0, c->d_cadj_pair_col, c->d_cadj_pair_elem,
                   c->d_cadj_dptr, c->d_cadj_dent, c->d_cadj_w, c->d_nonpml, c->d_cdist, c->d_prim, c->d_desc,
-                  c->d_tc_tab, c->d_qp, c->d_qs};
+                  c->d_tc_tab, c->d_qp, c->d_qs, c->d_cov};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &e : c->ev)
@@ -664,19 +664,72 @@ int fem25_addblk_dev(fem25_ctx *h, int nsrc, const float *ue, float *sol, void *
   return FEM25_OK;
 }
 
-int fem25_gradient_dev(fem25_ctx *h, int npairs, const double *freq, const double *py, int nsrc,
-                       const double *u, const double *lam, int prec, double *grad, void *stream) {
-  if (!h || !freq || !py || !u || !lam || !grad || npairs <= 0 || nsrc <= 0) return FEM25_ERR_ARG;
-  Ctx *c = &h->c;
+// Checks shared by the gradient entry points; 0 or an error status.
+static int grad_args(Ctx *c, int npairs, const double *freq, const double *py, int nsrc,
+                     const double *u, const double *lam) {
+  if (!freq || !py || !u || !lam || npairs <= 0 || nsrc <= 0) return FEM25_ERR_ARG;
   if (c->mesh_scalars.ldisp)
     return fail(c, FEM25_ERR_UNSUPPORTED, "gradient: dispersive media are not supported");
-  if (prec != FEM25_PREC_FP64 && prec != FEM25_PREC_TF32X3)
-    return fail(c, FEM25_ERR_ARG, "gradient: unknown precision");
   if ((long long)npairs * nsrc > (1LL << 30))
     return fail(c, FEM25_ERR_ARG, "gradient: more than 2^30 (pair, source) fields");
+  return 0;
+}
+
+// (omega, omega * py) of pairs [p0, p0 + np) as one launch's parameter table
+static PairTable pair_table(const double *freq, const double *py, int p0, int np) {
+  PairTable pt;
+  for (int k = 0; k < kMaxPairs; k++) {
+    const double omega = k < np ? 6.2831853071795862 * freq[p0 + k] : 0.0;
+    pt.p[k] = make_double2(omega, k < np ? omega * py[p0 + k] : 0.0);
+  }
+  return pt;
+}
+
+// One-time set-up of the covariance gradient (allocates: not inside a capture).
+static int ensure_cov(Ctx *c, cudaStream_t st) {
+  if (c->d_cov) return 0;
+  if (capturing(st))
+    return fail(c, FEM25_ERR_ARG,
+                "gradient: make one uncaptured split-precision call before capturing");
+  cudaError_t e = prepare_grad_cov(c);
+  if (e == cudaErrorNotSupported)
+    return fail(c, FEM25_ERR_UNSUPPORTED, "gradient: split-precision path not available");
+  if (e != cudaSuccess) return fail(c, FEM25_ERR_CUDA, std::string("gradient (tf32x3) set-up: ") +
+                                                           cudaGetErrorString(e));
+  return 0;
+}
+
+// Adds the covariances of pairs' fields into the context's accumulators, 64
+// pairs per launch.
+static int cov_accumulate(Ctx *c, int npairs, const double *freq, const double *py, int nsrc,
+                          const double *u, const double *lam, cudaStream_t st) {
+  const size_t per_pair = (size_t)nsrc * c->ndof * 2;  // doubles of one pair's fields
+  for (int p0 = 0; p0 < npairs; p0 += kMaxPairs) {
+    const int np = std::min(kMaxPairs, npairs - p0);
+    CK(launch_grad_cov(c, pair_table(freq, py, p0, np), np, nsrc, u + p0 * per_pair,
+                       lam + p0 * per_pair, st),
+       "gradient (tf32x3) accumulation");
+  }
+  return FEM25_OK;
+}
+
+int fem25_gradient_dev(fem25_ctx *h, int npairs, const double *freq, const double *py, int nsrc,
+                       const double *u, const double *lam, int prec, double *grad, void *stream) {
+  if (!h || !grad) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  int r = grad_args(c, npairs, freq, py, nsrc, u, lam);
+  if (r) return r;
+  if (prec != FEM25_PREC_FP64 && prec != FEM25_PREC_TF32X3 && prec != FEM25_PREC_TF32X3_POINTWISE)
+    return fail(c, FEM25_ERR_ARG, "gradient: unknown precision");
   cudaStream_t st = (cudaStream_t)stream;
   CK(cudaSetDevice(c->device), "set device");
-  if (prec == FEM25_PREC_TF32X3 && !c->d_tc_tab) {
+  if (prec == FEM25_PREC_TF32X3) {
+    if ((r = ensure_cov(c, st))) return r;
+    if ((r = cov_accumulate(c, npairs, freq, py, nsrc, u, lam, st))) return r;
+    CK(launch_grad_cov_fin(c, grad, st), "gradient (tf32x3) contraction");
+    return FEM25_OK;
+  }
+  if (prec == FEM25_PREC_TF32X3_POINTWISE && !c->d_tc_tab) {
     if (capturing(st))
       return fail(c, FEM25_ERR_ARG,
                   "gradient: make one uncaptured split-precision call before capturing");
@@ -690,11 +743,7 @@ int fem25_gradient_dev(fem25_ctx *h, int npairs, const double *freq, const doubl
   const size_t per_pair = (size_t)nsrc * c->ndof * 2;  // doubles of one pair's fields
   for (int p0 = 0; p0 < npairs; p0 += kMaxPairs) {
     const int np = std::min(kMaxPairs, npairs - p0);
-    PairTable pt;
-    for (int k = 0; k < kMaxPairs; k++) {
-      const double omega = k < np ? 6.2831853071795862 * freq[p0 + k] : 0.0;
-      pt.p[k] = make_double2(omega, k < np ? omega * py[p0 + k] : 0.0);
-    }
+    const PairTable pt = pair_table(freq, py, p0, np);
     const double *uk = u + p0 * per_pair, *lk = lam + p0 * per_pair;
     if (prec == FEM25_PREC_FP64) {
       CK(launch_grad_plain(c, pt, np, nsrc, uk, lk, grad, st), "gradient");
@@ -702,6 +751,29 @@ int fem25_gradient_dev(fem25_ctx *h, int npairs, const double *freq, const doubl
       CK(launch_grad_tc(c, pt, np, nsrc, uk, lk, grad, st), "gradient (tf32x3)");
     }
   }
+  return FEM25_OK;
+}
+
+int fem25_gradient_accumulate_dev(fem25_ctx *h, int npairs, const double *freq, const double *py,
+                                  int nsrc, const double *u, const double *lam, void *stream) {
+  if (!h) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  int r = grad_args(c, npairs, freq, py, nsrc, u, lam);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaSetDevice(c->device), "set device");
+  if ((r = ensure_cov(c, st))) return r;
+  return cov_accumulate(c, npairs, freq, py, nsrc, u, lam, st);
+}
+
+int fem25_gradient_finalize_dev(fem25_ctx *h, double *grad, void *stream) {
+  if (!h || !grad) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  if (c->mesh_scalars.ldisp)
+    return fail(c, FEM25_ERR_UNSUPPORTED, "gradient: dispersive media are not supported");
+  CK(cudaSetDevice(c->device), "set device");
+  if (!c->d_cov || !c->cov_pending) return FEM25_OK;  // nothing accumulated
+  CK(launch_grad_cov_fin(c, grad, (cudaStream_t)stream), "gradient (tf32x3) contraction");
   return FEM25_OK;
 }
 

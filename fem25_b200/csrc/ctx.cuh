@@ -130,6 +130,10 @@ struct Ctx {
   int *d_nonpml = nullptr;       // ids of the elements outside the PML
   int n_nonpml = 0;
   unsigned char *d_tc_tab = nullptr;  // SHL tables of the tensor-core gradient (tf32 hi/lo)
+  // covariance gradient: per element outside the PML, 15 FP64 blocks of
+  // 25 x 25 field covariances; pending = holds sums not yet contracted
+  double *d_cov = nullptr;
+  bool cov_pending = false;
   // cached COMPLEX*8 device buffer of fem25_asmble_driver, and its pipeline:
   // element chunk k = [drv_elem[k], drv_elem[k+1]) completes the CSR rows
   // [drv_row[k], drv_row[k+1]), whose values are gathered and copied to the
@@ -167,6 +171,10 @@ cudaError_t launch_grad_plain(Ctx *c, const PairTable &pt, int npairs, int nsrc,
 cudaError_t prepare_grad_tc(Ctx *c);
 cudaError_t launch_grad_tc(Ctx *c, const PairTable &pt, int npairs, int nsrc, const double *u,
                            const double *lam, double *grad, cudaStream_t st);
+cudaError_t prepare_grad_cov(Ctx *c);
+cudaError_t launch_grad_cov(Ctx *c, const PairTable &pt, int npairs, int nsrc, const double *u,
+                            const double *lam, cudaStream_t st);
+cudaError_t launch_grad_cov_fin(Ctx *c, double *grad, cudaStream_t st);
 cudaError_t launch_ref_cfmat(Ctx *c, int lisp, double vpvs, double omega, double py,
                              const float *wave, int accumulate, cudaStream_t st);
 cudaError_t launch_ref_adjflam(Ctx *c, const float *adjlam, float *gradl, cudaStream_t st);

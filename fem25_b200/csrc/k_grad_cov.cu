@@ -1,0 +1,739 @@
+// Exact lambda/mu/rho adjoint gradient through per-element field
+// covariances: a tcgen05 accumulation in split precision (3xTF32, FP32 in
+// TMEM, FP64 across (omega, py) pairs) followed by an FP64 contraction.
+//
+// For an element outside the PML the 2.5D operator is affine in the pair
+// weights (estiff25.f:64-154): A = K0 + i wpy K1 - w^2 M + wpy^2 Mc with
+// w = omega, wpy = omega * py, and every part is bilinear in the nodal
+// values.  The gradient sum over pairs p and sources s,
+//     g_m = sum_{p,s} Re( lam_ps^H (dA_p/dm) u_ps ),
+// therefore only needs, per element, the weighted covariances of the nodal
+// fields (c, d: component of lam, u; i, j: element node; C = conj(lam) u^T)
+//     R_cd = sum Re C_cd              (c,d) in {00, 02, 20, 22, 11}
+//     P_c  = sum wpy^2 Re C_cc        W_c = sum w^2 Re C_cc
+//     I_cd = sum wpy Im C_cd          (c,d) in {01, 21, 10, 12}
+// fifteen 25 x 25 blocks whose sums run over every (pair, source) of every
+// call, and one contraction of the blocks with the shape-function tables,
+// the inverse Jacobian and the anchor weights W_q SF_a(q) at the 169
+// points (the bilinear forms of KM25ISOQ, estiff25.f:64-154, written out in
+// the blocks).  The per-(element, pair, source) work is a rank-2 real update
+// of a 75 x 150 matrix -- a GEMM over the sources -- instead of
+// interpolating both fields at the 169 points.
+//
+// Accumulation (k_grad_cov): one persistent CTA per SM.  Per element and
+// pair, D[lam row][u column] += sum_k A[row][k] B[column][k] with
+// K = (source, re/im):
+//     A[32c + a][2s, 2s+1]     = (Re lam, Im lam)           of component c, node a
+//     B[25d + b][2s, 2s+1]     = (Re u, Im u)               -> D = Re conj(lam) u
+//     B[80 + 25d + b][2s, 2s+1] = (Im u, -Re u)             -> D = Im conj(lam) u
+// M = 128 (75 rows used), N = 160 (150 used), 16 sources (K = 32) per
+// stage, x = hi + lo split with D = A_hi B_hi + A_lo B_hi + A_hi B_lo.
+//   warps 7, 11, 15, 19, 20-23  producers: copy the stage's nodal values
+//                (complex128) into one of 5 raw shared-memory stages
+//   warp 3       MMA issuer (one thread), two TMEM accumulators of 160
+//                columns (one per stage in flight)
+//   15 warps     epilogue: convert the next stage's raw values into tf32
+//                hi/lo operand tiles (one of 3), then drain this stage:
+//                warp w (w < 20, w % 4 = c < 3) owns one of the five blocks
+//                of lam component c (TMEM lanes 32c..32c+24, lane = node),
+//                reads its 25 columns and adds them, weighted, into 25 FP64
+//                registers; at the end of the element it writes (or adds)
+//                the block row to memory.
+// The epilogue warps sit on scheduler partitions 0-2 (their TMEM lane
+// quarters), so the conversion, the largest share of the instructions, is
+// spread over three partitions instead of queueing behind the copies.
+// Hand-offs are mbarriers; every wait is bounded and a wait that runs out
+// sets the error word and drains the schedule without waiting.
+//
+// Contraction (k_grad_cov_fin, FP64): per element the blocks are combined
+// (symmetric parts of R_00, R_22, R_11; S = R_02 + R_20^T;
+// G_1 = I_01 - I_10^T, G_2 = I_21 - I_12^T; P_1, P_0 + P_2, W_0 + W_1 + W_2)
+// and each is contracted with the tensor-product shape functions,
+// N_a(xi_x, eta_z) = l_ax(xi_x) l_ae(eta_z) (dshl.f:100-243), by sum
+// factorisation: Z = B l_e, Y = Z l_x, F(q) = T(q)^T Y(q), about 0.6 M FMA
+// per element, independent of the number of pairs and sources.
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "ctx.cuh"
+#include "kcommon.cuh"
+#include "tcgen05.cuh"
+
+namespace fem25 {
+
+namespace cov {
+constexpr int kG = 8;                        // sources per stage
+constexpr int kGhBits = 2;                   // log2(kG / 2)
+constexpr int kK = 2 * kG;                   // K columns per stage (re, im)
+constexpr int kM = 128;
+constexpr int kN = 192;                      // B rows: a 32-row slot per (part, component)
+constexpr int kNIm = 96;                     // first row of the Im part
+constexpr uint32_t kALbo = kM / 8 * 128;     // 2048 B between K chunks of A
+constexpr uint32_t kBLbo = kN / 8 * 128;     // 3072 B between K chunks of B
+constexpr int kATile = (int)kALbo * (kK / 4);  // 8 KB
+constexpr int kBTile = (int)kBLbo * (kK / 4);  // 12 KB
+constexpr int kBImOff = kNIm / 8 * 128;      // 1536 B from a Re row of B to its Im row
+constexpr int kStage = 2 * kATile + 2 * kBTile;  // A_hi, A_lo, B_hi, B_lo: 40 KB
+constexpr int kNB = 3;                       // operand stages in the ring
+constexpr int kThreads = 768;                // 24 warps
+constexpr int kMmaWarp = 3;
+constexpr int kEpiWarps = 15;
+constexpr int kProdWarps = 8;
+constexpr int kEpiThreads = kEpiWarps * 32;
+constexpr int kProdThreads = kProdWarps * 32;
+constexpr int kSlotsPer = 6;                 // values per producer thread and stage: 2 fields x 3 components
+constexpr int kRawStage = kSlotsPer * kProdThreads * 16;  // 24 KB of raw complex128 values per stage
+constexpr int kRawD = 4;                     // raw stages (kRawD - 1 copy groups in flight)
+constexpr int kSmemBytes = kNB * kStage + kRawD * kRawStage;  // 216 KB
+constexpr int kDrain = 2;                    // stages per TMEM accumulation (FP32 sums of 2 kDrain kG)
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kTmemStage = 256;
+constexpr int kBlocks = 15;
+constexpr int kBlk = kNen * kNen + 1;        // 625 doubles per block, padded to 16 bytes
+static_assert(kProdThreads == 32 * kG, "one producer thread per (node slot, source)");
+static_assert((1 << kGhBits) == kG / 2, "source-pair bits");
+static_assert(kSmemBytes <= 227 * 1024, "shared memory");
+}  // namespace cov
+
+constexpr uint32_t kCovIdesc = tf32_idesc(cov::kM, cov::kN);
+
+// Epilogue role of warp w (w < 20, c = w % 4 < 3, k = w / 4): the block it
+// accumulates (index into R00 R02 R20 R22 R11 P0 P1 P2 W0 W1 W2 I01 I21 I10
+// I12), its first TMEM column and its weight (0: 1, 1: wpy^2, 2: w^2, 3: wpy).
+__device__ __forceinline__ void cov_role(int c, int k, int &blk, int &col, int &wt) {
+  // g: 0-2 Re of u component g, 3-5 Im of u component g-3; column 32g
+  int g;
+  switch (c * 5 + k) {
+    case 0: blk = 0; g = 0; wt = 0; break;    // lam_0: R00
+    case 1: blk = 1; g = 2; wt = 0; break;    //        R02
+    case 2: blk = 5; g = 0; wt = 1; break;    //        P0
+    case 3: blk = 8; g = 0; wt = 2; break;    //        W0
+    case 4: blk = 11; g = 4; wt = 3; break;   //        I01
+    case 5: blk = 4; g = 1; wt = 0; break;    // lam_1: R11
+    case 6: blk = 13; g = 3; wt = 3; break;   //        I10
+    case 7: blk = 6; g = 1; wt = 1; break;    //        P1
+    case 8: blk = 9; g = 1; wt = 2; break;    //        W1
+    case 9: blk = 14; g = 5; wt = 3; break;   //        I12
+    case 10: blk = 2; g = 0; wt = 0; break;   // lam_2: R20
+    case 11: blk = 3; g = 2; wt = 0; break;   //        R22
+    case 12: blk = 7; g = 2; wt = 1; break;   //        P2
+    case 13: blk = 10; g = 2; wt = 2; break;  //        W2
+    default: blk = 12; g = 4; wt = 3; break;  //        I21
+  }
+  col = 32 * g;
+}
+
+struct CovArgs {
+  int npairs, nsrc, ndof, n_elem;
+  int add;  // 1: add into the accumulators, 0: overwrite them
+};
+
+__global__ void __launch_bounds__(cov::kThreads, 1)
+    k_grad_cov(CovArgs ga, const int *__restrict__ elems, const int *__restrict__ lm, PairTable pt,
+               const double2 *__restrict__ u, const double2 *__restrict__ lam,
+               double *__restrict__ acc_out, int *__restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  __shared__ uint64_t bar_bfull[cov::kNB], bar_bempty[cov::kNB], bar_tfull[2], bar_tempty[2];
+  __shared__ uint64_t bar_drain;
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int drain_s;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  volatile int *drain = &drain_s;
+
+  // ---- set-up: zeroed stages (rows and columns no conversion writes stay
+  // zero), barriers, TMEM
+  for (int i = tid * 16; i < cov::kSmemBytes; i += cov::kThreads * 16)
+    *reinterpret_cast<uint4 *>(sm + i) = make_uint4(0, 0, 0, 0);
+  if (tid == 0) {
+    drain_s = 0;
+    // multi-warp hand-offs count warps: each warp syncs, then one lane arrives
+    for (int b = 0; b < cov::kNB; b++) {
+      mbar_init(smem_u32(&bar_bfull[b]), cov::kProdWarps);
+      mbar_init(smem_u32(&bar_bempty[b]), 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(smem_u32(&bar_tfull[b]), 1);
+      mbar_init(smem_u32(&bar_tempty[b]), cov::kEpiWarps);
+    }
+    mbar_init(smem_u32(&bar_drain), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == cov::kMmaWarp) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_s)),
+                 "r"(cov::kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base_s;
+  const int nch = (ga.nsrc + cov::kG - 1) / cov::kG;  // stages per (element, pair)
+  const int my_elems = (ga.n_elem - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const uint32_t total = (uint32_t)max(my_elems, 0) * (uint32_t)ga.npairs * (uint32_t)nch;
+  const bool epi = warp < 20 && (warp & 3) != 3;
+
+  if (warp != cov::kMmaWarp && !epi) {
+    // =================== producers (warps 7, 11, 15, 19, 20-23)
+    // Thread pt (0..255) owns node a = 8 ah + a7 and source g = 2 gh + g1 of
+    // every stage (a7 = pt bits 0-2, g1 = bit 3, ah = bits 4-5, gh = bits
+    // 6-7; a >= 25: no node): it copies the node's three DOFs of u and of
+    // lam (two 48-byte runs; GENID numbers a node's DOFs consecutively) into
+    // its own raw slots by cp.async (zero-filled for a fixed node or a
+    // source past nsrc), kRawD - 1 stages ahead, and converts them itself
+    // (FP64 -> tf32 hi/lo) into A rows 32c + a (lam) and B rows 32c + a,
+    // 96 + 32c + a (u) at K = 2g.  A warp's 32 threads cover the 16
+    // (row mod 8, g mod 2) shared-memory bank classes twice, so each 8-byte
+    // tile store is two wavefronts.
+    const int pt0 = (warp < 20 ? (warp >> 2) - 1 : warp - 16) * 32 + lane;
+    const int a = ((pt0 >> 4) & 3) * 8 + (pt0 & 7);
+    const int g = ((pt0 >> 6) & (cov::kG / 2 - 1)) * 2 + ((pt0 >> 3) & 1);
+    const bool node = a < kNen;
+    const uint32_t to_a = kmajor_off(a, 2 * g, cov::kALbo);                        // A row a
+    const uint32_t to_b = 2 * cov::kATile + kmajor_off(a, 2 * g, cov::kBLbo);      // B row a
+    uint8_t *raw = sm + cov::kNB * cov::kStage;
+    int d0 = 0, d0_next = 0;  // first DOF of the node in this / the next element (0: fixed)
+    int iei = blockIdx.x, ip = 0, ich = 0;  // next stage to copy
+    uint32_t issued = 0;
+    auto node_dof = [&](int eidx) -> int {
+      return (node && eidx < ga.n_elem) ? __ldg(lm + (size_t)elems[eidx] * kNee + 3 * a) : 0;
+    };
+    auto issue = [&]() {
+      const bool act = d0 > 0 && g < ga.nsrc - ich * cov::kG;
+      const size_t off = act ? ((size_t)ip * ga.nsrc + (size_t)ich * cov::kG + g) * ga.ndof + d0 - 1 : 0;
+      const uint32_t rs = smem_u32(raw + (issued % cov::kRawD) * cov::kRawStage) + pt0 * 16;
+      const uint32_t n = act ? 16u : 0u;
+      if (node) {
+#pragma unroll
+        for (int j = 0; j < cov::kSlotsPer; j++) {
+          const double2 *src = (j < 3 ? u : lam) + off + j % 3;
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(
+                           rs + j * cov::kProdThreads * 16),
+                       "l"(src), "r"(n)
+                       : "memory");
+        }
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+      issued++;
+      if (++ich == nch) {
+        ich = 0;
+        if (++ip == ga.npairs) {
+          ip = 0;
+          iei += gridDim.x;
+          d0 = d0_next;
+          d0_next = node_dof(iei + (int)gridDim.x);  // in flight until the next element
+        }
+      }
+    };
+    if (total > 0) {
+      d0 = node_dof(iei);
+      d0_next = node_dof(iei + (int)gridDim.x);
+    }
+    while (issued < total && issued < (uint32_t)(cov::kRawD - 1)) issue();
+    for (uint32_t s = 0; s < total; s++) {
+      if (issued < total) issue();  // stage s + kRawD - 1 into this thread's slots of s - 1
+      // copy groups still allowed in flight once stage s has landed
+      switch (issued - s - 1) {
+        case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+        case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+        case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+        default: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+      }
+      const int bs = (int)(s % cov::kNB);
+      mbar_wait(smem_u32(&bar_bempty[bs]), ((s / cov::kNB) & 1u) ^ 1u, drain, err, -2000001);
+      if (node) {
+        const uint8_t *rs = raw + (s % cov::kRawD) * cov::kRawStage + pt0 * 16;
+        uint8_t *st = sm + bs * cov::kStage;
+#pragma unroll
+        for (int j = 0; j < cov::kSlotsPer; j++) {
+          const double2 v = *reinterpret_cast<const double2 *>(rs + j * cov::kProdThreads * 16);
+          const float xr = (float)v.x, xi = (float)v.y;
+          const uint32_t hr = to_tf32(xr), hi = to_tf32(xi);
+          const uint32_t lr = to_tf32(xr - __uint_as_float(hr));
+          const uint32_t li = to_tf32(xi - __uint_as_float(hi));
+          const int c = j % 3;  // rows 32c + a: 4c core-matrix groups further
+          if (j < 3) {  // u -> B Re row and Im row, hi then lo
+            uint8_t *d = st + to_b + 512 * c;
+            *reinterpret_cast<uint2 *>(d) = make_uint2(hr, hi);
+            *reinterpret_cast<uint2 *>(d + cov::kBTile) = make_uint2(lr, li);
+            *reinterpret_cast<uint2 *>(d + cov::kBImOff) = make_uint2(hi, hr ^ 0x80000000u);
+            *reinterpret_cast<uint2 *>(d + cov::kBTile + cov::kBImOff) =
+                make_uint2(li, lr ^ 0x80000000u);
+          } else {  // lam -> A row (hi, then lo)
+            uint8_t *d = st + to_a + 512 * c;
+            *reinterpret_cast<uint2 *>(d) = make_uint2(hr, hi);
+            *reinterpret_cast<uint2 *>(d + cov::kATile) = make_uint2(lr, li);
+          }
+        }
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&bar_bfull[bs]));
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (warp == cov::kMmaWarp) {
+    // =================== MMA issuer
+    if (lane == 0) {
+      const uint32_t sbase = smem_u32(sm);
+      const uint64_t adesc = umma_desc(sbase, cov::kALbo, 128);
+      const uint64_t bdesc = umma_desc(sbase, cov::kBLbo, 128);
+      uint32_t s = 0, unit = 0;
+      for (int ei = blockIdx.x; ei < ga.n_elem; ei += gridDim.x) {
+        for (int p = 0; p < ga.npairs; p++) {
+          for (int ch = 0; ch < nch; ch++, s++) {
+            // a TMEM accumulator takes kDrain stages of one pair (FP32 sums
+            // of at most 2 kDrain kG products), then the epilogue adds it in FP64
+            const bool first = ch % cov::kDrain == 0;
+            const bool last = ch % cov::kDrain == cov::kDrain - 1 || ch == nch - 1;
+            const int ts = (int)(unit & 1u), bs = (int)(s % cov::kNB);
+            if (first)
+              mbar_wait(smem_u32(&bar_tempty[ts]), ((unit >> 1) & 1u) ^ 1u, drain, err, -2000002);
+            mbar_wait(smem_u32(&bar_bfull[bs]), (s / cov::kNB) & 1u, drain, err, -2000003);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t td = tmem + (uint32_t)ts * cov::kTmemStage;
+            const int nact = min(cov::kG, ga.nsrc - ch * cov::kG);
+            const int nks = (nact + 3) / 4;  // K steps of 8 = 4 sources
+            const uint32_t so = (uint32_t)(bs * cov::kStage);
+            for (int ks = 0; ks < nks; ks++) {
+              const uint64_t ahi = adesc + (uint64_t)((so + 2 * ks * cov::kALbo) >> 4);
+              const uint64_t alo = ahi + (uint64_t)(cov::kATile >> 4);
+              const uint64_t bhi =
+                  bdesc + (uint64_t)((so + 2 * cov::kATile + 2 * ks * cov::kBLbo) >> 4);
+              const uint64_t blo = bhi + (uint64_t)(cov::kBTile >> 4);
+              mma_tf32(td, ahi, bhi, kCovIdesc, (first && ks == 0) ? 0u : 1u);
+              mma_tf32(td, alo, bhi, kCovIdesc, 1u);
+              mma_tf32(td, ahi, blo, kCovIdesc, 1u);
+            }
+            mma_commit(smem_u32(&bar_bempty[bs]));
+            if (last) {
+              mma_commit(smem_u32(&bar_tfull[ts]));
+              unit++;
+            }
+          }
+        }
+      }
+      // every MMA issued above has completed once this commit arrives
+      mma_commit(smem_u32(&bar_drain));
+      const long long t0 = clock64();
+      while (!mbar_try_wait(smem_u32(&bar_drain), 0u)) {
+        if (clock64() - t0 > kTcSpinCycles) {
+          atomicCAS(err, 0, -2000004);
+          break;
+        }
+      }
+    }
+    __syncwarp();
+  } else {
+    // =================== epilogue (15 warps)
+    const int c = warp & 3, k = warp >> 2;
+    int blk, col0, wt;
+    cov_role(c, k, blk, col0, wt);
+    const uint32_t lane_base = (uint32_t)(32 * c) << 16;
+    double acc[kNen];
+#pragma unroll
+    for (int j = 0; j < kNen; j++) acc[j] = 0.0;
+    uint32_t unit = 0;  // TMEM accumulations so far
+    for (int ei = blockIdx.x; ei < ga.n_elem; ei += gridDim.x) {
+      for (int p = 0; p < ga.npairs; p++) {
+        const double2 pr = pt.p[p];
+        const double w = wt == 0 ? 1.0 : wt == 1 ? pr.y * pr.y : wt == 2 ? pr.x * pr.x : pr.y;
+        for (int ch = 0; ch < nch; ch += cov::kDrain, unit++) {
+          const int ts = (int)(unit & 1u);
+          mbar_wait(smem_u32(&bar_tfull[ts]), (unit >> 1) & 1u, drain, err, -2000005);
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t tb = tmem + lane_base + (uint32_t)ts * cov::kTmemStage + (uint32_t)col0;
+          __syncwarp();
+          uint32_t r[16];
+          tmem_ld16(tb, r);
+          tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 16; j++) acc[j] += w * (double)__uint_as_float(r[j]);
+          tmem_ld16(tb + 16u, r);
+          tmem_wait_ld();
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(smem_u32(&bar_tempty[ts]));
+#pragma unroll
+          for (int j = 16; j < kNen; j++) acc[j] += w * (double)__uint_as_float(r[j - 16]);
+        }
+      }
+      // block row `lane` of this element, stored transposed ([j][i]) so that
+      // the 25 lanes of a store are consecutive
+      if (lane < kNen) {
+        double *dst = acc_out + ((size_t)ei * cov::kBlocks + blk) * cov::kBlk + lane;
+        if (ga.add) {
+#pragma unroll
+          for (int j = 0; j < kNen; j++) atomicAdd(dst + kNen * j, acc[j]);  // one adder per word
+        } else {
+#pragma unroll
+          for (int j = 0; j < kNen; j++) dst[kNen * j] = acc[j];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kNen; j++) acc[j] = 0.0;
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == cov::kMmaWarp) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cov::kTmemCols)
+                 : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 contraction of the accumulated blocks
+// ---------------------------------------------------------------------------
+// Per element and combined block B (9 of them), with the shape functions
+// T_t(q)_(ix + 5 ie) = X_t(qx, ix) E_t(qz, ie) for t = N (X = l, E = l),
+// xi (l', l), eta (l, l'):
+//   Z_A[i][jx][qz]      = sum_je B[i][jx + 5 je] A(qz, je)                A = l, l'
+//   W_EA[ix][jx][qz]    = sum_ie E(qz, ie) Z_A[ix + 5 ie][jx][qz]        E = l, l'
+//   F^{t1 t2}(qz, qx)   = sum_jx X_t2(qx, jx) sum_ix X_t1(qx, ix) W_{E_t1 A_t2}[ix][jx][qz]
+// = T_t1(q)^T B T_t2(q): about 0.28 M FMA per element.
+namespace covf {
+constexpr int kThreads = 256;
+constexpr int kRawMax = 3;                   // raw blocks behind one combined block
+constexpr int kRaw = kRawMax * cov::kBlk;    // doubles per raw buffer
+constexpr int kZ = kNen * kNl * kNint;       // 1625: Z[i][jx][qz]
+constexpr int kW = kNl * kNl * kNint;        // 325: W[ix][jx][qz]
+constexpr int kSmemDoubles = 2 * kRaw + 2 * kZ + 4 * kW + 2 * kNint * kNl + 4 * kNq;
+constexpr int kSmemBytes = kSmemDoubles * 8;  // 72 KB: three CTAs per SM
+}  // namespace covf
+
+// 1D Lagrange factors of the element's shape functions at the 13 points:
+// l[q][i] = l_i(x_q), d[q][i] = l_i'(x_q)  (SHL = l(xi) l(eta), dshl.f:100-243)
+struct CovFinTabs {
+  double l[kNint][kNl];
+  double d[kNint][kNl];
+};
+
+// raw blocks behind combined block b (stored [j][i]): first index and count
+__device__ __forceinline__ void cov_raw_of(int b, int *ids, int &n) {
+  switch (b) {
+    case 0: ids[0] = 0; n = 1; break;                  // R00
+    case 1: ids[0] = 3; n = 1; break;                  // R22
+    case 2: ids[0] = 4; n = 1; break;                  // R11
+    case 3: ids[0] = 1; ids[1] = 2; n = 2; break;      // R02, R20
+    case 4: ids[0] = 11; ids[1] = 13; n = 2; break;    // I01, I10
+    case 5: ids[0] = 12; ids[1] = 14; n = 2; break;    // I21, I12
+    case 6: ids[0] = 6; n = 1; break;                  // P1
+    case 7: ids[0] = 5; ids[1] = 7; n = 2; break;      // P0, P2
+    default: ids[0] = 8; ids[1] = 9; ids[2] = 10; n = 3; break;  // W0, W1, W2
+  }
+}
+
+// combined block b at (i, j) from its raw blocks r (r + k * kBlk: k-th raw)
+__device__ __forceinline__ double cov_bval(int b, const double *r, int i, int j) {
+  const int ij = j * kNen + i, ji = i * kNen + j;  // r[ij] = R[i][j]
+  switch (b) {
+    case 0: case 1: case 2: return 0.5 * (r[ij] + r[ji]);           // symmetric part
+    case 3: return r[ij] + r[cov::kBlk + ji];                        // R02 + R20^T
+    case 4: case 5: return r[ij] - r[cov::kBlk + ji];                // I01 - I10^T, I21 - I12^T
+    case 6: return r[ij];
+    case 7: return r[ij] + r[cov::kBlk + ij];
+    default: return r[ij] + r[cov::kBlk + ij] + r[2 * cov::kBlk + ij];
+  }
+}
+
+// sum_jx x2[jx] sum_ix x1[ix] W[ix][jx][qz]
+__device__ __forceinline__ double cov_fw(const double *W, int qz, const double *x1,
+                                         const double *x2) {
+  double f = 0.0;
+#pragma unroll
+  for (int jx = 0; jx < kNl; jx++) {
+    double h = 0.0;
+#pragma unroll
+    for (int ix = 0; ix < kNl; ix++) h = fma(x1[ix], W[(ix * kNl + jx) * kNint + qz], h);
+    f = fma(x2[jx], h, f);
+  }
+  return f;
+}
+
+__global__ void __launch_bounds__(covf::kThreads, 3)
+    k_grad_cov_fin(MeshView mv, DevTables dt, int n_elem, int nnpg, const int *__restrict__ elems,
+                   const double *__restrict__ accb, CovFinTabs tb, double *__restrict__ grad,
+                   int *__restrict__ err) {
+  extern __shared__ __align__(16) double fs[];
+  double *rawb = fs;                          // [2][kRaw]
+  double *zl = rawb + 2 * covf::kRaw, *zd = zl + covf::kZ;
+  double *wb = zd + covf::kZ;                 // [4][kW]: (E, A) = (l,l) (l,l') (l',l) (l',l')
+  double *tl_s = wb + 4 * covf::kW, *td_s = tl_s + kNint * kNl;  // 1D tables
+  double *wsf_s = td_s + kNint * kNl;         // [4][169] W_q SF_a(q)
+  __shared__ double red[12][covf::kThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int k = tid; k < kNint * kNl; k += covf::kThreads) {
+    tl_s[k] = tb.l[k / kNl][k % kNl];
+    td_s[k] = tb.d[k / kNl][k % kNl];
+  }
+  const bool ptq = tid < kNq;
+  const int q = ptq ? tid : 0, qx = q % kNint, qz = q / kNint;
+  const int my_elems = (n_elem - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int ntask = max(my_elems, 0) * 9;     // tasks (element, combined block)
+
+  // copies the raw blocks of task k into raw buffer k & 1 (16-byte cp.async)
+  auto fetch = [&](int k) {
+    if (k < ntask) {
+      const int ei = (int)blockIdx.x + (k / 9) * (int)gridDim.x, b = k % 9;
+      int ids[covf::kRawMax], n;
+      cov_raw_of(b, ids, n);
+      double *dst = rawb + (k & 1) * covf::kRaw;
+      const double *src = accb + (size_t)ei * cov::kBlocks * cov::kBlk;
+      constexpr int kV = cov::kBlk / 2;  // 16-byte vectors per block
+      for (int v = tid; v < n * kV; v += covf::kThreads) {
+        const int r = v / kV, o = 2 * (v % kV);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst + r * cov::kBlk + o)),
+                     "l"(src + (size_t)ids[r] * cov::kBlk + o)
+                     : "memory");
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+
+  double ax = 0.0, bx = 0.0, az = 0.0, bz = 0.0;  // inverse Jacobian rows at point q
+  double xl[kNl], xd[kNl];                         // l(qx, .), l'(qx, .)
+  double tl = 0.0, tm = 0.0, tr = 0.0;
+  fetch(0);
+  for (int k = 0; k < ntask; k++) {
+    const int ei = (int)blockIdx.x + (k / 9) * (int)gridDim.x, b = k % 9;
+    const int4 ie = mv.ieng[elems[ei]];
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();  // task k's raw blocks visible; task k - 1 done with every buffer
+    fetch(k + 1);
+    if (b == 0) {
+      if (k == 0) {
+#pragma unroll
+        for (int i = 0; i < kNl; i++) {
+          xl[i] = tl_s[qx * kNl + i];
+          xd[i] = td_s[qx * kNl + i];
+        }
+      }
+      tl = tm = tr = 0.0;
+      if (ptq) {
+        QGeo g;
+        if (!quad_geo(mv, dt, ie, q, false, g)) atomicCAS(err, 0, elems[ei] + 1);
+        ax = g.dzdeta / g.rjac;
+        bx = -g.dzdxi / g.rjac;
+        az = -g.dxdeta / g.rjac;
+        bz = g.dxdxi / g.rjac;
+        const double wq = dt.wts[qx] * dt.wts[qz] * g.rjac;
+#pragma unroll
+        for (int a = 0; a < 4; a++) wsf_s[a * kNq + q] = dt.sf[4 * q + a] * wq;
+      }
+    }
+    const double *r = rawb + (k & 1) * covf::kRaw;
+    const bool two = b < 6;  // Z_l' and the W's beyond (l, l) needed
+    // ---- Z stage: task (i, jx)
+    if (tid < kNen * kNl) {
+      const int i = tid / kNl, jx = tid % kNl;
+      double bv[kNl];
+#pragma unroll
+      for (int je = 0; je < kNl; je++) bv[je] = cov_bval(b, r, i, jx + kNl * je);
+      double *ol = zl + (i * kNl + jx) * kNint, *od = zd + (i * kNl + jx) * kNint;
+#pragma unroll
+      for (int z = 0; z < kNint; z++) {
+        double sl = 0.0, sd = 0.0;
+#pragma unroll
+        for (int je = 0; je < kNl; je++) {
+          sl = fma(bv[je], tb.l[z][je], sl);
+          sd = fma(bv[je], tb.d[z][je], sd);
+        }
+        ol[z] = sl;
+        if (two) od[z] = sd;
+      }
+    }
+    __syncthreads();
+    // ---- W stage: task (ix, jx, qz)
+    for (int t = tid; t < covf::kW; t += covf::kThreads) {
+      const int z = t % kNint, ixjx = t / kNint, ix = ixjx / kNl, jx = ixjx % kNl;
+      double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
+#pragma unroll
+      for (int ie2 = 0; ie2 < kNl; ie2++) {
+        const int zi = ((ix + kNl * ie2) * kNl + jx) * kNint + z;
+        const double a = zl[zi];
+        const double el = tl_s[z * kNl + ie2], ed = td_s[z * kNl + ie2];
+        w0 = fma(el, a, w0);
+        if (two) {
+          const double c = zd[zi];
+          w1 = fma(el, c, w1);
+          w2 = fma(ed, a, w2);
+          w3 = fma(ed, c, w3);
+        }
+      }
+      wb[t] = w0;
+      if (two) {
+        wb[covf::kW + t] = w1;
+        wb[2 * covf::kW + t] = w2;
+        wb[3 * covf::kW + t] = w3;
+      }
+    }
+    __syncthreads();
+    // ---- F stage: point q
+    if (ptq) {
+      const double *W0 = wb, *W1 = wb + covf::kW, *W2 = wb + 2 * covf::kW, *W3 = wb + 3 * covf::kW;
+      if (b < 3) {
+        const double fxx = cov_fw(W0, qz, xd, xd), fxe = cov_fw(W1, qz, xd, xl);
+        const double fee = cov_fw(W3, qz, xl, xl);
+        const double xx = ax * ax * fxx + 2.0 * ax * bx * fxe + bx * bx * fee;
+        const double zz = az * az * fxx + 2.0 * az * bz * fxe + bz * bz * fee;
+        if (b == 0) {
+          tl += xx;
+          tm += 2.0 * xx + zz;
+        } else if (b == 1) {
+          tl += zz;
+          tm += xx + 2.0 * zz;
+        } else {
+          tm += xx + zz;
+        }
+      } else if (b == 3) {
+        const double fxx = cov_fw(W0, qz, xd, xd), fxe = cov_fw(W1, qz, xd, xl);
+        const double fex = cov_fw(W2, qz, xl, xd), fee = cov_fw(W3, qz, xl, xl);
+        tl += ax * az * fxx + ax * bz * fxe + bx * az * fex + bx * bz * fee;  // x^T S z
+        tm += az * ax * fxx + az * bx * fxe + bz * ax * fex + bz * bx * fee;  // z^T S x
+      } else if (b < 6) {
+        const double fxn = cov_fw(W0, qz, xd, xl), fen = cov_fw(W2, qz, xl, xl);
+        const double fnx = cov_fw(W0, qz, xl, xd), fne = cov_fw(W1, qz, xl, xl);
+        if (b == 4) {
+          tl += ax * fxn + bx * fen;  // x^T G1 v
+          tm -= ax * fnx + bx * fne;  // v^T G1 x
+        } else {
+          tl += az * fxn + bz * fen;  // z^T G2 v
+          tm -= az * fnx + bz * fne;  // v^T G2 z
+        }
+      } else {
+        const double fnn = cov_fw(W0, qz, xl, xl);
+        if (b == 6) {
+          tl += fnn;
+          tm += 2.0 * fnn;
+        } else if (b == 7) {
+          tm += fnn;
+        } else {
+          tr -= fnn;
+        }
+      }
+    }
+    if (b == 8) {
+      // ---- g_{m, anchor a} += sum_q W_q SF_a(q) T_m(q)
+      double v[12];
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const double w = ptq ? wsf_s[a * kNq + q] : 0.0;
+        v[3 * a + 0] = w * tl;
+        v[3 * a + 1] = w * tm;
+        v[3 * a + 2] = w * tr;
+      }
+#pragma unroll
+      for (int kk = 0; kk < 12; kk++) {
+        double x = v[kk];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        v[kk] = x;
+      }
+      if (lane == 0)
+        for (int kk = 0; kk < 12; kk++) red[kk][warp] = v[kk];
+      __syncthreads();
+      if (tid < 12) {
+        double x = 0.0;
+        for (int w = 0; w < covf::kThreads / 32; w++) x += red[tid][w];
+        const int a = tid / 3, m = tid % 3;
+        const int anchor = (a == 0 ? ie.x : a == 1 ? ie.y : a == 2 ? ie.z : ie.w) - 1;
+        atomicAdd(&grad[(size_t)m * nnpg + anchor], x);
+      }
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// host
+// ---------------------------------------------------------------------------
+static CovFinTabs cov_fin_tables(const Tables &t) {
+  // Lagrange basis on the 5 GLL points (the factors of SHL, dshl.f:100-243)
+  CovFinTabs tb;
+  for (int q = 0; q < kNint; q++) {
+    const double x = t.xigll[q];
+    for (int i = 0; i < kNl; i++) {
+      double v = 1.0, dsum = 0.0;
+      for (int k = 0; k < kNl; k++)
+        if (k != i) v *= (x - t.xipts[k]) / (t.xipts[i] - t.xipts[k]);
+      for (int m = 0; m < kNl; m++) {
+        if (m == i) continue;
+        double p = 1.0 / (t.xipts[i] - t.xipts[m]);
+        for (int k = 0; k < kNl; k++)
+          if (k != i && k != m) p *= (x - t.xipts[k]) / (t.xipts[i] - t.xipts[k]);
+        dsum += p;
+      }
+      tb.l[q][i] = v;
+      tb.d[q][i] = dsum;
+    }
+  }
+  return tb;
+}
+
+// One-time set-up of the covariance gradient: the gather's DOF-layout check,
+// the kernels' shared-memory attributes and the FP64 accumulators
+// (15 x 625 doubles per element outside the PML).  Allocates, so it runs
+// outside any stream capture.
+cudaError_t prepare_grad_cov(Ctx *c) {
+  if (c->d_cov) return cudaSuccess;
+  for (size_t i = 0; i + 2 < c->h_lm.size(); i += 3) {
+    const int d = c->h_lm[i];
+    const bool ok = d > 0 ? (c->h_lm[i + 1] == d + 1 && c->h_lm[i + 2] == d + 2)
+                          : (c->h_lm[i + 1] == 0 && c->h_lm[i + 2] == 0);
+    if (!ok) return cudaErrorNotSupported;
+  }
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_grad_cov, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                cov::kSmemBytes)))
+    return e;
+  if ((e = cudaFuncSetAttribute(k_grad_cov_fin, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                covf::kSmemBytes)))
+    return e;
+  const size_t n = (size_t)std::max(c->n_nonpml, 1) * cov::kBlocks * cov::kBlk;
+  double *d = nullptr;
+  if ((e = cudaMalloc(&d, n * sizeof(double)))) return e;
+  c->d_cov = d;
+  c->cov_pending = false;
+  return cudaSuccess;
+}
+
+cudaError_t launch_grad_cov(Ctx *c, const PairTable &pt, int npairs, int nsrc, const double *u,
+                            const double *lam, cudaStream_t st) {
+  if (!c->d_cov) return cudaErrorNotReady;
+  if (c->n_nonpml == 0) return cudaSuccess;
+  CovArgs ga;
+  ga.npairs = npairs;
+  ga.nsrc = nsrc;
+  ga.ndof = c->ndof;
+  ga.n_elem = c->n_nonpml;
+  ga.add = c->cov_pending ? 1 : 0;
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  const int grid = std::min(nsm, c->n_nonpml);
+  k_grad_cov<<<grid, cov::kThreads, cov::kSmemBytes, st>>>(ga, c->d_nonpml, c->d_lm, pt,
+                                                           (const double2 *)u,
+                                                           (const double2 *)lam, c->d_cov,
+                                                           c->d_err);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) c->cov_pending = true;
+  return e;
+}
+
+cudaError_t launch_grad_cov_fin(Ctx *c, double *grad, cudaStream_t st) {
+  if (!c->d_cov) return cudaErrorNotReady;
+  if (!c->cov_pending || c->n_nonpml == 0) return cudaSuccess;
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  const int grid = std::min(3 * nsm, c->n_nonpml);
+  k_grad_cov_fin<<<grid, covf::kThreads, covf::kSmemBytes, st>>>(
+      c->mv, c->dt, c->n_nonpml, c->nnpg, c->d_nonpml, c->d_cov, cov_fin_tables(c->tab), grad,
+      c->d_err);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) c->cov_pending = false;
+  return e;
+}
+
+}  // namespace fem25

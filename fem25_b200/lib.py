@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(_HERE, "libfem25gpu.so")
 FEM25_OK = 0
 FEM25_PREC_FP64 = 0
 FEM25_PREC_TF32X3 = 1
+FEM25_PREC_TF32X3_POINTWISE = 2
 _CODES = {1: "ERR_ARG", 2: "ERR_JACOBIAN", 3: "ERR_PATTERN", 4: "ERR_CUDA", 5: "ERR_ALLOC",
           6: "ERR_GRAPH", 7: "ERR_UNSUPPORTED", 8: "ERR_NOMESH"}
 
@@ -71,6 +72,8 @@ def lib():
         L.fem25_dense_factor_dev.argtypes = [vp, vp, vp]
         L.fem25_dense_solve_dev.argtypes = [vp, i, i, vp, vp]
         L.fem25_gradient_dev.argtypes = [vp, i, vp, vp, i, vp, vp, i, vp, vp]
+        L.fem25_gradient_accumulate_dev.argtypes = [vp, i, vp, vp, i, vp, vp, vp]
+        L.fem25_gradient_finalize_dev.argtypes = [vp, vp, vp]
         L.fem25_ref_gradient_dev.argtypes = [vp, C.c_char_p, d, d, d, vp, vp, i, vp, vp]
         L.fem25_ref_gradient_info.argtypes = [vp, C.POINTER(i), C.POINTER(ll), vp]
         L.fem25_ref_vforce2_dev.argtypes = [vp, C.c_char_p, d, d, vp, vp, vp]
@@ -344,6 +347,19 @@ class Context:
         p = np.ascontiguousarray(pys, np.float64)
         self._check(lib().fem25_gradient_dev(self.h, len(f), _np(f), _np(p), nsrc, _ptr(u),
                                              _ptr(lam), prec, _ptr(grad), _stream(stream)))
+
+    def gradient_accumulate(self, freqs, pys, nsrc, u, lam, stream=None):
+        """Adds the field covariances of the pairs into the context's
+        accumulators (split-precision gradient, see gradient_finalize)."""
+        f = np.ascontiguousarray(freqs, np.float64)
+        p = np.ascontiguousarray(pys, np.float64)
+        self._check(lib().fem25_gradient_accumulate_dev(self.h, len(f), _np(f), _np(p), nsrc,
+                                                        _ptr(u), _ptr(lam), _stream(stream)))
+
+    def gradient_finalize(self, grad, stream=None):
+        """grad += the gradient of everything accumulated since the last
+        finalize; empties the accumulators."""
+        self._check(lib().fem25_gradient_finalize_dev(self.h, _ptr(grad), _stream(stream)))
 
     def ref_gradient_info(self):
         n, nz = C.c_int(), C.c_longlong()

@@ -179,17 +179,53 @@ int fem25_addblk_dev(fem25_ctx *ctx, int nsrc, const float *ue, float *sol, void
  * rho:  grad[m*NNPG + p] += sum_s Re( lam_s^H (dA/dm_p) u_s )
  * for m = lambda, mu, rho, summed over the n (omega, py) pairs; fields are
  * complex128 device arrays [pair][src][NDOF]; grad is FP64 on the device.
+ * Replaces the per-source CFMAT_DIST + ADJGRAD sums (hessloc.f90:1-133,
+ * adjgrad.f90:1-145) and the MPI_REDUCE of GRADL (funcgradh.f90:428) for an
+ * exact (not Vp/Vs-masked) parameterisation.
  * Elements of domain 'A' (PML) do not contribute.
- * prec: FEM25_PREC_FP64 (plain FP64 kernels) or FEM25_PREC_TF32X3
- * (split-precision tensor-core contraction, FP64 cross-pair reduction).
+ * prec:
+ *   FEM25_PREC_FP64             plain FP64 kernels, per (pair, source) at the
+ *                               169 quadrature points;
+ *   FEM25_PREC_TF32X3           split-precision tensor cores (3xTF32, FP32
+ *                               accumulation in TMEM, FP64 across pairs):
+ *                               per element the weighted covariances
+ *                               sum conj(lam) u^T of the nodal fields are
+ *                               accumulated over all pairs and sources, then
+ *                               contracted once in FP64.  Equivalent to
+ *                               fem25_gradient_accumulate_dev followed by
+ *                               fem25_gradient_finalize_dev, so it also adds
+ *                               any accumulation still pending on the context;
+ *   FEM25_PREC_TF32X3_POINTWISE split-precision tensor cores interpolating
+ *                               both fields at the 169 points per (pair,
+ *                               source), no accumulator memory.
  * Pairs are passed to the kernels by value, 64 per launch; the call only
  * enqueues work and may be recorded into a CUDA graph once the first
- * TF32X3 call on the context (which uploads its tables) has returned. */
+ * split-precision call of that kind on the context (which allocates or
+ * uploads its tables) has returned. */
 #define FEM25_PREC_FP64 0
 #define FEM25_PREC_TF32X3 1
+#define FEM25_PREC_TF32X3_POINTWISE 2
 int fem25_gradient_dev(fem25_ctx *ctx, int npairs, const double *freq, const double *py,
                        int nsrc, const double *u, const double *lam, int prec, double *grad,
                        void *stream);
+
+/* Split form of the FEM25_PREC_TF32X3 gradient for inversion loops that
+ * solve one pair at a time (funcgradh.f90:191-420: every frequency's forward
+ * and adjoint fields add into GRADL before one reduction).
+ * fem25_gradient_accumulate_dev adds the covariances of npairs pairs'
+ * fields (same arguments as fem25_gradient_dev) into the context's
+ * accumulators: 15 x 625 doubles per element outside the PML (75 KB each),
+ * allocated by the first call, which must not be inside a stream capture.
+ * fem25_gradient_finalize_dev contracts everything accumulated since the
+ * last finalize into grad (+=) and empties the accumulators; with nothing
+ * accumulated it leaves grad unchanged.  The first accumulation after a
+ * finalize overwrites the accumulators instead of adding, a choice made
+ * when the call is made: a CUDA graph should record accumulate calls
+ * together with the finalize that consumes them. */
+int fem25_gradient_accumulate_dev(fem25_ctx *ctx, int npairs, const double *freq,
+                                  const double *py, int nsrc, const double *u, const double *lam,
+                                  void *stream);
+int fem25_gradient_finalize_dev(fem25_ctx *ctx, double *grad, void *stream);
 
 /* Reference-compatible gradient (CFMAT_DIST hessloc.f90:1-133 + ADJFLAM_DIST
  * adjgrad.f90:88-145 + SAXPY adjgrad.f90:76): derivative in Vp ('PP') or Vs

@@ -13,7 +13,8 @@ import numpy as np
 import pytest
 
 import oracle
-from fem25_b200 import FEM25_PREC_FP64, FEM25_PREC_TF32X3, Context, Fem25Error, synth
+from fem25_b200 import (FEM25_PREC_FP64, FEM25_PREC_TF32X3, FEM25_PREC_TF32X3_POINTWISE,
+                        Context, Fem25Error, synth)
 from tests import helpers
 
 torch = pytest.importorskip("torch")
@@ -28,7 +29,8 @@ def _rel(a, b):
     return float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
 
 
-@pytest.mark.parametrize("prec", [FEM25_PREC_FP64, FEM25_PREC_TF32X3])
+@pytest.mark.parametrize("prec", [FEM25_PREC_FP64, FEM25_PREC_TF32X3,
+                                  FEM25_PREC_TF32X3_POINTWISE])
 def test_graph_replay_matches_eager(prec):
     mesh, pairs, _ = synth.make_config(0, nx=12, nz=8)
     g = oracle.graph_build(mesh)
@@ -106,7 +108,8 @@ def test_gradient_more_pairs_than_one_launch():
         oracle.grad_exact(mesh, g, f, py, u[p], lam[p], out=ref)
     d_u = torch.from_numpy(u).to(_dev())
     d_l = torch.from_numpy(lam).to(_dev())
-    for prec, tol in ((FEM25_PREC_FP64, 1e-10), (FEM25_PREC_TF32X3, 2e-5)):
+    for prec, tol in ((FEM25_PREC_FP64, 1e-10), (FEM25_PREC_TF32X3, 2e-5),
+                      (FEM25_PREC_TF32X3_POINTWISE, 2e-5)):
         d_g = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=_dev())
         ctx.gradient([p[0] for p in use], [p[1] for p in use], nsrc, d_u, d_l, d_g, prec)
         got = d_g.cpu().numpy()
@@ -132,9 +135,9 @@ def test_capture_before_setup_is_rejected():
             st = torch.cuda.current_stream()
             with pytest.raises(Fem25Error):
                 ctx.assemble_batch("B", [pairs[0][0]], [pairs[0][1]], ring, stride, 1, stream=st)
-            with pytest.raises(Fem25Error):
-                ctx.gradient([pairs[0][0]], [pairs[0][1]], 1, u, u, grad, FEM25_PREC_TF32X3,
-                             stream=st)
+            for prec in (FEM25_PREC_TF32X3, FEM25_PREC_TF32X3_POINTWISE):
+                with pytest.raises(Fem25Error):
+                    ctx.gradient([pairs[0][0]], [pairs[0][1]], 1, u, u, grad, prec, stream=st)
             with pytest.raises(Fem25Error):
                 ctx.assemble("B", pairs[0][0], pairs[0][1], ring, stream=st)
     torch.cuda.current_stream().wait_stream(side)
@@ -142,6 +145,7 @@ def test_capture_before_setup_is_rejected():
     del graph
     # the same calls work once made outside a capture
     ctx.assemble_batch("B", [pairs[0][0]], [pairs[0][1]], ring, stride, 1)
-    ctx.gradient([pairs[0][0]], [pairs[0][1]], 1, u, u, grad, FEM25_PREC_TF32X3)
+    for prec in (FEM25_PREC_TF32X3, FEM25_PREC_TF32X3_POINTWISE):
+        ctx.gradient([pairs[0][0]], [pairs[0][1]], 1, u, u, grad, prec)
     torch.cuda.synchronize()
     ctx.close()

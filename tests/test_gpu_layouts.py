@@ -8,6 +8,7 @@ rectangular half-space the other parity tests use.
 Tolerances as in test_gpu_parity.py: plain FP64 CSR and the reference's
 COMPLEX*8 CDIST bit-exact (dispersive media included); batched CSR <= 1e-12
 per row; exact gradient FP64 <= 1e-10 and 3xTF32 <= 2e-5 relative (2-norm);
+both split-precision forms (covariance and pointwise) as well;
 reference-compatible gradient and the Hessian-path kernels (MET225_MOD,
 CADJ_NU_ALPHA, PCHADJ) bit-exact.
 """
@@ -15,7 +16,8 @@ import numpy as np
 import pytest
 
 import oracle
-from fem25_b200 import FEM25_PREC_FP64, FEM25_PREC_TF32X3, Context, synth
+from fem25_b200 import (FEM25_PREC_FP64, FEM25_PREC_TF32X3, FEM25_PREC_TF32X3_POINTWISE,
+                        Context, synth)
 from tests import helpers
 
 torch = pytest.importorskip("torch")
@@ -72,7 +74,8 @@ def test_exact_gradient_both_precisions(layout):
     for p, (f, py) in enumerate(use):
         oracle.grad_exact(mesh, g, f, py, u[p], lam[p], out=ref)
     d_u, d_l = torch.from_numpy(u).to(_dev()), torch.from_numpy(lam).to(_dev())
-    for prec, tol in ((FEM25_PREC_FP64, 1e-10), (FEM25_PREC_TF32X3, 2e-5)):
+    for prec, tol in ((FEM25_PREC_FP64, 1e-10), (FEM25_PREC_TF32X3, 2e-5),
+                      (FEM25_PREC_TF32X3_POINTWISE, 2e-5)):
         d_g = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=_dev())
         ctx.gradient([p[0] for p in use], [p[1] for p in use], nsrc, d_u, d_l, d_g, prec)
         got = d_g.cpu().numpy()

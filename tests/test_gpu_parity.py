@@ -13,7 +13,8 @@ import numpy as np
 import pytest
 
 import oracle
-from fem25_b200 import FEM25_PREC_FP64, FEM25_PREC_TF32X3, Context, Fem25Error, synth
+from fem25_b200 import (FEM25_PREC_FP64, FEM25_PREC_TF32X3, FEM25_PREC_TF32X3_POINTWISE,
+                        Context, Fem25Error, synth)
 from tests import helpers
 
 torch = pytest.importorskip("torch")
@@ -265,10 +266,14 @@ def test_gradient_fp64_source_tiles_agree(tile, monkeypatch):
     ctx.close()
 
 
+@pytest.mark.parametrize("prec", [FEM25_PREC_TF32X3, FEM25_PREC_TF32X3_POINTWISE],
+                         ids=["covariance", "pointwise"])
 @pytest.mark.parametrize("nsrc", [1, 7])
-def test_gradient_tf32x3_matches_oracle(nsrc):
-    """Split-precision tensor-core gradient; 3 pairs x 7 sources = 21 combos
-    exercises two full batches of 10 and a ragged one, nsrc=1 a batch of 3."""
+def test_gradient_tf32x3_matches_oracle(nsrc, prec):
+    """Split-precision tensor-core gradients.  Pointwise form: 3 pairs x 7
+    sources = 21 combos exercises four full stages of 5 combos and a ragged
+    one, nsrc=1 a stage of 3.  Covariance form: a partly filled 16-source
+    stage per pair."""
     mesh, pairs, _ = synth.make_config(0, nx=10, nz=6)
     g = oracle.graph_build(mesh)
     ctx = Context(mesh, g)
@@ -284,8 +289,7 @@ def test_gradient_tf32x3_matches_oracle(nsrc):
     d_l = torch.from_numpy(lam).to(_dev())
     for rep in range(2):
         d_g = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=_dev())
-        ctx.gradient([p[0] for p in use], [p[1] for p in use], nsrc, d_u, d_l, d_g,
-                     FEM25_PREC_TF32X3)
+        ctx.gradient([p[0] for p in use], [p[1] for p in use], nsrc, d_u, d_l, d_g, prec)
         got = d_g.cpu().numpy()
         for m in range(3):
             rel = np.linalg.norm(got[m] - ref[m]) / np.linalg.norm(ref[m])

@@ -404,3 +404,117 @@ def test_pchadj_matches_numpy_restatement(small_case):
         assert np.allclose(jacl[2 * col:2 * col + 2].T, j, rtol=0, atol=1e-4 * np.abs(j).max())
         ref_h[4 * col:4 * col + 4] += np.real(j.conj().T @ j).reshape(-1)
     assert np.max(np.abs(hess - ref_h)) <= 2e-5 * np.max(np.abs(ref_h))
+
+
+def test_gradient_covariance_form():
+    """The algebra of the covariance gradient (k_grad_cov.cu) restated in
+    numpy: per element the 15 weighted blocks of sum conj(lam) u^T, the 9
+    combined blocks and the sum-factorised contraction with the 1D Lagrange
+    factors of SHL, against the oracle's exact gradient (grad_exact) on a
+    jittered, topographic layout, several pairs and sources."""
+    mesh, pairs, _ = synth.make_config(4, nx=8, nz=6)
+    g = oracle.graph_build(mesh)
+    lm = np.asarray(g.lm).reshape(mesh.nelem, 75)
+    use = [pairs[1], pairs[len(pairs) // 2], pairs[-1]]
+    nsrc = 3
+    rng = np.random.default_rng(91)
+    shape = (len(use), nsrc, g.ndof)
+    u = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    lam = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    ref = np.zeros((3, mesh.nnpg))
+    for p, (f, py) in enumerate(use):
+        oracle.grad_exact(mesh, g, f, py, u[p], lam[p], out=ref)
+    xig, shl = oracle.tables()
+    xq, wq = xig[0], xig[1]
+    xn, _ = oracle.lobatto(5)
+    xn[2] = 0.0
+    # 1D Lagrange values l[q][i] and derivatives d[q][i] on the 5 GLL nodes
+    lg = np.ones((13, 5))
+    dg = np.zeros((13, 5))
+    for i in range(5):
+        oth = [k for k in range(5) if k != i]
+        for k in oth:
+            lg[:, i] *= (xq - xn[k]) / (xn[i] - xn[k])
+        for m in oth:
+            t = np.full(13, 1.0 / (xn[i] - xn[m]))
+            for k in oth:
+                if k != m:
+                    t *= (xq - xn[k]) / (xn[i] - xn[k])
+            dg[:, i] += t
+    # SHL is the tensor product (node a = ix + 5 ie, point q = qx + 13 qz)
+    assert np.allclose(np.einsum("xi,ze->zxei", lg, lg).reshape(13, 13, 25), shl[:, :, :, 2],
+                       atol=1e-14)
+    fx = {"N": lg, "X": dg, "E": lg}  # factor on xi for T_N, T_xi, T_eta
+    fe = {"N": lg, "X": lg, "E": dg}  # factor on eta
+
+    def Y(B, t):  # [ie][ix][qz][qx]
+        return np.einsum("iej,ze,xj->izx", B.reshape(25, 5, 5), fe[t], fx[t]).reshape(5, 5, 13, 13)
+
+    def F(Yt, t1):  # T_t1(q)^T Y(q)
+        return np.einsum("eizx,xi,ze->zx", Yt, fx[t1], fe[t1])
+
+    X, Z = np.meshgrid(xq, xq)  # [qz][qx]: X = xi, Z = eta
+    W = np.outer(wq, wq)
+    sf = 0.25 * np.array([(1 - X) * (1 - Z), (1 + X) * (1 - Z), (1 + X) * (1 + Z), (1 - X) * (1 + Z)])
+    dsx = 0.25 * np.array([-(1 - Z), (1 - Z), (1 + Z), -(1 + Z)])
+    dse = 0.25 * np.array([-(1 - X), -(1 + X), (1 + X), (1 - X)])
+    out = np.zeros((3, mesh.nnpg))
+    for e in range(mesh.nelem):
+        if chr(mesh.cdomain[e]) == "A":
+            continue
+        dofs = lm[e]
+        on = dofs > 0
+
+        def gather(fld):
+            v = np.zeros((len(use), nsrc, 75), complex)
+            v[:, :, on] = fld[:, :, dofs[on] - 1]
+            return v.reshape(len(use), nsrc, 25, 3).transpose(0, 1, 3, 2)  # [p][s][comp][node]
+
+        U, L = gather(u), gather(lam)
+        blk = {k: np.zeros((25, 25)) for k in ("R00", "R02", "R20", "R22", "R11", "P0", "P1",
+                                               "P2", "W0", "W1", "W2", "I01", "I21", "I10", "I12")}
+        for p, (f, py) in enumerate(use):
+            om = 2.0 * np.pi * f
+            wpy = om * py
+            C = np.einsum("sci,sdj->cdij", np.conj(L[p]), U[p])
+            for c, d in ((0, 0), (0, 2), (2, 0), (2, 2), (1, 1)):
+                blk[f"R{c}{d}"] += C[c, d].real
+            for c in range(3):
+                blk[f"P{c}"] += wpy * wpy * C[c, c].real
+                blk[f"W{c}"] += om * om * C[c, c].real
+            for c, d in ((0, 1), (2, 1), (1, 0), (1, 2)):
+                blk[f"I{c}{d}"] += wpy * C[c, d].imag
+        sym = [0.5 * (blk[k] + blk[k].T) for k in ("R00", "R22", "R11")]
+        S = blk["R02"] + blk["R20"].T
+        G = [blk["I01"] - blk["I10"].T, blk["I21"] - blk["I12"].T]
+        VA, VB, VC = blk["P1"], blk["P0"] + blk["P2"], blk["W0"] + blk["W1"] + blk["W2"]
+        ie = mesh.ieng[e] - 1
+        xa, za = mesh.xlocs[ie], mesh.zlocs[ie]
+        dxdxi, dxdeta = np.tensordot(xa, dsx, 1), np.tensordot(xa, dse, 1)
+        dzdxi, dzdeta = np.tensordot(za, dsx, 1), np.tensordot(za, dse, 1)
+        rj = dxdxi * dzdeta - dxdeta * dzdxi
+        ax, bx, az, bz = dzdeta / rj, -dzdxi / rj, -dxdeta / rj, dxdxi / rj
+        xx, zz = [], []
+        for B in sym:
+            yx, ye = Y(B, "X"), Y(B, "E")
+            fxx, fxe, fee = F(yx, "X"), F(ye, "X"), F(ye, "E")
+            xx.append(ax * ax * fxx + 2 * ax * bx * fxe + bx * bx * fee)
+            zz.append(az * az * fxx + 2 * az * bz * fxe + bz * bz * fee)
+        yx, ye = Y(S, "X"), Y(S, "E")
+        sxx, sxe, sex, see = F(yx, "X"), F(ye, "X"), F(yx, "E"), F(ye, "E")
+        xsz = ax * az * sxx + ax * bz * sxe + bx * az * sex + bx * bz * see
+        zsx = az * ax * sxx + az * bx * sxe + bz * ax * sex + bz * bx * see
+        gl, gm = 0.0, 0.0
+        for Gk, (c1, c2) in zip(G, ((ax, bx), (az, bz))):
+            yn, yx, ye = Y(Gk, "N"), Y(Gk, "X"), Y(Gk, "E")
+            gl = gl + c1 * F(yn, "X") + c2 * F(yn, "E")
+            gm = gm - (c1 * F(yx, "N") + c2 * F(ye, "N"))
+        va, vb, vc = (F(Y(V, "N"), "N") for V in (VA, VB, VC))
+        tl = xx[0] + xsz + zz[1] + gl + va
+        tm = 2 * xx[0] + zz[0] + zsx + xx[1] + 2 * zz[1] + xx[2] + zz[2] + gm + 2 * va + vb
+        tr = -vc
+        wgt = W * rj
+        for a in range(4):
+            out[:, ie[a]] += [np.sum(sf[a] * wgt * t) for t in (tl, tm, tr)]
+    for m in range(3):
+        assert np.linalg.norm(out[m] - ref[m]) <= 1e-12 * np.linalg.norm(ref[m]), m
