@@ -179,11 +179,14 @@ def pipeline_uneven(local, dev):
     0.1), 4800 systems, 64 sources).  The batched assembly runs all 4800
     systems; the plain assembly runs one system per frequency and each
     gradient one (omega, py) pair with all 64 sources, scaled to the 4800 pairs
-    (per-system and per-pair costs do not depend on the pair).  Parity at full
-    size: the last batched system against the plain FP64 CSR, the
-    split-precision gradient against the FP64 one."""
+    (per-system and per-pair costs do not depend on the pair).  The batched
+    gradient adds each pair's field covariances as the pair's solutions
+    arrive (fem25_gradient_accumulate_dev) and contracts them once
+    (fem25_gradient_finalize_dev); the plain one runs the FP64 kernel per
+    pair.  Parity at full size: the last batched system against the plain
+    FP64 CSR, the split-precision gradient against the FP64 one."""
     import torch
-    from fem25_b200 import FEM25_PREC_FP64, FEM25_PREC_TF32X3, Context, synth
+    from fem25_b200 import FEM25_PREC_FP64, FEM25_PREC_TF32X3_POINTWISE, Context, synth
     mesh, pairs, cfg = synth.make_config(4)
     nsrc = cfg["nsrc"]
     t0 = time.perf_counter()
@@ -255,9 +258,11 @@ def pipeline_uneven(local, dev):
     gp = pairs[npairs // 2]
     g64 = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=dev)
     g32 = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=dev)
-    # untimed first calls: they upload the tensor-core tables and tune the FP64
-    # gradient's source tile
-    ctx.gradient([gp[0]], [gp[1]], nsrc, u, lam, g32, FEM25_PREC_TF32X3, stream=stream)
+    # untimed first calls: they allocate the covariance accumulators, upload
+    # the pointwise tensor-core tables and tune the FP64 gradient's source tile
+    ctx.gradient_accumulate([gp[0]], [gp[1]], nsrc, u, lam, stream=stream)
+    ctx.gradient_finalize(g32, stream=stream)
+    ctx.gradient([gp[0]], [gp[1]], nsrc, u, lam, g32, FEM25_PREC_TF32X3_POINTWISE, stream=stream)
     ctx.gradient([gp[0]], [gp[1]], nsrc, u, lam, g64, FEM25_PREC_FP64, stream=stream)
     torch.cuda.synchronize()
 
@@ -265,7 +270,15 @@ def pipeline_uneven(local, dev):
         out.zero_()
         ctx.gradient([gp[0]], [gp[1]], nsrc, u, lam, out, prec, stream=stream)
     t_g64 = timed(lambda: run_grad(g64, FEM25_PREC_FP64), reps=2)
-    t_g32 = timed(lambda: run_grad(g32, FEM25_PREC_TF32X3), reps=3)
+    t_gpw = timed(lambda: run_grad(g32, FEM25_PREC_TF32X3_POINTWISE), reps=2)
+    # per pair: the covariance accumulation; per gradient: one contraction
+    t_acc = timed(lambda: ctx.gradient_accumulate([gp[0]], [gp[1]], nsrc, u, lam, stream=stream),
+                  reps=3)
+    g32.zero_()
+    ctx.gradient_finalize(g32, stream=stream)  # empties the timing runs' sums
+    g32.zero_()
+    ctx.gradient_accumulate([gp[0]], [gp[1]], nsrc, u, lam, stream=stream)
+    t_fin = timed(lambda: ctx.gradient_finalize(g32, stream=stream))
     grel = max(float(torch.linalg.norm(g32[m] - g64[m]) / torch.linalg.norm(g64[m]))
                for m in range(3))
     del u, lam, g64, g32
@@ -273,8 +286,8 @@ def pipeline_uneven(local, dev):
     ctx.close()
     torch.cuda.empty_cache()
     plain_total = (t_pasm + t_g64) * npairs
-    batched_total = t_basm + t_g32 * npairs
-    batched_graph_total = t_basm_graph + t_g32 * npairs
+    batched_total = t_basm + t_acc * npairs + t_fin
+    batched_graph_total = t_basm_graph + t_acc * npairs + t_fin
     units = mesh.nelem * nsrc
     return {"workload": f"uneven batch: 600x200 jittered deg-4 mesh with topography, strip 4 "
                         f"({mesh.nelem} elements, NDOF {ndof}, NNZ {nz}), "
@@ -286,13 +299,15 @@ def pipeline_uneven(local, dev):
             "batched_assembly_s": t_basm, "batched_assemblies_per_s": npairs / t_basm,
             "batched_assembly_graph_s": t_basm_graph,
             "plain_assembly_s_per_system": t_pasm,
-            "gradient_tf32x3_s_per_pair": t_g32, "gradient_fp64_s_per_pair": t_g64,
-            "gradient_tf32x3_elem_rhs_per_s": units / t_g32,
+            "gradient_tf32x3_s_per_pair": t_acc, "gradient_tf32x3_contraction_s": t_fin,
+            "gradient_fp64_s_per_pair": t_g64,
+            "gradient_tf32x3_pointwise_s_per_pair": t_gpw,
+            "gradient_tf32x3_elem_rhs_per_s": units / t_acc,
             "gradient_fp64_elem_rhs_per_s": units / t_g64,
             "gradient_rel_err_vs_fp64": grel, "csr_rel_err_batched_vs_plain": csr_rel,
             "sample": f"batched assembly: all {npairs} systems; plain assembly: 1 system per "
-                      f"frequency ({len(sel)}); gradients: 1 pair x {nsrc} sources; totals scaled "
-                      f"to {npairs} pairs",
+                      f"frequency ({len(sel)}); gradients: 1 pair x {nsrc} sources per pair, "
+                      f"scaled to {npairs} pairs, plus one contraction for the batched path",
             "setup_s": round(setup_s, 1), "autotuned": tuned}
 
 
@@ -323,7 +338,8 @@ def main():
     import torch.distributed as dist
     from datetime import timedelta
 
-    from fem25_b200 import FEM25_PREC_FP64, FEM25_PREC_TF32X3, Context, synth
+    from fem25_b200 import (FEM25_PREC_FP64, FEM25_PREC_TF32X3, FEM25_PREC_TF32X3_POINTWISE,
+                            Context, synth)
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -470,22 +486,57 @@ def main():
 
         gms, g64 = time_grad(FEM25_PREC_FP64)
         tms, g32 = time_grad(FEM25_PREC_TF32X3)
+        pms, gpw = time_grad(FEM25_PREC_TF32X3_POINTWISE)
         rel = max(float(torch.linalg.norm(g32[m] - g64[m]) / torch.linalg.norm(g64[m]))
                   for m in range(3))
+        prel = max(float(torch.linalg.norm(gpw[m] - g64[m]) / torch.linalg.norm(g64[m]))
+                   for m in range(3))
+        # the covariance path's two kernels on their own: accumulation (per
+        # pair in an inversion loop) and contraction (once per gradient)
+        fr_, py_ = [p[0] for p in gp], [p[1] for p in gp]
+        acc_ms, fin_ms = [], []
+        for _ in range(3):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            ev[0].record(stream)
+            ctx.gradient_accumulate(fr_, py_, nsrc, u, lam, stream=stream)  # one k_grad_cov launch
+            ev[1].record(stream)
+            ctx.gradient_finalize(g32, stream=stream)  # one k_grad_cov_fin launch
+            ev[2].record(stream)
+            torch.cuda.synchronize()
+            acc_ms.append(ev[0].elapsed_time(ev[1]))
+            fin_ms.append(ev[1].elapsed_time(ev[2]))
+        acc_ms, fin_ms = min(acc_ms), min(fin_ms)
         nelem_phys = int(np.sum(mesh.cdomain != ord("A")))
         units = mesh.nelem * nsrc * npool
         grad = {"metric": "gradient elem·rhs/s", "unit": "elem·rhs/s",
                 "plain_fp64": units / (gms / 1e3), "ms": gms,
                 "tf32x3": units / (tms / 1e3), "tf32x3_ms": tms, "tf32x3_rel_err": rel,
+                "tf32x3_form": "field covariances accumulated per element on tcgen05, "
+                               "contracted once in FP64 (k_grad_cov + k_grad_cov_fin)",
+                "tf32x3_accumulate_ms": acc_ms, "tf32x3_contraction_ms": fin_ms,
+                "tf32x3_accumulate_elem_rhs_per_s": units / (acc_ms / 1e3),
+                "tf32x3_pointwise": units / (pms / 1e3), "tf32x3_pointwise_ms": pms,
+                "tf32x3_pointwise_rel_err": prel,
                 "units": f"{mesh.nelem} elements x {nsrc} sources x {npool} (omega,py) pairs "
                          f"({nelem_phys} non-PML elements computed)",
                 "algorithmic_tflops_fp64": units * 547200 / (gms / 1e3) / 1e12}
-        # split-precision kernel against the tensor roofline: the metric's fixed
+        # covariance accumulation against HBM: the algorithmic bytes are the
+        # two complex128 fields read once (2 x pairs x sources x NDOF x 16 B)
+        hpk, hkind = peaks()
+        fbytes = 2.0 * npool * nsrc * ctx.ndof * 16
+        gbs = fbytes / (acc_ms / 1e3) / 1e9
+        grad["covariance_roofline"] = {"bound": "hbm", "kernel": "k_grad_cov", "achieved": gbs,
+                                       "peak": hpk, "unit": "GB/s", "frac": gbs / hpk,
+                                       "peak_kind": hkind,
+                                       "algorithmic_bytes": "u and lambda read once, "
+                                                            f"{fbytes / 1e9:.2f} GB per launch"}
+        # the pointwise kernel against the tensor roofline: the metric's fixed
         # 547 200 flop per elem.rhs over a 3xTF32 peak (bf16 burst / 2 / 3)
         bpk, bkind = bf16_peak()
-        tf = units * 547200 / (tms / 1e3) / 1e12
-        grad["tf32x3_roofline"] = {"bound": "tensor", "kernel": "k_grad_tc", "achieved": tf,
-                                   "peak": bpk / 6.0, "unit": "TFLOP/s", "frac": tf / (bpk / 6.0),
+        tf = units * 547200 / (pms / 1e3) / 1e12
+        grad["tf32x3_roofline"] = {"bound": "tensor", "kernel": "k_grad_tc (pointwise form)",
+                                   "achieved": tf, "peak": bpk / 6.0, "unit": "TFLOP/s",
+                                   "frac": tf / (bpk / 6.0),
                                    "peak_kind": f"{bkind} bf16 burst {bpk:g} / 2 (TF32) / 3 "
                                                 f"(split products)"}
         # the reference-compatible drop-in (CFMAT_DIST + ADJGRAD, COMPLEX*8,

@@ -196,12 +196,12 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
   if (tid == 0) {
     drain_s = 0;
     for (int b = 0; b < tc::kNB; b++) {
-      mbar_init(smem_u32(&bar_bfull[b]), tc::kProdThreads);
+      mbar_init(smem_u32(&bar_bfull[b]), tc::kProdThreads / 32);  // one arrival per warp
       mbar_init(smem_u32(&bar_bempty[b]), 1);
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(smem_u32(&bar_tfull[b]), 1);
-      mbar_init(smem_u32(&bar_tempty[b]), tc::kEpiThreads);
+      mbar_init(smem_u32(&bar_tempty[b]), tc::kEpiThreads / 32);
     }
     mbar_init(smem_u32(&bar_drain), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -303,7 +303,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
           }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive(smem_u32(&bar_bfull[bs]));
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&bar_bfull[bs]));
         int ein = ei, bn = b + 1;
         if (bn == nb) {
           bn = 0;
@@ -412,7 +413,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
           const int cend = min(clast, nc - 1);
           if (cend < cfirst) {
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            mbar_arrive(smem_u32(&bar_tempty[ts]));
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&bar_tempty[ts]));
           }
           for (int c = cfirst; c <= cend; c++) {
             __syncwarp();
@@ -425,7 +427,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             tmem_wait_ld();
             if (c == cend) {
               asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-              mbar_arrive(smem_u32(&bar_tempty[ts]));
+              __syncwarp();
+              if (lane == 0) mbar_arrive(smem_u32(&bar_tempty[ts]));
             }
             const double2 pr = pt.p[(c0 + c) / ga.nsrc];
             point_forms(pg, (float)(pr.x * pr.x), (float)pr.y, val, tl, tm, tr);
@@ -451,7 +454,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             }
           }
           asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-          mbar_arrive(smem_u32(&bar_tempty[ts]));
+          __syncwarp();
+          if (lane == 0) mbar_arrive(smem_u32(&bar_tempty[ts]));
           __syncwarp();
           if (quarter < 2) named_bar(3, 64);  // point 168's rows visible
           const int j3 = min(lane / 3, 9);  // lanes 30, 31 (no point of their own) read rows 27-29
