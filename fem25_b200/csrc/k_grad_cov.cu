@@ -24,24 +24,22 @@
 // pair, D[lam row][u column] += sum_k A[row][k] B[column][k] with
 // K = (source, re/im):
 //     A[32c + a][2s, 2s+1]     = (Re lam, Im lam)           of component c, node a
-//     B[25d + b][2s, 2s+1]     = (Re u, Im u)               -> D = Re conj(lam) u
-//     B[80 + 25d + b][2s, 2s+1] = (Im u, -Re u)             -> D = Im conj(lam) u
-// M = 128 (75 rows used), N = 160 (150 used), 16 sources (K = 32) per
+//     B[32d + b][2s, 2s+1]      = (Re u, Im u)              -> D = Re conj(lam) u
+//     B[96 + 32d + b][2s, 2s+1] = (Im u, -Re u)             -> D = Im conj(lam) u
+// M = 128 (100 rows used: component 1's rows also at 96 + a), N = 192
+// (150 used, a 32-column slot per part and component), 8 sources (K = 16) per
 // stage, x = hi + lo split with D = A_hi B_hi + A_lo B_hi + A_hi B_lo.
-//   warps 7, 11, 15, 19, 20-23  producers: copy the stage's nodal values
-//                (complex128) into one of 5 raw shared-memory stages
-//   warp 3       MMA issuer (one thread), two TMEM accumulators of 160
-//                columns (one per stage in flight)
-//   15 warps     epilogue: convert the next stage's raw values into tf32
-//                hi/lo operand tiles (one of 3), then drain this stage:
-//                warp w (w < 20, w % 4 = c < 3) owns one of the five blocks
-//                of lam component c (TMEM lanes 32c..32c+24, lane = node),
-//                reads its 25 columns and adds them, weighted, into 25 FP64
+//   8 producer warps  each thread owns one (node, source) of every stage: it
+//                copies the node's u and lam runs (complex128) into its raw
+//                shared-memory slots and converts them itself to tf32 hi/lo
+//                operand tiles (one of 3 stages)
+//   warp 3       MMA issuer (one thread), two TMEM accumulators of 192
+//                columns (each takes 2 stages of one pair)
+//   15 epilogue warps  one block each: the warp's TMEM lane quarter holds
+//                the lam component (lane = node); it reads its 25 columns
+//                and adds them, weighted by the pair, into 25 FP64
 //                registers; at the end of the element it writes (or adds)
 //                the block row to memory.
-// The epilogue warps sit on scheduler partitions 0-2 (their TMEM lane
-// quarters), so the conversion, the largest share of the instructions, is
-// spread over three partitions instead of queueing behind the copies.
 // Hand-offs are mbarriers; every wait is bounded and a wait that runs out
 // sets the error word and drains the schedule without waiting.
 //
@@ -98,7 +96,7 @@ static_assert(kSmemBytes <= 227 * 1024, "shared memory");
 
 constexpr uint32_t kCovIdesc = tf32_idesc(cov::kM, cov::kN);
 
-// Epilogue role of warp w (w < 20, c = w % 4 < 3, k = w / 4): the block it
+// Epilogue block k (0-4) of lam component c: the block it
 // accumulates (index into R00 R02 R20 R22 R11 P0 P1 P2 W0 W1 W2 I01 I21 I10
 // I12), its first TMEM column and its weight (0: 1, 1: wpy^2, 2: w^2, 3: wpy).
 __device__ __forceinline__ void cov_role(int c, int k, int &blk, int &col, int &wt) {
@@ -122,6 +120,46 @@ __device__ __forceinline__ void cov_role(int c, int k, int &blk, int &col, int &
     default: blk = 12; g = 4; wt = 3; break;  //        I21
   }
   col = 32 * g;
+}
+
+// Warp roles.  A warp reads the TMEM lanes of its quarter (warp % 4), which
+// is also its scheduler partition.  The lam rows of component c sit in lane
+// quarter c, and those of component 1 a second time in quarter 3, so the 15
+// epilogue warps take partitions 0 (component 0, five blocks), 1 (component
+// 1, three blocks), 2 (component 2, five blocks) and 3 (component 1, two
+// blocks); with the MMA warp on partition 3 the 8 producer warps, which issue
+// most of the instructions, spread 1 / 3 / 1 / 3 over the partitions.
+// Returns 0 (epilogue: component c, block k of it), 1 (MMA) or 2 (producer
+// number pidx).
+__device__ __forceinline__ int cov_warp_role(int w, int &c, int &k, int &pidx) {
+  const int q = w & 3, r = w >> 2;  // partition, rank on it (0..5)
+  c = k = pidx = 0;
+  if (q == 0 || q == 2) {
+    if (r < 5) {
+      c = q;
+      k = r;
+      return 0;
+    }
+    pidx = q == 0 ? 0 : 1;  // warps 20, 22
+    return 2;
+  }
+  if (q == 1) {
+    if (r < 3) {
+      c = 1;
+      k = r;  // blocks 0-2 of component 1
+      return 0;
+    }
+    pidx = 2 + (r - 3);  // warps 13, 17, 21
+    return 2;
+  }
+  if (r == 0) return 1;  // warp 3
+  if (r < 3) {
+    c = 1;
+    k = 2 + r;  // blocks 3, 4 of component 1, lane quarter 3
+    return 0;
+  }
+  pidx = 5 + (r - 3);  // warps 15, 19, 23
+  return 2;
 }
 
 struct CovArgs {
@@ -174,10 +212,11 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
   const int nch = (ga.nsrc + cov::kG - 1) / cov::kG;  // stages per (element, pair)
   const int my_elems = (ga.n_elem - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
   const uint32_t total = (uint32_t)max(my_elems, 0) * (uint32_t)ga.npairs * (uint32_t)nch;
-  const bool epi = warp < 20 && (warp & 3) != 3;
+  int rc, rk, rp;
+  const int role = cov_warp_role(warp, rc, rk, rp);
 
-  if (warp != cov::kMmaWarp && !epi) {
-    // =================== producers (warps 7, 11, 15, 19, 20-23)
+  if (role == 2) {
+    // =================== producers (warps 13, 15, 17, 19, 20-23)
     // Thread pt (0..255) owns node a = 8 ah + a7 and source g = 2 gh + g1 of
     // every stage (a7 = pt bits 0-2, g1 = bit 3, ah = bits 4-5, gh = bits
     // 6-7; a >= 25: no node): it copies the node's three DOFs of u and of
@@ -188,7 +227,7 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
     // 96 + 32c + a (u) at K = 2g.  A warp's 32 threads cover the 16
     // (row mod 8, g mod 2) shared-memory bank classes twice, so each 8-byte
     // tile store is two wavefronts.
-    const int pt0 = (warp < 20 ? (warp >> 2) - 1 : warp - 16) * 32 + lane;
+    const int pt0 = rp * 32 + lane;
     const int a = ((pt0 >> 4) & 3) * 8 + (pt0 & 7);
     const int g = ((pt0 >> 6) & (cov::kG / 2 - 1)) * 2 + ((pt0 >> 3) & 1);
     const bool node = a < kNen;
@@ -262,10 +301,14 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
             *reinterpret_cast<uint2 *>(d + cov::kBImOff) = make_uint2(hi, hr ^ 0x80000000u);
             *reinterpret_cast<uint2 *>(d + cov::kBTile + cov::kBImOff) =
                 make_uint2(li, lr ^ 0x80000000u);
-          } else {  // lam -> A row (hi, then lo)
+          } else {  // lam -> A row (hi, then lo); component 1 also to row 96 + a
             uint8_t *d = st + to_a + 512 * c;
             *reinterpret_cast<uint2 *>(d) = make_uint2(hr, hi);
             *reinterpret_cast<uint2 *>(d + cov::kATile) = make_uint2(lr, li);
+            if (c == 1) {
+              *reinterpret_cast<uint2 *>(d + 1024) = make_uint2(hr, hi);
+              *reinterpret_cast<uint2 *>(d + 1024 + cov::kATile) = make_uint2(lr, li);
+            }
           }
         }
       }
@@ -274,7 +317,7 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
       if (lane == 0) mbar_arrive(smem_u32(&bar_bfull[bs]));
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
-  } else if (warp == cov::kMmaWarp) {
+  } else if (role == 1) {
     // =================== MMA issuer
     if (lane == 0) {
       const uint32_t sbase = smem_u32(sm);
@@ -328,10 +371,9 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
     __syncwarp();
   } else {
     // =================== epilogue (15 warps)
-    const int c = warp & 3, k = warp >> 2;
     int blk, col0, wt;
-    cov_role(c, k, blk, col0, wt);
-    const uint32_t lane_base = (uint32_t)(32 * c) << 16;
+    cov_role(rc, rk, blk, col0, wt);
+    const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;  // lane quarter = partition
     double acc[kNen];
 #pragma unroll
     for (int j = 0; j < kNen; j++) acc[j] = 0.0;
