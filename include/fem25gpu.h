@@ -197,7 +197,11 @@ int fem25_addblk_dev(fem25_ctx *ctx, int nsrc, const float *ue, float *sol, void
  *                               any accumulation still pending on the context;
  *   FEM25_PREC_TF32X3_POINTWISE split-precision tensor cores interpolating
  *                               both fields at the 169 points per (pair,
- *                               source), no accumulator memory.
+ *                               source), no accumulator memory; faster for
+ *                               one-shot calls with few (pair, source)
+ *                               fields, as the covariance form's contraction
+ *                               is a fixed cost per call (about 40 fields on
+ *                               a 48 000-element mesh break even).
  * Pairs are passed to the kernels by value, 64 per launch; the call only
  * enqueues work and may be recorded into a CUDA graph once the first
  * split-precision call of that kind on the context (which allocates or

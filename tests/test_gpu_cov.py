@@ -5,9 +5,10 @@ Per element the weighted covariances sum conj(lam) u^T of the nodal fields
 are accumulated over (pair, source) on tcgen05 tensor cores in 3xTF32 and
 contracted once in FP64.  Checks: the oracle's exact gradient (grad_exact,
 a loop-for-loop restatement of the KM25ISOQ derivative sums) on the
-half-space, jittered and topographic layouts with source counts that fill
-part of a 16-source stage; the FP64 kernel; the split calls against the
-one-shot call; and the accumulator's empty / pending states.
+half-space, jittered, topographic and layered layouts with source counts
+that fill 8-source stages partly (1, 5, 17, 33 sources); the FP64 kernel; the
+split calls against the one-shot call; the accumulator's empty / pending
+states; split calls recorded into a CUDA graph.
 
 Tolerances: 2e-5 relative (2-norm per parameter) against the oracle, as
 for the pointwise split-precision kernel; split vs one-shot 1e-12 (the same
@@ -95,4 +96,51 @@ def test_split_calls_equal_one_shot():
     ctx.gradient(freqs[2:], pys[2:], nsrc, d_u[2:], d_l[2:], both, FEM25_PREC_TF32X3)
     rel = float(torch.linalg.norm(both - one) / torch.linalg.norm(one))
     assert rel <= 1e-12
+    ctx.close()
+
+
+def test_split_calls_record_into_a_graph():
+    """Accumulate calls recorded together with the finalize that consumes
+    them replay to the eager result on every replay, including after the
+    fields are overwritten in place."""
+    mesh, pairs, _ = synth.make_config(0, nx=10, nz=6)
+    g = oracle.graph_build(mesh)
+    ctx = Context(mesh, g)
+    use = [pairs[2], pairs[7], pairs[12]]
+    nsrc = 5
+    rng = np.random.default_rng(83)
+    u, lam = _fields(rng, len(use), nsrc, g.ndof)
+    d_u, d_l = torch.from_numpy(u).to(_dev()), torch.from_numpy(lam).to(_dev())
+    freqs, pys = [p[0] for p in use], [p[1] for p in use]
+    eager = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=_dev())
+    for k in range(len(use)):  # the uncaptured first call allocates the accumulators
+        ctx.gradient_accumulate([freqs[k]], [pys[k]], nsrc, d_u[k:k + 1], d_l[k:k + 1])
+    ctx.gradient_finalize(eager)
+    torch.cuda.synchronize()
+    got = torch.zeros_like(eager)
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(graph, stream=side):
+            st = torch.cuda.current_stream()
+            got.zero_()
+            for k in range(len(use)):
+                ctx.gradient_accumulate([freqs[k]], [pys[k]], nsrc, d_u[k:k + 1], d_l[k:k + 1],
+                                        stream=st)
+            ctx.gradient_finalize(got, stream=st)
+    torch.cuda.current_stream().wait_stream(side)
+    for rep in range(2):
+        graph.replay()
+        torch.cuda.synchronize()
+        rel = float(torch.linalg.norm(got - eager) / torch.linalg.norm(eager))
+        assert rel <= 1e-12, (rep, rel)
+    d_u.mul_(0.5 - 0.5j)
+    graph.replay()
+    again = torch.zeros_like(eager)
+    ctx.gradient(freqs, pys, nsrc, d_u, d_l, again, FEM25_PREC_TF32X3)
+    torch.cuda.synchronize()
+    assert float(torch.linalg.norm(got - again) / torch.linalg.norm(again)) <= 1e-12
+    assert float(torch.linalg.norm(got - eager) / torch.linalg.norm(eager)) > 1e-3
+    del graph
     ctx.close()

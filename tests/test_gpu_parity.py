@@ -272,7 +272,7 @@ def test_gradient_fp64_source_tiles_agree(tile, monkeypatch):
 def test_gradient_tf32x3_matches_oracle(nsrc, prec):
     """Split-precision tensor-core gradients.  Pointwise form: 3 pairs x 7
     sources = 21 combos exercises four full stages of 5 combos and a ragged
-    one, nsrc=1 a stage of 3.  Covariance form: a partly filled 16-source
+    one, nsrc=1 a stage of 3.  Covariance form: a partly filled 8-source
     stage per pair."""
     mesh, pairs, _ = synth.make_config(0, nx=10, nz=6)
     g = oracle.graph_build(mesh)
