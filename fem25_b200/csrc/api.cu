@@ -117,12 +117,25 @@ int read_err_word(Ctx *c, cudaStream_t st) {
     cudaMemsetAsync(c->d_err, 0, sizeof(int), st);
     return fail(c, FEM25_ERR_JACOBIAN, buf);
   }
+  if (h <= -1000000) {
+    // a bounded wait of a tensor-core gradient kernel ran out (-1000001..:
+    // pointwise form, -2000001..: covariance form; the last digit names the
+    // hand-off); the kernel drained its schedule and returned
+    char buf[160];
+    std::snprintf(buf, sizeof buf,
+                  "gradient: a tensor-core pipeline wait timed out (code %d); results of that "
+                  "launch are invalid",
+                  h);
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), st);
+    return fail(c, FEM25_ERR_CUDA, buf);
+  }
   if (h < 0) {
     cudaMemsetAsync(c->d_err, 0, sizeof(int), st);
     return fail(c, FEM25_ERR_PATTERN, "element entry without a CSR / CSC slot");
   }
   return FEM25_OK;
 }
+
 
 int upload_model(Ctx *c, const double *ecoeff, const double *dens) {
   const size_t n = c->nnpg;
@@ -596,6 +609,13 @@ int fem25_assemble_batch_dev(fem25_ctx *h, int n, const char *cftype, const doub
   CK(launch_stream_batch(c, n, sys.data(), ring_base, slot_stride, nslots, st), "stream kernel");
   if (c->prof) CK(cudaEventRecord(c->ev[1], st), "event");
   return FEM25_OK;
+}
+
+int fem25_sync_status(fem25_ctx *h, void *stream) {
+  if (!h) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  CK(cudaSetDevice(c->device), "set device");
+  return read_err_word(c, (cudaStream_t)stream);
 }
 
 int fem25_tuning(const fem25_ctx *h, int *stream_variant, int *grad_tile) {

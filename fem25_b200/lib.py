@@ -74,6 +74,7 @@ def lib():
         L.fem25_gradient_dev.argtypes = [vp, i, vp, vp, i, vp, vp, i, vp, vp]
         L.fem25_gradient_accumulate_dev.argtypes = [vp, i, vp, vp, i, vp, vp, vp]
         L.fem25_gradient_finalize_dev.argtypes = [vp, vp, vp]
+        L.fem25_sync_status.argtypes = [vp, vp]
         L.fem25_ref_gradient_dev.argtypes = [vp, C.c_char_p, d, d, d, vp, vp, i, vp, vp]
         L.fem25_ref_gradient_info.argtypes = [vp, C.POINTER(i), C.POINTER(ll), vp]
         L.fem25_ref_vforce2_dev.argtypes = [vp, C.c_char_p, d, d, vp, vp, vp]
@@ -355,6 +356,11 @@ class Context:
         p = np.ascontiguousarray(pys, np.float64)
         self._check(lib().fem25_gradient_accumulate_dev(self.h, len(f), _np(f), _np(p), nsrc,
                                                         _ptr(u), _ptr(lam), _stream(stream)))
+
+    def sync_status(self, stream=None):
+        """Waits for the stream; raises Fem25Error for what kernels recorded
+        on the device (Jacobian failures, timed-out pipeline waits)."""
+        self._check(lib().fem25_sync_status(self.h, _stream(stream)))
 
     def gradient_finalize(self, grad, stream=None):
         """grad += the gradient of everything accumulated since the last

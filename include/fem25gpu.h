@@ -359,6 +359,15 @@ int fem25_misfit_noalloc_dev(fem25_ctx *ctx, int nsrc, int nrec, const int *mrdo
  * and the source tile of the FP64 gradient (2, 4 or 8 sources per
  * shared-memory pass). */
 int fem25_tuning(const fem25_ctx *ctx, int *stream_variant, int *grad_tile);
+
+/* Waits for the stream and reports what the context's kernels recorded on
+ * the device since the last check: FEM25_ERR_JACOBIAN for an element whose
+ * Jacobian the gradient kernels found undefined or negative, FEM25_ERR_CUDA
+ * for a bounded pipeline wait of a tensor-core gradient kernel that ran out
+ * (that launch's results are invalid).  The asynchronous entry points
+ * (gradient, batch) do not wait; call this where the stream is synchronised
+ * anyway (after a gradient, before reading it back). */
+int fem25_sync_status(fem25_ctx *ctx, void *stream);
 int fem25_profile_enable(fem25_ctx *ctx, int enable);
 int fem25_profile_ms(fem25_ctx *ctx, int which, double *ms);
 
