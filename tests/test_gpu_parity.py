@@ -546,6 +546,13 @@ def test_dispersive_batched_and_gradient_rejected(case_disp):
     assert ei.value.code == 7
     u = torch.zeros((1, 1, g.ndof), dtype=torch.complex128, device=_dev())
     d_g = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=_dev())
+    for prec in (FEM25_PREC_FP64, FEM25_PREC_TF32X3, FEM25_PREC_TF32X3_POINTWISE):
+        with pytest.raises(Fem25Error) as ei:
+            ctx.gradient([0.5], [0.0], 1, u, u, d_g, prec)
+        assert ei.value.code == 7
     with pytest.raises(Fem25Error) as ei:
-        ctx.gradient([0.5], [0.0], 1, u, u, d_g)
+        ctx.gradient_accumulate([0.5], [0.0], 1, u, u)
+    assert ei.value.code == 7
+    with pytest.raises(Fem25Error) as ei:
+        ctx.gradient_finalize(d_g)
     assert ei.value.code == 7
