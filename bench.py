@@ -12,11 +12,15 @@ Also reported on the same line:
   * plain_fp64: the per-(omega, py) FP64 element + gather kernels (systems/s)
   * e2e: ASMBLE_DRIVER through the C ABI with host buffers (model upload from
     pinned memory, COMPLEX*8 CDIST read back to pinned memory) -- systems/s
-  * gradient: exact adjoint gradient, elem.rhs/s, 400x120 layered mesh, 32 sources
+  * gradient: exact adjoint gradient, elem.rhs/s, 400x120 layered mesh, 32
+    sources x 2 pairs: FP64; split precision in the covariance form (one-shot
+    call, and its accumulation and contraction kernels apart, with an HBM
+    roofline of the accumulation) and in the pointwise form (tensor roofline)
   * pipeline: the uneven-batch workload (600x200 jittered mesh with
     topography, 24 frequencies 0.1-2.4 Hz x ceil(16 f / 0.1) ky = 4800 systems,
-    64 sources): batched assembly + split-precision gradient against the plain
-    per-(omega, py) FP64 assembly + FP64 gradient
+    64 sources): batched assembly + split-precision covariance accumulation per
+    pair + one contraction, against the plain per-(omega, py) FP64 assembly +
+    FP64 gradient per pair
   * roofline of the streaming kernel and the CPU baseline (the oracle).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
