@@ -45,6 +45,12 @@ STREAM_KERNELS = {0: "k_stream<1>", 1: "k_stream<2>", 2: "k_stream<4>", 3: "k_st
                   4: "k_stream_tma<64>", 5: "k_stream_tma<128>", 6: "k_stream_ring<256, 4>",
                   7: "k_stream_ring<512, 4>", 8: "k_stream_big<512, 4>", 9: "k_stream_big<256, 4>"}
 UNIT = "assemblies/s"
+# DRAM traffic of k_stream_big<512, 4> from one ncu capture of the 100x40
+# layout of the same 400x120 layered mesh (NNZ 20 418 489), 16 systems per
+# launch: 329.8 MB read (the entry basis and block terms, once per launch)
+# and 5.168 GB written (the values; the last ~60 MB still in L2 at kernel end)
+STREAM_BIG_READ_PER_ENTRY = 329.8e6 / 20418489           # bytes per CSR entry and launch
+STREAM_BIG_WRITE_PER_ENTRY = 5.168e9 / (16 * 20418489)   # bytes per CSR entry and system
 
 
 def peaks():
@@ -416,6 +422,12 @@ def main():
     # variants 8 and 9, up to 1024 systems each, never more than the ring)
     per_launch = min(1024 if ctx.tuning()["stream_variant"] >= 8 else 16, nslots)
     launches_per_step = 2 * len(set(freqs)) + -(-nsys // per_launch)
+    # DRAM bytes of one launch of the captured kernel, scaled from the small
+    # case: reads by the entries, writes by entries x systems per launch
+    traffic = None
+    if ctx.tuning()["stream_variant"] == 8:
+        traffic = (STREAM_BIG_READ_PER_ENTRY * nz +
+                   STREAM_BIG_WRITE_PER_ENTRY * nz * per_launch)
 
     # ---------------- plain FP64 per-system path (device buffers)
     o128 = torch.empty(nz, dtype=torch.complex128, device=dev)
@@ -593,7 +605,13 @@ def main():
                       "setup_s": round(setup_s, 2)},
            "plain_fp64": {"value": plain_rate, "unit": UNIT, "speedup_batched": value / world / plain_rate},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "traffic": None,
+                        "frac": achieved / peak, "traffic": traffic,
+                        "traffic_unit": "bytes per launch",
+                        "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a "
+                                        "100x40 capture of the same kernel, scaled to this "
+                                        "launch (reads by CSR entries, writes by entries x "
+                                        "systems); null when another variant is tuned",
+                        "algorithmic_bytes_per_launch": 16.0 * nz * per_launch,
                         "kernel": STREAM_KERNELS.get(tuning["stream_variant"], "k_stream"),
                         "kernel_ms": kms, "peak_kind": peak_kind,
                         "algorithmic_bytes": "16 B x NNZ per system (complex128 values written)"},
