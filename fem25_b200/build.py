@@ -4,7 +4,9 @@
 
 nvcc cross-compiles without a GPU.  The plain-assembly and reference-
 bookkeeping kernels are compiled with -fmad=false (no FMA contraction, the
-reference's separately rounded arithmetic); everything else uses FMA.
+reference's separately rounded arithmetic); everything else uses FMA.  The
+plain element kernels are also compiled a second time with FMA allowed
+(k_plain_fma.cu.o), the benchmark option of fem25_plain_fma.
 """
 from __future__ import annotations
 
@@ -24,6 +26,7 @@ COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp
 
 UNITS = [
     ("k_plain.cu", ["-fmad=false"]),
+    ("k_plain.cu", ["-DFEM25_PLAIN_FMA"], "k_plain_fma.cu.o"),
     ("k_ref.cu", ["-fmad=false"]),
     ("k_batch.cu", []),
     ("k_grad.cu", []),
@@ -57,9 +60,10 @@ def build(verbose=False, extra=()):
     headers = [os.path.join(SRC, f) for f in os.listdir(SRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(ROOT, "include", "fem25gpu.h"))
     objs = []
-    for name, flags in UNITS:
+    for unit in UNITS:
+        name, flags = unit[0], unit[1]
         src = os.path.join(SRC, name)
-        obj = os.path.join(OBJ, name + ".o")
+        obj = os.path.join(OBJ, unit[2] if len(unit) > 2 else name + ".o")
         objs.append(obj)
         if _stale(obj, [src, __file__] + headers):
             out = _run([NVCC] + COMMON + list(flags) + list(extra) + ["-Xptxas", "-v", "-c", "-o", obj, src])

@@ -121,12 +121,13 @@ int read_err_word(Ctx *c, cudaStream_t st) {
     // a bounded wait of a tensor-core gradient kernel ran out (-1000001..:
     // pointwise form, -2000001..: covariance form; the last digit names the
     // hand-off); the kernel drained its schedule and returned
-    char buf[160];
+    char buf[200];
     std::snprintf(buf, sizeof buf,
                   "gradient: a tensor-core pipeline wait timed out (code %d); results of that "
-                  "launch are invalid",
+                  "launch, and covariances accumulated since the last finalize, are discarded",
                   h);
     cudaMemsetAsync(c->d_err, 0, sizeof(int), st);
+    c->cov_pending = false;  // the next accumulation overwrites the sums
     return fail(c, FEM25_ERR_CUDA, buf);
   }
   if (h < 0) {
@@ -514,7 +515,10 @@ int fem25_assemble_dev(fem25_ctx *h, char cftype, double freq, double py, double
   int r = ensure_plain(c, st);
   if (r) return r;
   if (c->prof) CK(cudaEventRecord(c->ev[2], st), "event");
-  CK(launch_elem_plain(c, cftype, freq, py, 0, c->nelem, st), "element kernel");
+  if (c->plain_fma)
+    CK(launch_elem_plain_fma(c, cftype, freq, py, 0, c->nelem, st), "element kernel (FMA)");
+  else
+    CK(launch_elem_plain(c, cftype, freq, py, 0, c->nelem, st), "element kernel");
   CK(launch_gather_plain(c, csr128, csr64, 0, c->nzero, st), "gather kernel");
   if (c->prof) CK(cudaEventRecord(c->ev[3], st), "event");
   return FEM25_OK;
@@ -616,6 +620,19 @@ int fem25_sync_status(fem25_ctx *h, void *stream) {
   Ctx *c = &h->c;
   CK(cudaSetDevice(c->device), "set device");
   return read_err_word(c, (cudaStream_t)stream);
+}
+
+int fem25_plain_fma(fem25_ctx *h, int enable) {
+  if (!h) return FEM25_ERR_ARG;
+  h->c.plain_fma = enable != 0;
+  return FEM25_OK;
+}
+
+int fem25_test_waits(fem25_ctx *h, long long limit_cycles, int inject) {
+  if (!h || (inject != 0 && inject != 1)) return FEM25_ERR_ARG;
+  h->c.wait_limit = limit_cycles > 0 ? limit_cycles : 0;
+  h->c.wait_inject = inject;
+  return FEM25_OK;
 }
 
 int fem25_tuning(const fem25_ctx *h, int *stream_variant, int *grad_tile) {

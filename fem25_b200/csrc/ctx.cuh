@@ -143,6 +143,12 @@ struct Ctx {
   cudaStream_t copy_st = nullptr;
   std::vector<cudaEvent_t> drv_ev;
   DenseLU *dense = nullptr;
+  // fem25_assemble_dev with the FMA build of the element kernels
+  bool plain_fma = false;
+  // bounded waits of the tensor-core gradient kernels: limit in SM clocks
+  // (0: the default, about half a second) and the time-out test hook
+  long long wait_limit = 0;
+  int wait_inject = 0;
   // optional CUDA-event timing of the dominant kernels
   bool prof = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -151,6 +157,9 @@ struct Ctx {
 // kernels / launchers (defined in the .cu files)
 cudaError_t launch_elem_plain(Ctx *c, char cftype, double freq, double py, int e0, int e1,
                               cudaStream_t st);
+// the same element kernels compiled with FMA contraction (fem25_plain_fma)
+cudaError_t launch_elem_plain_fma(Ctx *c, char cftype, double freq, double py, int e0, int e1,
+                                  cudaStream_t st);
 cudaError_t launch_gather_plain(Ctx *c, double *csr128, float *csr64, long long nz0,
                                 long long nz1, cudaStream_t st);
 cudaError_t build_gather_map(Ctx *c, cudaStream_t st);

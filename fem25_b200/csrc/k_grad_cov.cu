@@ -164,7 +164,11 @@ __device__ __forceinline__ int cov_warp_role(int w, int &c, int &k, int &pidx) {
 
 struct CovArgs {
   int npairs, nsrc, ndof, n_elem;
-  int add;  // 1: add into the accumulators, 0: overwrite them
+  int add;          // 1: add into the accumulators, 0: overwrite them
+  int inject;       // 1: producer warp 0 of CTA 0 withholds its first stage
+                    // arrival, so the MMA thread's wait runs out (a test of
+                    // the time-out path)
+  long long spin;   // SM clocks a pipeline wait may take before it gives up
 };
 
 __global__ void __launch_bounds__(cov::kThreads, 1)
@@ -282,7 +286,8 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
         default: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
       }
       const int bs = (int)(s % cov::kNB);
-      mbar_wait(smem_u32(&bar_bempty[bs]), ((s / cov::kNB) & 1u) ^ 1u, drain, err, -2000001);
+      mbar_wait(smem_u32(&bar_bempty[bs]), ((s / cov::kNB) & 1u) ^ 1u, drain, err, -2000001,
+                ga.spin);
       if (node) {
         const uint8_t *rs = raw + (s % cov::kRawD) * cov::kRawStage + pt0 * 16;
         uint8_t *st = sm + bs * cov::kStage;
@@ -314,7 +319,8 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
-      if (lane == 0) mbar_arrive(smem_u32(&bar_bfull[bs]));
+      const bool withhold = ga.inject && blockIdx.x == 0 && rp == 0 && s == 0;
+      if (lane == 0 && !withhold) mbar_arrive(smem_u32(&bar_bfull[bs]));
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
   } else if (role == 1) {
@@ -333,8 +339,10 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
             const bool last = ch % cov::kDrain == cov::kDrain - 1 || ch == nch - 1;
             const int ts = (int)(unit & 1u), bs = (int)(s % cov::kNB);
             if (first)
-              mbar_wait(smem_u32(&bar_tempty[ts]), ((unit >> 1) & 1u) ^ 1u, drain, err, -2000002);
-            mbar_wait(smem_u32(&bar_bfull[bs]), (s / cov::kNB) & 1u, drain, err, -2000003);
+              mbar_wait(smem_u32(&bar_tempty[ts]), ((unit >> 1) & 1u) ^ 1u, drain, err, -2000002,
+                        ga.spin);
+            mbar_wait(smem_u32(&bar_bfull[bs]), (s / cov::kNB) & 1u, drain, err, -2000003,
+                      ga.spin);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t td = tmem + (uint32_t)ts * cov::kTmemStage;
             const int nact = min(cov::kG, ga.nsrc - ch * cov::kG);
@@ -384,7 +392,7 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
         const double w = wt == 0 ? 1.0 : wt == 1 ? pr.y * pr.y : wt == 2 ? pr.x * pr.x : pr.y;
         for (int ch = 0; ch < nch; ch += cov::kDrain, unit++) {
           const int ts = (int)(unit & 1u);
-          mbar_wait(smem_u32(&bar_tfull[ts]), (unit >> 1) & 1u, drain, err, -2000005);
+          mbar_wait(smem_u32(&bar_tfull[ts]), (unit >> 1) & 1u, drain, err, -2000005, ga.spin);
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint32_t tb = tmem + lane_base + (uint32_t)ts * cov::kTmemStage + (uint32_t)col0;
           __syncwarp();
@@ -752,6 +760,8 @@ cudaError_t launch_grad_cov(Ctx *c, const PairTable &pt, int npairs, int nsrc, c
   ga.ndof = c->ndof;
   ga.n_elem = c->n_nonpml;
   ga.add = c->cov_pending ? 1 : 0;
+  ga.inject = c->wait_inject;
+  ga.spin = c->wait_limit > 0 ? c->wait_limit : kTcSpinCycles;
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
   const int grid = std::min(nsm, c->n_nonpml);

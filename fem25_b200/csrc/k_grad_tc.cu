@@ -106,7 +106,11 @@ __host__ __device__ __forceinline__ int tail_lane(int d, int qt) {
 
 struct TcArgs {
   int npairs, nsrc, ndof, nnpg, n_elem;
-  int ncombo;  // npairs * nsrc
+  int ncombo;      // npairs * nsrc
+  int inject;      // 1: the first producer warp of CTA 0 withholds its first
+                   // stage arrival, so the MMA thread's wait runs out (a test
+                   // of the time-out path)
+  long long spin;  // SM clocks a pipeline wait may take before it gives up
 };
 
 // Per-point geometry of the epilogue: inverse-Jacobian rows and W_q SF_a(q).
@@ -271,7 +275,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
       FEM25_TC_LOAD_STAGE(0);
       for (uint32_t s = 0;; s++) {
         const int bs = (int)(s % tc::kNB);
-        mbar_wait(smem_u32(&bar_bempty[bs]), ((s / tc::kNB) & 1u) ^ 1u, drain, err, -1000001);
+        mbar_wait(smem_u32(&bar_bempty[bs]), ((s / tc::kNB) & 1u) ^ 1u, drain, err, -1000001,
+                  ga.spin);
         uint8_t *bh = sB + bs * tc::kBStage;
         // items past the last combo of the stage store zeros into rows the
         // epilogue ignores; empty slots store nothing
@@ -304,7 +309,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();
-        if (lane == 0) mbar_arrive(smem_u32(&bar_bfull[bs]));
+        const bool withhold = ga.inject && blockIdx.x == 0 && warp == tc::kProdWarp0 && s == 0;
+        if (lane == 0 && !withhold) mbar_arrive(smem_u32(&bar_bfull[bs]));
         int ein = ei, bn = b + 1;
         if (bn == nb) {
           bn = 0;
@@ -331,8 +337,9 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
       for (int ei = blockIdx.x; ei < ga.n_elem; ei += gridDim.x) {
         for (int b = 0; b < nb; b++, s++) {
           const int bs = (int)(s % tc::kNB), ts = (int)(s & 1u);
-          mbar_wait(smem_u32(&bar_bfull[bs]), (s / tc::kNB) & 1u, drain, err, -1000002);
-          mbar_wait(smem_u32(&bar_tempty[ts]), ((s >> 1) & 1u) ^ 1u, drain, err, -1000003);
+          mbar_wait(smem_u32(&bar_bfull[bs]), (s / tc::kNB) & 1u, drain, err, -1000002, ga.spin);
+          mbar_wait(smem_u32(&bar_tempty[ts]), ((s >> 1) & 1u) ^ 1u, drain, err, -1000003,
+                    ga.spin);
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint64_t bstage = bdesc + (uint64_t)((bs * tc::kBStage) >> 4);
           const uint32_t tstage = tmem + (uint32_t)(ts * tc::kTmemStage);
@@ -405,7 +412,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         const int ts = (int)(s & 1u);
         const int c0 = b * tc::kC;
         const int nc = min(tc::kC, ga.ncombo - c0);
-        mbar_wait(smem_u32(&bar_tfull[ts]), (s >> 1) & 1u, drain, err, -1000005);
+        mbar_wait(smem_u32(&bar_tfull[ts]), (s >> 1) & 1u, drain, err, -1000005, ga.spin);
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t tbase = tmem + lane_base + (uint32_t)(ts * tc::kTmemStage);
         float tl = 0.f, tm = 0.f, tr = 0.f;
@@ -640,6 +647,8 @@ cudaError_t launch_grad_tc(Ctx *c, const PairTable &pt, int npairs, int nsrc, co
   ga.nnpg = c->nnpg;
   ga.n_elem = c->n_nonpml;
   ga.ncombo = npairs * nsrc;
+  ga.inject = c->wait_inject;
+  ga.spin = c->wait_limit > 0 ? c->wait_limit : kTcSpinCycles;
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
   const int grid = std::min(nsm, c->n_nonpml);

@@ -5,13 +5,22 @@
 //
 // This translation unit is compiled with -fmad=false: every multiply and add
 // is rounded separately, in the order the reference writes them, so the FP64
-// sums are the reference arithmetic without FMA contraction.
+// sums are the reference arithmetic without FMA contraction.  It is compiled
+// a second time with FEM25_PLAIN_FMA defined and FMA contraction allowed,
+// into the nested namespace fem25::plain_fma, for launch_elem_plain_fma (the
+// same element kernels with fused multiply-adds, a benchmark option of
+// fem25_assemble_dev).
 #include <cub/device/device_scan.cuh>
 
 #include "ctx.cuh"
 #include "kcommon.cuh"
 
+#ifdef FEM25_PLAIN_FMA
 namespace fem25 {
+namespace plain_fma {
+#else
+namespace fem25 {
+#endif
 
 struct PlainArgs {
   double w2, py2, wpy, omega;
@@ -472,6 +481,7 @@ __global__ void __launch_bounds__(kPlainThreads, 1)
   }
 }
 
+#ifndef FEM25_PLAIN_FMA
 // Sum of the element contributions of every nonzero of [nz0, nz1) in element order:
 // FP64 (complex128 output) and the reference's COMPLEX*8 accumulation
 // CDIST = CDIST + CMPLX(CARG) (asmble.f90:302-305).
@@ -586,11 +596,13 @@ PmlParams pml_params(const Ctx *c, char cftype, double freq) {
   return p;
 }
 
+#endif  // FEM25_PLAIN_FMA
+
 cudaError_t launch_elem_plain(Ctx *c, char cftype, double freq, double py, int e0, int e1,
                               cudaStream_t st) {
   if (e1 <= e0) return cudaSuccess;
   PlainArgs pa;
-  pa.pml = pml_params(c, cftype, freq);
+  pa.pml = fem25::pml_params(c, cftype, freq);
   pa.omega = pa.pml.omega;
   pa.w2 = ipow2(pa.omega);  // OMEGA**2
   pa.py2 = ipow2(py);       // PY**2
@@ -617,6 +629,7 @@ cudaError_t launch_elem_plain(Ctx *c, char cftype, double freq, double py, int e
   return cudaGetLastError();
 }
 
+#ifndef FEM25_PLAIN_FMA
 cudaError_t launch_gather_plain(Ctx *c, double *csr128, float *csr64, long long nz0,
                                 long long nz1, cudaStream_t st) {
   if (nz1 <= nz0) return cudaSuccess;
@@ -673,4 +686,14 @@ cudaError_t build_gather_map(Ctx *c, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+#endif  // FEM25_PLAIN_FMA
+
+#ifdef FEM25_PLAIN_FMA
+}  // namespace plain_fma
+
+cudaError_t launch_elem_plain_fma(Ctx *c, char cftype, double freq, double py, int e0, int e1,
+                                  cudaStream_t st) {
+  return plain_fma::launch_elem_plain(c, cftype, freq, py, e0, e1, st);
+}
+#endif
 }  // namespace fem25

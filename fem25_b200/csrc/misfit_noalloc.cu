@@ -22,7 +22,15 @@
 // Set-up: the first call on each device (with that device current) looks up
 // the scratch's device address with cudaGetSymbolAddress and caches it; this
 // may load the library's device code on that device, so make the first call
-// before any stream capture begins.
+// before any stream capture begins.  The cached address belongs to the
+// device's primary context: after a cudaDeviceReset in the process (or a
+// library that destroys the primary context) it is stale, so the entry point
+// must not be used across a device reset.
+//
+// Host staging: the receiver tables pass through stack buffers of this call
+// with cudaMemcpyAsync, so a call on a stream that is being captured returns
+// FEM25_ERR_ARG (a recorded copy would read those buffers after the call has
+// returned).
 //
 // Concurrency: the scratch is one array per device, shared by every context
 // on it.  Calls that overlap in time on one device (two host threads, or two
@@ -132,13 +140,22 @@ extern "C" int fem25_misfit_noalloc_dev(fem25_ctx *h, int nsrc, int nrec, const 
   }
   cudaError_t e = cudaSetDevice(c->device);
   if (e != cudaSuccess) return cuda_fail(c, e, "set device");
+  cudaStream_t st = (cudaStream_t)stream;
+  {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if ((e = cudaStreamIsCapturing(st, &cs)) != cudaSuccess)
+      return cuda_fail(c, e, "misfit_noalloc: stream status");
+    if (cs != cudaStreamCaptureStatusNone)
+      return fail(c, FEM25_ERR_ARG,
+                  "misfit_noalloc: the stream is being captured; the receiver tables are "
+                  "staged from host buffers that do not outlive the call");
+  }
   unsigned char *base = nullptr;
   if ((e = scratch_on(c->device, &base)) != cudaSuccess) return cuda_fail(c, e, "misfit scratch");
   int *d_mrdof = reinterpret_cast<int *>(base + kOffMrdof);
   float *d_trig = reinterpret_cast<float *>(base + kOffTrig);
   float *d_recv = reinterpret_cast<float *>(base + kOffRecv);
   float *d_part = reinterpret_cast<float *>(base + kOffPart);
-  cudaStream_t st = (cudaStream_t)stream;
   // receiver tables: staged through pageable stack buffers, so the caller's
   // host arrays are no longer needed when the call returns
   const double omega = 6.2831853071795862 * freq;

@@ -7,7 +7,8 @@
 
 namespace fem25 {
 
-// A bounded wait gives up after this many SM clocks (about half a second).
+// A bounded wait gives up after this many SM clocks (about half a second)
+// unless the launch passes another limit.
 constexpr long long kTcSpinCycles = 1000000000LL;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -72,14 +73,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t phase) {
 }
 
 // Bounded wait on an mbarrier phase.  Returns at once in drain mode; on
-// running out it sets the error word and puts the CTA in drain mode.
+// running out (after `limit` SM clocks) it sets the error word and puts the
+// CTA in drain mode.
 __device__ __forceinline__ void mbar_wait(uint32_t mbar, uint32_t phase, volatile int *drain,
-                                          int *err, int code) {
+                                          int *err, int code, long long limit) {
   if (*drain) return;
   const long long t0 = clock64();
   while (!mbar_try_wait(mbar, phase)) {
     if (*drain) return;
-    if (clock64() - t0 > kTcSpinCycles) {
+    if (clock64() - t0 > limit) {
       atomicCAS(err, 0, code);
       *drain = 1;
       return;

@@ -75,6 +75,8 @@ def lib():
         L.fem25_gradient_accumulate_dev.argtypes = [vp, i, vp, vp, i, vp, vp, vp]
         L.fem25_gradient_finalize_dev.argtypes = [vp, vp, vp]
         L.fem25_sync_status.argtypes = [vp, vp]
+        L.fem25_test_waits.argtypes = [vp, ll, i]
+        L.fem25_plain_fma.argtypes = [vp, i]
         L.fem25_ref_gradient_dev.argtypes = [vp, C.c_char_p, d, d, d, vp, vp, i, vp, vp]
         L.fem25_ref_gradient_info.argtypes = [vp, C.POINTER(i), C.POINTER(ll), vp]
         L.fem25_ref_vforce2_dev.argtypes = [vp, C.c_char_p, d, d, vp, vp, vp]
@@ -309,6 +311,11 @@ class Context:
         self._check(lib().fem25_asmble_driver(self.h, self.nzero, cftype.encode(), freq, py, ptr))
         return out
 
+    def plain_fma(self, enable=True):
+        """Benchmark option: assemble() with the FMA build of the element
+        kernels (not bit-identical to the reference arithmetic)."""
+        self._check(lib().fem25_plain_fma(self.h, 1 if enable else 0))
+
     def assemble(self, cftype, freq, py, out128=None, out64=None, stream=None):
         self._check(lib().fem25_assemble_dev(self.h, cftype.encode(), freq, py, _ptr(out128),
                                              _ptr(out64), _stream(stream)))
@@ -361,6 +368,12 @@ class Context:
         """Waits for the stream; raises Fem25Error for what kernels recorded
         on the device (Jacobian failures, timed-out pipeline waits)."""
         self._check(lib().fem25_sync_status(self.h, _stream(stream)))
+
+    def test_waits(self, limit_cycles=0, inject=False):
+        """Test hook of the tensor-core kernels' bounded waits: the limit in SM
+        clocks (0: default) and whether launches withhold one producer arrival
+        so that a wait runs out (see fem25_test_waits)."""
+        self._check(lib().fem25_test_waits(self.h, int(limit_cycles), 1 if inject else 0))
 
     def gradient_finalize(self, grad, stream=None):
         """grad += the gradient of everything accumulated since the last

@@ -132,6 +132,14 @@ int fem25_asmble_driver(fem25_ctx *ctx, int nzloc, char cftype, double freq, dou
 int fem25_assemble_dev(fem25_ctx *ctx, char cftype, double freq, double py, double *csr128,
                        float *csr64, void *stream);
 
+/* Benchmark option of fem25_assemble_dev (no counterpart in the reference):
+ * enable = 1 computes the element matrices with the same kernels compiled
+ * with fused multiply-adds, so the CSR is no longer bit-identical to the
+ * reference arithmetic (it stays within about 1e-15 of it per row);
+ * enable = 0 (the default) restores the separately rounded operations.
+ * fem25_asmble_driver always uses the reference arithmetic. */
+int fem25_plain_fma(fem25_ctx *ctx, int enable);
+
 /* Batched assembly of n systems (cftype[k], freq[k], py[k]) into complex128
  * device slots: system k goes to ring_base + (k % nslots) * slot_stride
  * doubles (slot_stride even and >= 2*NZERO).  Uses the per-mesh affine basis
@@ -336,7 +344,10 @@ int fem25_misfit_dev(fem25_ctx *ctx, int nsrc, int nrec, const int *mrdof, const
  * threads, or two streams with no ordering between them) race on it and give
  * wrong results.  The first call on each device sets the scratch up (looks up
  * its address, which may load the library's device code); make that first
- * call before any stream capture begins. */
+ * call before any stream capture begins.  That address is kept for the life
+ * of the process: do not use this entry point across a cudaDeviceReset.
+ * The receiver tables are staged from host buffers that live only during the
+ * call, so a call on a stream that is being captured returns FEM25_ERR_ARG. */
 #define FEM25_NOALLOC_MAX_REC 2048
 #define FEM25_NOALLOC_MAX_SRC_REC 262144
 int fem25_misfit_noalloc_dev(fem25_ctx *ctx, int nsrc, int nrec, const int *mrdof,
@@ -368,6 +379,15 @@ int fem25_tuning(const fem25_ctx *ctx, int *stream_variant, int *grad_tile);
  * (gradient, batch) do not wait; call this where the stream is synchronised
  * anyway (after a gradient, before reading it back). */
 int fem25_sync_status(fem25_ctx *ctx, void *stream);
+
+/* Test hook of the bounded waits above (no counterpart in the reference):
+ * limit_cycles > 0 sets the SM clocks a pipeline wait of the tensor-core
+ * gradient kernels may take before it gives up (<= 0: the default, about half
+ * a second); inject = 1 makes the next launches withhold one producer
+ * arrival in their first CTA, so that a wait runs out, the launch drains and
+ * fem25_sync_status reports FEM25_ERR_CUDA (the covariances accumulated since
+ * the last finalize are then discarded).  inject = 0 restores normal runs. */
+int fem25_test_waits(fem25_ctx *ctx, long long limit_cycles, int inject);
 int fem25_profile_enable(fem25_ctx *ctx, int enable);
 int fem25_profile_ms(fem25_ctx *ctx, int which, double *ms);
 

@@ -57,7 +57,7 @@ def _setup(L):
     L.orc_asmble.argtypes = [vp, vp, vp, vp, C.c_int, C.c_char, C.c_double, C.c_double,
                              C.c_int, C.c_int, vp, vp]
     L.orc_asmble_rows.argtypes = [vp, vp, vp, vp, C.c_int, vp, C.c_char, C.c_double,
-                                  C.c_double, vp]
+                                  C.c_double, vp, vp]
     L.orc_graph_build.argtypes = [vp, C.POINTER(C.c_int)]
     L.orc_graph_build.restype = vp
     L.orc_graph_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
@@ -191,31 +191,50 @@ def dabm_element(mesh, ielem, inpg, freq, py):
     return out
 
 
-def asmble(mesh, g, cftype, freq, py, elo=0, ehi=None, want64=True):
-    """ASMBLE_DRIVER over elements [elo, ehi): (csr128, csr64)."""
+def asmble(mesh, g, cftype, freq, py, elo=0, ehi=None, want64=True, want128=True, out=None):
+    """ASMBLE_DRIVER over elements [elo, ehi): (csr128, csr64).  ``out`` =
+    (csr128, csr64) arrays to add into instead of fresh zeroed ones (either
+    may be None, which skips that output)."""
     om = OracleMesh(mesh)
     ehi = mesh.nelem if ehi is None else ehi
-    c128 = np.zeros(g.nzero, np.complex128)
-    c64 = np.zeros(g.nzero, np.complex64) if want64 else None
+    if out is not None:
+        c128, c64 = out
+    else:
+        c128 = np.zeros(g.nzero, np.complex128) if want128 else None
+        c64 = np.zeros(g.nzero, np.complex64) if want64 else None
     ierr = lib().orc_asmble(om.ptr, _p(g.lm), _p(g.irptr), _p(g.jcptr), g.ndof,
-                            cftype.encode(), freq, py, elo, ehi, _p(c128),
-                            _p(c64) if want64 else None)
+                            cftype.encode(), freq, py, elo, ehi,
+                            _p(c128) if c128 is not None else None,
+                            _p(c64) if c64 is not None else None)
     if ierr:
         raise RuntimeError(f"oracle asmble ierr={ierr}")
     return c128, c64
 
 
-def asmble_rows(mesh, lm, irptr, jcptr, ndof, rows, cftype, freq, py):
-    """CSR values of the given 1-based DOF rows only (others left zero)."""
+def asmble_rows(mesh, g, rows, cftype, freq, py):
+    """CSR values of the given 1-based DOF rows only: (idx, csr128, csr64) with
+    idx the 0-based CSR positions of the rows' entries (rows in the given
+    order, each in JCPTR order) and the values at those positions, equal bit
+    for bit to the full ``asmble`` there."""
     om = OracleMesh(mesh)
-    mask = np.zeros(ndof, np.uint8)
-    mask[np.asarray(rows) - 1] = 1
-    out = np.zeros(len(jcptr), np.complex128)
-    ierr = lib().orc_asmble_rows(om.ptr, _p(lm), _p(irptr), _p(jcptr), ndof, _p(mask),
-                                 cftype.encode(), freq, py, _p(out))
+    rows = np.asarray(rows, np.int64)
+    if len(np.unique(rows)) != len(rows) or rows.min() < 1 or rows.max() > g.ndof:
+        raise ValueError("rows must be distinct 1-based DOFs")
+    starts = g.irptr[rows - 1].astype(np.int64) - 1
+    lens = (g.irptr[rows] - g.irptr[rows - 1]).astype(np.int64)
+    rowoff = np.full(g.ndof, -1, np.int64)
+    rowoff[rows - 1] = np.concatenate([[0], np.cumsum(lens)[:-1]])
+    n = int(lens.sum())
+    idx = np.concatenate([np.arange(s0, s0 + l) for s0, l in zip(starts, lens)])
+    c128 = np.zeros(n, np.complex128)
+    c64 = np.zeros(n, np.complex64)
+    ierr = lib().orc_asmble_rows(om.ptr, _p(np.ascontiguousarray(g.lm, np.int32)),
+                                 _p(np.ascontiguousarray(g.irptr, np.int32)),
+                                 _p(np.ascontiguousarray(g.jcptr, np.int32)), g.ndof, _p(rowoff),
+                                 cftype.encode(), freq, py, _p(c128), _p(c64))
     if ierr:
         raise RuntimeError(f"oracle asmble_rows ierr={ierr}")
-    return out
+    return idx, c128, c64
 
 
 def peff(g, cdist64, ue64):
@@ -231,6 +250,21 @@ def addblk(g, ue64, sol64):
     out = np.array(sol64, np.complex64, copy=True)
     lib().orc_addblk(g.ndof, _p(g.cnp), _p(np.ascontiguousarray(ue64, np.complex64)), _p(out))
     return out
+
+
+def verify_steve(g, cdist64, u0, sol):
+    """VERIFY_STEVE: (DIF1, BUFF1, BUFF2) of the Bielak identity on the 'E'
+    rows for the COMPLEX*8 CSR, background field u0 and total solution sol."""
+    L = lib()
+    L.orc_verify_steve.restype = C.c_float
+    L.orc_verify_steve.argtypes = [C.c_int] + [C.c_void_p] * 8
+    b1 = np.zeros(g.ndof, np.complex64)
+    b2 = np.zeros(g.ndof, np.complex64)
+    d = L.orc_verify_steve(g.ndof, _p(g.irptr), _p(g.jcptr), _p(g.cnp),
+                           _p(np.ascontiguousarray(cdist64, np.complex64)),
+                           _p(np.ascontiguousarray(u0, np.complex64)),
+                           _p(np.ascontiguousarray(sol, np.complex64)), _p(b1), _p(b2))
+    return float(d), b1, b2
 
 
 def grad_exact(mesh, g, freq, py, u, lam, out=None):

@@ -975,13 +975,18 @@ int orc_asmble(const orc_mesh *m, const int *lm, const int *irptr, const int *jc
 }
 
 /*
- * Row-restricted assembly: fills only CSR rows whose 1-based DOF has
- * rowmask[dof-1] != 0.  Same arithmetic and order as orc_asmble, used for
- * spot checks of full-size systems (only elements touching the rows run).
+ * Row-restricted assembly (ASMBLE_DRIVER / ASMBLE_CDIST, asmble.f90:140-305,
+ * for a subset of rows): rowoff[dof-1] >= 0 selects a 1-based DOF row and
+ * gives the compact offset of its first entry in out128 / out64 (either may
+ * be NULL); the row's entries follow in JCPTR order.  Same arithmetic and
+ * element order as orc_asmble (FP64 sums and the reference's FP32
+ * cast-then-add), so the selected rows equal the full assembly's bit for
+ * bit; only the elements touching a selected row are integrated, which
+ * makes spot checks of full-size systems cheap.
  */
 int orc_asmble_rows(const orc_mesh *m, const int *lm, const int *irptr, const int *jcptr,
-                    int ndof, const unsigned char *rowmask, char cftype, double freq, double py,
-                    double *csr128)
+                    int ndof, const long long *rowoff, char cftype, double freq, double py,
+                    double *out128, float *out64)
 {
     orc_ws w;
     ws_init(&w, m->nord);
@@ -990,13 +995,13 @@ int orc_asmble_rows(const orc_mesh *m, const int *lm, const int *irptr, const in
         const int *lme = lm + (size_t)3 * nen * ielem;
         int touch = 0;
         for (int ipe = 0; ipe < nee; ipe++)
-            if (lme[ipe] > 0 && rowmask[lme[ipe] - 1]) { touch = 1; break; }
+            if (lme[ipe] > 0 && lme[ipe] <= ndof && rowoff[lme[ipe] - 1] >= 0) { touch = 1; break; }
         if (!touch) continue;
         ierr = element_mats(m, &w, ielem, cftype, freq, py);
         if (ierr) break;
         for (int ipe = 0; ipe < nee; ipe++) {
             int idof = lme[ipe];
-            if (idof == 0 || !rowmask[idof - 1]) continue;
+            if (idof == 0 || rowoff[idof - 1] < 0) continue;
             int jbeg = irptr[idof - 1], jend = irptr[idof] - 1;
             int nvar = jend - jbeg + 1;
             for (int iqe = 0; iqe < nee; iqe++) {
@@ -1004,10 +1009,20 @@ int orc_asmble_rows(const orc_mesh *m, const int *lm, const int *irptr, const in
                 if (jdof == 0) continue;
                 int indx = ibsect(nvar, jdof, jcptr + (jbeg - 1));
                 if (indx <= 0) { ierr = 2; break; }
-                size_t iz = (size_t)(jbeg - 1 + indx - 1);
-                csr128[2 * iz] = csr128[2 * iz] + (w.me[ipe + nee * iqe] + w.ke[ipe + nee * iqe].re);
-                csr128[2 * iz + 1] = csr128[2 * iz + 1] + w.ke[ipe + nee * iqe].im;
+                size_t iz = (size_t)(rowoff[idof - 1] + indx - 1);
+                double r1 = w.me[ipe + nee * iqe] + w.ke[ipe + nee * iqe].re;
+                double q1 = w.ke[ipe + nee * iqe].im;
+                if (out128) {
+                    out128[2 * iz] = out128[2 * iz] + r1;
+                    out128[2 * iz + 1] = out128[2 * iz + 1] + q1;
+                }
+                if (out64) {
+                    float fr = (float)r1, fq = (float)q1;
+                    out64[2 * iz] = out64[2 * iz] + fr;
+                    out64[2 * iz + 1] = out64[2 * iz + 1] + fq;
+                }
             }
+            if (ierr) break;
         }
     }
     ws_free(&w);
@@ -1461,6 +1476,43 @@ void orc_addblk(int ndof, const char *cnp, const float *u0, float *sol)
         sol[2 * (idof - 1)] = sol[2 * (idof - 1)] + u0[2 * (idof - 1)];
         sol[2 * (idof - 1) + 1] = sol[2 * (idof - 1) + 1] + u0[2 * (idof - 1) + 1];
     }
+}
+
+/* VERIFY_STEVE (asmble.f90:381-433), the Bielak identity check: on every
+ * exterior ('E') row, BUFF1 = sum over 'E' and 'B' columns of S_ij U0_j and
+ * BUFF2 = the same sum over the solved total field SOL (after ADDBLK), in
+ * COMPLEX*8 and the row's column order; returns DIF1 = max |BUFF1 - BUFF2|
+ * (the reference prints it).  With P_eff from ASMB_PEFF the two agree up to
+ * the solve's residual on the 'E' rows; buff1 / buff2 (nullable, COMPLEX*8
+ * [NDOF], zero off the 'E' rows) return the sums. */
+float orc_verify_steve(int ndof, const int *irptr, const int *jcptr, const char *cnp,
+                       const float *cdist, const float *u0, const float *sol, float *buff1,
+                       float *buff2)
+{
+    float dif1 = 0.0f;
+    for (int idof = 1; idof <= ndof; idof++) {
+        float b1r = 0.0f, b1i = 0.0f, b2r = 0.0f, b2i = 0.0f;
+        if (cnp[idof - 1] == 'E') {
+            for (int j = irptr[idof - 1]; j <= irptr[idof] - 1; j++) {
+                int jdof = jcptr[j - 1];
+                char c2 = cnp[jdof - 1];
+                if (c2 != 'B' && c2 != 'E') continue;
+                float ar = cdist[2 * (j - 1)], ai = cdist[2 * (j - 1) + 1];
+                float ur = u0[2 * (jdof - 1)], ui = u0[2 * (jdof - 1) + 1];
+                float sr = sol[2 * (jdof - 1)], si = sol[2 * (jdof - 1) + 1];
+                b1r = b1r + (ar * ur - ai * ui);
+                b1i = b1i + (ar * ui + ai * ur);
+                b2r = b2r + (ar * sr - ai * si);
+                b2i = b2i + (ar * si + ai * sr);
+            }
+        }
+        if (buff1) { buff1[2 * (idof - 1)] = b1r; buff1[2 * (idof - 1) + 1] = b1i; }
+        if (buff2) { buff2[2 * (idof - 1)] = b2r; buff2[2 * (idof - 1) + 1] = b2i; }
+        float dr = b1r - b2r, di = b1i - b2i;
+        float d = sqrtf(dr * dr + di * di);
+        if (d > dif1) dif1 = d;
+    }
+    return dif1;
 }
 
 /* ------------------------------------------------------------------------ */

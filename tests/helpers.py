@@ -72,3 +72,38 @@ class DirectFWI:
         r[self.rdofs] = res
         lam = lu.solve(r, trans="H")  # lam = A^{-H} R^T r
         return chi, u, lam
+
+
+def sample_rows(mesh, g, per_class=12, seed=0):
+    """A seeded set of 1-based CSR rows covering every DOF class of CNMESH
+    (PML 'A', Bielak strip 'E', interior 'I', strip boundary 'B'), rows of
+    free-surface nodes (topography included) and the first and last rows."""
+    rng = np.random.default_rng(seed)
+    rows = {1, g.ndof}
+    cnp = np.asarray(g.cnp)
+    for c in b"AEIB":
+        cand = np.nonzero(cnp == c)[0] + 1
+        if len(cand):
+            rows.update(int(r) for r in rng.choice(cand, min(per_class, len(cand)), replace=False))
+    nl = mesh.nord + 1
+    fs = np.array([bytes(mesh.cnnpg[p]) == b"FS" for p in range(mesh.nnpg)])
+    top = np.nonzero(fs[mesh.ieng[:, 2] - 1] | fs[mesh.ieng[:, 3] - 1])[0]
+    surf = set()
+    for e in top:
+        for ilxi in range(nl):
+            surf.update(int(d) for d in g.lm[e, (nl - 1) * nl + ilxi] if d > 0)
+    surf = np.array(sorted(surf))
+    rows.update(int(r) for r in rng.choice(surf, min(per_class, len(surf)), replace=False))
+    return np.array(sorted(rows), np.int64)
+
+
+def rows_err(a, ref, idx, g, rows):
+    """CSR value error of the sampled rows: max over rows of
+    max_j |a - ref| / max_j |ref| (the per-row definition of row_norm_err)."""
+    lens = (g.irptr[rows] - g.irptr[rows - 1]).astype(np.int64)
+    starts = np.concatenate([[0], np.cumsum(lens)[:-1]])
+    d = np.abs(np.asarray(a) - np.asarray(ref))
+    r = np.abs(np.asarray(ref))
+    dm = np.maximum.reduceat(d, starts)
+    rm = np.maximum.reduceat(r, starts)
+    return float((dm / np.where(rm > 0, rm, 1.0)).max())
