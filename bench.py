@@ -210,31 +210,8 @@ def run_reference(args, rank):
     print(json.dumps(out))
 
 
-def pipeline_uneven(local, dev):
-    """Batched split-precision path against the plain per-(omega, py) FP64 path
-    on the uneven-batch workload (600x200 jittered mesh with +-200 m
-    topography, Bielak strip 4, 24 frequencies 0.1-2.4 Hz, nky = ceil(16 f /
-    0.1), 4800 systems, 64 sources).  The batched assembly runs all 4800
-    systems; the plain assembly runs one system per frequency and each
-    gradient one (omega, py) pair with all 64 sources, scaled to the 4800 pairs
-    (per-system and per-pair costs do not depend on the pair).  The batched
-    gradient adds each pair's field covariances as the pair's solutions
-    arrive (fem25_gradient_accumulate_dev) and contracts them once
-    (fem25_gradient_finalize_dev); the plain one runs the FP64 kernel per
-    pair.  Parity at full size: the last batched system against the plain
-    FP64 CSR, the split-precision gradient against the FP64 one."""
-    import torch
-    from fem25_b200 import FEM25_PREC_FP64, FEM25_PREC_TF32X3_POINTWISE, Context, synth
-    mesh, pairs, cfg = synth.make_config(4)
-    nsrc = cfg["nsrc"]
-    t0 = time.perf_counter()
-    ctx = Context(mesh, device=local)
-    setup_s = time.perf_counter() - t0
-    nz, ndof, npairs = ctx.nzero, ctx.ndof, len(pairs)
-    stream = torch.cuda.current_stream(dev)
-    freqs = [p[0] for p in pairs]
-    pys = [p[1] for p in pairs]
-
+def _timer(torch, stream):
+    """fn -> best device seconds of ``reps`` runs, CUDA events on ``stream``."""
     def timed(fn, reps=1):
         best = None
         for _ in range(reps):
@@ -247,38 +224,73 @@ def pipeline_uneven(local, dev):
             ms = e0.elapsed_time(e1)
             best = ms if best is None else min(best, ms)
         return best / 1e3
+    return timed
 
-    # batched assembly: every system, ring of 8 complex128 slots
-    nslots = 8
-    sst = (2 * nz + 15) // 16 * 16  # 128-byte aligned ring slots
-    ring = torch.empty(nslots * sst, dtype=torch.float64, device=dev)
-    ctx.assemble_batch("B", freqs[:nslots], pys[:nslots], ring, sst, nslots, stream=stream)
-    torch.cuda.synchronize()
-    t_basm = timed(lambda: ctx.assemble_batch("B", freqs, pys, ring, sst, nslots, stream=stream))
-    # the same batch recorded once into a CUDA graph and replayed: no host
-    # work per launch (system tables are kernel parameters)
-    graph = torch.cuda.CUDAGraph()
-    side = torch.cuda.Stream(dev)
-    side.wait_stream(stream)
-    with torch.cuda.stream(side):
-        with torch.cuda.graph(graph, stream=side):
-            ctx.assemble_batch("B", freqs, pys, ring, sst, nslots,
-                               stream=torch.cuda.current_stream(dev))
-    stream.wait_stream(side)
-    graph.replay()
-    torch.cuda.synchronize()
-    t_basm_graph = timed(graph.replay, reps=3)
-    del graph
-    k = npairs - 1
-    slot = ring[(k % nslots) * sst:(k % nslots) * sst + 2 * nz].clone()
-    del ring
-    torch.cuda.empty_cache()
-    plain = torch.empty(2 * nz, dtype=torch.float64, device=dev)
-    ctx.assemble("B", freqs[k], pys[k], plain, None, stream=stream)
-    torch.cuda.synchronize()
-    csr_rel = float((slot - plain).abs().max() / plain.abs().max())
-    del slot
-    # plain assembly: the middle ky of every frequency
+
+def _per_param(torch, got, ref):
+    """relative 2-norm error per parameter (lambda, mu, rho)."""
+    return [float(torch.linalg.norm(got[m] - ref[m]) / torch.linalg.norm(ref[m])) for m in range(3)]
+
+
+def pipeline_uneven(local, dev, rank=0, world=1, max_over_ranks=None):
+    """The target comparison on the uneven-batch workload (600x200 jittered
+    mesh with +-200 m topography, 4-element strip, 24 frequencies 0.1-2.4 Hz,
+    nky = ceil(16 f / 0.1): 4800 (omega, py) systems, 64 sources).
+
+    Batched split-precision side, measured end to end: one CUDA graph holds
+    the batched assembly of every system of this rank (ring of 8 complex128
+    slots), one covariance accumulation (fem25_gradient_accumulate_dev) per
+    pair with that pair's 64 source fields (a pool of 2 field sets of the
+    adjoint-gradient kind, cycled: the operator and the kernels do not depend
+    on the values), and the contraction (fem25_gradient_finalize_dev); the
+    graph is replayed once under CUDA events.  With several ranks the pairs
+    are sharded longest-processing-time first and the FP64 gradients summed
+    by one NCCL all-reduce, timed apart.
+    Plain side (sampled): the per-(omega, py) FP64 assembly of the middle ky
+    of each frequency, in the reference arithmetic (-fmad=false) and with the
+    FMA build of the same kernels, plus the FP64 gradient of one pair with 64
+    sources; per-system and per-pair costs do not depend on the pair and are
+    scaled to the 4800 pairs.
+    Accuracy: per-parameter error of both split-precision forms against the
+    FP64 kernel on one pair; sampled rows (every DOF class, free surface) of
+    the last batched system against the plain FP64 assembly."""
+    import torch
+    from fem25_b200 import (FEM25_PREC_FP64, FEM25_PREC_TF32X3, FEM25_PREC_TF32X3_POINTWISE,
+                            Context, graph_build, synth)
+    from fem25_b200.parallel import pair_costs, shard_lpt
+    mesh, pairs, cfg = synth.make_config(4)
+    nsrc = cfg["nsrc"]
+    npairs = len(pairs)
+    freqs = [p[0] for p in pairs]
+    pys = [p[1] for p in pairs]
+    mine = shard_lpt(pair_costs(freqs, nsrc), world)[rank]
+    stream = torch.cuda.current_stream(dev)
+    timed = _timer(torch, stream)
+    t0 = time.perf_counter()
+    g = graph_build(mesh)
+    # a pool of 2 field sets [pair][64 sources][NDOF] (u and lambda)
+    pool_pairs = [pairs[npairs // 3], pairs[(2 * npairs) // 3]]
+    pool_u = synth.smooth_fields(mesh, g, pool_pairs, nsrc, seed=4041, device=dev)
+    pool_l = synth.smooth_fields(mesh, g, pool_pairs, nsrc, seed=4042, device=dev)
+    rows = None
+    if rank == 0:
+        import numpy as np
+        rng = np.random.default_rng(4)
+        cnp = np.asarray(g.cnp)
+        rows = [1, g.ndof]
+        for c in b"AEIB":
+            cand = np.nonzero(cnp == c)[0] + 1
+            rows += [int(r) for r in rng.choice(cand, min(12, len(cand)), replace=False)]
+        rows = np.array(sorted(set(rows)), np.int64)
+        lens = g.irptr[rows] - g.irptr[rows - 1]
+        ridx = torch.from_numpy(np.concatenate(
+            [np.arange(a - 1, a - 1 + n) for a, n in zip(g.irptr[rows - 1], lens)])).to(dev)
+
+    # ---------------- plain side (sampled) and the accuracy reference
+    ctx = Context(mesh, g, device=local)
+    setup_s = time.perf_counter() - t0
+    nz, ndof = ctx.nzero, ctx.ndof
+    plain = torch.empty(nz, dtype=torch.complex128, device=dev)
     sel = []
     for f in cfg["freqs"]:
         idx = [i for i, p in enumerate(pairs) if p[0] == f]
@@ -287,66 +299,193 @@ def pipeline_uneven(local, dev):
     torch.cuda.synchronize()
     t_pasm = timed(lambda: [ctx.assemble("B", freqs[i], pys[i], plain, None, stream=stream)
                             for i in sel]) / len(sel)
+    ctx.plain_fma(True)
+    ctx.assemble("B", freqs[sel[0]], pys[sel[0]], plain, None, stream=stream)
+    torch.cuda.synchronize()
+    t_pasm_fma = timed(lambda: [ctx.assemble("B", freqs[i], pys[i], plain, None, stream=stream)
+                                for i in sel]) / len(sel)
+    ctx.plain_fma(False)
+    klast = mine[-1] if mine else npairs - 1
+    plain_rows = None
+    if rank == 0:
+        ctx.assemble("B", freqs[klast], pys[klast], plain, None, stream=stream)
+        plain_rows = plain[ridx].clone()
     del plain
-    # gradient: one pair, all sources, both precisions
-    gen = torch.Generator(device=dev)
-    gen.manual_seed(2031)
-    u = torch.randn((1, nsrc, ndof), dtype=torch.complex128, device=dev, generator=gen)
-    lam = torch.randn((1, nsrc, ndof), dtype=torch.complex128, device=dev, generator=gen)
-    gp = pairs[npairs // 2]
+    torch.cuda.empty_cache()
+    gp = pool_pairs[0]
+    u1, l1 = pool_u[:1], pool_l[:1]
     g64 = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=dev)
-    g32 = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=dev)
-    # untimed first calls: they allocate the covariance accumulators, upload
-    # the pointwise tensor-core tables and tune the FP64 gradient's source tile
-    ctx.gradient_accumulate([gp[0]], [gp[1]], nsrc, u, lam, stream=stream)
-    ctx.gradient_finalize(g32, stream=stream)
-    ctx.gradient([gp[0]], [gp[1]], nsrc, u, lam, g32, FEM25_PREC_TF32X3_POINTWISE, stream=stream)
-    ctx.gradient([gp[0]], [gp[1]], nsrc, u, lam, g64, FEM25_PREC_FP64, stream=stream)
+    gcv = torch.zeros_like(g64)
+    gpw = torch.zeros_like(g64)
+    ctx.gradient([gp[0]], [gp[1]], nsrc, u1, l1, g64, FEM25_PREC_FP64, stream=stream)
+    ctx.gradient([gp[0]], [gp[1]], nsrc, u1, l1, gpw, FEM25_PREC_TF32X3_POINTWISE, stream=stream)
     torch.cuda.synchronize()
 
     def run_grad(out, prec):
         out.zero_()
-        ctx.gradient([gp[0]], [gp[1]], nsrc, u, lam, out, prec, stream=stream)
+        ctx.gradient([gp[0]], [gp[1]], nsrc, u1, l1, out, prec, stream=stream)
     t_g64 = timed(lambda: run_grad(g64, FEM25_PREC_FP64), reps=2)
-    t_gpw = timed(lambda: run_grad(g32, FEM25_PREC_TF32X3_POINTWISE), reps=2)
-    # per pair: the covariance accumulation; per gradient: one contraction
-    t_acc = timed(lambda: ctx.gradient_accumulate([gp[0]], [gp[1]], nsrc, u, lam, stream=stream),
-                  reps=3)
-    g32.zero_()
-    ctx.gradient_finalize(g32, stream=stream)  # empties the timing runs' sums
-    g32.zero_()
-    ctx.gradient_accumulate([gp[0]], [gp[1]], nsrc, u, lam, stream=stream)
-    t_fin = timed(lambda: ctx.gradient_finalize(g32, stream=stream))
-    grel = max(float(torch.linalg.norm(g32[m] - g64[m]) / torch.linalg.norm(g64[m]))
-               for m in range(3))
-    del u, lam, g64, g32
-    tuned = ctx.tuning()
+    t_gpw = timed(lambda: run_grad(gpw, FEM25_PREC_TF32X3_POINTWISE), reps=2)
+    run_grad(gcv, FEM25_PREC_TF32X3)
+    ctx.sync_status(stream)
+    err_cov = _per_param(torch, gcv, g64)
+    err_pw = _per_param(torch, gpw, g64)
+    del g64, gcv, gpw
+    tuned_plain = ctx.tuning()
     ctx.close()
     torch.cuda.empty_cache()
-    plain_total = (t_pasm + t_g64) * npairs
-    batched_total = t_basm + t_acc * npairs + t_fin
-    batched_graph_total = t_basm_graph + t_acc * npairs + t_fin
+
+    # ---------------- batched side: one CUDA graph, replayed once
+    ctx = Context(mesh, g, device=local)
+    nslots = 8
+    sst = (2 * nz + 15) // 16 * 16  # 128-byte aligned ring slots
+    ring = torch.empty(nslots * sst, dtype=torch.float64, device=dev)
+    gsum = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=dev)
+    # set-up calls outside the graph: basis, variant timing, the PML deltas
+    # of every frequency, accumulators
+    one_per_f = sorted({freqs[k]: k for k in (mine or [0])}.values())
+    ctx.assemble_batch("B", [freqs[k] for k in one_per_f], [pys[k] for k in one_per_f], ring, sst,
+                       nslots, stream=stream)
+    ctx.gradient_accumulate([gp[0]], [gp[1]], nsrc, u1, l1, stream=stream)
+    ctx.gradient_finalize(gsum, stream=stream)
+    torch.cuda.synchronize()
+    # the accumulation of one pair and the contraction, eager, for the record
+    t_acc = timed(lambda: ctx.gradient_accumulate([gp[0]], [gp[1]], nsrc, u1, l1, stream=stream),
+                  reps=3)
+    t_fin = timed(lambda: ctx.gradient_finalize(gsum, stream=stream))
+    ctx.sync_status(stream)
+    gsum.zero_()
+    mine_f = [freqs[k] for k in mine]
+    mine_p = [pys[k] for k in mine]
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(stream)
+    nlaunch = 0
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(graph, stream=side):
+            cur = torch.cuda.current_stream(dev)
+            if mine:
+                ctx.assemble_batch("B", mine_f, mine_p, ring, sst, nslots, stream=cur)
+            for j, k in enumerate(mine):
+                q = k % len(pool_pairs)
+                ctx.gradient_accumulate([freqs[k]], [pys[k]], nsrc, pool_u[q:q + 1],
+                                        pool_l[q:q + 1], stream=cur)
+            ctx.gradient_finalize(gsum, stream=cur)
+    stream.wait_stream(side)
+    torch.cuda.synchronize()
+    t_graph = timed(graph.replay)
+    ctx.sync_status(stream)
+    tuned = ctx.tuning()
+    t_allreduce = 0.0
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        t_allreduce = timed(lambda: dist.all_reduce(gsum, op=dist.ReduceOp.SUM))
+    t_job = t_graph + t_allreduce
+    if max_over_ranks is not None:
+        t_job = max_over_ranks(t_job)
+    csr_rel = None
+    if rank == 0 and mine:
+        import numpy as np
+        k = len(mine) - 1
+        slot = ring[(k % nslots) * sst:(k % nslots) * sst + 2 * nz].view(-1, 2)[ridx]
+        b = torch.complex(slot[:, 0], slot[:, 1])
+        d = (b - plain_rows).abs().cpu().numpy()
+        r = plain_rows.abs().cpu().numpy()
+        lens = (g.irptr[rows] - g.irptr[rows - 1]).astype(np.int64)
+        st = np.concatenate([[0], np.cumsum(lens)[:-1]])
+        csr_rel = float((np.maximum.reduceat(d, st) / np.maximum.reduceat(r, st)).max())
+    del graph, ring, pool_u, pool_l
+    ctx.close()
+    torch.cuda.empty_cache()
+    n_launch = (len(set(mine_f)) * 2 + -(-len(mine) // nslots) + len(mine) + 1)
     units = mesh.nelem * nsrc
-    return {"workload": f"uneven batch: 600x200 jittered deg-4 mesh with topography, strip 4 "
-                        f"({mesh.nelem} elements, NDOF {ndof}, NNZ {nz}), "
-                        f"24 f x ceil(16 f/0.1) ky = {npairs} systems, {nsrc} sources",
-            "batched_tf32x3_s": batched_total, "plain_fp64_s": plain_total,
-            "speedup": plain_total / batched_total,
-            "batched_tf32x3_graph_s": batched_graph_total,
-            "speedup_graph": plain_total / batched_graph_total,
-            "batched_assembly_s": t_basm, "batched_assemblies_per_s": npairs / t_basm,
-            "batched_assembly_graph_s": t_basm_graph,
-            "plain_assembly_s_per_system": t_pasm,
-            "gradient_tf32x3_s_per_pair": t_acc, "gradient_tf32x3_contraction_s": t_fin,
-            "gradient_fp64_s_per_pair": t_g64,
-            "gradient_tf32x3_pointwise_s_per_pair": t_gpw,
-            "gradient_tf32x3_elem_rhs_per_s": units / t_acc,
-            "gradient_fp64_elem_rhs_per_s": units / t_g64,
-            "gradient_rel_err_vs_fp64": grel, "csr_rel_err_batched_vs_plain": csr_rel,
-            "sample": f"batched assembly: all {npairs} systems; plain assembly: 1 system per "
-                      f"frequency ({len(sel)}); gradients: 1 pair x {nsrc} sources per pair, "
-                      f"scaled to {npairs} pairs, plus one contraction for the batched path",
-            "setup_s": round(setup_s, 1), "autotuned": tuned}
+    out = {"workload": f"uneven batch: 600x200 jittered deg-4 mesh with topography, strip 4 "
+                       f"({mesh.nelem} elements, NDOF {ndof}, NNZ {nz}), "
+                       f"24 f x ceil(16 f/0.1) ky = {npairs} systems, {nsrc} sources",
+           "batched_measured_s": t_job, "batched_graph_s": t_graph,
+           "batched_form": "one CUDA graph: batched assembly of every system + one covariance "
+                           "accumulation per (omega, py) pair (64 sources) + one contraction",
+           "pairs_this_rank": len(mine), "allreduce_s": t_allreduce,
+           "gradient_tf32x3_s_per_pair": t_acc, "gradient_tf32x3_contraction_s": t_fin,
+           "gradient_tf32x3_elem_rhs_per_s": units / t_acc,
+           "plain_assembly_s_per_system": t_pasm, "plain_assembly_fma_s_per_system": t_pasm_fma,
+           "gradient_fp64_s_per_pair": t_g64, "gradient_tf32x3_pointwise_s_per_pair": t_gpw,
+           "gradient_fp64_elem_rhs_per_s": units / t_g64,
+           "gradient_rel_err_vs_fp64": {"covariance (lambda, mu, rho)": err_cov,
+                                        "pointwise (lambda, mu, rho)": err_pw},
+           "csr_rel_err_batched_vs_plain_rows": csr_rel,
+           "graph_kernel_launches": n_launch,
+           "setup_s": round(setup_s, 1), "autotuned": tuned, "autotuned_plain": tuned_plain}
+    if world == 1:
+        plain_total = (t_pasm + t_g64) * npairs
+        plain_total_fma = (t_pasm_fma + t_g64) * npairs
+        out.update({"plain_fp64_s": plain_total, "plain_fp64_fma_s": plain_total_fma,
+                    "speedup_measured": plain_total / t_job,
+                    "speedup_measured_vs_fma_plain": plain_total_fma / t_job,
+                    "sample": f"batched: all {npairs} systems and pairs measured in one graph; "
+                              f"plain: assembly of 1 system per frequency ({len(sel)}) and the "
+                              f"FP64 gradient of 1 pair x {nsrc} sources, scaled to {npairs} "
+                              f"pairs"})
+    return out
+
+
+def split_precision_leg(local, dev):
+    """The split-precision contraction workload (300x150 jittered mesh,
+    128 sources, a sample of its 96 ky x 12 f pairs): elem.rhs/s of the FP64
+    kernel and of both split-precision forms, and their relative error
+    against FP64 per parameter, on seeded smooth fields of the adjoint-
+    gradient kind (unit RMS, lognormal amplitude, 5 km-correlated phase)."""
+    import torch
+    from fem25_b200 import (FEM25_PREC_FP64, FEM25_PREC_TF32X3, FEM25_PREC_TF32X3_POINTWISE,
+                            Context, graph_build, synth)
+    mesh, pairs, cfg = synth.make_config(3)
+    nsrc = cfg["nsrc"]
+    g = graph_build(mesh)
+    ctx = Context(mesh, g, device=local)
+    stream = torch.cuda.current_stream(dev)
+    timed = _timer(torch, stream)
+    use = [pairs[96 * 2 + 80], pairs[96 * 9 + 30]]  # (0.6 Hz, high ky), (2.0 Hz, low ky)
+    u = synth.smooth_fields(mesh, g, use, nsrc, seed=3031, device=dev)
+    lam = synth.smooth_fields(mesh, g, use, nsrc, seed=3032, device=dev)
+    fr, py = [p[0] for p in use], [p[1] for p in use]
+    res = {}
+    outs = {}
+    for name, prec in (("fp64", FEM25_PREC_FP64), ("tf32x3_covariance", FEM25_PREC_TF32X3),
+                       ("tf32x3_pointwise", FEM25_PREC_TF32X3_POINTWISE)):
+        out = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=dev)
+        ctx.gradient(fr, py, nsrc, u, lam, out, prec, stream=stream)  # set-up / tuning
+
+        def run():
+            out.zero_()
+            ctx.gradient(fr, py, nsrc, u, lam, out, prec, stream=stream)
+        t = timed(run, reps=2)
+        ctx.sync_status(stream)
+        outs[name] = out
+        res[name] = {"s": t, "elem_rhs_per_s": mesh.nelem * nsrc * len(use) / t}
+    for name in ("tf32x3_covariance", "tf32x3_pointwise"):
+        res[name]["rel_err_vs_fp64"] = dict(zip(("lambda", "mu", "rho"),
+                                                _per_param(torch, outs[name], outs["fp64"])))
+    # the covariance form's two kernels: accumulation per pair, contraction once
+    acc = timed(lambda: ctx.gradient_accumulate(fr, py, nsrc, u, lam, stream=stream), reps=2)
+    tmp = torch.zeros_like(outs["fp64"])
+    fin = timed(lambda: ctx.gradient_finalize(tmp, stream=stream))
+    ctx.sync_status(stream)
+    res["tf32x3_covariance"]["accumulate_s_per_pair"] = acc / len(use)
+    res["tf32x3_covariance"]["contraction_s"] = fin
+    res["tf32x3_covariance"]["full_workload_s_estimate"] = acc / len(use) * len(pairs) + fin
+    res["fp64"]["full_workload_s_estimate"] = res["fp64"]["s"] / len(use) * len(pairs)
+    del u, lam, outs, tmp
+    ctx.close()
+    torch.cuda.empty_cache()
+    return {"workload": f"split-precision contraction: 300x150 jittered deg-4 mesh "
+                        f"({mesh.nelem} elements, NDOF {g.ndof}), {nsrc} sources, "
+                        f"{len(pairs)} (omega, py) pairs (12 f x 96 ky)",
+            "sample": f"{len(use)} pairs x {nsrc} sources measured (f = {use[0][0]:.1f} and "
+                      f"{use[1][0]:.1f} Hz); full-workload times scale per pair",
+            "fields": "seeded smooth fields: unit RMS per (pair, source), lognormal(0, 0.1) "
+                      "amplitude, exp(i (omega x / 2500 m/s + phi)), phi 5 km-correlated",
+            "units": "elem.rhs = element x source x (omega, py) pair", **res}
 
 
 def main():
@@ -401,6 +540,13 @@ def main():
         mesh, pairs, cfg = synth.make_config(1, nx=100, nz=40)
     else:
         mesh, pairs, cfg = synth.make_config(1)
+    if world > 1:
+        # weak scaling over distinct systems: rank r's 8 frequencies sit
+        # r * 0.2 / world Hz above the single-GPU workload's, 64 ky each
+        vmin = synth.vs_min(mesh)
+        df = 0.2 * rank / world
+        pairs = [(float(f + df), float(py)) for f in cfg["freqs"]
+                 for py in synth.ky_list(f + df, 64, vmin)]
     ctx = Context(mesh, device=local)
     nz = ctx.nzero
     ndof_main = ctx.ndof
@@ -494,21 +640,28 @@ def main():
            "path": "fem25_update_model + fem25_asmble_driver (ASMBLE_DRIVER drop-in), "
                    "COMPLEX*8 CDIST to pinned host memory"}
     del h_cdist
-    # batched basis is rebuilt after update_model: restore it outside any timing
+    # a model-update step: fem25_update_model invalidates the affine basis, so
+    # the next batch rebuilds it (element basis integrals, gather, per-entry
+    # primaries) before its 512 systems; wall clock around both, synchronised
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.update_model(h_e.numpy(), h_d.numpy())
     step()
     torch.cuda.synchronize()
+    upd_s = max_over_ranks(time.perf_counter() - t0)
+    model_update = {"s": upd_s, "assemblies_per_s": nsys * world / upd_s,
+                    "basis_rebuild_s": max(0.0, upd_s - ms_step / 1e3),
+                    "what": "fem25_update_model (host model upload) + one 512-system batch "
+                            "that first rebuilds the affine basis"}
 
     # ---------------- gradient (exact lambda/mu/rho), 400x120 mesh, 32 sources x 2 pairs
     grad = None
     if not args.no_grad:
         nsrc = 32
         npool = 2
-        gen = torch.Generator(device=dev)
-        gen.manual_seed(2027)
-        shape = (npool, nsrc, ctx.ndof)
-        u = torch.randn(shape, dtype=torch.complex128, device=dev, generator=gen)
-        lam = torch.randn(shape, dtype=torch.complex128, device=dev, generator=gen)
         gp = pairs[::64][:npool]
+        u = synth.smooth_fields(mesh, ctx.g, gp, nsrc, seed=2027, device=dev)
+        lam = synth.smooth_fields(mesh, ctx.g, gp, nsrc, seed=2028, device=dev)
 
         def time_grad(prec, reps=3):
             out = torch.zeros((3, mesh.nnpg), dtype=torch.float64, device=dev)
@@ -531,10 +684,9 @@ def main():
         gms, g64 = time_grad(FEM25_PREC_FP64)
         tms, g32 = time_grad(FEM25_PREC_TF32X3)
         pms, gpw = time_grad(FEM25_PREC_TF32X3_POINTWISE)
-        rel = max(float(torch.linalg.norm(g32[m] - g64[m]) / torch.linalg.norm(g64[m]))
-                  for m in range(3))
-        prel = max(float(torch.linalg.norm(gpw[m] - g64[m]) / torch.linalg.norm(g64[m]))
-                   for m in range(3))
+        ctx.sync_status(stream)
+        rel = dict(zip(("lambda", "mu", "rho"), _per_param(torch, g32, g64)))
+        prel = dict(zip(("lambda", "mu", "rho"), _per_param(torch, gpw, g64)))
         # the covariance path's two kernels on their own: accumulation (per
         # pair in an inversion loop) and contraction (once per gradient)
         fr_, py_ = [p[0] for p in gp], [p[1] for p in gp]
@@ -553,14 +705,18 @@ def main():
         nelem_phys = int(np.sum(mesh.cdomain != ord("A")))
         units = mesh.nelem * nsrc * npool
         grad = {"metric": "gradient elem·rhs/s", "unit": "elem·rhs/s",
+                "workload": "adjoint gradient: 400x120 layered mesh, 32 sources, 2 of the "
+                            "8 f x 64 ky pairs; seeded smooth fields (unit RMS, lognormal "
+                            "amplitude, 5 km-correlated phase)",
                 "plain_fp64": units / (gms / 1e3), "ms": gms,
-                "tf32x3": units / (tms / 1e3), "tf32x3_ms": tms, "tf32x3_rel_err": rel,
+                "tf32x3": units / (tms / 1e3), "tf32x3_ms": tms,
+                "tf32x3_rel_err_vs_fp64": rel,
                 "tf32x3_form": "field covariances accumulated per element on tcgen05, "
                                "contracted once in FP64 (k_grad_cov + k_grad_cov_fin)",
                 "tf32x3_accumulate_ms": acc_ms, "tf32x3_contraction_ms": fin_ms,
                 "tf32x3_accumulate_elem_rhs_per_s": units / (acc_ms / 1e3),
                 "tf32x3_pointwise": units / (pms / 1e3), "tf32x3_pointwise_ms": pms,
-                "tf32x3_pointwise_rel_err": prel,
+                "tf32x3_pointwise_rel_err_vs_fp64": prel,
                 "units": f"{mesh.nelem} elements x {nsrc} sources x {npool} (omega,py) pairs "
                          f"({nelem_phys} non-PML elements computed)",
                 "algorithmic_tflops_fp64": units * 547200 / (gms / 1e3) / 1e12}
@@ -607,13 +763,16 @@ def main():
         del u, lam, w32, l32, gl
     tuning = ctx.tuning()
 
+    del ring
+    ctx.close()
+    torch.cuda.empty_cache()
+    ctx = None
+    split = None
+    if not args.no_grad and not args.small and rank == 0:
+        split = split_precision_leg(local, dev)
     pipe = None
-    if world == 1 and not args.no_pipeline and not args.small:
-        del ring
-        ctx.close()
-        torch.cuda.empty_cache()
-        ctx = None
-        pipe = pipeline_uneven(local, dev)
+    if not args.no_pipeline and not args.small:
+        pipe = pipeline_uneven(local, dev, rank, world, max_over_ranks)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -642,7 +801,8 @@ def main():
                         "kernel": STREAM_KERNELS.get(tuning["stream_variant"], "k_stream"),
                         "kernel_ms": kms, "peak_kind": peak_kind,
                         "algorithmic_bytes": "16 B x NNZ per system (complex128 values written)"},
-           "cpu_baseline": cpu, "e2e": e2e, "gradient": grad, "pipeline": pipe,
+           "cpu_baseline": cpu, "e2e": e2e, "model_update_step": model_update,
+           "gradient": grad, "split_precision": split, "pipeline": pipe,
            "gpu_launches": launches_per_step * args.steps, "clocks": clocks}
     if rank == 0:
         print(json.dumps(out))

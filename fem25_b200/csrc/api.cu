@@ -96,7 +96,8 @@ void free_ctx(Ctx *c) {
                   c->d_pml_delta, c->d_jcsc, c->d_icsc, c->d_rg_anchor, c->d_mconn,
                   c->d_elem_wts, c->d_fmat, c->d_cadj_col0, c->d_cadj_pair_col, c->d_cadj_pair_elem,
                   c->d_cadj_dptr, c->d_cadj_dent, c->d_cadj_w, c->d_nonpml, c->d_cdist, c->d_prim, c->d_desc,
-                  c->d_tc_tab, c->d_qp, c->d_qs, c->d_cov};
+                  c->d_tc_tab, c->d_qp, c->d_qs, c->d_cov, c->d_cov_ops, c->d_cov_opptr,
+                  c->d_cov_tx, c->d_cov_node, c->d_maskg, c->d_avg_work};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &e : c->ev)
@@ -232,6 +233,9 @@ int ensure_refgrad(Ctx *c) {
   CK(dalloc_copy(&c->d_icsc, c->rg.icsc.data(), c->rg.icsc.size()), "ref grad");
   CK(dalloc_copy(&c->d_rg_anchor, c->rg.anchor_of_col.data(), c->rg.anchor_of_col.size()), "ref grad");
   CK(dalloc_copy(&c->d_mconn, c->rg.mconn.data(), c->rg.mconn.size()), "ref grad");
+  CK(dalloc_copy(&c->d_maskg, c->rg.maskg.data(), c->rg.maskg.size()), "ref grad");
+  CK(cudaMalloc(&c->d_avg_work, sizeof(double) * 2 * (size_t)std::max(c->rg.nnpinv, 1)),
+     "ref grad");
   CK(dalloc_copy(&c->d_elem_wts, c->rg.elem_wts.data(), c->rg.elem_wts.size()), "ref grad");
   CK(cudaMalloc(&c->d_fmat, sizeof(float2) * (c->rg.nz ? c->rg.nz : 1)), "ref grad");
   c->refgrad_ready = true;
@@ -926,6 +930,62 @@ int fem25_ref_vforce2_dev(fem25_ctx *h, const char *cinvtype, double freq, doubl
   return FEM25_OK;
 }
 
+int fem25_wtgrad_dev(fem25_ctx *h, int na35, const float *wgrad, float *grad, void *stream) {
+  if (!h || !wgrad || !grad || na35 <= 0) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  CK(cudaSetDevice(c->device), "set device");
+  CK(launch_wtgrad(na35, wgrad, grad, (cudaStream_t)stream), "wtgrad");
+  return FEM25_OK;
+}
+
+// shared checks of AVGRAD / AVGRAD8: the GENGMASK tables, set up outside a capture
+static int avgrad_args(Ctx *c, int nvinv, int ncasc, const void *grad, cudaStream_t st) {
+  if (!grad || nvinv < 1 || nvinv > 2 || ncasc < 0) return FEM25_ERR_ARG;
+  if (!c->refgrad_ready && capturing(st))
+    return fail(c, FEM25_ERR_ARG,
+                "avgrad: the inversion tables are built on the first call; make one uncaptured "
+                "call before capturing");
+  return ensure_refgrad(c);
+}
+
+int fem25_avgrad_dev(fem25_ctx *h, int nvinv, int ncasc, float *grad, void *stream) {
+  if (!h) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  CK(cudaSetDevice(c->device), "set device");
+  int r = avgrad_args(c, nvinv, ncasc, grad, (cudaStream_t)stream);
+  if (r) return r;
+  CK(launch_avgrad(c, nvinv, ncasc, grad, (cudaStream_t)stream), "avgrad");
+  return FEM25_OK;
+}
+
+int fem25_avgrad8_dev(fem25_ctx *h, int nvinv, int ncasc, double *grad, void *stream) {
+  if (!h) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  CK(cudaSetDevice(c->device), "set device");
+  int r = avgrad_args(c, nvinv, ncasc, grad, (cudaStream_t)stream);
+  if (r) return r;
+  CK(launch_avgrad8(c, nvinv, ncasc, grad, (cudaStream_t)stream), "avgrad8");
+  return FEM25_OK;
+}
+
+int fem25_misfit_options(fem25_ctx *h, int norm, int irestp, int ibphase, float eps, float thresh,
+                         float dtmax, float dtmax_obj) {
+  if (!h) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  if (norm < 1 || norm > 4) return fail(c, FEM25_ERR_ARG, "misfit options: NORM must be 1-4");
+  if (irestp < 1 || irestp > 3) return fail(c, FEM25_ERR_ARG, "misfit options: IRESTP must be 1-3");
+  if (ibphase < 0 || ibphase > 6)
+    return fail(c, FEM25_ERR_ARG, "misfit options: IBPHASE must be 0-6");
+  c->mopt.norm = norm;
+  c->mopt.irestp = irestp;
+  c->mopt.ibphase = ibphase;
+  c->mopt.eps = eps;
+  c->mopt.thresh = thresh;
+  c->mopt.dtmax = dtmax;
+  c->mopt.dtmax_obj = dtmax_obj;
+  return FEM25_OK;
+}
+
 int fem25_misfit_dev(fem25_ctx *h, int nsrc, int nrec, const int *mrdof, const double *yrec,
                      double freq, double py, double azmod, const float *recv, const float *sol,
                      const float *obs, const float *wghts, float *est, float *rhs, float *misfit,
@@ -970,7 +1030,7 @@ int fem25_misfit_dev(fem25_ctx *h, int nsrc, int nrec, const int *mrdof, const d
     CK(dalloc_copy(&d_w, wghts, ns3), "misfit");
     CK(cudaMalloc(&d_est, sizeof(float) * 2 * ns3), "misfit");
     CK(cudaMalloc(&d_mis, sizeof(float) * nsrc), "misfit");
-    CK(launch_misfit(c, nsrc, nrec, d_mrdof, d_trig, omega, py, azmod, d_recv, sol, d_obs, d_w,
+    CK(launch_misfit(c, nsrc, nrec, d_mrdof, d_trig, freq, py, azmod, d_recv, sol, d_obs, d_w,
                      d_est, rhs, d_mis, st),
        "misfit");
     CK(cudaMemcpyAsync(est, d_est, sizeof(float) * 2 * ns3, cudaMemcpyDeviceToHost, st), "misfit");

@@ -62,6 +62,17 @@ struct PairTable {
   double2 p[kMaxPairs];
 };
 
+// Options of the misfit / adjoint source (the reference's INV_INFO fields
+// NORM, IRESTP, IBPHASE, the thresholds of COBJ4 and the DTMAX phase-jump
+// tests), and the per-call values the kernel needs.
+struct MisfitOpts {
+  int norm, irestp, ibphase;
+  float eps, thresh;       // COBJ4's EPS = EPSS * CRESMN, THRESH = THRESHS * CRESMN
+  float dtmax, dtmax_obj;  // BPRESID4's and COBJ4's DTMAX (0 = off)
+  double freq;             // FREQ of the call
+  float2 hfact;            // HDIFFER(IBPHASE, FREQ) of the call
+};
+
 struct DenseLU;  // dense LU of the small-mesh direct solve (dense_solve.cu)
 
 struct Ctx {
@@ -116,6 +127,8 @@ struct Ctx {
   bool refgrad_ready = false;
   RefGradSetup rg;
   int *d_jcsc = nullptr, *d_icsc = nullptr, *d_rg_anchor = nullptr, *d_mconn = nullptr;
+  int *d_maskg = nullptr;          // MASKG(NNPG) of GENGMASK
+  void *d_avg_work = nullptr;      // AVGRAD / AVGRAD8 workspace (2 x NNPINV doubles)
   double *d_elem_wts = nullptr;
   float2 *d_fmat = nullptr;
   // CADJ_NU_ALPHA: (anchor column, connected element) pairs in the reference's
@@ -134,6 +147,11 @@ struct Ctx {
   // 25 x 25 field covariances; pending = holds sums not yet contracted
   double *d_cov = nullptr;
   bool cov_pending = false;
+  // its gather plan (TMA boxes per element) and the tensor-map encoder
+  int2 *d_cov_ops = nullptr;
+  int *d_cov_opptr = nullptr, *d_cov_tx = nullptr;
+  uint32_t *d_cov_node = nullptr;
+  void *tmap_encode = nullptr;
   // cached COMPLEX*8 device buffer of fem25_asmble_driver, and its pipeline:
   // element chunk k = [drv_elem[k], drv_elem[k+1]) completes the CSR rows
   // [drv_row[k], drv_row[k+1]), whose values are gathered and copied to the
@@ -149,6 +167,8 @@ struct Ctx {
   // (0: the default, about half a second) and the time-out test hook
   long long wait_limit = 0;
   int wait_inject = 0;
+  // misfit options (fem25_misfit_options); the defaults of the reference
+  MisfitOpts mopt{2, 3, 0, 0.0f, 0.0f, 0.0f, 0.0f, 0.0, {1.0f, 0.0f}};
   // optional CUDA-event timing of the dominant kernels
   bool prof = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -187,6 +207,9 @@ cudaError_t launch_grad_cov_fin(Ctx *c, double *grad, cudaStream_t st);
 cudaError_t launch_ref_cfmat(Ctx *c, int lisp, double vpvs, double omega, double py,
                              const float *wave, int accumulate, cudaStream_t st);
 cudaError_t launch_ref_adjflam(Ctx *c, const float *adjlam, float *gradl, cudaStream_t st);
+cudaError_t launch_wtgrad(int na35, const float *wgrad, float *grad, cudaStream_t st);
+cudaError_t launch_avgrad(Ctx *c, int nvinv, int ncasc, float *grad, cudaStream_t st);
+cudaError_t launch_avgrad8(Ctx *c, int nvinv, int ncasc, double *grad, cudaStream_t st);
 cudaError_t launch_ref_pchadj(Ctx *c, int nvinv, int nrhs, const float *grns, const float *fmat,
                               float *hessb, float *jacl, cudaStream_t st);
 int prepare_cadj(Ctx *c, std::string *msg);
@@ -200,12 +223,12 @@ cudaError_t launch_ref_met225(Ctx *c, int lisp, int liss, double omega, double p
 cudaError_t launch_ref_vforce2(Ctx *c, int lisp, int liss, double omega, double py,
                                const float *wave, float *fmat, cudaStream_t st);
 cudaError_t launch_misfit(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const float *d_trig,
-                          double omega, double py, double azmod, const float *d_recv,
+                          double freq, double py, double azmod, const float *d_recv,
                           const float *sol, const float *d_obs, const float *d_wghts,
                           float *d_est, float *rhs, float *d_misfit, cudaStream_t st);
 
 cudaError_t launch_misfit_part(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const float *d_trig,
-                               double azmod, const float *d_recv, const float *sol,
+                               double freq, double azmod, const float *d_recv, const float *sol,
                                const float *d_obs, const float *d_wghts, float *d_est, float *rhs,
                                float *d_part, float *d_misfit, cudaStream_t st);
 

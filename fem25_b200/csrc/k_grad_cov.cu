@@ -17,31 +17,42 @@
 // the inverse Jacobian and the anchor weights W_q SF_a(q) at the 169
 // points (the bilinear forms of KM25ISOQ, estiff25.f:64-154, written out in
 // the blocks).  The per-(element, pair, source) work is a rank-2 real update
-// of a 75 x 150 matrix -- a GEMM over the sources -- instead of
-// interpolating both fields at the 169 points.
+// -- a GEMM over the sources -- instead of interpolating both fields at the
+// 169 points.
 //
 // Accumulation (k_grad_cov): one persistent CTA per SM.  Per element and
 // pair, D[lam row][u column] += sum_k A[row][k] B[column][k] with
-// K = (source, re/im):
-//     A[32c + a][2s, 2s+1]     = (Re lam, Im lam)           of component c, node a
-//     B[32d + b][2s, 2s+1]      = (Re u, Im u)              -> D = Re conj(lam) u
-//     B[96 + 32d + b][2s, 2s+1] = (Im u, -Re u)             -> D = Im conj(lam) u
-// M = 128 (100 rows used: component 1's rows also at 96 + a), N = 192
-// (150 used, a 32-column slot per part and component), 8 sources (K = 16) per
-// stage, x = hi + lo split with D = A_hi B_hi + A_lo B_hi + A_hi B_lo.
-//   8 producer warps  each thread owns one (node, source) of every stage: it
-//                copies the node's u and lam runs (complex128) into its raw
-//                shared-memory slots and converts them itself to tf32 hi/lo
-//                operand tiles (one of 3 stages)
-//   warp 3       MMA issuer (one thread), two TMEM accumulators of 192
-//                columns (each takes 2 stages of one pair)
+// K = (source, two real parts).  Only nine (lam component, u component,
+// Re / Im) products are needed, and they fit one 75 x 75 product when the
+// u components enter as
+//     B[a][2s, 2s+1]      = (Re u0, Im u0)     slot 0
+//     B[32 + a][..]       = (Im u1, -Re u1)    slot 1
+//     B[64 + a][..]       = (Re u2, Im u2)     slot 2
+// and the lam components as (Re, Im) for components 0 and 2 and as
+// (-Im lam1, Re lam1) for component 1 (rows 32 c + a; component 1 again at
+// rows 96 + a): row c = 0 then gives Re C00, Im C01, Re C02 in slots 0-2,
+// c = 2 gives Re C20, Im C21, Re C22, and c = 1 gives Im C10, -Re C11,
+// Im C12.  M = 128, N = 96, 8 sources (K = 16) per stage, x = hi + lo with
+// D = A_hi B_hi + A_lo B_hi + A_hi B_lo.
+//   loader / MMA   one thread (warp 3): fetches each stage's nodal values
+//                with 2D TMA loads -- per element a precomputed list of
+//                boxes covering its nodes' DOF runs (16-, 4- or 1-node
+//                boxes, 8 source rows each, from u and from lam) -- into a
+//                raw ring of kRawD stages, kRawD - 1 stages ahead, and
+//                issues the MMAs into one of 4 TMEM accumulators of 128
+//                columns (each takes kDrain stages of one pair)
+//   8 converter warps  thread (node, source) reads its node's six complex
+//                values from the raw stage and writes them (FP64 -> tf32
+//                hi/lo, signs and swaps above) into one of 3 operand stages
 //   15 epilogue warps  one block each: the warp's TMEM lane quarter holds
 //                the lam component (lane = node); it reads its 25 columns
-//                and adds them, weighted by the pair, into 25 FP64
-//                registers; at the end of the element it writes (or adds)
-//                the block row to memory.
-// Hand-offs are mbarriers; every wait is bounded and a wait that runs out
-// sets the error word and drains the schedule without waiting.
+//                and adds them, weighted (and signed) by the pair, into 25
+//                FP64 registers; at the end of the element it writes (or
+//                adds) the block row to memory.
+// Hand-offs are mbarriers (the raw stages complete by TMA transaction
+// bytes); every wait is bounded and a wait that runs out sets the error
+// word and drains the schedule without waiting (the loader stops issuing
+// and waits, bounded, for the loads in flight before the CTA exits).
 //
 // Contraction (k_grad_cov_fin, FP64): per element the blocks are combined
 // (symmetric parts of R_00, R_22, R_11; S = R_02 + R_20^T;
@@ -50,6 +61,10 @@
 // N_a(xi_x, eta_z) = l_ax(xi_x) l_ae(eta_z) (dshl.f:100-243), by sum
 // factorisation: Z = B l_e, Y = Z l_x, F(q) = T(q)^T Y(q), about 0.6 M FMA
 // per element, independent of the number of pairs and sources.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -62,64 +77,64 @@ namespace fem25 {
 
 namespace cov {
 constexpr int kG = 8;                        // sources per stage
-constexpr int kGhBits = 2;                   // log2(kG / 2)
-constexpr int kK = 2 * kG;                   // K columns per stage (re, im)
+constexpr int kK = 2 * kG;                   // K columns per stage
 constexpr int kM = 128;
-constexpr int kN = 192;                      // B rows: a 32-row slot per (part, component)
-constexpr int kNIm = 96;                     // first row of the Im part
+constexpr int kN = 96;                       // B rows: slot k (u component k) at rows 32 k + node
 constexpr uint32_t kALbo = kM / 8 * 128;     // 2048 B between K chunks of A
-constexpr uint32_t kBLbo = kN / 8 * 128;     // 3072 B between K chunks of B
+constexpr uint32_t kBLbo = kN / 8 * 128;     // 1536 B between K chunks of B
 constexpr int kATile = (int)kALbo * (kK / 4);  // 8 KB
-constexpr int kBTile = (int)kBLbo * (kK / 4);  // 12 KB
-constexpr int kBImOff = kNIm / 8 * 128;      // 1536 B from a Re row of B to its Im row
-constexpr int kStage = 2 * kATile + 2 * kBTile;  // A_hi, A_lo, B_hi, B_lo: 40 KB
+constexpr int kBTile = (int)kBLbo * (kK / 4);  // 6 KB
+constexpr int kStage = 2 * kATile + 2 * kBTile;  // A_hi, A_lo, B_hi, B_lo: 28 KB
 constexpr int kNB = 3;                       // operand stages in the ring
+constexpr int kNodeBytes = 48;               // one node's three complex128 DOFs
+constexpr int kRawField = kNen * kG * kNodeBytes;  // 9600 B: 25 nodes x 8 sources
+constexpr int kRawStage = 2 * kRawField;     // u then lam
+constexpr int kRawD = 5;                     // raw stages (kRawD - 1 fetched ahead)
+constexpr int kSmemBytes = kNB * kStage + kRawD * kRawStage;  // 180 KB
 constexpr int kThreads = 768;                // 24 warps
 constexpr int kMmaWarp = 3;
 constexpr int kEpiWarps = 15;
 constexpr int kProdWarps = 8;
-constexpr int kEpiThreads = kEpiWarps * 32;
 constexpr int kProdThreads = kProdWarps * 32;
-constexpr int kSlotsPer = 6;                 // values per producer thread and stage: 2 fields x 3 components
-constexpr int kRawStage = kSlotsPer * kProdThreads * 16;  // 24 KB of raw complex128 values per stage
-constexpr int kRawD = 4;                     // raw stages (kRawD - 1 copy groups in flight)
-constexpr int kSmemBytes = kNB * kStage + kRawD * kRawStage;  // 216 KB
 constexpr int kDrain = 2;                    // stages per TMEM accumulation (FP32 sums of 2 kDrain kG)
+constexpr int kUnits = 4;                    // TMEM accumulators
 constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kTmemStage = 256;
+constexpr uint32_t kTmemUnit = 128;          // columns per accumulator (96 used)
 constexpr int kBlocks = 15;
 constexpr int kBlk = kNen * kNen + 1;        // 625 doubles per block, padded to 16 bytes
-static_assert(kProdThreads == 32 * kG, "one producer thread per (node slot, source)");
-static_assert((1 << kGhBits) == kG / 2, "source-pair bits");
+constexpr int kBoxNodes[3] = {16, 4, 1};     // TMA box widths (nodes)
+static_assert(kProdThreads == 32 * kG, "one converter thread per (node slot, source)");
+static_assert(kRawField % 128 == 0, "raw regions keep the 128-byte alignment of TMA boxes");
 static_assert(kSmemBytes <= 227 * 1024, "shared memory");
+static_assert(kUnits * kTmemUnit <= kTmemCols, "tensor memory");
 }  // namespace cov
 
 constexpr uint32_t kCovIdesc = tf32_idesc(cov::kM, cov::kN);
 
-// Epilogue block k (0-4) of lam component c: the block it
-// accumulates (index into R00 R02 R20 R22 R11 P0 P1 P2 W0 W1 W2 I01 I21 I10
-// I12), its first TMEM column and its weight (0: 1, 1: wpy^2, 2: w^2, 3: wpy).
-__device__ __forceinline__ void cov_role(int c, int k, int &blk, int &col, int &wt) {
-  // g: 0-2 Re of u component g, 3-5 Im of u component g-3; column 32g
-  int g;
+// Epilogue block k (0-4) of lam component c: the block it accumulates
+// (index into R00 R02 R20 R22 R11 P0 P1 P2 W0 W1 W2 I01 I21 I10 I12), its
+// u slot (TMEM column 32 slot), its weight (0: 1, 1: wpy^2, 2: w^2, 3: wpy)
+// and whether the product enters with a minus sign (component 1's slot 1
+// holds -Re C11).
+__device__ __forceinline__ void cov_role(int c, int k, int &blk, int &slot, int &wt, bool &neg) {
+  neg = false;
   switch (c * 5 + k) {
-    case 0: blk = 0; g = 0; wt = 0; break;    // lam_0: R00
-    case 1: blk = 1; g = 2; wt = 0; break;    //        R02
-    case 2: blk = 5; g = 0; wt = 1; break;    //        P0
-    case 3: blk = 8; g = 0; wt = 2; break;    //        W0
-    case 4: blk = 11; g = 4; wt = 3; break;   //        I01
-    case 5: blk = 4; g = 1; wt = 0; break;    // lam_1: R11
-    case 6: blk = 13; g = 3; wt = 3; break;   //        I10
-    case 7: blk = 6; g = 1; wt = 1; break;    //        P1
-    case 8: blk = 9; g = 1; wt = 2; break;    //        W1
-    case 9: blk = 14; g = 5; wt = 3; break;   //        I12
-    case 10: blk = 2; g = 0; wt = 0; break;   // lam_2: R20
-    case 11: blk = 3; g = 2; wt = 0; break;   //        R22
-    case 12: blk = 7; g = 2; wt = 1; break;   //        P2
-    case 13: blk = 10; g = 2; wt = 2; break;  //        W2
-    default: blk = 12; g = 4; wt = 3; break;  //        I21
+    case 0: blk = 0; slot = 0; wt = 0; break;               // lam_0: R00
+    case 1: blk = 1; slot = 2; wt = 0; break;               //        R02
+    case 2: blk = 5; slot = 0; wt = 1; break;               //        P0
+    case 3: blk = 8; slot = 0; wt = 2; break;               //        W0
+    case 4: blk = 11; slot = 1; wt = 3; break;              //        I01
+    case 5: blk = 4; slot = 1; wt = 0; neg = true; break;   // lam_1: R11
+    case 6: blk = 13; slot = 0; wt = 3; break;              //        I10
+    case 7: blk = 6; slot = 1; wt = 1; neg = true; break;   //        P1
+    case 8: blk = 9; slot = 1; wt = 2; neg = true; break;   //        W1
+    case 9: blk = 14; slot = 2; wt = 3; break;              //        I12
+    case 10: blk = 2; slot = 0; wt = 0; break;              // lam_2: R20
+    case 11: blk = 3; slot = 2; wt = 0; break;              //        R22
+    case 12: blk = 7; slot = 2; wt = 1; break;              //        P2
+    case 13: blk = 10; slot = 2; wt = 2; break;             //        W2
+    default: blk = 12; slot = 1; wt = 3; break;             //        I21
   }
-  col = 32 * g;
 }
 
 // Warp roles.  A warp reads the TMEM lanes of its quarter (warp % 4), which
@@ -127,10 +142,10 @@ __device__ __forceinline__ void cov_role(int c, int k, int &blk, int &col, int &
 // quarter c, and those of component 1 a second time in quarter 3, so the 15
 // epilogue warps take partitions 0 (component 0, five blocks), 1 (component
 // 1, three blocks), 2 (component 2, five blocks) and 3 (component 1, two
-// blocks); with the MMA warp on partition 3 the 8 producer warps, which issue
-// most of the instructions, spread 1 / 3 / 1 / 3 over the partitions.
-// Returns 0 (epilogue: component c, block k of it), 1 (MMA) or 2 (producer
-// number pidx).
+// blocks); with the loader / MMA warp on partition 3 the 8 converter warps
+// spread 1 / 3 / 1 / 3 over the partitions.
+// Returns 0 (epilogue: component c, block k of it), 1 (loader / MMA) or 2
+// (converter number pidx).
 __device__ __forceinline__ int cov_warp_role(int w, int &c, int &k, int &pidx) {
   const int q = w & 3, r = w >> 2;  // partition, rank on it (0..5)
   c = k = pidx = 0;
@@ -165,18 +180,57 @@ __device__ __forceinline__ int cov_warp_role(int w, int &c, int &k, int &pidx) {
 struct CovArgs {
   int npairs, nsrc, ndof, n_elem;
   int add;          // 1: add into the accumulators, 0: overwrite them
-  int inject;       // 1: producer warp 0 of CTA 0 withholds its first stage
+  int inject;       // 1: converter warp 0 of CTA 0 withholds its first stage
                     // arrival, so the MMA thread's wait runs out (a test of
                     // the time-out path)
   long long spin;   // SM clocks a pipeline wait may take before it gives up
 };
 
+// The 2D TMA views of the launch's fields: [field: u, lam][box width code],
+// each a row of 2 NDOF doubles per (pair, source), box = (6 x width doubles,
+// kG rows).
+struct CovMaps {
+  CUtensorMap m[2][3];
+};
+
+// Per-element gather plan (elements outside the PML, kernel order):
+//   op = {x: first double of the box (2 (DOF - 1)), code | raw 128-B granule << 8}
+//   node[a] = raw byte offset of the node's source-0 values | box code << 16,
+//             or 0xFFFFFFFF for a node without DOFs (fixed)
+//   tx = TMA bytes of one stage (both fields)
+struct CovPlan {
+  const int2 *ops;
+  const int *opptr;    // [n_elem + 1]
+  const uint32_t *node;  // [n_elem][25]
+  const int *tx;       // [n_elem]
+};
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\t"
+      "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(mbar),
+      "r"(bytes)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                            uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
+}
+
 __global__ void __launch_bounds__(cov::kThreads, 1)
-    k_grad_cov(CovArgs ga, const int *__restrict__ elems, const int *__restrict__ lm, PairTable pt,
-               const double2 *__restrict__ u, const double2 *__restrict__ lam,
+    k_grad_cov(const __grid_constant__ CovMaps maps, CovArgs ga, CovPlan plan, PairTable pt,
                double *__restrict__ acc_out, int *__restrict__ err) {
-  extern __shared__ __align__(1024) uint8_t sm[];
-  __shared__ uint64_t bar_bfull[cov::kNB], bar_bempty[cov::kNB], bar_tfull[2], bar_tempty[2];
+  extern __shared__ __align__(1024) uint8_t sm_dyn[];
+  // 128-byte aligned base (TMA destinations); the launch adds 128 bytes
+  uint8_t *sm = sm_dyn + ((128u - (smem_u32(sm_dyn) & 127u)) & 127u);
+  __shared__ uint64_t bar_bfull[cov::kNB], bar_bempty[cov::kNB];
+  __shared__ uint64_t bar_rfull[cov::kRawD], bar_rempty[cov::kRawD];
+  __shared__ uint64_t bar_tfull[cov::kUnits], bar_tempty[cov::kUnits];
   __shared__ uint64_t bar_drain;
   __shared__ uint32_t tmem_base_s;
   __shared__ int drain_s;
@@ -194,7 +248,11 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
       mbar_init(smem_u32(&bar_bfull[b]), cov::kProdWarps);
       mbar_init(smem_u32(&bar_bempty[b]), 1);
     }
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < cov::kRawD; b++) {
+      mbar_init(smem_u32(&bar_rfull[b]), 1);
+      mbar_init(smem_u32(&bar_rempty[b]), cov::kProdWarps);
+    }
+    for (int b = 0; b < cov::kUnits; b++) {
       mbar_init(smem_u32(&bar_tfull[b]), 1);
       mbar_init(smem_u32(&bar_tempty[b]), cov::kEpiWarps);
     }
@@ -216,103 +274,68 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
   const int nch = (ga.nsrc + cov::kG - 1) / cov::kG;  // stages per (element, pair)
   const int my_elems = (ga.n_elem - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
   const uint32_t total = (uint32_t)max(my_elems, 0) * (uint32_t)ga.npairs * (uint32_t)nch;
+  uint8_t *raw = sm + cov::kNB * cov::kStage;
   int rc, rk, rp;
   const int role = cov_warp_role(warp, rc, rk, rp);
 
   if (role == 2) {
-    // =================== producers (warps 13, 15, 17, 19, 20-23)
+    // =================== converters (warps 13, 15, 17, 19, 20-23)
     // Thread pt (0..255) owns node a = 8 ah + a7 and source g = 2 gh + g1 of
     // every stage (a7 = pt bits 0-2, g1 = bit 3, ah = bits 4-5, gh = bits
-    // 6-7; a >= 25: no node): it copies the node's three DOFs of u and of
-    // lam (two 48-byte runs; GENID numbers a node's DOFs consecutively) into
-    // its own raw slots by cp.async (zero-filled for a fixed node or a
-    // source past nsrc), kRawD - 1 stages ahead, and converts them itself
-    // (FP64 -> tf32 hi/lo) into A rows 32c + a (lam) and B rows 32c + a,
-    // 96 + 32c + a (u) at K = 2g.  A warp's 32 threads cover the 16
-    // (row mod 8, g mod 2) shared-memory bank classes twice, so each 8-byte
-    // tile store is two wavefronts.
+    // 6-7; a >= 25: no node): it reads the node's u and lam values of source
+    // g from the raw stage (the node's box and place in it come from the
+    // element's plan) and writes them (FP64 -> tf32 hi/lo) into A rows
+    // 32c + a (lam; component 1 also at 96 + a) and B rows 32c + a (u) at
+    // K = 2g.  A warp's 32 threads cover the 16 (row mod 8, g mod 2)
+    // shared-memory bank classes twice, so each 8-byte tile store is two
+    // wavefronts.
     const int pt0 = rp * 32 + lane;
     const int a = ((pt0 >> 4) & 3) * 8 + (pt0 & 7);
     const int g = ((pt0 >> 6) & (cov::kG / 2 - 1)) * 2 + ((pt0 >> 3) & 1);
     const bool node = a < kNen;
     const uint32_t to_a = kmajor_off(a, 2 * g, cov::kALbo);                        // A row a
     const uint32_t to_b = 2 * cov::kATile + kmajor_off(a, 2 * g, cov::kBLbo);      // B row a
-    uint8_t *raw = sm + cov::kNB * cov::kStage;
-    int d0 = 0, d0_next = 0;  // first DOF of the node in this / the next element (0: fixed)
-    int iei = blockIdx.x, ip = 0, ich = 0;  // next stage to copy
-    uint32_t issued = 0;
-    auto node_dof = [&](int eidx) -> int {
-      return (node && eidx < ga.n_elem) ? __ldg(lm + (size_t)elems[eidx] * kNee + 3 * a) : 0;
-    };
-    auto issue = [&]() {
-      const bool act = d0 > 0 && g < ga.nsrc - ich * cov::kG;
-      const size_t off = act ? ((size_t)ip * ga.nsrc + (size_t)ich * cov::kG + g) * ga.ndof + d0 - 1 : 0;
-      const uint32_t rs = smem_u32(raw + (issued % cov::kRawD) * cov::kRawStage) + pt0 * 16;
-      const uint32_t n = act ? 16u : 0u;
-      if (node) {
-#pragma unroll
-        for (int j = 0; j < cov::kSlotsPer; j++) {
-          const double2 *src = (j < 3 ? u : lam) + off + j % 3;
-          asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(
-                           rs + j * cov::kProdThreads * 16),
-                       "l"(src), "r"(n)
-                       : "memory");
-        }
-      }
-      asm volatile("cp.async.commit_group;" ::: "memory");
-      issued++;
-      if (++ich == nch) {
-        ich = 0;
-        if (++ip == ga.npairs) {
-          ip = 0;
-          iei += gridDim.x;
-          d0 = d0_next;
-          d0_next = node_dof(iei + (int)gridDim.x);  // in flight until the next element
-        }
-      }
-    };
-    if (total > 0) {
-      d0 = node_dof(iei);
-      d0_next = node_dof(iei + (int)gridDim.x);
-    }
-    while (issued < total && issued < (uint32_t)(cov::kRawD - 1)) issue();
+    int iei = blockIdx.x, ip = 0, ich = 0;
+    uint32_t nodeinfo = node && iei < ga.n_elem ? __ldg(plan.node + (size_t)iei * kNen + a)
+                                                : 0xFFFFFFFFu;
     for (uint32_t s = 0; s < total; s++) {
-      if (issued < total) issue();  // stage s + kRawD - 1 into this thread's slots of s - 1
-      // copy groups still allowed in flight once stage s has landed
-      switch (issued - s - 1) {
-        case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
-        case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
-        case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
-        default: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
-      }
-      const int bs = (int)(s % cov::kNB);
+      const int rs = (int)(s % cov::kRawD), bs = (int)(s % cov::kNB);
+      mbar_wait(smem_u32(&bar_rfull[rs]), (s / cov::kRawD) & 1u, drain, err, -2000006, ga.spin);
       mbar_wait(smem_u32(&bar_bempty[bs]), ((s / cov::kNB) & 1u) ^ 1u, drain, err, -2000001,
                 ga.spin);
       if (node) {
-        const uint8_t *rs = raw + (s % cov::kRawD) * cov::kRawStage + pt0 * 16;
+        const bool act = nodeinfo != 0xFFFFFFFFu && g < ga.nsrc - ich * cov::kG;
+        const uint32_t code = (nodeinfo >> 16) & 3u;
+        const uint32_t rowb = (code == 0 ? 16u : code == 1 ? 4u : 1u) * cov::kNodeBytes;
+        const uint8_t *src = raw + rs * cov::kRawStage + (act ? (nodeinfo & 0xFFFFu) + g * rowb : 0u);
         uint8_t *st = sm + bs * cov::kStage;
 #pragma unroll
-        for (int j = 0; j < cov::kSlotsPer; j++) {
-          const double2 v = *reinterpret_cast<const double2 *>(rs + j * cov::kProdThreads * 16);
-          const float xr = (float)v.x, xi = (float)v.y;
-          const uint32_t hr = to_tf32(xr), hi = to_tf32(xi);
-          const uint32_t lr = to_tf32(xr - __uint_as_float(hr));
-          const uint32_t li = to_tf32(xi - __uint_as_float(hi));
-          const int c = j % 3;  // rows 32c + a: 4c core-matrix groups further
-          if (j < 3) {  // u -> B Re row and Im row, hi then lo
+        for (int j = 0; j < 6; j++) {  // j < 3: u component j; else lam component j - 3
+          const int c = j % 3;
+          double2 v = act ? *reinterpret_cast<const double2 *>(src + (j < 3 ? 0 : cov::kRawField) +
+                                                                16 * c)
+                          : make_double2(0.0, 0.0);
+          // the sign / swap of the layout: u1 -> (Im, -Re), lam1 -> (-Im, Re)
+          float x0 = (float)v.x, x1 = (float)v.y;
+          if (c == 1) {
+            const float t = x0;
+            x0 = j < 3 ? x1 : -x1;
+            x1 = j < 3 ? -t : t;
+          }
+          const uint32_t h0 = to_tf32(x0), h1 = to_tf32(x1);
+          const uint32_t l0 = to_tf32(x0 - __uint_as_float(h0));
+          const uint32_t l1 = to_tf32(x1 - __uint_as_float(h1));
+          if (j < 3) {  // u -> B row 32c + a, hi then lo
             uint8_t *d = st + to_b + 512 * c;
-            *reinterpret_cast<uint2 *>(d) = make_uint2(hr, hi);
-            *reinterpret_cast<uint2 *>(d + cov::kBTile) = make_uint2(lr, li);
-            *reinterpret_cast<uint2 *>(d + cov::kBImOff) = make_uint2(hi, hr ^ 0x80000000u);
-            *reinterpret_cast<uint2 *>(d + cov::kBTile + cov::kBImOff) =
-                make_uint2(li, lr ^ 0x80000000u);
-          } else {  // lam -> A row (hi, then lo); component 1 also to row 96 + a
+            *reinterpret_cast<uint2 *>(d) = make_uint2(h0, h1);
+            *reinterpret_cast<uint2 *>(d + cov::kBTile) = make_uint2(l0, l1);
+          } else {  // lam -> A row 32c + a (hi, then lo); component 1 also to row 96 + a
             uint8_t *d = st + to_a + 512 * c;
-            *reinterpret_cast<uint2 *>(d) = make_uint2(hr, hi);
-            *reinterpret_cast<uint2 *>(d + cov::kATile) = make_uint2(lr, li);
+            *reinterpret_cast<uint2 *>(d) = make_uint2(h0, h1);
+            *reinterpret_cast<uint2 *>(d + cov::kATile) = make_uint2(l0, l1);
             if (c == 1) {
-              *reinterpret_cast<uint2 *>(d + 1024) = make_uint2(hr, hi);
-              *reinterpret_cast<uint2 *>(d + 1024 + cov::kATile) = make_uint2(lr, li);
+              *reinterpret_cast<uint2 *>(d + 1024) = make_uint2(h0, h1);
+              *reinterpret_cast<uint2 *>(d + 1024 + cov::kATile) = make_uint2(l0, l1);
             }
           }
         }
@@ -321,30 +344,73 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
       __syncwarp();
       const bool withhold = ga.inject && blockIdx.x == 0 && rp == 0 && s == 0;
       if (lane == 0 && !withhold) mbar_arrive(smem_u32(&bar_bfull[bs]));
+      if (lane == 0) mbar_arrive(smem_u32(&bar_rempty[rs]));
+      if (++ich == nch) {
+        ich = 0;
+        if (++ip == ga.npairs) {
+          ip = 0;
+          iei += gridDim.x;
+          nodeinfo = node && iei < ga.n_elem ? __ldg(plan.node + (size_t)iei * kNen + a)
+                                             : 0xFFFFFFFFu;
+        }
+      }
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
   } else if (role == 1) {
-    // =================== MMA issuer
+    // =================== loader and MMA issuer
     if (lane == 0) {
       const uint32_t sbase = smem_u32(sm);
+      const uint32_t rbase = smem_u32(raw);
       const uint64_t adesc = umma_desc(sbase, cov::kALbo, 128);
       const uint64_t bdesc = umma_desc(sbase, cov::kBLbo, 128);
+      // TMA fetch of stage s (element iei, pair ip, chunk ich: the issue
+      // pointer) into raw stage s % kRawD
+      int iei = blockIdx.x, ip = 0, ich = 0;
+      uint32_t issued = 0;
+      auto issue = [&]() {
+        const int rs = (int)(issued % cov::kRawD);
+        if (issued >= (uint32_t)cov::kRawD)
+          mbar_wait(smem_u32(&bar_rempty[rs]), ((issued / cov::kRawD) & 1u) ^ 1u, drain, err,
+                    -2000007, ga.spin);
+        if (*drain) return;  // no new loads once the CTA drains
+        const uint32_t full = smem_u32(&bar_rfull[rs]);
+        mbar_arrive_expect_tx(full, (uint32_t)__ldg(plan.tx + iei));
+        const int y = ip * ga.nsrc + ich * cov::kG;
+        const uint32_t dst0 = rbase + (uint32_t)(rs * cov::kRawStage);
+        for (int k = __ldg(plan.opptr + iei), k1 = __ldg(plan.opptr + iei + 1); k < k1; k++) {
+          const int2 op = __ldg(plan.ops + k);
+          const int code = op.y & 0xFF;
+          const uint32_t off = (uint32_t)(op.y >> 8) * 128u;
+          tma_load_2d(dst0 + off, &maps.m[0][code], op.x, y, full);
+          tma_load_2d(dst0 + cov::kRawField + off, &maps.m[1][code], op.x, y, full);
+        }
+        issued++;
+        if (++ich == nch) {
+          ich = 0;
+          if (++ip == ga.npairs) {
+            ip = 0;
+            iei += gridDim.x;
+          }
+        }
+      };
+      while (issued < total && issued < (uint32_t)(cov::kRawD - 1)) issue();
       uint32_t s = 0, unit = 0;
       for (int ei = blockIdx.x; ei < ga.n_elem; ei += gridDim.x) {
         for (int p = 0; p < ga.npairs; p++) {
           for (int ch = 0; ch < nch; ch++, s++) {
+            // fetch stage s + kRawD - 1 (its raw slot was freed by stage s - 1)
+            if (issued < total && !*drain) issue();
             // a TMEM accumulator takes kDrain stages of one pair (FP32 sums
             // of at most 2 kDrain kG products), then the epilogue adds it in FP64
             const bool first = ch % cov::kDrain == 0;
             const bool last = ch % cov::kDrain == cov::kDrain - 1 || ch == nch - 1;
-            const int ts = (int)(unit & 1u), bs = (int)(s % cov::kNB);
+            const int ts = (int)(unit % cov::kUnits), bs = (int)(s % cov::kNB);
             if (first)
-              mbar_wait(smem_u32(&bar_tempty[ts]), ((unit >> 1) & 1u) ^ 1u, drain, err, -2000002,
-                        ga.spin);
+              mbar_wait(smem_u32(&bar_tempty[ts]), ((unit / cov::kUnits) & 1u) ^ 1u, drain, err,
+                        -2000002, ga.spin);
             mbar_wait(smem_u32(&bar_bfull[bs]), (s / cov::kNB) & 1u, drain, err, -2000003,
                       ga.spin);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t td = tmem + (uint32_t)ts * cov::kTmemStage;
+            const uint32_t td = tmem + (uint32_t)ts * cov::kTmemUnit;
             const int nact = min(cov::kG, ga.nsrc - ch * cov::kG);
             const int nks = (nact + 3) / 4;  // K steps of 8 = 4 sources
             const uint32_t so = (uint32_t)(bs * cov::kStage);
@@ -368,19 +434,35 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
       }
       // every MMA issued above has completed once this commit arrives
       mma_commit(smem_u32(&bar_drain));
-      const long long t0 = clock64();
+      long long t0 = clock64();
       while (!mbar_try_wait(smem_u32(&bar_drain), 0u)) {
         if (clock64() - t0 > kTcSpinCycles) {
           atomicCAS(err, 0, -2000004);
           break;
         }
       }
+      // loads still in flight (a drained CTA may have issued stages nobody
+      // consumed): wait, bounded, for the last phase issued into each raw slot
+      if (*drain) {
+        for (int r = 0; r < cov::kRawD; r++) {
+          const uint32_t n = issued > (uint32_t)r ? (issued - 1 - (uint32_t)r) / cov::kRawD + 1 : 0u;
+          if (n == 0) continue;
+          t0 = clock64();
+          while (!mbar_try_wait(smem_u32(&bar_rfull[r]), (n - 1) & 1u)) {
+            if (clock64() - t0 > kTcSpinCycles) {
+              atomicCAS(err, 0, -2000008);
+              break;
+            }
+          }
+        }
+      }
     }
     __syncwarp();
   } else {
     // =================== epilogue (15 warps)
-    int blk, col0, wt;
-    cov_role(rc, rk, blk, col0, wt);
+    int blk, slot, wt;
+    bool neg;
+    cov_role(rc, rk, blk, slot, wt, neg);
     const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;  // lane quarter = partition
     double acc[kNen];
 #pragma unroll
@@ -389,12 +471,14 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
     for (int ei = blockIdx.x; ei < ga.n_elem; ei += gridDim.x) {
       for (int p = 0; p < ga.npairs; p++) {
         const double2 pr = pt.p[p];
-        const double w = wt == 0 ? 1.0 : wt == 1 ? pr.y * pr.y : wt == 2 ? pr.x * pr.x : pr.y;
+        double w = wt == 0 ? 1.0 : wt == 1 ? pr.y * pr.y : wt == 2 ? pr.x * pr.x : pr.y;
+        if (neg) w = -w;
         for (int ch = 0; ch < nch; ch += cov::kDrain, unit++) {
-          const int ts = (int)(unit & 1u);
-          mbar_wait(smem_u32(&bar_tfull[ts]), (unit >> 1) & 1u, drain, err, -2000005, ga.spin);
+          const int ts = (int)(unit % cov::kUnits);
+          mbar_wait(smem_u32(&bar_tfull[ts]), (unit / cov::kUnits) & 1u, drain, err, -2000005,
+                    ga.spin);
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint32_t tb = tmem + lane_base + (uint32_t)ts * cov::kTmemStage + (uint32_t)col0;
+          const uint32_t tb = tmem + lane_base + (uint32_t)ts * cov::kTmemUnit + 32u * (uint32_t)slot;
           __syncwarp();
           uint32_t r[16];
           tmem_ld16(tb, r);
@@ -723,10 +807,54 @@ static CovFinTabs cov_fin_tables(const Tables &t) {
   return tb;
 }
 
+// Gather plan of the covariance accumulation for every element outside the
+// PML (kernel order): the element's nodes, sorted by first DOF, split into
+// runs of consecutive nodes (GENID numbers an element's new nodes
+// consecutively, so a structured mesh gives one 16-node run, one 4-node run
+// and five single nodes); each run is covered by TMA boxes of 16, 4 and 1
+// nodes, packed one after the other (8 source rows each) into the 9600-byte
+// raw region of a field.
+static void build_cov_plan(const Ctx *c, const std::vector<int> &elems, std::vector<int2> &ops,
+                           std::vector<int> &opptr, std::vector<uint32_t> &node,
+                           std::vector<int> &tx) {
+  const int n = (int)elems.size();
+  opptr.assign(n + 1, 0);
+  node.assign((size_t)n * kNen, 0xFFFFFFFFu);
+  tx.assign(n, 0);
+  ops.clear();
+  for (int k = 0; k < n; k++) {
+    const int *lme = c->h_lm.data() + (size_t)elems[k] * kNee;
+    int ord[kNen], cnt = 0;
+    for (int a = 0; a < kNen; a++)
+      if (lme[3 * a] > 0) ord[cnt++] = a;
+    std::sort(ord, ord + cnt, [&](int x, int y) { return lme[3 * x] < lme[3 * y]; });
+    uint32_t off = 0;  // bytes into the field's raw region
+    for (int i = 0; i < cnt;) {
+      int len = 1;
+      while (i + len < cnt && lme[3 * ord[i + len]] == lme[3 * ord[i]] + 3 * len) len++;
+      // boxes of 16, 4 and 1 nodes over the run
+      int done = 0;
+      while (done < len) {
+        const int code = len - done >= 16 ? 0 : len - done >= 4 ? 1 : 2;
+        const int w = cov::kBoxNodes[code];
+        const int d0 = lme[3 * ord[i + done]];
+        ops.push_back(make_int2(2 * (d0 - 1), code | (int)(off / 128u) << 8));
+        for (int j = 0; j < w; j++) node[(size_t)k * kNen + ord[i + done + j]] =
+            (off + (uint32_t)(j * cov::kNodeBytes)) | ((uint32_t)code << 16);
+        off += (uint32_t)(w * cov::kNodeBytes * cov::kG);
+        done += w;
+      }
+      i += len;
+    }
+    opptr[k + 1] = (int)ops.size();
+    tx[k] = (int)(2 * off);
+  }
+}
+
 // One-time set-up of the covariance gradient: the gather's DOF-layout check,
-// the kernels' shared-memory attributes and the FP64 accumulators
-// (15 x 625 doubles per element outside the PML).  Allocates, so it runs
-// outside any stream capture.
+// the gather plan, the kernels' shared-memory attributes and the FP64
+// accumulators (15 x 625 doubles per element outside the PML).  Allocates,
+// so it runs outside any stream capture.
 cudaError_t prepare_grad_cov(Ctx *c) {
   if (c->d_cov) return cudaSuccess;
   for (size_t i = 0; i + 2 < c->h_lm.size(); i += 3) {
@@ -735,12 +863,36 @@ cudaError_t prepare_grad_cov(Ctx *c) {
                           : (c->h_lm[i + 1] == 0 && c->h_lm[i + 2] == 0);
     if (!ok) return cudaErrorNotSupported;
   }
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+          cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn)
+    return cudaErrorNotSupported;
+  c->tmap_encode = fn;
+  std::vector<int> elems;
+  for (int e = 0; e < c->nelem; e++)
+    if (c->h_cdomain[e] != 'A') elems.push_back(e);
+  std::vector<int2> ops;
+  std::vector<int> opptr, tx;
+  std::vector<uint32_t> node;
+  build_cov_plan(c, elems, ops, opptr, node, tx);
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(k_grad_cov, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                cov::kSmemBytes)))
+                                cov::kSmemBytes + 128)))
     return e;
   if ((e = cudaFuncSetAttribute(k_grad_cov_fin, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 covf::kSmemBytes)))
+    return e;
+  auto up = [&](void **d, const void *h, size_t bytes) -> cudaError_t {
+    cudaError_t r = cudaMalloc(d, bytes ? bytes : 16);
+    if (r == cudaSuccess && bytes) r = cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice);
+    return r;
+  };
+  if ((e = up((void **)&c->d_cov_ops, ops.data(), ops.size() * sizeof(int2))) ||
+      (e = up((void **)&c->d_cov_opptr, opptr.data(), opptr.size() * sizeof(int))) ||
+      (e = up((void **)&c->d_cov_node, node.data(), node.size() * sizeof(uint32_t))) ||
+      (e = up((void **)&c->d_cov_tx, tx.data(), tx.size() * sizeof(int))))
     return e;
   const size_t n = (size_t)std::max(c->n_nonpml, 1) * cov::kBlocks * cov::kBlk;
   double *d = nullptr;
@@ -750,10 +902,37 @@ cudaError_t prepare_grad_cov(Ctx *c) {
   return cudaSuccess;
 }
 
+// The 2D TMA views of one launch's fields: rows of 2 NDOF doubles, one per
+// (pair, source), for each box width.  cudaErrorInvalidValue for a field
+// pointer off a 16-byte boundary.
+static cudaError_t cov_maps(const Ctx *c, const double *u, const double *lam, int rows,
+                            CovMaps &maps) {
+  auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(c->tmap_encode);
+  const double *base[2] = {u, lam};
+  for (int f = 0; f < 2; f++) {
+    if (reinterpret_cast<uintptr_t>(base[f]) % 16) return cudaErrorInvalidValue;
+    for (int code = 0; code < 3; code++) {
+      const cuuint64_t dim[2] = {(cuuint64_t)2 * c->ndof, (cuuint64_t)rows};
+      const cuuint64_t stride[1] = {(cuuint64_t)c->ndof * 16};
+      const cuuint32_t box[2] = {(cuuint32_t)(6 * cov::kBoxNodes[code]), (cuuint32_t)cov::kG};
+      const cuuint32_t estr[2] = {1, 1};
+      CUresult r = encode(&maps.m[f][code], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
+                          const_cast<double *>(base[f]), dim, stride, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    }
+  }
+  return cudaSuccess;
+}
+
 cudaError_t launch_grad_cov(Ctx *c, const PairTable &pt, int npairs, int nsrc, const double *u,
                             const double *lam, cudaStream_t st) {
   if (!c->d_cov) return cudaErrorNotReady;
   if (c->n_nonpml == 0) return cudaSuccess;
+  CovMaps maps;
+  cudaError_t e = cov_maps(c, u, lam, npairs * nsrc, maps);
+  if (e != cudaSuccess) return e;
   CovArgs ga;
   ga.npairs = npairs;
   ga.nsrc = nsrc;
@@ -762,14 +941,13 @@ cudaError_t launch_grad_cov(Ctx *c, const PairTable &pt, int npairs, int nsrc, c
   ga.add = c->cov_pending ? 1 : 0;
   ga.inject = c->wait_inject;
   ga.spin = c->wait_limit > 0 ? c->wait_limit : kTcSpinCycles;
+  CovPlan plan{c->d_cov_ops, c->d_cov_opptr, c->d_cov_node, c->d_cov_tx};
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
   const int grid = std::min(nsm, c->n_nonpml);
-  k_grad_cov<<<grid, cov::kThreads, cov::kSmemBytes, st>>>(ga, c->d_nonpml, c->d_lm, pt,
-                                                           (const double2 *)u,
-                                                           (const double2 *)lam, c->d_cov,
-                                                           c->d_err);
-  cudaError_t e = cudaGetLastError();
+  k_grad_cov<<<grid, cov::kThreads, cov::kSmemBytes + 128, st>>>(maps, ga, plan, pt, c->d_cov,
+                                                                 c->d_err);
+  e = cudaGetLastError();
   if (e == cudaSuccess) c->cov_pending = true;
   return e;
 }

@@ -8,6 +8,8 @@
 // on its own, as the reference writes it.
 #include <algorithm>
 
+#include <complex>
+
 #include "ctx.cuh"
 #include "kcommon.cuh"
 
@@ -76,6 +78,14 @@ cudaError_t launch_addblk(Ctx *c, int nsrc, const float *u0, float *sol, cudaStr
 // misfit + adjoint source, one thread per (source, receiver)
 //   trig[ir] = (cos, sin) of omega*py*yrec in single precision; rot = (cos th,
 //   sin th, cos -th, sin -th) of the model azimuth (computed on the host).
+//   The COBJ4 term (objfn.f:60-125) and the BPRESID4 residual
+//   (objfn.f:795-843) follow the context's misfit options (NORM, IRESTP,
+//   DTMAX, COBJ4's EPS / THRESH); the residual is scaled by HDIFFER
+//   (adjgrad.f90:528-566, evaluated on the host) in RESID_DRHS.
+//   |z| = sqrt(re^2 + im^2); complex products (ac - bd, ad + bc); this unit
+//   is compiled without FMA contraction, so every result is bit-identical to
+//   the oracle except where IRESTP = 1 or a DTMAX test takes phases
+//   (atan2f, cosf, sinf of the device against the host's libm).
 // ---------------------------------------------------------------------------
 struct cfl {
   float re, im;
@@ -83,11 +93,45 @@ struct cfl {
 __device__ __forceinline__ cfl cmulf(cfl a, cfl b) {
   return cfl{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
 }
+__device__ __forceinline__ float cabsf_(cfl z) { return sqrtf(z.re * z.re + z.im * z.im); }
+
+// CRESID (objfn.f:953-1010)
+__device__ __forceinline__ cfl cresid(int irestp, cfl obs, cfl est) {
+  if (obs.re == 0.0f && obs.im == 0.0f) return cfl{0.0f, 0.0f};
+  if (irestp == 1 || irestp == 2) {
+    float adata, pdata, aest, pest;
+    if (irestp == 2) {
+      adata = sqrtf(obs.re * obs.re + obs.im * obs.im);
+      pdata = 0.0f;
+      aest = sqrtf(est.re * est.re + est.im * est.im);
+      pest = 0.0f;
+    } else {
+      adata = 1.0f;
+      pdata = atan2f(obs.im, obs.re);
+      aest = 1.0f;
+      pest = atan2f(est.im, est.re);
+    }
+    const cfl a = cmulf(cfl{adata, 0.0f}, cfl{cosf(pdata), sinf(pdata)});
+    const cfl b = cmulf(cfl{aest, 0.0f}, cfl{cosf(pest), sinf(pest)});
+    return cfl{a.re - b.re, a.im - b.im};
+  }
+  return cfl{obs.re - est.re, obs.im - est.im};
+}
+
+// the wrapped phase difference SPHASE(obs) - SPHASE(est) exceeds dtmax as a
+// time shift (objfn.f:106-112, :826-832)
+__device__ __forceinline__ bool phase_jump(cfl obs, cfl est, double freq, float dtmax) {
+  const float kTwoPi = 6.283185307179586f, kPi = 3.1415926535897931f;
+  float dphi = atan2f(obs.im, obs.re) - atan2f(est.im, est.re);
+  if (dphi < -kPi) dphi = dphi + kTwoPi;
+  if (dphi > +kPi) dphi = dphi - kTwoPi;
+  return fabs((double)dphi / ((double)kTwoPi * freq)) > (double)dtmax;
+}
 
 __global__ void k_misfit(int nsrc, int nrec, int ndof, const int *__restrict__ mrdof,
                          const float4 *__restrict__ trig, float4 rot, const float2 *__restrict__ recv,
                          const float2 *__restrict__ sol, const float2 *__restrict__ obs,
-                         const float *__restrict__ wghts, float2 *__restrict__ est,
+                         const float *__restrict__ wghts, MisfitOpts mo, float2 *__restrict__ est,
                          float2 *__restrict__ rhs, float *__restrict__ part) {
   int gid = blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= nsrc * nrec) return;
@@ -117,25 +161,66 @@ __global__ void k_misfit(int nsrc, int nrec, int ndof, const int *__restrict__ m
     res[i] = cfl{0.0f, 0.0f};
     part[(size_t)gid * 3 + i] = 0.0f;
     if (o3[i].re == 0.0f && o3[i].im == 0.0f) continue;
-    cfl ob = cmulf(o3[i], cf2), es = cmulf(er[i], cf2);
-    cfl dif = cfl{ob.re - es.re, ob.im - es.im};
-    float wv = fabsf(wghts[((size_t)s * nrec + ir) * 3 + i]);
-    float w2 = wv * wv;
-    res[i] = cfl{w2 * dif.re, w2 * dif.im};
-    cfl dif0 = cfl{o3[i].re - er[i].re, o3[i].im - er[i].im};
-    part[(size_t)gid * 3 + i] = w2 * (dif0.re * dif0.re + dif0.im * dif0.im);
+    const float w = wghts[((size_t)s * nrec + ir) * 3 + i];
+    const cfl S = cfl{w, 0.0f};
+    const float sabs = fabsf(w);
+    // ---- COBJ4 term on the unshifted pair
+    {
+      const cfl dif = cresid(mo.irestp, o3[i], er[i]);
+      float c;
+      if (mo.norm == 1) {
+        c = cabsf_(cmulf(S, dif));
+      } else if (mo.norm == 3) {
+        const float arg = cabsf_(cmulf(S, dif));
+        c = arg <= mo.eps ? arg * arg / (2.0f * mo.eps) : arg - mo.eps / 2.0f;
+      } else if (mo.norm == 4) {
+        const float arg = cabsf_(dif), sd = cabsf_(cmulf(S, dif));
+        c = arg <= mo.thresh ? sd * sd / (2.0f * (mo.eps * mo.eps)) : sd / mo.eps;
+      } else {
+        const cfl cd = cmulf(cfl{dif.re, -dif.im}, dif);
+        c = sabs * sabs * cd.re;
+        if (mo.dtmax_obj > 0.0f && phase_jump(o3[i], er[i], mo.freq, mo.dtmax_obj)) {
+          const float damp = cabsf_(o3[i]) - cabsf_(er[i]);
+          c = mo.irestp == 1 ? sabs * sabs * 4.0f : sabs * sabs * (damp * damp);
+        }
+      }
+      part[(size_t)gid * 3 + i] = c;
+    }
+    // ---- BPRESID4 residual on the shifted pair (EPS = 0, objfn.f:795-797)
+    {
+      const cfl ob = cmulf(o3[i], cf2), es = cmulf(er[i], cf2);
+      const cfl dif = cresid(mo.irestp, ob, es);
+      const float e0 = 0.0f;
+      if (mo.norm == 1 || (mo.norm == 3 && !(cabsf_(cmulf(S, dif)) <= e0))) {
+        const cfl num = cmulf(S, dif);  // CONJG(WEIGHT) = WEIGHT
+        const float den = cabsf_(dif);
+        res[i] = cfl{num.re / den, num.im / den};
+      } else if (mo.norm == 3) {
+        res[i] = cmulf(cfl{sabs * sabs / e0, 0.0f}, dif);
+      } else if (mo.norm == 4) {
+        const float eps2 = 0.0f;  // EPSS * EPS**2 with EPS = 0
+        const float sd = cabsf_(cmulf(S, dif));
+        const float denon = eps2 * sqrtf(1.0f + sd * sd / eps2);
+        res[i] = cmulf(cfl{sabs * sabs / denon, 0.0f}, dif);
+      } else {
+        res[i] = cmulf(cfl{sabs * sabs, 0.0f}, dif);
+        if (mo.dtmax > 0.0f && phase_jump(ob, es, mo.freq, mo.dtmax)) res[i] = cfl{0.0f, 0.0f};
+      }
+    }
   }
   const float ct2 = rot.z, st2 = rot.w;
   cfl rr[3];
   rr[0] = cfl{res[0].re * ct2 - res[1].re * st2, res[0].im * ct2 - res[1].im * st2};
   rr[1] = cfl{res[0].re * st2 + res[1].re * ct2, res[0].im * st2 + res[1].im * ct2};
   rr[2] = res[2];
+  const cfl hf = cfl{mo.hfact.x, mo.hfact.y};
   for (int i = 0; i < 3; i++) {
     int d = mrdof[3 * ir + i];
     if (d <= 0 || d > ndof) continue;
-    // receivers map to distinct DOFs (checked by the host); conjugate for
-    // the transpose solve (adjgrad.f90:519-521)
-    rhs[(size_t)s * ndof + d - 1] = make_float2(0.0f + rr[i].re, -(0.0f + rr[i].im));
+    // receivers map to distinct DOFs (checked by the host): RHS = 0 + HFACT
+    // RESID, conjugated for the transpose solve (adjgrad.f90:509-521)
+    const cfl t = cmulf(hf, rr[i]);
+    rhs[(size_t)s * ndof + d - 1] = make_float2(0.0f + t.re, -(0.0f + t.im));
   }
 }
 
@@ -160,12 +245,34 @@ __global__ void k_misfit_sum(int nsrc, int nrec, const float *__restrict__ part,
   out[s] = acc;
 }
 
+// The call's options: the context's, with FREQ and HDIFFER (adjgrad.f90:528-566)
+// evaluated on the host (REAL*4 OMEGA, the C library's complex square root).
+static MisfitOpts misfit_opts(const Ctx *c, double freq) {
+  MisfitOpts mo = c->mopt;
+  mo.freq = freq;
+  const float omega = (float)(2.0 * 3.1415926535897932384626434 * freq);
+  std::complex<float> h(1.0f, 0.0f);
+  if (mo.ibphase == 1 || mo.ibphase == 2) {
+    h = std::sqrt(std::complex<float>(0.0f, -omega));
+    if (mo.ibphase == 2) h = -h;
+  } else if (mo.ibphase == 3 || mo.ibphase == 4) {
+    h = std::sqrt(std::complex<float>(0.0f, omega));
+    if (mo.ibphase == 4) h = -h;
+  } else if (mo.ibphase == 5) {
+    h = std::complex<float>(0.0f, omega);
+  } else if (mo.ibphase == 6) {
+    h = std::complex<float>(0.0f, 1.0f);
+  }
+  mo.hfact = make_float2(h.real(), h.imag());
+  return mo;
+}
+
 cudaError_t launch_misfit(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const float *d_trig,
-                          double omega, double py, double azmod, const float *d_recv,
+                          double freq, double py, double azmod, const float *d_recv,
                           const float *sol, const float *d_obs, const float *d_wghts,
                           float *d_est, float *rhs, float *d_misfit, cudaStream_t st) {
-  (void)omega;
   (void)py;
+  const MisfitOpts mo = misfit_opts(c, freq);
   float th = (float)azmod * 0.017453292519943295f;
   float4 rot = make_float4(cosf(th), sinf(th), cosf(-th), sinf(-th));
   float *d_part = nullptr;
@@ -176,7 +283,7 @@ cudaError_t launch_misfit(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const 
   int n = nsrc * nrec;
   k_misfit<<<(n + 127) / 128, 128, 0, st>>>(nsrc, nrec, c->ndof, d_mrdof, (const float4 *)d_trig,
                                             rot, (const float2 *)d_recv, (const float2 *)sol,
-                                            (const float2 *)d_obs, d_wghts, (float2 *)d_est,
+                                            (const float2 *)d_obs, d_wghts, mo, (float2 *)d_est,
                                             (float2 *)rhs, d_part);
   k_misfit_sum<<<(nsrc + 127) / 128, 128, 0, st>>>(nsrc, nrec, d_part, d_misfit);
   cudaFreeAsync(d_part, st);
@@ -187,9 +294,10 @@ cudaError_t launch_misfit(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const 
 // caller-provided device buffer of 3 * nsrc * nrec floats (every entry is
 // written by k_misfit before k_misfit_sum reads it).
 cudaError_t launch_misfit_part(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const float *d_trig,
-                               double azmod, const float *d_recv, const float *sol,
+                               double freq, double azmod, const float *d_recv, const float *sol,
                                const float *d_obs, const float *d_wghts, float *d_est, float *rhs,
                                float *d_part, float *d_misfit, cudaStream_t st) {
+  const MisfitOpts mo = misfit_opts(c, freq);
   float th = (float)azmod * 0.017453292519943295f;
   float4 rot = make_float4(cosf(th), sinf(th), cosf(-th), sinf(-th));
   const long long nrhs = (long long)nsrc * c->ndof;
@@ -197,7 +305,7 @@ cudaError_t launch_misfit_part(Ctx *c, int nsrc, int nrec, const int *d_mrdof, c
   int n = nsrc * nrec;
   k_misfit<<<(n + 127) / 128, 128, 0, st>>>(nsrc, nrec, c->ndof, d_mrdof, (const float4 *)d_trig,
                                             rot, (const float2 *)d_recv, (const float2 *)sol,
-                                            (const float2 *)d_obs, d_wghts, (float2 *)d_est,
+                                            (const float2 *)d_obs, d_wghts, mo, (float2 *)d_est,
                                             (float2 *)rhs, d_part);
   k_misfit_sum<<<(nsrc + 127) / 128, 128, 0, st>>>(nsrc, nrec, d_part, d_misfit);
   return cudaGetLastError();
@@ -1078,6 +1186,81 @@ cudaError_t launch_ref_adjflam(Ctx *c, const float *adjlam, float *gradl, cudaSt
   k_ref_adjflam<<<(n + 255) / 256, 256, 0, st>>>(n, c->d_jcsc, c->d_icsc, c->d_fmat,
                                                  (const float2 *)adjlam, gradl);
   return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// gradient post-processing of FUNCGRADH25 (funcgradh.f90:436-443)
+// ---------------------------------------------------------------------------
+// WTGRAD (gengmask.f90:384-416): GRAD(IA35) = GRAD(IA35) * WGRAD(IA35)
+__global__ void k_wtgrad(int na35, const float *__restrict__ wgrad, float *__restrict__ grad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < na35) grad[i] = grad[i] * wgrad[i];
+}
+
+cudaError_t launch_wtgrad(int na35, const float *wgrad, float *grad, cudaStream_t st) {
+  k_wtgrad<<<(na35 + 255) / 256, 256, 0, st>>>(na35, wgrad, grad);
+  return cudaGetLastError();
+}
+
+// One cascade of AVGRAD / AVGRAD8 (gengmask.f90:1202-1332), one thread per
+// anchor INPG: the mean of the gradient over the inversion anchors of every
+// element connected to INPG (MCONN order, anchors IA = 1..4 of each
+// element, counted with repetition as in the reference), written to `out`;
+// anchors outside the inversion and entries without neighbours keep `in`.
+template <typename T>
+__global__ void k_avgrad(int nnpg, int ncon, int nvinv, const int *__restrict__ maskg,
+                         const int *__restrict__ mconn, const int4 *__restrict__ ieng,
+                         const T *__restrict__ in, T *__restrict__ out) {
+  const int inpg = blockIdx.x * blockDim.x + threadIdx.x;
+  if (inpg >= nnpg) return;
+  const int inpinv = maskg[inpg];
+  if (inpinv <= 0) return;
+  T xavg[2] = {T(0), T(0)};
+  int navg[2] = {0, 0};
+  for (int icon = 0; icon < ncon; icon++) {
+    const int ielem = mconn[inpg + (size_t)nnpg * icon];
+    if (ielem == 0) break;
+    const int4 ie = ieng[ielem - 1];
+    const int an[4] = {ie.x, ie.y, ie.z, ie.w};
+    for (int ia = 0; ia < 4; ia++) {
+      const int jnpg = an[ia];
+      if (jnpg == 0) break;
+      const int jnpinv = maskg[jnpg - 1];
+      if (jnpinv > 0)
+        for (int iv = 0; iv < nvinv; iv++) {
+          xavg[iv] = xavg[iv] + in[(size_t)(jnpinv - 1) * nvinv + iv];
+          navg[iv] = navg[iv] + 1;
+        }
+    }
+  }
+  for (int iv = 0; iv < nvinv; iv++) {
+    const size_t ia35 = (size_t)(inpinv - 1) * nvinv + iv;
+    if (navg[iv] > 0) out[ia35] = xavg[iv] / (T)navg[iv];
+  }
+}
+
+// NCASC cascades; each starts from a copy of the gradient (SCOPY / DCOPY)
+template <typename T>
+cudaError_t launch_avgrad_t(Ctx *c, int nvinv, int ncasc, T *grad, T *work, cudaStream_t st) {
+  const size_t na35 = (size_t)c->rg.nnpinv * nvinv;
+  for (int k = 0; k < ncasc; k++) {
+    cudaError_t e = cudaMemcpyAsync(work, grad, sizeof(T) * na35, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+    k_avgrad<T><<<(c->nnpg + 255) / 256, 256, 0, st>>>(c->nnpg, c->rg.ncon, nvinv, c->d_maskg,
+                                                       c->d_mconn, c->d_ieng, grad, work);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    e = cudaMemcpyAsync(grad, work, sizeof(T) * na35, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_avgrad(Ctx *c, int nvinv, int ncasc, float *grad, cudaStream_t st) {
+  return launch_avgrad_t<float>(c, nvinv, ncasc, grad, (float *)c->d_avg_work, st);
+}
+
+cudaError_t launch_avgrad8(Ctx *c, int nvinv, int ncasc, double *grad, cudaStream_t st) {
+  return launch_avgrad_t<double>(c, nvinv, ncasc, grad, (double *)c->d_avg_work, st);
 }
 
 }  // namespace fem25

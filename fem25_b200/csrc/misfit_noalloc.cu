@@ -182,8 +182,8 @@ extern "C" int fem25_misfit_noalloc_dev(fem25_ctx *h, int nsrc, int nrec, const 
                              cudaMemcpyHostToDevice, st)) != cudaSuccess)
       return cuda_fail(c, e, "misfit receiver tables");
   }
-  e = launch_misfit_part(c, nsrc, nrec, d_mrdof, d_trig, azmod, d_recv, sol, obs, wghts, est, rhs,
-                         d_part, misfit, st);
+  e = launch_misfit_part(c, nsrc, nrec, d_mrdof, d_trig, freq, azmod, d_recv, sol, obs, wghts, est,
+                         rhs, d_part, misfit, st);
   if (e != cudaSuccess) return cuda_fail(c, e, "misfit");
   return FEM25_OK;
 }

@@ -85,6 +85,11 @@ def lib():
         L.fem25_ref_cadj_nu_alpha_dev.argtypes = [vp, C.c_char_p, C.c_double, C.c_double, vp,
                                                   vp, vp, i, vp, vp, vp, vp]
         L.fem25_ref_pchadj_dev.argtypes = [vp, i, i, vp, vp, vp, vp, vp]
+        L.fem25_wtgrad_dev.argtypes = [vp, i, vp, vp, vp]
+        L.fem25_avgrad_dev.argtypes = [vp, i, i, vp, vp]
+        L.fem25_avgrad8_dev.argtypes = [vp, i, i, vp, vp]
+        L.fem25_misfit_options.argtypes = [vp, i, i, i, C.c_float, C.c_float, C.c_float,
+                                           C.c_float]
         L.fem25_misfit_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp, vp]
         L.fem25_misfit_noalloc_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp,
                                                vp]
@@ -392,6 +397,18 @@ class Context:
                                                  _ptr(wave), _ptr(adjlam), 1 if accumulate else 0,
                                                  _ptr(gradl), _stream(stream)))
 
+    def wtgrad(self, wgrad, grad, stream=None):
+        """WTGRAD: grad *= wgrad (REAL*4 device arrays, in place)."""
+        self._check(lib().fem25_wtgrad_dev(self.h, grad.numel(), _ptr(wgrad), _ptr(grad),
+                                           _stream(stream)))
+
+    def avgrad(self, nvinv, ncasc, grad, stream=None):
+        """AVGRAD (REAL*4) or AVGRAD8 (REAL*8, by the tensor's dtype) on
+        grad[NNPINV * nvinv] in place."""
+        import torch
+        fn = lib().fem25_avgrad8_dev if grad.dtype == torch.float64 else lib().fem25_avgrad_dev
+        self._check(fn(self.h, nvinv, ncasc, _ptr(grad), _stream(stream)))
+
     def met225(self, cinvtype, freq, py, adjlam, nu, alpha, wave, p1buf, p2buf,
                accumulate=False, stream=None):
         """MET225_MOD Hessian-vector buffers (REAL*4 [nnpinv * nvinv] each)."""
@@ -419,6 +436,14 @@ class Context:
                                                 _ptr(fmat), _stream(stream)))
 
     # ---- misfit
+    def misfit_options(self, norm=2, irestp=3, ibphase=0, eps=0.0, thresh=0.0, dtmax=0.0,
+                       dtmax_obj=0.0):
+        """NORM, IRESTP, IBPHASE, COBJ4's EPS / THRESH and the DTMAX tests of the
+        misfit entry points (see fem25_misfit_options); no arguments restore
+        the defaults."""
+        self._check(lib().fem25_misfit_options(self.h, norm, irestp, ibphase, eps, thresh, dtmax,
+                                               dtmax_obj))
+
     def misfit(self, nsrc, mrdof, yrec, freq, py, azmod, recv, sol, obs, wghts, rhs, stream=None):
         nrec = mrdof.shape[0]
         est = np.zeros((nsrc, nrec, 3), np.complex64)

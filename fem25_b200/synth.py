@@ -324,3 +324,61 @@ def make_config(idx, nx=None, nz=None):
         for py in ky_list(f, nk, vmin):
             pairs.append((float(f), float(py)))
     return mesh, pairs, c
+
+
+def dof_coords(mesh: Mesh, g) -> tuple[np.ndarray, np.ndarray]:
+    """(x, z) of every DOF: the element's GLL node (ILXI, ILETA)
+    (node IAE = (ILETA-1) NLXI + ILXI, dshl.f:41-62) mapped through the
+    bilinear anchor map (csf2d.f:45-66).  Fixed DOFs (LM = 0) are skipped."""
+    nl = mesh.nord + 1
+    gll = {4: np.array([-1.0, -math.sqrt(3.0 / 7.0), 0.0, math.sqrt(3.0 / 7.0), 1.0])}.get(
+        mesh.nord)
+    if gll is None:
+        raise ValueError("dof_coords: GLL nodes tabulated for NORD = 4 only")
+    xi = np.tile(gll, nl)
+    eta = np.repeat(gll, nl)
+    sf = 0.25 * np.stack([(1 - xi) * (1 - eta), (1 + xi) * (1 - eta), (1 + xi) * (1 + eta),
+                          (1 - xi) * (1 + eta)], axis=1)            # [nen, 4]
+    xe = mesh.xlocs[mesh.ieng - 1] @ sf.T                          # [nelem, nen]
+    ze = mesh.zlocs[mesh.ieng - 1] @ sf.T
+    x = np.zeros(g.ndof)
+    z = np.zeros(g.ndof)
+    lm = np.asarray(g.lm)                                          # [nelem, nen, 3]
+    for c in range(3):
+        d = lm[:, :, c].reshape(-1)
+        keep = d > 0
+        x[d[keep] - 1] = xe.reshape(-1)[keep]
+        z[d[keep] - 1] = ze.reshape(-1)[keep]
+    return x, z
+
+
+def smooth_fields(mesh: Mesh, g, pairs, nsrc: int, seed: int, device="cpu", speed=2500.0,
+                  corr_len=5000.0, sigma_amp=0.1, nmodes=64):
+    """Seeded complex128 nodal fields [len(pairs), nsrc, NDOF] of the adjoint-
+    gradient workload: per (pair, source) a lognormal(0, sigma_amp) amplitude
+    times exp(i (k0 x + phi)), k0 = omega / speed along x and phi a smooth
+    random phase with a Gaussian correlation of length corr_len (a sum of
+    nmodes random Fourier modes), scaled to unit RMS.  Built with torch on
+    ``device``."""
+    import torch
+    x, z = dof_coords(mesh, g)
+    gen = torch.Generator(device="cpu")
+    gen.manual_seed(seed)
+    xt = torch.from_numpy(x).to(device)
+    zt = torch.from_numpy(z).to(device)
+    out = torch.empty((len(pairs), nsrc, g.ndof), dtype=torch.complex128, device=device)
+    for p, (f, _py) in enumerate(pairs):
+        k0 = TWOPI * f / speed
+        for s in range(nsrc):
+            kx = (torch.randn(nmodes, generator=gen, dtype=torch.float64) / corr_len).to(device)
+            kz = (torch.randn(nmodes, generator=gen, dtype=torch.float64) / corr_len).to(device)
+            b = (torch.rand(nmodes, generator=gen, dtype=torch.float64) * TWOPI).to(device)
+            phi = torch.zeros(g.ndof, dtype=torch.float64, device=device)
+            for m in range(nmodes):
+                phi += torch.cos(kx[m] * xt + kz[m] * zt + b[m])
+            phi *= math.sqrt(2.0 / nmodes)
+            amp = torch.exp(sigma_amp * torch.randn(g.ndof, generator=gen,
+                                                    dtype=torch.float64).to(device))
+            v = amp * torch.exp(1j * (k0 * xt + phi))
+            out[p, s] = v / torch.sqrt(torch.mean(torch.abs(v) ** 2))
+    return out

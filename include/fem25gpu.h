@@ -252,6 +252,21 @@ int fem25_ref_gradient_dev(fem25_ctx *ctx, const char *cinvtype, double vpvs, do
 int fem25_ref_gradient_info(fem25_ctx *ctx, int *nnpinv, long long *nz_fdist,
                             int *maskg /* [NNPG], nullable */);
 
+/* Post-processing of the reduced gradient in FUNCGRADH25
+ * (funcgradh.f90:436-443), on device arrays in place:
+ * fem25_wtgrad_dev is WTGRAD (gengmask.f90:384-416),
+ * GRAD(IA35) = GRAD(IA35) * WGRAD(IA35) for na35 REAL*4 values;
+ * fem25_avgrad_dev / fem25_avgrad8_dev are AVGRAD / AVGRAD8
+ * (gengmask.f90:1202-1332): ncasc cascades of replacing every inversion
+ * anchor's value by the mean over the inversion anchors of its connected
+ * elements (MCONN, IENG, MASKG of GENGMASK, as fem25_ref_gradient_info
+ * reports them), for nvinv (1 or 2) values per anchor, grad REAL*4 /
+ * REAL*8 [NNPINV * nvinv] with index (inpinv - 1) * nvinv + ivinv.  The
+ * first AVGRAD call builds the GENGMASK tables (outside any capture). */
+int fem25_wtgrad_dev(fem25_ctx *ctx, int na35, const float *wgrad, float *grad, void *stream);
+int fem25_avgrad_dev(fem25_ctx *ctx, int nvinv, int ncasc, float *grad, void *stream);
+int fem25_avgrad8_dev(fem25_ctx *ctx, int nvinv, int ncasc, double *grad, void *stream);
+
 /* Virtual forces of VFORCE25_2 (vforce25.f:373-607) with the alpha / beta
  * derivative matrices of DABMKISOB25 (dstiff25.f:1-203), the convention of
  * the reference's Gauss-Newton / Hessian routines (qpmfree.f90:1119): for
@@ -315,13 +330,35 @@ int fem25_ref_pchadj_dev(fem25_ctx *ctx, int nvinv, int nrhs, const float *grns,
                          const float *fmat, float *hessb, float *jacl, void *stream);
 
 /* ---- forward misfit + adjoint source ---------------------------------------
- * EXRESP25D (locrec2d.f:867-925) + rotation + CRESID/BPRESID4 L2 + COBJ4 +
- * RESID_DRHS (adjgrad.f90:448-523) for nsrc solutions at once.
+ * Options of fem25_misfit_dev and fem25_misfit_noalloc_dev, kept by the
+ * context (the reference's INV_INFO fields; defaults NORM 2, IRESTP 3,
+ * IBPHASE 0, no thresholds, no phase-jump tests):
+ *   norm     NORM of COBJ4 / BPRESID4 (objfn.f:5-175, :757-847):
+ *            1 L1, 2 L2, 3 Huber, 4 L1/L2 combination;
+ *   irestp   IRESTP of CRESID (objfn.f:953-1012): 1 phase only,
+ *            2 amplitude only, 3 phase and amplitude;
+ *   ibphase  IBPHASE of HDIFFER (adjgrad.f90:528-566): 0 none, 1 sqrt(-iw),
+ *            2 -sqrt(-iw), 3 sqrt(iw), 4 -sqrt(iw), 5 iw, 6 i;
+ *   eps, thresh  COBJ4's EPS = EPSS * CRESMN and THRESH = THRESHS * CRESMN
+ *            (NORM 3 and 4), computed by the caller over its data set;
+ *   dtmax    BPRESID4's DTMAX (L2: residuals whose phase difference is a
+ *            time shift above dtmax are zeroed; 0 = off);
+ *   dtmax_obj COBJ4's DTMAX (L2; FUNCGRADH25 passes 0, funcgradh.f90:405).
+ * As in the reference, BPRESID4 uses EPS = 0 for every norm
+ * (objfn.f:795-797): its NORM 3 residual equals the L1 one unless W DIF = 0,
+ * and its NORM 4 residual is not finite.  IRESTP 1 and the DTMAX tests take
+ * phases with the device's atan2f / cosf / sinf. */
+int fem25_misfit_options(fem25_ctx *ctx, int norm, int irestp, int ibphase, float eps,
+                         float thresh, float dtmax, float dtmax_obj);
+
+/* EXRESP25D (locrec2d.f:867-925) + rotation + CRESID + BPRESID4 + COBJ4 +
+ * RESID_DRHS with HDIFFER (adjgrad.f90:448-566) for nsrc solutions at once.
  * sol: COMPLEX*8 [nsrc][NDOF] device; mrdof: MRDOF(3,NREC) host;
  * yrec[NREC], recv COMPLEX*8 (3,NREC), obs COMPLEX*8 [nsrc](3,NREC),
  * wghts REAL*4 [nsrc](3,NREC) host; outputs: est COMPLEX*8 [nsrc](3,NREC)
  * host, rhs COMPLEX*8 [nsrc][NDOF] device (conjugated, ready for the
- * transpose solve), misfit[nsrc] host (sum |w|^2 |obs-est|^2, not halved). */
+ * transpose solve), misfit[nsrc] host (the source's sum of COBJ4's terms,
+ * for L2 sum |w|^2 |obs-est|^2, not halved). */
 int fem25_misfit_dev(fem25_ctx *ctx, int nsrc, int nrec, const int *mrdof, const double *yrec,
                      double freq, double py, double azmod, const float *recv, const float *sol,
                      const float *obs, const float *wghts, float *est, float *rhs, float *misfit,

@@ -380,6 +380,17 @@ class RefGrad:
                          _p(jacl) if jacl is not None else None)
         return jacl
 
+    def avgrad(self, nvinv, ncasc, grad):
+        """AVGRAD (float32 grad) or AVGRAD8 (float64 grad): a smoothed copy."""
+        L = lib()
+        g = np.array(grad, copy=True)
+        ieng = np.ascontiguousarray(self.mesh.ieng, np.int32)
+        fn = L.orc_avgrad8 if g.dtype == np.float64 else L.orc_avgrad
+        fn.argtypes = [C.c_int] * 4 + [C.c_void_p] * 3 + [C.c_int, C.c_void_p]
+        fn(self.mesh.nnpg, self.ncon, nvinv, ncasc, _p(self.maskg), _p(self.mconn), _p(ieng),
+           g.size, _p(g))
+        return g
+
     def adjflam(self, fmat, adjlam64, gradl=None):
         if gradl is None:
             gradl = np.zeros(self.nnpinv, np.float32)
@@ -389,15 +400,39 @@ class RefGrad:
         return gradl
 
 
-def misfit(ndof, mrdof, yrec, freq, py, azmod, recv, sol64, obs, wghts):
-    """(est[nrec,3] c64, rhs[ndof] c64, sum |w|^2 |obs-est|^2)."""
+def wtgrad(wgrad, grad):
+    """WTGRAD: grad * wgrad in REAL*4 (a new array)."""
+    g = np.array(grad, np.float32, copy=True)
+    lib().orc_wtgrad.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+    lib().orc_wtgrad(g.size, _p(np.ascontiguousarray(wgrad, np.float32)), _p(g))
+    return g
+
+
+def misfit(ndof, mrdof, yrec, freq, py, azmod, recv, sol64, obs, wghts, norm=2, irestp=3,
+           ibphase=0, eps=0.0, thresh=0.0, dtmax=0.0, dtmax_obj=0.0):
+    """(est[nrec,3] c64, rhs[ndof] c64, the source's sum of COBJ4 terms)."""
+    L = lib()
+    L.orc_misfit_opt.restype = C.c_float
+    L.orc_misfit_opt.argtypes = ([C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double,
+                                  C.c_double, C.c_double] + [C.c_void_p] * 4 +
+                                 [C.c_int] * 3 + [C.c_float] * 4 + [C.c_void_p] * 2)
     nrec = mrdof.shape[0]
     est = np.zeros((nrec, 3), np.complex64)
     rhs = np.zeros(ndof, np.complex64)
-    val = lib().orc_misfit(ndof, nrec, _p(np.ascontiguousarray(mrdof, np.int32)),
+    val = L.orc_misfit_opt(ndof, nrec, _p(np.ascontiguousarray(mrdof, np.int32)),
                            _p(np.ascontiguousarray(yrec, np.float64)), freq, py, azmod,
                            _p(np.ascontiguousarray(recv, np.complex64)),
                            _p(np.ascontiguousarray(sol64, np.complex64)),
                            _p(np.ascontiguousarray(obs, np.complex64)),
-                           _p(np.ascontiguousarray(wghts, np.float32)), _p(est), _p(rhs))
+                           _p(np.ascontiguousarray(wghts, np.float32)), norm, irestp, ibphase,
+                           eps, thresh, dtmax, dtmax_obj, _p(est), _p(rhs))
     return est, rhs, float(val)
+
+
+def hdiffer(ibphase, freq):
+    """HDIFFER(IBPHASE, FREQ) as COMPLEX*8."""
+    L = lib()
+    L.orc_hdiffer.argtypes = [C.c_int, C.c_double, C.c_void_p]
+    h = np.zeros(2, np.float32)
+    L.orc_hdiffer(ibphase, freq, _p(h))
+    return complex(h[0], h[1])

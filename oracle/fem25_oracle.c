@@ -22,6 +22,7 @@
  * assemble + direct solve, (iv) the Bielak identity.  Parity with the
  * reference's own binary output is unpinned.
  */
+#include <complex.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -2372,23 +2373,171 @@ void orc_adjflam(int nnpinv, const int *jcsc, const int *icsc, const float *fmat
     free(vwork);
 }
 
+/* WTGRAD (gengmask.f90:384-416) */
+void orc_wtgrad(int na35, const float *wgrad, float *grad)
+{
+    for (int i = 0; i < na35; i++) grad[i] = grad[i] * wgrad[i];
+}
+
+/* AVGRAD (gengmask.f90:1202-1266), REAL*4; mconn MCONN(NNPG,NCON) and ieng
+ * IENG(4,NELEM) column-major, 1-based */
+void orc_avgrad(int nnpg, int ncon, int nvinv, int ncasc, const int *maskg, const int *mconn,
+                const int *ieng, int na35, float *grad)
+{
+    if (ncasc <= 0) return;
+    float *work = (float *)malloc(sizeof(float) * (size_t)na35);
+    for (int icasc = 0; icasc < ncasc; icasc++) {
+        memcpy(work, grad, sizeof(float) * (size_t)na35);
+        for (int inpg = 1; inpg <= nnpg; inpg++) {
+            int inpinv = maskg[inpg - 1];
+            if (inpinv <= 0) continue;
+            float xavg[2] = {0.0f, 0.0f};
+            int navg[2] = {0, 0};
+            for (int icon = 1; icon <= ncon; icon++) {
+                int ielem = mconn[(inpg - 1) + (size_t)nnpg * (icon - 1)];
+                if (ielem == 0) break;
+                for (int ia = 1; ia <= 4; ia++) {
+                    int jnpg = ieng[4 * (ielem - 1) + ia - 1];
+                    if (jnpg == 0) break;
+                    int jnpinv = maskg[jnpg - 1];
+                    if (jnpinv > 0)
+                        for (int iv = 1; iv <= nvinv; iv++) {
+                            xavg[iv - 1] = xavg[iv - 1] + grad[(jnpinv - 1) * nvinv + iv - 1];
+                            navg[iv - 1] = navg[iv - 1] + 1;
+                        }
+                }
+            }
+            for (int iv = 1; iv <= nvinv; iv++)
+                if (navg[iv - 1] > 0)
+                    work[(inpinv - 1) * nvinv + iv - 1] = xavg[iv - 1] / (float)navg[iv - 1];
+        }
+        memcpy(grad, work, sizeof(float) * (size_t)na35);
+    }
+    free(work);
+}
+
+/* AVGRAD8 (gengmask.f90:1270-1332), REAL*8 */
+void orc_avgrad8(int nnpg, int ncon, int nvinv, int ncasc, const int *maskg, const int *mconn,
+                 const int *ieng, int na35, double *grad)
+{
+    if (ncasc <= 0) return;
+    double *work = (double *)malloc(sizeof(double) * (size_t)na35);
+    for (int icasc = 0; icasc < ncasc; icasc++) {
+        memcpy(work, grad, sizeof(double) * (size_t)na35);
+        for (int inpg = 1; inpg <= nnpg; inpg++) {
+            int inpinv = maskg[inpg - 1];
+            if (inpinv <= 0) continue;
+            double xavg[2] = {0.0, 0.0};
+            int navg[2] = {0, 0};
+            for (int icon = 1; icon <= ncon; icon++) {
+                int ielem = mconn[(inpg - 1) + (size_t)nnpg * (icon - 1)];
+                if (ielem == 0) break;
+                for (int ia = 1; ia <= 4; ia++) {
+                    int jnpg = ieng[4 * (ielem - 1) + ia - 1];
+                    if (jnpg == 0) break;
+                    int jnpinv = maskg[jnpg - 1];
+                    if (jnpinv > 0)
+                        for (int iv = 1; iv <= nvinv; iv++) {
+                            xavg[iv - 1] = xavg[iv - 1] + grad[(jnpinv - 1) * nvinv + iv - 1];
+                            navg[iv - 1] = navg[iv - 1] + 1;
+                        }
+                }
+            }
+            for (int iv = 1; iv <= nvinv; iv++)
+                if (navg[iv - 1] > 0)
+                    work[(inpinv - 1) * nvinv + iv - 1] = xavg[iv - 1] / (double)navg[iv - 1];
+        }
+        memcpy(grad, work, sizeof(double) * (size_t)na35);
+    }
+    free(work);
+}
+
 /* ------------------------------------------------------------------------ */
 /* forward misfit and adjoint source                                          */
 /* EXRESP25D (locrec2d.f:867-925) -> CROTATE (wrapph.f:178) -> CRESID         */
-/* (objfn.f:953-1010) -> BPRESID4 L2 (objfn.f:757-845) / COBJ4 L2             */
-/* (objfn.f:5-172) -> RESID_DRHS (adjgrad.f90:448-523) with HDIFFER=1.        */
+/* (objfn.f:953-1010) -> COBJ4 (objfn.f:5-172) and BPRESID4 (objfn.f:757-845) */
+/* -> RESID_DRHS (adjgrad.f90:448-523) with HDIFFER (adjgrad.f90:528-566).    */
 /* Single precision as in the reference.                                      */
 /*   sol: COMPLEX*8 [ndof]; mrdof: MRDOF(3,NREC); obs, wghts: (3,NREC)        */
 /*   rhs: COMPLEX*8 [ndof] adjoint RHS (conjugated, as handed to the solver)  */
-/* returns the source's contribution to sum |w|^2 |obs - est|^2 (not halved)  */
+/* returns the source's sum of COBJ4's terms C (not halved)                   */
+/* Options (the INV_INFO fields of the reference's .spec file):               */
+/*   norm   NORM: 1 L1, 3 Huber, 4 L1/L2 combination, else L2                  */
+/*   irestp IRESTP: 1 phase only, 2 amplitude only, else both                 */
+/*   ibphase IBPHASE of HDIFFER (0-6)                                         */
+/*   eps, thresh  COBJ4's EPS = EPSS*CRESMN and THRESH = THRESHS*CRESMN       */
+/*   dtmax  BPRESID4's DTMAX, dtmax_obj COBJ4's DTMAX (L2 only, 0 = off)      */
+/* |z| is restated as sqrt(re^2 + im^2) and complex products in the order     */
+/* (ac - bd, ad + bc); BPRESID4's EPS is 0 for every norm (objfn.f:795-797),  */
+/* as in the reference.                                                       */
 /* ------------------------------------------------------------------------ */
-float orc_misfit(int ndof, int nrec, const int *mrdof, const double *yrec, double freq, double py,
-                 double azmod, const float *recv, const float *sol, const float *obs,
-                 const float *wghts, float *est, float *rhs)
+static float cabsf_(cc z) { return sqrtf(z.re * z.re + z.im * z.im); }
+
+/* CRESID (objfn.f:953-1010) */
+static cc cresid(int irestp, cc obs, cc est)
+{
+    if (obs.re == 0.0f && obs.im == 0.0f) return cmk(0.0f, 0.0f);
+    if (irestp == 1 || irestp == 2) {
+        float adata, pdata, aest, pest;
+        if (irestp == 2) {
+            adata = sqrtf(obs.re * obs.re + obs.im * obs.im);
+            pdata = 0.0f;
+            aest = sqrtf(est.re * est.re + est.im * est.im);
+            pest = 0.0f;
+        } else {
+            adata = 1.0f;
+            pdata = atan2f(obs.im, obs.re);
+            aest = 1.0f;
+            pest = atan2f(est.im, est.re);
+        }
+        cc a = cmulf(cmk(adata, 0.0f), cmk(cosf(pdata), sinf(pdata)));
+        cc b = cmulf(cmk(aest, 0.0f), cmk(cosf(pest), sinf(pest)));
+        return cmk(a.re - b.re, a.im - b.im);
+    }
+    return cmk(obs.re - est.re, obs.im - est.im);
+}
+
+/* wrapped phase difference SPHASE(obs) - SPHASE(est) exceeds dtmax in time */
+static int phase_jump(cc obs, cc est, double freq, float dtmax)
+{
+    const float TWOPI_F = (float)6.283185307179586, PI_F = (float)3.1415926535897931;
+    float dphi = atan2f(obs.im, obs.re) - atan2f(est.im, est.re);
+    if (dphi < -PI_F) dphi = dphi + TWOPI_F;
+    if (dphi > +PI_F) dphi = dphi - TWOPI_F;
+    return fabs((double)dphi / ((double)TWOPI_F * freq)) > (double)dtmax;
+}
+
+/* HDIFFER (adjgrad.f90:528-566) */
+void orc_hdiffer(int ibphase, double freq, float *h)
+{
+    float omega = (float)(2.0 * 3.1415926535897932384626434 * freq);
+    float complex z = 1.0f;
+    if (ibphase == 1 || ibphase == 2) {
+        z = csqrtf(CMPLXF(0.0f, -omega));
+        if (ibphase == 2) z = -z;
+    } else if (ibphase == 3 || ibphase == 4) {
+        z = csqrtf(CMPLXF(0.0f, omega));
+        if (ibphase == 4) z = -z;
+    } else if (ibphase == 5) {
+        z = CMPLXF(0.0f, omega);
+    } else if (ibphase == 6) {
+        z = CMPLXF(0.0f, 1.0f);
+    }
+    h[0] = crealf(z);
+    h[1] = cimagf(z);
+}
+
+float orc_misfit_opt(int ndof, int nrec, const int *mrdof, const double *yrec, double freq,
+                     double py, double azmod, const float *recv, const float *sol,
+                     const float *obs, const float *wghts, int norm, int irestp, int ibphase,
+                     float eps, float thresh, float dtmax, float dtmax_obj, float *est, float *rhs)
 {
     const double TWOPI = 6.2831853071795862;
     double omega = TWOPI * freq;
     float cobj = 0.0f;
+    float hf[2];
+    orc_hdiffer(ibphase, freq, hf);
+    const cc hfact = cmk(hf[0], hf[1]);
     if (rhs) for (int i = 0; i < 2 * ndof; i++) rhs[i] = 0.0f;
     for (int ir = 0; ir < nrec; ir++) {
         float ph = (float)(omega * py * yrec[ir]);
@@ -2417,13 +2566,52 @@ float orc_misfit(int ndof, int nrec, const int *mrdof, const double *yrec, doubl
         for (int i = 0; i < 3; i++) {
             res[i] = cmk(0.0f, 0.0f);
             if (o3[i].re == 0.0f && o3[i].im == 0.0f) continue;
-            cc ob = cmulf(o3[i], cf2), es = cmulf(er[i], cf2);
-            cc dif = cmk(ob.re - es.re, ob.im - es.im);
-            float w2 = fabsf(wghts[3 * ir + i]) * fabsf(wghts[3 * ir + i]);
-            res[i] = cmk(w2 * dif.re, w2 * dif.im);
-            /* objective uses the unshifted pair: |exp(i phi)| = 1 */
-            cc dif0 = cmk(o3[i].re - er[i].re, o3[i].im - er[i].im);
-            cobj = cobj + w2 * (dif0.re * dif0.re + dif0.im * dif0.im);
+            const float w = wghts[3 * ir + i];
+            const cc S = cmk(w, 0.0f);
+            const float sabs = fabsf(w);
+            /* ---- COBJ4 term on the unshifted pair */
+            {
+                cc dif = cresid(irestp, o3[i], er[i]);
+                float c;
+                if (norm == 1) {
+                    c = cabsf_(cmulf(S, dif));
+                } else if (norm == 3) {
+                    float arg = cabsf_(cmulf(S, dif));
+                    c = arg <= eps ? arg * arg / (2.0f * eps) : arg - eps / 2.0f;
+                } else if (norm == 4) {
+                    float arg = cabsf_(dif), sd = cabsf_(cmulf(S, dif));
+                    c = arg <= thresh ? sd * sd / (2.0f * (eps * eps)) : sd / eps;
+                } else {
+                    cc cd = cmulf(cmk(dif.re, -dif.im), dif);
+                    c = sabs * sabs * cd.re;
+                    if (dtmax_obj > 0.0f && phase_jump(o3[i], er[i], freq, dtmax_obj)) {
+                        float damp = cabsf_(o3[i]) - cabsf_(er[i]);
+                        c = irestp == 1 ? sabs * sabs * 4.0f : sabs * sabs * (damp * damp);
+                    }
+                }
+                cobj = cobj + c;
+            }
+            /* ---- BPRESID4 residual on the shifted pair (EPS = 0) */
+            {
+                cc ob = cmulf(o3[i], cf2), es = cmulf(er[i], cf2);
+                cc dif = cresid(irestp, ob, es);
+                const float e0 = 0.0f;
+                if (norm == 1 || (norm == 3 && !(cabsf_(cmulf(S, dif)) <= e0))) {
+                    cc num = cmulf(S, dif);  /* CONJG(WEIGHT) = WEIGHT */
+                    float den = cabsf_(dif);
+                    res[i] = cmk(num.re / den, num.im / den);
+                } else if (norm == 3) {
+                    res[i] = cmulf(cmk(sabs * sabs / e0, 0.0f), dif);
+                } else if (norm == 4) {
+                    float eps2 = 0.0f;  /* EPSS * EPS**2 with EPS = 0 */
+                    float sd = cabsf_(cmulf(S, dif));
+                    float denon = eps2 * sqrtf(1.0f + sd * sd / eps2);
+                    res[i] = cmulf(cmk(sabs * sabs / denon, 0.0f), dif);
+                } else {
+                    res[i] = cmulf(cmk(sabs * sabs, 0.0f), dif);
+                    if (dtmax > 0.0f && phase_jump(ob, es, freq, dtmax)) res[i] = cmk(0.0f, 0.0f);
+                }
+            }
         }
         if (!rhs) continue;
         /* unrotate residual */
@@ -2435,10 +2623,21 @@ float orc_misfit(int ndof, int nrec, const int *mrdof, const double *yrec, doubl
         for (int i = 0; i < 3; i++) {
             int d = mrdof[3 * ir + i];
             if (d <= 0 || d > ndof) continue;
-            rhs[2 * (d - 1)] = rhs[2 * (d - 1)] + rr[i].re;
-            rhs[2 * (d - 1) + 1] = rhs[2 * (d - 1) + 1] + rr[i].im;
+            cc t = cmulf(hfact, rr[i]);
+            rhs[2 * (d - 1)] = rhs[2 * (d - 1)] + t.re;
+            rhs[2 * (d - 1) + 1] = rhs[2 * (d - 1) + 1] + t.im;
         }
     }
     if (rhs) for (int i = 0; i < ndof; i++) rhs[2 * i + 1] = -rhs[2 * i + 1];
     return cobj;
+}
+
+/* the defaults of the reference's .spec file: L2, phase and amplitude, no
+ * back-propagation filter, no phase-jump test */
+float orc_misfit(int ndof, int nrec, const int *mrdof, const double *yrec, double freq, double py,
+                 double azmod, const float *recv, const float *sol, const float *obs,
+                 const float *wghts, float *est, float *rhs)
+{
+    return orc_misfit_opt(ndof, nrec, mrdof, yrec, freq, py, azmod, recv, sol, obs, wghts, 2, 3, 0,
+                          0.0f, 0.0f, 0.0f, 0.0f, est, rhs);
 }
