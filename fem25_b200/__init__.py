@@ -6,11 +6,13 @@ The entry points mirror the reference Fortran routines they replace:
     graph_build(mesh)                  GEN_GRAPH25        graph25_driver.f90:2
     Context.asmble_driver(...)         ASMBLE_DRIVER      asmble.f90:1
     Context.assemble(...)              ASMBLE_DRIVER into complex128 / complex64 device CSR
-    Context.assemble_batch(...)        many (omega, py) systems, one streaming launch
+    Context.assemble_batch(...)        many (omega, py) systems per call (streaming launches of
+                                       up to min(nslots, 1024) systems each)
     Context.asmb_peff(...)             ASMB_PEFF          asmble.f90:318
     Context.gradient(...)              exact adjoint gradient in lambda, mu, rho
     Context.cfmat_adjgrad(...)         CFMAT_DIST + ADJFLAM_DIST (reference-compatible)
-    Context.misfit(...)                EXRESP25D + COBJ4 + RESID_DRHS
+    Context.misfit(...)                EXRESP25D + COBJ4 + BPRESID4 + RESID_DRHS
+    Context.postsolve(...)             ADDBLK + the misfit pass, one kernel
 
 Errors follow the reference's IERR convention: a nonzero status raises
 ``Fem25Error`` carrying the status code and the library's message.  There is

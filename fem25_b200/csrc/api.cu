@@ -97,7 +97,8 @@ void free_ctx(Ctx *c) {
                   c->d_elem_wts, c->d_fmat, c->d_cadj_col0, c->d_cadj_pair_col, c->d_cadj_pair_elem,
                   c->d_cadj_dptr, c->d_cadj_dent, c->d_cadj_w, c->d_nonpml, c->d_cdist, c->d_prim, c->d_desc,
                   c->d_tc_tab, c->d_qp, c->d_qs, c->d_cov, c->d_cov_ops, c->d_cov_opptr,
-                  c->d_cov_tx, c->d_cov_node, c->d_maskg, c->d_avg_work};
+                  c->d_cov_tx, c->d_cov_node, c->d_maskg, c->d_avg_work, c->d_post_mrdof,
+                  c->d_post_bits, c->d_hvec, c->d_hgrad};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &e : c->ev)
@@ -966,6 +967,128 @@ int fem25_avgrad8_dev(fem25_ctx *h, int nvinv, int ncasc, double *grad, void *st
   if (r) return r;
   CK(launch_avgrad8(c, nvinv, ncasc, grad, (cudaStream_t)stream), "avgrad8");
   return FEM25_OK;
+}
+
+int fem25_postsolve_dev(fem25_ctx *h, int nsrc, int nrec, const int *mrdof, const double *yrec,
+                        double freq, double py, double azmod, const float *recv, const float *ue,
+                        float *sol, const float *obs, const float *wghts, float *est, float *rhs,
+                        float *misfit, void *stream) {
+  if (!h || nsrc <= 0 || nrec <= 0 || !mrdof || !yrec || !recv || !ue || !sol || !obs || !wghts ||
+      !est || !rhs || !misfit)
+    return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  if (nrec > FEM25_POSTSOLVE_MAX_REC)
+    return fail(c, FEM25_ERR_ARG, "postsolve: nrec exceeds FEM25_POSTSOLVE_MAX_REC");
+  {
+    std::vector<int> seen;
+    for (int k = 0; k < 3 * nrec; k++) {
+      if (mrdof[k] < 0 || mrdof[k] > c->ndof)
+        return fail(c, FEM25_ERR_ARG, "postsolve: MRDOF entry out of range");
+      if (mrdof[k] > 0) seen.push_back(mrdof[k]);
+    }
+    std::sort(seen.begin(), seen.end());
+    if (std::adjacent_find(seen.begin(), seen.end()) != seen.end())
+      return fail(c, FEM25_ERR_ARG, "postsolve: two receiver components share a DOF");
+  }
+  CK(cudaSetDevice(c->device), "set device");
+  cudaStream_t st = (cudaStream_t)stream;
+  // receiver tables: rebuilt only when MRDOF differs from the last call's
+  if (c->post_mrdof.size() != 3 * (size_t)nrec ||
+      !std::equal(c->post_mrdof.begin(), c->post_mrdof.end(), mrdof)) {
+    CK(cudaStreamSynchronize(st), "synchronize");
+    if (c->d_post_mrdof) cudaFree(c->d_post_mrdof);
+    if (c->d_post_bits) cudaFree(c->d_post_bits);
+    c->d_post_mrdof = nullptr;
+    c->d_post_bits = nullptr;
+    c->post_mrdof.clear();
+    std::vector<uint32_t> bits(((size_t)c->ndof + 31) / 32, 0u);
+    for (int k = 0; k < 3 * nrec; k++)
+      if (mrdof[k] > 0) bits[(mrdof[k] - 1) >> 5] |= 1u << ((mrdof[k] - 1) & 31);
+    CK(dalloc_copy(&c->d_post_mrdof, mrdof, 3 * (size_t)nrec), "postsolve");
+    CK(dalloc_copy(&c->d_post_bits, bits.data(), bits.size()), "postsolve");
+    c->post_mrdof.assign(mrdof, mrdof + 3 * (size_t)nrec);
+  }
+  const double omega = 6.2831853071795862 * freq;
+  std::vector<float> trig(4 * (size_t)nrec);
+  for (int ir = 0; ir < nrec; ir++) {
+    float ph = (float)(omega * py * yrec[ir]);
+    float ph2 = -(float)(omega * py * yrec[ir]);
+    trig[4 * ir + 0] = cosf(ph);
+    trig[4 * ir + 1] = sinf(ph);
+    trig[4 * ir + 2] = cosf(ph2);
+    trig[4 * ir + 3] = sinf(ph2);
+  }
+  float *d_trig = nullptr, *d_recv = nullptr, *d_obs = nullptr, *d_w = nullptr, *d_est = nullptr,
+        *d_mis = nullptr;
+  const size_t nr3 = 3 * (size_t)nrec, ns3 = nr3 * nsrc;
+  auto run = [&]() -> int {
+    CK(dalloc_copy(&d_trig, trig.data(), trig.size()), "postsolve");
+    CK(dalloc_copy(&d_recv, recv, 2 * nr3), "postsolve");
+    CK(dalloc_copy(&d_obs, obs, 2 * ns3), "postsolve");
+    CK(dalloc_copy(&d_w, wghts, ns3), "postsolve");
+    CK(cudaMalloc(&d_est, sizeof(float) * 2 * ns3), "postsolve");
+    CK(cudaMalloc(&d_mis, sizeof(float) * nsrc), "postsolve");
+    CK(launch_postsolve(c, nsrc, nrec, c->d_post_mrdof, c->d_post_bits, d_trig, freq, azmod, d_recv,
+                        ue, sol, d_obs, d_w, d_est, rhs, d_mis, st),
+       "postsolve");
+    CK(cudaMemcpyAsync(est, d_est, sizeof(float) * 2 * ns3, cudaMemcpyDeviceToHost, st), "postsolve");
+    CK(cudaMemcpyAsync(misfit, d_mis, sizeof(float) * nsrc, cudaMemcpyDeviceToHost, st),
+       "postsolve");
+    CK(cudaStreamSynchronize(st), "postsolve");
+    return FEM25_OK;
+  };
+  int r = run();
+  for (void *p : {(void *)d_trig, (void *)d_recv, (void *)d_obs, (void *)d_w, (void *)d_est,
+                  (void *)d_mis})
+    if (p) cudaFree(p);
+  return r;
+}
+
+int fem25_asmb_peff(fem25_ctx *h, int ndof, const float *cdist, const float *ue, float *peff) {
+  if (!h || !ue || !peff) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  if (ndof != c->ndof) return fail(c, FEM25_ERR_ARG, "asmb_peff: NDOF differs from the context");
+  CK(cudaSetDevice(c->device), "set device");
+  const size_t n = (size_t)c->ndof;
+  if (!c->d_hvec) CK(cudaMalloc(&c->d_hvec, sizeof(float2) * 3 * n), "host-buffer scratch");
+  const float2 *a_loc = c->d_cdist;
+  if (cdist) {
+    if (!c->d_cdist) CK(cudaMalloc(&c->d_cdist, sizeof(float2) * (size_t)c->nzero), "cdist buffer");
+    CK(cudaMemcpy(c->d_cdist, cdist, sizeof(float2) * (size_t)c->nzero, cudaMemcpyHostToDevice),
+       "cdist upload");
+    a_loc = c->d_cdist;
+  } else if (!a_loc) {
+    return fail(c, FEM25_ERR_NOMESH,
+                "asmb_peff: CDIST = NULL needs a fem25_asmble_driver call on this context first");
+  }
+  CK(cudaMemcpy(c->d_hvec, ue, sizeof(float2) * n, cudaMemcpyHostToDevice), "ue upload");
+  CK(launch_peff(c, 1, (const float *)a_loc, (const float *)c->d_hvec, (float *)(c->d_hvec + n), 0),
+     "peff");
+  CK(cudaMemcpy(peff, c->d_hvec + n, sizeof(float2) * n, cudaMemcpyDeviceToHost), "peff copy");
+  return read_err_word(c, 0);
+}
+
+int fem25_cfmat_adjgrad(fem25_ctx *h, const char *cinvtype, double vpvs, double freq, double py,
+                        const float *wave, const float *adjlam, int accumulate, float *gradl) {
+  if (!h || !cinvtype || !wave || !adjlam || !gradl) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  CK(cudaSetDevice(c->device), "set device");
+  int r = ensure_refgrad(c);
+  if (r) return r;
+  const size_t n = (size_t)c->ndof;
+  if (!c->d_hvec) CK(cudaMalloc(&c->d_hvec, sizeof(float2) * 3 * n), "host-buffer scratch");
+  if (!c->d_hgrad)
+    CK(cudaMalloc(&c->d_hgrad, sizeof(float) * (size_t)std::max(c->rg.nnpinv, 1)), "gradl buffer");
+  CK(cudaMemcpy(c->d_hvec, wave, sizeof(float2) * n, cudaMemcpyHostToDevice), "wave upload");
+  CK(cudaMemcpy(c->d_hvec + n, adjlam, sizeof(float2) * n, cudaMemcpyHostToDevice), "adjlam upload");
+  CK(cudaMemcpy(c->d_hgrad, gradl, sizeof(float) * (size_t)c->rg.nnpinv, cudaMemcpyHostToDevice),
+     "gradl upload");
+  r = fem25_ref_gradient_dev(h, cinvtype, vpvs, freq, py, (const float *)c->d_hvec,
+                             (const float *)(c->d_hvec + n), accumulate, c->d_hgrad, nullptr);
+  if (r) return r;
+  CK(cudaMemcpy(gradl, c->d_hgrad, sizeof(float) * (size_t)c->rg.nnpinv, cudaMemcpyDeviceToHost),
+     "gradl copy");
+  return read_err_word(c, 0);
 }
 
 int fem25_misfit_options(fem25_ctx *h, int norm, int irestp, int ibphase, float eps, float thresh,

@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include <string>
 #include <vector>
 
@@ -167,6 +169,15 @@ struct Ctx {
   // (0: the default, about half a second) and the time-out test hook
   long long wait_limit = 0;
   int wait_inject = 0;
+  // receiver tables of the fused post-solve pass, kept while MRDOF repeats:
+  // the receiver DOFs as a bitmap (one bit per DOF) and MRDOF itself
+  std::vector<int> post_mrdof;
+  int *d_post_mrdof = nullptr;
+  uint32_t *d_post_bits = nullptr;
+  // device scratch of the host-buffer drop-ins (fem25_asmb_peff,
+  // fem25_cfmat_adjgrad): 3 COMPLEX*8 [NDOF] vectors and GRADL
+  float2 *d_hvec = nullptr;
+  float *d_hgrad = nullptr;
   // misfit options (fem25_misfit_options); the defaults of the reference
   MisfitOpts mopt{2, 3, 0, 0.0f, 0.0f, 0.0f, 0.0f, 0.0, {1.0f, 0.0f}};
   // optional CUDA-event timing of the dominant kernels
@@ -231,6 +242,11 @@ cudaError_t launch_misfit_part(Ctx *c, int nsrc, int nrec, const int *d_mrdof, c
                                double freq, double azmod, const float *d_recv, const float *sol,
                                const float *d_obs, const float *d_wghts, float *d_est, float *rhs,
                                float *d_part, float *d_misfit, cudaStream_t st);
+
+cudaError_t launch_postsolve(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const uint32_t *d_bits,
+                             const float *d_trig, double freq, double azmod, const float *d_recv,
+                             const float *ue, float *sol, const float *d_obs, const float *d_wghts,
+                             float *d_est, float *rhs, float *d_misfit, cudaStream_t st);
 
 PmlParams pml_params(const Ctx *c, char cftype, double freq);
 

@@ -128,22 +128,23 @@ __device__ __forceinline__ bool phase_jump(cfl obs, cfl est, double freq, float 
   return fabs((double)dphi / ((double)kTwoPi * freq)) > (double)dtmax;
 }
 
-__global__ void k_misfit(int nsrc, int nrec, int ndof, const int *__restrict__ mrdof,
-                         const float4 *__restrict__ trig, float4 rot, const float2 *__restrict__ recv,
-                         const float2 *__restrict__ sol, const float2 *__restrict__ obs,
-                         const float *__restrict__ wghts, MisfitOpts mo, float2 *__restrict__ est,
-                         float2 *__restrict__ rhs, float *__restrict__ part) {
-  int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= nsrc * nrec) return;
-  const int s = gid / nrec, ir = gid % nrec;
-  const float4 tg = trig[ir];
+// Receiver ir of source s: the estimates, the three COBJ4 terms (part[0..2])
+// and the right-hand-side entries at its DOFs; sv[i] is the solution at
+// MRDOF(i, ir) (unused where MRDOF is 0).
+__device__ __forceinline__ void misfit_one(int s, int ir, int nrec, int ndof,
+                                           const int *__restrict__ mrdof, const float4 tg,
+                                           float4 rot, const float2 *__restrict__ recv,
+                                           const float2 *sv, const float2 *__restrict__ obs,
+                                           const float *__restrict__ wghts, const MisfitOpts &mo,
+                                           float2 *__restrict__ est, float2 *__restrict__ rhs,
+                                           float *part) {
   const cfl cf = cfl{tg.x, tg.y}, cf2 = cfl{tg.z, tg.w};
   cfl e3[3], o3[3];
   for (int i = 0; i < 3; i++) {
     int d = mrdof[3 * ir + i];
     if (d != 0) {
-      float2 rv = recv[3 * ir + i], sv = sol[(size_t)s * ndof + d - 1];
-      e3[i] = cmulf(cmulf(cfl{rv.x, rv.y}, cfl{sv.x, sv.y}), cf);
+      float2 rv = recv[3 * ir + i];
+      e3[i] = cmulf(cmulf(cfl{rv.x, rv.y}, cfl{sv[i].x, sv[i].y}), cf);
     } else {
       e3[i] = cfl{0.0f, 0.0f};
     }
@@ -159,7 +160,7 @@ __global__ void k_misfit(int nsrc, int nrec, int ndof, const int *__restrict__ m
   cfl res[3];
   for (int i = 0; i < 3; i++) {
     res[i] = cfl{0.0f, 0.0f};
-    part[(size_t)gid * 3 + i] = 0.0f;
+    part[i] = 0.0f;
     if (o3[i].re == 0.0f && o3[i].im == 0.0f) continue;
     const float w = wghts[((size_t)s * nrec + ir) * 3 + i];
     const cfl S = cfl{w, 0.0f};
@@ -184,7 +185,7 @@ __global__ void k_misfit(int nsrc, int nrec, int ndof, const int *__restrict__ m
           c = mo.irestp == 1 ? sabs * sabs * 4.0f : sabs * sabs * (damp * damp);
         }
       }
-      part[(size_t)gid * 3 + i] = c;
+      part[i] = c;
     }
     // ---- BPRESID4 residual on the shifted pair (EPS = 0, objfn.f:795-797)
     {
@@ -222,6 +223,23 @@ __global__ void k_misfit(int nsrc, int nrec, int ndof, const int *__restrict__ m
     const cfl t = cmulf(hf, rr[i]);
     rhs[(size_t)s * ndof + d - 1] = make_float2(0.0f + t.re, -(0.0f + t.im));
   }
+}
+
+__global__ void k_misfit(int nsrc, int nrec, int ndof, const int *__restrict__ mrdof,
+                         const float4 *__restrict__ trig, float4 rot, const float2 *__restrict__ recv,
+                         const float2 *__restrict__ sol, const float2 *__restrict__ obs,
+                         const float *__restrict__ wghts, MisfitOpts mo, float2 *__restrict__ est,
+                         float2 *__restrict__ rhs, float *__restrict__ part) {
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nsrc * nrec) return;
+  const int s = gid / nrec, ir = gid % nrec;
+  float2 sv[3];
+  for (int i = 0; i < 3; i++) {
+    const int d = mrdof[3 * ir + i];
+    sv[i] = d != 0 ? sol[(size_t)s * ndof + d - 1] : make_float2(0.0f, 0.0f);
+  }
+  misfit_one(s, ir, nrec, ndof, mrdof, trig[ir], rot, recv, sv, obs, wghts, mo, est, rhs,
+             part + (size_t)gid * 3);
 }
 
 // RESID_DRHS conjugates the whole right-hand side (adjgrad.f90:519-521): the
@@ -287,6 +305,94 @@ cudaError_t launch_misfit(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const 
                                             (float2 *)rhs, d_part);
   k_misfit_sum<<<(nsrc + 127) / 128, 128, 0, st>>>(nsrc, nrec, d_part, d_misfit);
   cudaFreeAsync(d_part, st);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// the pass after the solve, fused (one launch for all sources of a group):
+// ADDBLK (bielak_utils.f:1116-1125) on the exterior DOFs, EXRESP25D
+// receiver extraction (locrec2d.f:867-925) and the misfit / adjoint source
+// of k_misfit.  Block s < nsrc first handles the receivers of source s: each
+// thread adds the background field to its receiver DOFs itself (the same
+// FP32 add as ADDBLK), computes the receiver's terms with misfit_one into
+// shared memory, and thread 0 sums them in COBJ4 order.  Then every block
+// takes a grid-strided share of the [nsrc][NDOF] entries that are not
+// receiver DOFs (rbits): ADDBLK on 'E' DOFs, RESID_DRHS's conjugated zero in
+// the right-hand side.  Receiver DOFs are distinct, so no entry has two
+// writers; the results equal fem25_addblk_dev followed by fem25_misfit_dev
+// bit for bit.
+// ---------------------------------------------------------------------------
+__global__ void k_postsolve(int nsrc, int nrec, int ndof, const char *__restrict__ cnp,
+                            const uint32_t *__restrict__ rbits, const int *__restrict__ mrdof,
+                            const float4 *__restrict__ trig, float4 rot,
+                            const float2 *__restrict__ recv, const float2 *__restrict__ ue,
+                            float2 *__restrict__ sol, const float2 *__restrict__ obs,
+                            const float *__restrict__ wghts, MisfitOpts mo,
+                            float2 *__restrict__ est, float2 *__restrict__ rhs,
+                            float *__restrict__ misfit) {
+  extern __shared__ float ps[];  // [3 nrec] COBJ4 terms of this block's source
+  const int s = blockIdx.x;
+  if (s < nsrc) {
+    for (int ir = threadIdx.x; ir < nrec; ir += blockDim.x) {
+      float2 sv[3];
+      for (int i = 0; i < 3; i++) {
+        const int d = mrdof[3 * ir + i];
+        sv[i] = make_float2(0.0f, 0.0f);
+        if (d <= 0) continue;
+        const size_t k = (size_t)s * ndof + d - 1;
+        float2 v = sol[k];
+        if (cnp[d - 1] == 'E') {
+          const float2 b = ue[k];
+          v = make_float2(v.x + b.x, v.y + b.y);
+          sol[k] = v;
+        }
+        sv[i] = v;
+      }
+      misfit_one(s, ir, nrec, ndof, mrdof, trig[ir], rot, recv, sv, obs, wghts, mo, est, rhs,
+                 ps + 3 * ir);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float acc = 0.0f;
+      for (int k = 0; k < 3 * nrec; k++) {
+        const float v = ps[k];
+        if (v != 0.0f) acc = acc + v;
+      }
+      misfit[s] = acc;
+    }
+  }
+  const long long n = (long long)nsrc * ndof;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int d = (int)(idx % ndof);
+    if ((rbits[d >> 5] >> (d & 31)) & 1u) continue;
+    if (cnp[d] == 'E') {
+      const float2 a = sol[idx], b = ue[idx];
+      sol[idx] = make_float2(a.x + b.x, a.y + b.y);
+    }
+    rhs[idx] = make_float2(0.0f, -0.0f);
+  }
+}
+
+cudaError_t launch_postsolve(Ctx *c, int nsrc, int nrec, const int *d_mrdof, const uint32_t *d_bits,
+                             const float *d_trig, double freq, double azmod, const float *d_recv,
+                             const float *ue, float *sol, const float *d_obs, const float *d_wghts,
+                             float *d_est, float *rhs, float *d_misfit, cudaStream_t st) {
+  const MisfitOpts mo = misfit_opts(c, freq);
+  float th = (float)azmod * 0.017453292519943295f;
+  float4 rot = make_float4(cosf(th), sinf(th), cosf(-th), sinf(-th));
+  const size_t smem = sizeof(float) * 3 * (size_t)nrec;
+  cudaError_t e = cudaFuncSetAttribute(k_postsolve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)std::max(smem, (size_t)1));
+  if (e != cudaSuccess) return e;
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  const long long n = (long long)nsrc * c->ndof;
+  const int grid = (int)std::max<long long>(nsrc, std::min<long long>(8LL * nsm, (n + 255) / 256));
+  k_postsolve<<<grid, 256, smem, st>>>(nsrc, nrec, c->ndof, c->d_cnp, d_bits, d_mrdof,
+                                       (const float4 *)d_trig, rot, (const float2 *)d_recv,
+                                       (const float2 *)ue, (float2 *)sol, (const float2 *)d_obs,
+                                       d_wghts, mo, (float2 *)d_est, (float2 *)rhs, d_misfit);
   return cudaGetLastError();
 }
 

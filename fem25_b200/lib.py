@@ -88,6 +88,10 @@ def lib():
         L.fem25_wtgrad_dev.argtypes = [vp, i, vp, vp, vp]
         L.fem25_avgrad_dev.argtypes = [vp, i, i, vp, vp]
         L.fem25_avgrad8_dev.argtypes = [vp, i, i, vp, vp]
+        L.fem25_postsolve_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp,
+                                          vp, vp]
+        L.fem25_asmb_peff.argtypes = [vp, i, vp, vp, vp]
+        L.fem25_cfmat_adjgrad.argtypes = [vp, C.c_char_p, d, d, d, vp, vp, i, vp]
         L.fem25_misfit_options.argtypes = [vp, i, i, i, C.c_float, C.c_float, C.c_float,
                                            C.c_float]
         L.fem25_misfit_dev.argtypes = [vp, i, i, vp, vp, d, d, d, vp, vp, vp, vp, vp, vp, vp, vp]
@@ -340,6 +344,16 @@ class Context:
         self._check(lib().fem25_peff_dev(self.h, nsrc, _ptr(a_loc), _ptr(ue), _ptr(peff),
                                          _stream(stream)))
 
+    def asmb_peff_host(self, ue, cdist=None):
+        """ASMB_PEFF with host arrays: P_eff (COMPLEX*8 [NDOF]) of the host
+        background field ue; cdist = host COMPLEX*8 CDIST, or None for the
+        last asmble_driver system still on the device."""
+        peff = np.zeros(self.ndof, np.complex64)
+        cd = None if cdist is None else _np(np.ascontiguousarray(cdist, np.complex64))
+        self._check(lib().fem25_asmb_peff(self.h, self.ndof, cd,
+                                          _np(np.ascontiguousarray(ue, np.complex64)), _np(peff)))
+        return peff
+
     def dense_factor(self, csr128, stream=None):
         """LU of the assembled complex128 CSR (device) for the small-mesh solve."""
         self._check(lib().fem25_dense_factor_dev(self.h, _ptr(csr128), _stream(stream)))
@@ -409,6 +423,13 @@ class Context:
         fn = lib().fem25_avgrad8_dev if grad.dtype == torch.float64 else lib().fem25_avgrad_dev
         self._check(fn(self.h, nvinv, ncasc, _ptr(grad), _stream(stream)))
 
+    def cfmat_adjgrad_host(self, cinvtype, vpvs, freq, py, wave, adjlam, gradl, accumulate=False):
+        """CFMAT_DIST + ADJGRAD with host arrays; gradl (float32 numpy) updated in place."""
+        self._check(lib().fem25_cfmat_adjgrad(
+            self.h, cinvtype.encode(), vpvs, freq, py,
+            _np(np.ascontiguousarray(wave, np.complex64)),
+            _np(np.ascontiguousarray(adjlam, np.complex64)), 1 if accumulate else 0, _np(gradl)))
+
     def met225(self, cinvtype, freq, py, adjlam, nu, alpha, wave, p1buf, p2buf,
                accumulate=False, stream=None):
         """MET225_MOD Hessian-vector buffers (REAL*4 [nnpinv * nvinv] each)."""
@@ -452,6 +473,23 @@ class Context:
             self.h, nsrc, nrec, _np(np.ascontiguousarray(mrdof, np.int32)),
             _np(np.ascontiguousarray(yrec, np.float64)), freq, py, azmod,
             _np(np.ascontiguousarray(recv, np.complex64)), _ptr(sol),
+            _np(np.ascontiguousarray(obs, np.complex64)),
+            _np(np.ascontiguousarray(wghts, np.float32)), _np(est), _ptr(rhs), _np(mis),
+            _stream(stream)))
+        return est, mis
+
+    def postsolve(self, nsrc, mrdof, yrec, freq, py, azmod, recv, ue, sol, obs, wghts, rhs,
+                  stream=None):
+        """ADDBLK + EXRESP25D + misfit / adjoint source in one kernel: sol
+        (device, COMPLEX*8 [nsrc][NDOF]) gets ue added on the 'E' DOFs in
+        place; returns (est, misfit) like misfit()."""
+        nrec = mrdof.shape[0]
+        est = np.zeros((nsrc, nrec, 3), np.complex64)
+        mis = np.zeros(nsrc, np.float32)
+        self._check(lib().fem25_postsolve_dev(
+            self.h, nsrc, nrec, _np(np.ascontiguousarray(mrdof, np.int32)),
+            _np(np.ascontiguousarray(yrec, np.float64)), freq, py, azmod,
+            _np(np.ascontiguousarray(recv, np.complex64)), _ptr(ue), _ptr(sol),
             _np(np.ascontiguousarray(obs, np.complex64)),
             _np(np.ascontiguousarray(wghts, np.float32)), _np(est), _ptr(rhs), _np(mis),
             _stream(stream)))

@@ -161,6 +161,15 @@ int fem25_assemble_batch_dev(fem25_ctx *ctx, int n, const char *cftype, const do
 int fem25_peff_dev(fem25_ctx *ctx, int nsrc, const float *a_loc, const float *ue, float *peff,
                    void *stream);
 
+/* Host-buffer drop-in for ASMB_PEFF(MASTER, MYCOMM, NDOF, NDOFL, NZLOC, CNP,
+ * MYDOFS, IRPTR_LOC, JCPTR_LOC, CDIST, UE, PEFF) (asmble.f90:318-319;
+ * callers bielak25.f90:536, funcgradh.f90:233): ue and peff are host
+ * COMPLEX*8 [NDOF] arrays; cdist is the host COMPLEX*8 CDIST(NZLOC) to
+ * upload, or NULL to use the CDIST of the last fem25_asmble_driver call on
+ * this context, which is still on the device (the reference calls ASMB_PEFF
+ * right after ASMBLE_DRIVER for the same system).  Synchronous. */
+int fem25_asmb_peff(fem25_ctx *ctx, int ndof, const float *cdist, const float *ue, float *peff);
+
 /* ---- direct solve on the GPU (small meshes) ---------------------------------
  * Stands in for the host MUMPS factor / solve hop (forward solve
  * bielak25.f90:443-446, 545-551; transpose adjoint solve adjgrad.f90:327-341)
@@ -251,6 +260,12 @@ int fem25_ref_gradient_dev(fem25_ctx *ctx, const char *cinvtype, double vpvs, do
                            float *gradl, void *stream);
 int fem25_ref_gradient_info(fem25_ctx *ctx, int *nnpinv, long long *nz_fdist,
                             int *maskg /* [NNPG], nullable */);
+/* Host-buffer form of the same pair for the call sites of CFMAT_DIST +
+ * ADJGRAD (funcgradh.f90:279-295): wave and adjlam host COMPLEX*8 [NDOF],
+ * gradl host REAL*4 [NNPINV] updated in place (GRADL of ADJGRAD).
+ * Synchronous. */
+int fem25_cfmat_adjgrad(fem25_ctx *ctx, const char *cinvtype, double vpvs, double freq, double py,
+                        const float *wave, const float *adjlam, int accumulate, float *gradl);
 
 /* Post-processing of the reduced gradient in FUNCGRADH25
  * (funcgradh.f90:436-443), on device arrays in place:
@@ -363,6 +378,21 @@ int fem25_misfit_dev(fem25_ctx *ctx, int nsrc, int nrec, const int *mrdof, const
                      double freq, double py, double azmod, const float *recv, const float *sol,
                      const float *obs, const float *wghts, float *est, float *rhs, float *misfit,
                      void *stream);
+
+/* The pass after the solve, fused into one kernel for nsrc sources: ADDBLK
+ * (bielak_utils.f:1116-1125; sol += ue on the 'E' DOFs, in place), then
+ * EXRESP25D and the misfit / adjoint source of fem25_misfit_dev on the
+ * updated solutions (the three steps at funcgradh.f90:248-263 and
+ * adjgrad.f90:288-323).  Arguments as fem25_misfit_dev plus ue and sol
+ * (COMPLEX*8 [nsrc][NDOF] device, sol updated); results bit-identical to
+ * fem25_addblk_dev followed by fem25_misfit_dev.  nrec <=
+ * FEM25_POSTSOLVE_MAX_REC; the receiver bitmap is rebuilt (synchronously)
+ * when MRDOF differs from the previous call's. */
+#define FEM25_POSTSOLVE_MAX_REC 16384
+int fem25_postsolve_dev(fem25_ctx *ctx, int nsrc, int nrec, const int *mrdof, const double *yrec,
+                        double freq, double py, double azmod, const float *recv, const float *ue,
+                        float *sol, const float *obs, const float *wghts, float *est, float *rhs,
+                        float *misfit, void *stream);
 
 /* The same misfit and adjoint source without any device allocation, for
  * callers that must not allocate device memory while they run: an inversion

@@ -29,6 +29,25 @@ def test_library_exports_header():
         assert isinstance(getattr(L, s), ctypes._CFuncPtr)
 
 
+def test_fortran_module_binds_header_symbols():
+    """Every BIND(C, NAME=...) of the ISO_C_BINDING module names an entry point
+    of the header that the library exports, with the header's argument count."""
+    src = open(os.path.join(ROOT, "fortran", "fem25gpu_mod.f90")).read()
+    hdr = open(os.path.join(ROOT, "include", "fem25gpu.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    binds = re.findall(r"(?:FUNCTION|SUBROUTINE)[ \t]+\w+\(([^)]*)\)[^\n]*(?:\n[^\n]*?)??"
+                       r"BIND\(C,\s*NAME='(fem25_\w+)'\)", src)
+    assert len(binds) >= 12
+    L = lib()
+    for args, name in binds:
+        assert hasattr(L, name), name
+        m = re.search(r"(?:int|void)\s+" + name + r"\s*\(([^)]*)\)", hdr)
+        assert m, name
+        nargs_c = len([a for a in m.group(1).split(",") if a.strip()])
+        nargs_f = len([a for a in args.replace("&", " ").split(",") if a.strip()])
+        assert nargs_c == nargs_f, (name, nargs_c, nargs_f)
+
+
 @pytest.mark.parametrize("idx,kw", [(0, {}), (1, dict(nx=24, nz=8)), (3, dict(nx=20, nz=10)),
                                     (4, dict(nx=30, nz=12))])
 def test_graph_matches_oracle(idx, kw):
