@@ -3,24 +3,32 @@
 Headline workload (one step): the batched assembly of 512 complex128 CSR
 systems (8 frequencies 0.2-1.6 Hz x 64 ky) of the 400x120 degree-4 mesh of a
 layered model into a ring of 32 slots (--nslots) -- the "CSR assemblies/s"
-half of the metric.  Each rank does
-the full 512-system batch (weak scaling, no data-path collective: the
-(omega, py) systems are independent).  Inputs (the per-mesh basis, 2.6 GB)
-and outputs (3.98 GB per system) are larger than L2, so no flush is needed.
+half of the metric.  With N ranks every rank assembles 512 systems of its
+own (its frequencies offset by r * 0.2 / N Hz): weak scaling, no data-path
+collective (the (omega, py) systems are independent).  Inputs (the per-mesh
+basis, 2.6 GB) and outputs (3.98 GB per system) are larger than L2, so no
+flush is needed.
 
 Also reported on the same line:
   * plain_fp64: the per-(omega, py) FP64 element + gather kernels (systems/s)
   * e2e: ASMBLE_DRIVER through the C ABI with host buffers (model upload from
     pinned memory, COMPLEX*8 CDIST read back to pinned memory) -- systems/s
+  * model_update_step: fem25_update_model + one batch that rebuilds the basis
   * gradient: exact adjoint gradient, elem.rhs/s, 400x120 layered mesh, 32
-    sources x 2 pairs: FP64; split precision in the covariance form (one-shot
-    call, and its accumulation and contraction kernels apart, with an HBM
-    roofline of the accumulation) and in the pointwise form (tensor roofline)
+    sources x 2 pairs of seeded smooth fields: FP64; split precision in the
+    covariance form (one-shot call, and its accumulation and contraction
+    kernels apart, with an HBM roofline of the accumulation) and in the
+    pointwise form (tensor roofline); per-parameter error against FP64
+  * split_precision: the 300x150 jittered workload, 128 sources, 2 of its
+    1152 pairs: elem.rhs/s of the three gradient kernels and the per-
+    parameter error of both split-precision forms against FP64
   * pipeline: the uneven-batch workload (600x200 jittered mesh with
     topography, 24 frequencies 0.1-2.4 Hz x ceil(16 f / 0.1) ky = 4800 systems,
     64 sources): batched assembly + split-precision covariance accumulation per
-    pair + one contraction, against the plain per-(omega, py) FP64 assembly +
-    FP64 gradient per pair
+    pair + one contraction, measured in one CUDA graph over all 4800 pairs,
+    against the plain per-(omega, py) FP64 assembly (reference arithmetic and
+    FMA build) + FP64 gradient per pair (sampled, scaled); sharded over ranks
+    with one NCCL all-reduce when N > 1
   * roofline of the streaming kernel and the CPU baseline (the oracle).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]

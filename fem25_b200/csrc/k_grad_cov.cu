@@ -103,6 +103,7 @@ constexpr uint32_t kTmemUnit = 128;          // columns per accumulator (96 used
 constexpr int kBlocks = 15;
 constexpr int kBlk = kNen * kNen + 1;        // 625 doubles per block, padded to 16 bytes
 constexpr int kBoxNodes[3] = {16, 4, 1};     // TMA box widths (nodes)
+constexpr int kRefNode = 12;                 // the element's centre node: the reference values
 static_assert(kProdThreads == 32 * kG, "one converter thread per (node slot, source)");
 static_assert(kRawField % 128 == 0, "raw regions keep the 128-byte alignment of TMA boxes");
 static_assert(kSmemBytes <= 227 * 1024, "shared memory");
@@ -292,29 +293,49 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
     const int pt0 = rp * 32 + lane;
     const int a = ((pt0 >> 4) & 3) * 8 + (pt0 & 7);
     const int g = ((pt0 >> 6) & (cov::kG / 2 - 1)) * 2 + ((pt0 >> 3) & 1);
-    const bool node = a < kNen;
+    const bool node = a < kNen;    // a node's deviation from the reference node
+    const bool refw = a == kNen;   // the reference values themselves (row / slot row 25)
     const uint32_t to_a = kmajor_off(a, 2 * g, cov::kALbo);                        // A row a
     const uint32_t to_b = 2 * cov::kATile + kmajor_off(a, 2 * g, cov::kBLbo);      // B row a
+    auto node_info = [&](int e, int n) -> uint32_t {
+      return e < ga.n_elem ? __ldg(plan.node + (size_t)e * kNen + n) : 0xFFFFFFFFu;
+    };
     int iei = blockIdx.x, ip = 0, ich = 0;
-    uint32_t nodeinfo = node && iei < ga.n_elem ? __ldg(plan.node + (size_t)iei * kNen + a)
-                                                : 0xFFFFFFFFu;
+    // plan entries of this thread's node and of the reference node, for the
+    // current element and (prefetched) the next one
+    uint32_t ni = node ? node_info(iei, a) : 0xFFFFFFFFu;
+    uint32_t nr = node_info(iei, cov::kRefNode);
+    uint32_t ni_next = node ? node_info(iei + gridDim.x, a) : 0xFFFFFFFFu;
+    uint32_t nr_next = node_info(iei + gridDim.x, cov::kRefNode);
+    auto raw_of = [&](uint32_t info, int rs) -> const uint8_t * {
+      const uint32_t code = (info >> 16) & 3u;
+      const uint32_t rowb = (code == 0 ? 16u : code == 1 ? 4u : 1u) * cov::kNodeBytes;
+      return raw + rs * cov::kRawStage + (info & 0xFFFFu) + g * rowb;
+    };
     for (uint32_t s = 0; s < total; s++) {
       const int rs = (int)(s % cov::kRawD), bs = (int)(s % cov::kNB);
       mbar_wait(smem_u32(&bar_rfull[rs]), (s / cov::kRawD) & 1u, drain, err, -2000006, ga.spin);
       mbar_wait(smem_u32(&bar_bempty[bs]), ((s / cov::kNB) & 1u) ^ 1u, drain, err, -2000001,
                 ga.spin);
-      if (node) {
-        const bool act = nodeinfo != 0xFFFFFFFFu && g < ga.nsrc - ich * cov::kG;
-        const uint32_t code = (nodeinfo >> 16) & 3u;
-        const uint32_t rowb = (code == 0 ? 16u : code == 1 ? 4u : 1u) * cov::kNodeBytes;
-        const uint8_t *src = raw + rs * cov::kRawStage + (act ? (nodeinfo & 0xFFFFu) + g * rowb : 0u);
+      if (node || refw) {
+        const bool gact = g < ga.nsrc - ich * cov::kG;
+        const bool vact = gact && node && ni != 0xFFFFFFFFu;
+        const bool ract = gact && nr != 0xFFFFFFFFu;
+        const uint8_t *src = vact ? raw_of(ni, rs) : raw;
+        const uint8_t *rsrc = ract ? raw_of(nr, rs) : raw;
         uint8_t *st = sm + bs * cov::kStage;
 #pragma unroll
         for (int j = 0; j < 6; j++) {  // j < 3: u component j; else lam component j - 3
           const int c = j % 3;
-          double2 v = act ? *reinterpret_cast<const double2 *>(src + (j < 3 ? 0 : cov::kRawField) +
-                                                                16 * c)
-                          : make_double2(0.0, 0.0);
+          const int fo = (j < 3 ? 0 : cov::kRawField) + 16 * c;
+          const double2 r = ract ? *reinterpret_cast<const double2 *>(rsrc + fo)
+                                 : make_double2(0.0, 0.0);
+          double2 v = r;  // reference writers store the reference values
+          if (node) {     // node threads store the deviation (a fixed node's value is 0)
+            const double2 x = vact ? *reinterpret_cast<const double2 *>(src + fo)
+                                   : make_double2(0.0, 0.0);
+            v = make_double2(x.x - r.x, x.y - r.y);
+          }
           // the sign / swap of the layout: u1 -> (Im, -Re), lam1 -> (-Im, Re)
           float x0 = (float)v.x, x1 = (float)v.y;
           if (c == 1) {
@@ -350,66 +371,101 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
         if (++ip == ga.npairs) {
           ip = 0;
           iei += gridDim.x;
-          nodeinfo = node && iei < ga.n_elem ? __ldg(plan.node + (size_t)iei * kNen + a)
-                                             : 0xFFFFFFFFu;
+          ni = ni_next;
+          nr = nr_next;
+          ni_next = node ? node_info(iei + gridDim.x, a) : 0xFFFFFFFFu;
+          nr_next = node_info(iei + gridDim.x, cov::kRefNode);
         }
       }
     }
   } else if (role == 1) {
-    // =================== loader and MMA issuer
-    if (lane == 0) {
-      const uint32_t sbase = smem_u32(sm);
-      const uint32_t rbase = smem_u32(raw);
-      const uint64_t adesc = umma_desc(sbase, cov::kALbo, 128);
-      const uint64_t bdesc = umma_desc(sbase, cov::kBLbo, 128);
-      // TMA fetch of stage s (element iei, pair ip, chunk ich: the issue
-      // pointer) into raw stage s % kRawD
-      int iei = blockIdx.x, ip = 0, ich = 0;
-      uint32_t issued = 0;
-      auto issue = [&]() {
-        const int rs = (int)(issued % cov::kRawD);
-        if (issued >= (uint32_t)cov::kRawD)
-          mbar_wait(smem_u32(&bar_rempty[rs]), ((issued / cov::kRawD) & 1u) ^ 1u, drain, err,
-                    -2000007, ga.spin);
-        if (*drain) return;  // no new loads once the CTA drains
-        const uint32_t full = smem_u32(&bar_rfull[rs]);
-        mbar_arrive_expect_tx(full, (uint32_t)__ldg(plan.tx + iei));
-        const int y = ip * ga.nsrc + ich * cov::kG;
-        const uint32_t dst0 = rbase + (uint32_t)(rs * cov::kRawStage);
-        for (int k = __ldg(plan.opptr + iei), k1 = __ldg(plan.opptr + iei + 1); k < k1; k++) {
-          const int2 op = __ldg(plan.ops + k);
-          const int code = op.y & 0xFF;
-          const uint32_t off = (uint32_t)(op.y >> 8) * 128u;
-          tma_load_2d(dst0 + off, &maps.m[0][code], op.x, y, full);
-          tma_load_2d(dst0 + cov::kRawField + off, &maps.m[1][code], op.x, y, full);
+    // =================== loader and MMA issuer (the whole warp runs the
+    // schedule; lane 0 issues the TMA loads, MMAs and commits, the other
+    // lanes hold the plan's boxes, one per lane, prefetched an element ahead)
+    const uint32_t sbase = smem_u32(sm);
+    const uint32_t rbase = smem_u32(raw);
+    const uint64_t adesc = umma_desc(sbase, cov::kALbo, 128);
+    const uint64_t bdesc = umma_desc(sbase, cov::kBLbo, 128);
+    if (lane == 0)
+      for (int f = 0; f < 2; f++)
+        for (int cd = 0; cd < 3; cd++)
+          asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.m[f][cd]))
+                       : "memory");
+    // the boxes of element e: lane k holds box k; n boxes; tx bytes per stage
+    auto load_ops = [&](int e, int2 &op, int &n, uint32_t &tx) {
+      op = make_int2(0, 0);
+      n = 0;
+      tx = 0;
+      if (e < ga.n_elem) {
+        const int k0 = __ldg(plan.opptr + e);
+        n = __ldg(plan.opptr + e + 1) - k0;
+        if (lane < n) op = __ldg(plan.ops + k0 + lane);
+        tx = (uint32_t)__ldg(plan.tx + e);
+      }
+    };
+    // TMA fetch of stage `issued` (element iei, pair ip, chunk ich) into raw
+    // stage issued % kRawD
+    int iei = blockIdx.x, ip = 0, ich = 0;
+    int2 op_cur, op_nxt;
+    int n_cur, n_nxt;
+    uint32_t tx_cur, tx_nxt;
+    load_ops(iei, op_cur, n_cur, tx_cur);
+    load_ops(iei + (int)gridDim.x, op_nxt, n_nxt, tx_nxt);
+    uint32_t issued = 0;
+    // the drain flag as lane 0 reads it, so that the warp takes one branch
+    auto draining = [&]() -> bool { return __shfl_sync(0xffffffffu, *drain, 0) != 0; };
+    auto issue = [&]() {
+      const int rs = (int)(issued % cov::kRawD);
+      if (issued >= (uint32_t)cov::kRawD)
+        mbar_wait(smem_u32(&bar_rempty[rs]), ((issued / cov::kRawD) & 1u) ^ 1u, drain, err,
+                  -2000007, ga.spin);
+      if (draining()) return;  // no new loads once the CTA drains
+      const uint32_t full = smem_u32(&bar_rfull[rs]);
+      if (lane == 0) mbar_arrive_expect_tx(full, tx_cur);
+      const int y = ip * ga.nsrc + ich * cov::kG;
+      const uint32_t dst0 = rbase + (uint32_t)(rs * cov::kRawStage);
+      for (int k = 0; k < n_cur; k++) {
+        const int x = __shfl_sync(0xffffffffu, op_cur.x, k);
+        const int yk = __shfl_sync(0xffffffffu, op_cur.y, k);
+        if (lane == 0) {
+          const int code = yk & 0xFF;
+          const uint32_t off = (uint32_t)(yk >> 8) * 128u;
+          tma_load_2d(dst0 + off, &maps.m[0][code], x, y, full);
+          tma_load_2d(dst0 + cov::kRawField + off, &maps.m[1][code], x, y, full);
         }
-        issued++;
-        if (++ich == nch) {
-          ich = 0;
-          if (++ip == ga.npairs) {
-            ip = 0;
-            iei += gridDim.x;
-          }
+      }
+      __syncwarp();
+      issued++;
+      if (++ich == nch) {
+        ich = 0;
+        if (++ip == ga.npairs) {
+          ip = 0;
+          iei += gridDim.x;
+          op_cur = op_nxt;
+          n_cur = n_nxt;
+          tx_cur = tx_nxt;
+          load_ops(iei + (int)gridDim.x, op_nxt, n_nxt, tx_nxt);
         }
-      };
-      while (issued < total && issued < (uint32_t)(cov::kRawD - 1)) issue();
-      uint32_t s = 0, unit = 0;
-      for (int ei = blockIdx.x; ei < ga.n_elem; ei += gridDim.x) {
-        for (int p = 0; p < ga.npairs; p++) {
-          for (int ch = 0; ch < nch; ch++, s++) {
-            // fetch stage s + kRawD - 1 (its raw slot was freed by stage s - 1)
-            if (issued < total && !*drain) issue();
-            // a TMEM accumulator takes kDrain stages of one pair (FP32 sums
-            // of at most 2 kDrain kG products), then the epilogue adds it in FP64
-            const bool first = ch % cov::kDrain == 0;
-            const bool last = ch % cov::kDrain == cov::kDrain - 1 || ch == nch - 1;
-            const int ts = (int)(unit % cov::kUnits), bs = (int)(s % cov::kNB);
-            if (first)
-              mbar_wait(smem_u32(&bar_tempty[ts]), ((unit / cov::kUnits) & 1u) ^ 1u, drain, err,
-                        -2000002, ga.spin);
-            mbar_wait(smem_u32(&bar_bfull[bs]), (s / cov::kNB) & 1u, drain, err, -2000003,
-                      ga.spin);
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      }
+    };
+    while (issued < total && issued < (uint32_t)(cov::kRawD - 1)) issue();
+    uint32_t s = 0, unit = 0;
+    for (int ei = blockIdx.x; ei < ga.n_elem; ei += gridDim.x) {
+      for (int p = 0; p < ga.npairs; p++) {
+        for (int ch = 0; ch < nch; ch++, s++) {
+          // fetch stage s + kRawD - 1 (its raw slot was freed by stage s - 1)
+          if (issued < total && !draining()) issue();
+          // a TMEM accumulator takes kDrain stages of one pair (FP32 sums
+          // of at most 2 kDrain kG products), then the epilogue adds it in FP64
+          const bool first = ch % cov::kDrain == 0;
+          const bool last = ch % cov::kDrain == cov::kDrain - 1 || ch == nch - 1;
+          const int ts = (int)(unit % cov::kUnits), bs = (int)(s % cov::kNB);
+          if (first)
+            mbar_wait(smem_u32(&bar_tempty[ts]), ((unit / cov::kUnits) & 1u) ^ 1u, drain, err,
+                      -2000002, ga.spin);
+          mbar_wait(smem_u32(&bar_bfull[bs]), (s / cov::kNB) & 1u, drain, err, -2000003, ga.spin);
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          if (lane == 0) {
             const uint32_t td = tmem + (uint32_t)ts * cov::kTmemUnit;
             const int nact = min(cov::kG, ga.nsrc - ch * cov::kG);
             const int nks = (nact + 3) / 4;  // K steps of 8 = 4 sources
@@ -425,13 +481,14 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
               mma_tf32(td, ahi, blo, kCovIdesc, 1u);
             }
             mma_commit(smem_u32(&bar_bempty[bs]));
-            if (last) {
-              mma_commit(smem_u32(&bar_tfull[ts]));
-              unit++;
-            }
+            if (last) mma_commit(smem_u32(&bar_tfull[ts]));
           }
+          __syncwarp();
+          if (last) unit++;
         }
       }
+    }
+    if (lane == 0) {
       // every MMA issued above has completed once this commit arrives
       mma_commit(smem_u32(&bar_drain));
       long long t0 = clock64();
@@ -464,9 +521,13 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
     bool neg;
     cov_role(rc, rk, blk, slot, wt, neg);
     const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;  // lane quarter = partition
-    double acc[kNen];
+    // lane a < 25: row a of the deviations' covariance (columns 0-24) and its
+    // product with the reference (column 25); lane 25: the reference's
+    // product with the deviations (columns 0-24) and with itself (column 25)
+    constexpr int kAcc = kNen + 1;
+    double acc[kAcc];
 #pragma unroll
-    for (int j = 0; j < kNen; j++) acc[j] = 0.0;
+    for (int j = 0; j < kAcc; j++) acc[j] = 0.0;
     uint32_t unit = 0;  // TMEM accumulations so far
     for (int ei = blockIdx.x; ei < ga.n_elem; ei += gridDim.x) {
       for (int p = 0; p < ga.npairs; p++) {
@@ -491,8 +552,16 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
           __syncwarp();
           if (lane == 0) mbar_arrive(smem_u32(&bar_tempty[ts]));
 #pragma unroll
-          for (int j = 16; j < kNen; j++) acc[j] += w * (double)__uint_as_float(r[j - 16]);
+          for (int j = 16; j < kAcc; j++) acc[j] += w * (double)__uint_as_float(r[j - 16]);
         }
+      }
+      // the block of the fields themselves: C_aj = D_aj + D_a,25 + D_25,j + D_25,25
+      // (field = reference + deviation), in FP64; lane 25's row comes by shuffle
+      const double s_ref = __shfl_sync(0xffffffffu, acc[kNen], kNen);
+#pragma unroll
+      for (int j = 0; j < kNen; j++) {
+        const double bj = __shfl_sync(0xffffffffu, acc[j], kNen);
+        acc[j] = acc[j] + acc[kNen] + (bj + s_ref);
       }
       // block row `lane` of this element, stored transposed ([j][i]) so that
       // the 25 lanes of a store are consecutive
@@ -507,7 +576,7 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
         }
       }
 #pragma unroll
-      for (int j = 0; j < kNen; j++) acc[j] = 0.0;
+      for (int j = 0; j < kAcc; j++) acc[j] = 0.0;
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

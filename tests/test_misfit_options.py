@@ -9,9 +9,10 @@ as a scaling of the right-hand side, DTMAX switching residuals off).
 GPU part: fem25_misfit_dev and fem25_misfit_noalloc_dev against the oracle
 for every option set.  Tolerances: bit-identical wherever the arithmetic is
 + - * / sqrt (IRESTP 2, 3 without DTMAX), NaN where the reference's NORM 4
-residual is NaN; 1e-6 of the largest magnitude where phases are taken
-(IRESTP 1, DTMAX) because atan2f / cosf / sinf of the device and the host
-library differ in the last bits."""
+residual is NaN; where phases are taken (IRESTP 1, DTMAX), 1e-6 of the
+larger of the largest magnitude and w_max^2 = 2.25 (the phase-only residual
+is a difference of unit phasors times w^2), because atan2f / cosf / sinf of
+the device and the host library differ in the last bits."""
 import numpy as np
 import pytest
 
@@ -171,7 +172,9 @@ def _same(a, b, tol):
     else:
         fin = np.isfinite(bv)
         assert np.array_equal(np.isfinite(av), fin)
-        scale = max(np.abs(bv[fin]).max(), 1e-30) if fin.any() else 1.0
+        # phase-only residuals are differences of unit phasors scaled by w^2
+        # (w <= 1.5): rounding is relative to that scale, not to the result
+        scale = max(np.abs(bv[fin]).max() if fin.any() else 0.0, 2.25)
         assert np.abs(av[fin] - bv[fin]).max() <= tol * scale
 
 

@@ -91,3 +91,59 @@ def test_two_rank_gradient(mode):
     else:
         assert sorted(m[1] for m in msgs) == [0, 1]
         assert all("injected host failure" in m[2] for m in msgs)
+
+
+def _gpu_worker(rank, world, port, out):
+    """Rank 0 computes its share on the GPU (sharded_gradient's accumulate /
+    finalize on a Context), rank 1 with the oracle on the CPU; gloo sums."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    import oracle
+    from fem25_b200 import synth
+    from fem25_b200.parallel import distributed_gradient, sharded_gradient
+    mesh, pairs, _ = synth.make_config(2, nx=14, nz=8)
+    g = oracle.graph_build(mesh)
+    sel = [pairs[k] for k in (3, 70, 140, 200, 333, 480)]
+    nsrc = 8
+    u = synth.smooth_fields(mesh, g, sel, nsrc, seed=5).numpy()
+    lam = synth.smooth_fields(mesh, g, sel, nsrc, seed=6).numpy()
+    try:
+        if rank == 0:
+            from fem25_b200 import Context
+            ctx = Context(mesh, g)
+            dev = torch.device("cuda:0")
+            res = sharded_gradient(ctx, sel, nsrc, lambda k: (torch.from_numpy(u[k:k + 1]).to(dev),
+                                                              torch.from_numpy(lam[k:k + 1]).to(dev)))
+            res = res.cpu().numpy()
+            ref = np.zeros((3, mesh.nnpg))
+            for k in range(len(sel)):
+                oracle.grad_exact(mesh, g, sel[k][0], sel[k][1], u[k], lam[k], out=ref)
+            err = max(float(np.linalg.norm(res[m] - ref[m]) / np.linalg.norm(ref[m])) for m in range(3))
+            out.put(("ok", err))
+            ctx.close()
+        else:
+            def partial(idx):
+                o = np.zeros((3, mesh.nnpg))
+                for k in idx:
+                    oracle.grad_exact(mesh, g, sel[k][0], sel[k][1], u[k], lam[k], out=o)
+                return torch.from_numpy(o)
+            distributed_gradient(sel, partial, mesh.nnpg)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_two_rank_gradient_gpu_and_oracle_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gpu_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+        assert p.exitcode == 0
+    tag, err = q.get(timeout=5)
+    assert tag == "ok" and err <= 1e-6, err
