@@ -25,7 +25,12 @@
 //
 // Split precision: x = hi + lo with hi = tf32(x), lo = tf32(x - hi) for both
 // operands; D = A_hi B_hi + A_hi B_lo + A_lo B_hi (the A_lo B_lo term, ~2^-22
-// relative, is dropped).  With K segments of 28 columns (25 nodes + 3 zero):
+// relative, is dropped).  Fields enter centred: node column a holds the
+// node's deviation from the element's centre node (an FP64 difference) and
+// column 25 the centre value, which the tables weight by 1 in the value rows
+// and 0 in the derivative rows, so derivatives of smooth fields are formed
+// from the small deviations without cancellation.
+// With K segments of 28 columns (25 nodes, the centre value, 2 zero):
 //     A' = [A_hi | A_lo]                (56 columns, 7 MMA K-steps)
 //     B1 = [B_hi | B_hi],  B2 = [B_lo | 4 zero columns]
 //     D  = A' B1  (A_hi B_hi + A_lo B_hi)  +  A'[:, 0:32] B2  (A_hi B_lo)
@@ -88,6 +93,8 @@ constexpr int kStgBytes = 4 * kStgRows * kStgStride * 4;
 constexpr int kSmemBytes = kABytes + kNB * kBStage + kStgBytes;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kTmemStage = 256;
+constexpr int kRefNode = 12;                     // centre node: reference of the deviations
+constexpr int kRefCol = 25;                      // K column of the reference values
 constexpr int kNodeItems = 3;                    // gather items (nodes) per producer thread
 constexpr int kItemSlots = kProdThreads * kNodeItems;  // 288 slots for 250 items
 constexpr int kTabBytes = kABytes + kItemSlots * 4;    // A tables + slot -> item map
@@ -248,6 +255,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     }
     if (blockIdx.x < ga.n_elem) {
       int dn[tc::kNodeItems];        // first DOF of the item's node (0: fixed)
+      int dref = 0;                  // first DOF of the element's centre node
       double2 vn[tc::kNodeItems][3];  // the stage being gathered
       int ei = blockIdx.x, b = 0;
 #define FEM25_TC_LOAD_DOFS(EI)                                                   \
@@ -255,6 +263,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     const int e_ = elems[EI];                                                     \
     _Pragma("unroll") for (int j = 0; j < tc::kNodeItems; j++) dn[j] =            \
         meta[j] < 0 ? 0 : __ldg(lm + (size_t)e_ * kNee + 3 * (meta[j] >> 4));     \
+    dref = __ldg(lm + (size_t)e_ * kNee + 3 * tc::kRefNode);                      \
   } while (0)
 #define FEM25_TC_LOAD_STAGE(B)                                                   \
   do {                                                                            \
@@ -279,16 +288,32 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                   ga.spin);
         uint8_t *bh = sB + bs * tc::kBStage;
         // items past the last combo of the stage store zeros into rows the
-        // epilogue ignores; empty slots store nothing
+        // epilogue ignores; empty slots store nothing.  Centring: a node
+        // column holds the node's deviation from the element's centre node
+        // (FP64 difference), and column 25 the centre node's value itself,
+        // which the A tables weight by 1 in the value rows and by 0 in the
+        // derivative rows -- so derivatives are formed from the deviations
+        // alone (smooth fields lose no digits to cancellation) and values
+        // are centre + interpolated deviation.
+        const int c0s = b * tc::kC, ncs = min(tc::kC, ga.ncombo - c0s);
 #pragma unroll
         for (int j = 0; j < tc::kNodeItems; j++) {
           if (meta[j] >= 0) {
             const int row0 = (meta[j] & 7) * 12 + ((meta[j] >> 3) & 1) * 6, a = meta[j] >> 4;
+            const bool ract = (meta[j] & 7) < ncs && dref > 0;
+            const double2 *rp = ((meta[j] & 8) ? lam : u) +
+                                (ract ? (size_t)(c0s + (meta[j] & 7)) * ga.ndof + dref - 1 : 0);
+            double2 rv[3];
+#pragma unroll
+            for (int i = 0; i < 3; i++) rv[i] = ract ? __ldg(rp + i) : make_double2(0.0, 0.0);
             // B1 columns a and 28 + a hold hi, B2 column a (virtual column
             // 56 + a of the stage) holds lo
             const uint32_t o0 = kmajor_off(row0, a, tc::kBLbo);
             const uint32_t o1 = kmajor_off(row0, a + tc::kSeg, tc::kBLbo);
             const uint32_t o2 = kmajor_off(row0, a + tc::kB1Cols, tc::kBLbo);
+            const uint32_t r0 = kmajor_off(row0, tc::kRefCol, tc::kBLbo);
+            const uint32_t r1 = kmajor_off(row0, tc::kRefCol + tc::kSeg, tc::kBLbo);
+            const uint32_t r2 = kmajor_off(row0, tc::kRefCol + tc::kB1Cols, tc::kBLbo);
 #pragma unroll
             for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -298,12 +323,21 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 // recomputed per row
                 const int row = row0 + 2 * i + ri;
                 const uint32_t dr = (uint32_t)(((row >> 3) - (row0 >> 3)) * 128 + ((row & 7) - (row0 & 7)) * 16);
-                const float x = (float)(ri == 0 ? vn[j][i].x : vn[j][i].y);
+                const double rx = ri == 0 ? rv[i].x : rv[i].y;
+                const float x = (float)((ri == 0 ? vn[j][i].x : vn[j][i].y) - rx);
                 const uint32_t hi = to_tf32(x);
                 const uint32_t lo = to_tf32(x - __uint_as_float(hi));
                 *reinterpret_cast<uint32_t *>(bh + o0 + dr) = hi;
                 *reinterpret_cast<uint32_t *>(bh + o1 + dr) = hi;
                 *reinterpret_cast<uint32_t *>(bh + o2 + dr) = lo;
+                if (a == tc::kRefNode) {
+                  const float xr = (float)rx;
+                  const uint32_t hr = to_tf32(xr);
+                  const uint32_t lr = to_tf32(xr - __uint_as_float(hr));
+                  *reinterpret_cast<uint32_t *>(bh + r0 + dr) = hr;
+                  *reinterpret_cast<uint32_t *>(bh + r1 + dr) = hr;
+                  *reinterpret_cast<uint32_t *>(bh + r2 + dr) = lr;
+                }
               }
           }
         }
@@ -565,7 +599,7 @@ std::vector<uint8_t> build_tc_tables(const Tables &t) {
   };
   for (int d = 0; d < 3; d++) {
     const int comp = d == 0 ? 2 : d - 1;  // SHL(3,...) = N, SHL(1,...) = dN/dxi, SHL(2,...) = dN/deta
-    for (int q = 0; q < kNq; q++)
+    for (int q = 0; q < kNq; q++) {
       for (int a = 0; a < kNen; a++) {
         const double x = t.shl[3 * ((size_t)a + (size_t)kNen * q) + comp];
         if (q < 128)
@@ -573,6 +607,15 @@ std::vector<uint8_t> build_tc_tables(const Tables &t) {
         else
           put(3, tail_lane(d, q - 128), a, x);
       }
+      // column 25 carries the centre node's value: weight 1 in the value
+      // rows (the shape functions sum to 1), 0 in the derivative rows
+      if (d == 0) {
+        if (q < 128)
+          put(d, q, tc::kRefCol, 1.0);
+        else
+          put(3, tail_lane(d, q - 128), tc::kRefCol, 1.0);
+      }
+    }
   }
   // producer slot -> item map.  Item (combo c, field f, node a) = c*50 + f*25
   // + a writes rows c*12 + f*6 + (0..5) at columns a, a+28, a+56; the bank of
