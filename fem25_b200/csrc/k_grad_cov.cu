@@ -568,8 +568,14 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
       if (lane < kNen) {
         double *dst = acc_out + ((size_t)ei * cov::kBlocks + blk) * cov::kBlk + lane;
         if (ga.add) {
+          // this lane is the only writer of these words in the launch (one CTA
+          // per element, one warp per block, one lane per row): a plain
+          // read-modify-write, the 25 loads in flight together
+          double old[kNen];
 #pragma unroll
-          for (int j = 0; j < kNen; j++) atomicAdd(dst + kNen * j, acc[j]);  // one adder per word
+          for (int j = 0; j < kNen; j++) old[j] = dst[kNen * j];
+#pragma unroll
+          for (int j = 0; j < kNen; j++) dst[kNen * j] = old[j] + acc[j];
         } else {
 #pragma unroll
           for (int j = 0; j < kNen; j++) dst[kNen * j] = acc[j];
