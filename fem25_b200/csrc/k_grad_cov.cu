@@ -605,16 +605,13 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
 //   F^{t1 t2}(qz, qx)   = sum_jx X_t2(qx, jx) sum_ix X_t1(qx, ix) W_{E_t1 A_t2}[ix][jx][qz]
 // = T_t1(q)^T B T_t2(q): about 0.28 M FMA per element.
 namespace covf {
-// one warp per row qz of quadrature points (13 warps), the element's 15 raw
-// blocks in shared memory, warp-private Z / W slices
-constexpr int kWarps = kNint;
-constexpr int kThreads = 32 * kWarps;        // 416
+constexpr int kThreads = 256;
 constexpr int kRawMax = 3;                   // raw blocks behind one combined block
-constexpr int kRawAll = cov::kBlocks * cov::kBlk;  // 9 390 doubles: every raw block of an element
-constexpr int kZw = 2 * kNen * kNl;          // Z_l, Z_l' slices of one qz: [2][25 i][5 jx]
-constexpr int kWw = 4 * kNl * kNl;           // W slices of one qz: [4 (E, A)][5 ix][5 jx]
-constexpr int kSmemDoubles = kRawAll + kWarps * (kZw + kWw) + 12 * kWarps;
-constexpr int kSmemBytes = kSmemDoubles * 8;  // 112 KB: two CTAs per SM
+constexpr int kRaw = kRawMax * cov::kBlk;    // doubles per raw buffer
+constexpr int kZ = kNen * kNl * kNint;       // 1625: Z[i][jx][qz]
+constexpr int kW = kNl * kNl * kNint;        // 325: W[ix][jx][qz]
+constexpr int kSmemDoubles = 2 * kRaw + 2 * kZ + 4 * kW + 2 * kNint * kNl + 4 * kNq;
+constexpr int kSmemBytes = kSmemDoubles * 8;  // 72 KB: three CTAs per SM
 }  // namespace covf
 
 // 1D Lagrange factors of the element's shape functions at the 13 points:
@@ -639,204 +636,224 @@ __device__ __forceinline__ void cov_raw_of(int b, int *ids, int &n) {
   }
 }
 
-// Warp w handles the 13 points of row qz = w (lane qx < 13: point
-// q = 13 qz + qx) for every combined block of the element, in warp-private
-// shared memory: Z_A[i][jx] = sum_je B[i][jx + 5 je] A(qz, je) (A = l, l'),
-// W_EA[ix][jx] = sum_ie E(qz, ie) Z_A[ix + 5 ie][jx], then the bilinear
-// forms at its points -- so the only CTA barriers per element are the raw
-// blocks' arrival, the anchor reduction and the reuse of the raw buffer.
-__global__ void __launch_bounds__(covf::kThreads, 2)
+// combined block b at (i, j) from its raw blocks r (r + k * kBlk: k-th raw)
+__device__ __forceinline__ double cov_bval(int b, const double *r, int i, int j) {
+  const int ij = j * kNen + i, ji = i * kNen + j;  // r[ij] = R[i][j]
+  switch (b) {
+    case 0: case 1: case 2: return 0.5 * (r[ij] + r[ji]);           // symmetric part
+    case 3: return r[ij] + r[cov::kBlk + ji];                        // R02 + R20^T
+    case 4: case 5: return r[ij] - r[cov::kBlk + ji];                // I01 - I10^T, I21 - I12^T
+    case 6: return r[ij];
+    case 7: return r[ij] + r[cov::kBlk + ij];
+    default: return r[ij] + r[cov::kBlk + ij] + r[2 * cov::kBlk + ij];
+  }
+}
+
+// sum_jx x2[jx] sum_ix x1[ix] W[ix][jx][qz]
+__device__ __forceinline__ double cov_fw(const double *W, int qz, const double *x1,
+                                         const double *x2) {
+  double f = 0.0;
+#pragma unroll
+  for (int jx = 0; jx < kNl; jx++) {
+    double h = 0.0;
+#pragma unroll
+    for (int ix = 0; ix < kNl; ix++) h = fma(x1[ix], W[(ix * kNl + jx) * kNint + qz], h);
+    f = fma(x2[jx], h, f);
+  }
+  return f;
+}
+
+__global__ void __launch_bounds__(covf::kThreads, 3)
     k_grad_cov_fin(MeshView mv, DevTables dt, int n_elem, int nnpg, const int *__restrict__ elems,
                    const double *__restrict__ accb, CovFinTabs tb, double *__restrict__ grad,
                    int *__restrict__ err) {
   extern __shared__ __align__(16) double fs[];
-  double *raw = fs;                                   // [15][kBlk]
+  double *rawb = fs;                          // [2][kRaw]
+  double *zl = rawb + 2 * covf::kRaw, *zd = zl + covf::kZ;
+  double *wb = zd + covf::kZ;                 // [4][kW]: (E, A) = (l,l) (l,l') (l',l) (l',l')
+  double *tl_s = wb + 4 * covf::kW, *td_s = tl_s + kNint * kNl;  // 1D tables
+  double *wsf_s = td_s + kNint * kNl;         // [4][169] W_q SF_a(q)
+  __shared__ double red[12][covf::kThreads / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double *zw = raw + covf::kRawAll + warp * (covf::kZw + covf::kWw);  // [2][25][5]
-  double *ww = zw + covf::kZw;                                          // [4][5][5]
-  double *red = raw + covf::kRawAll + covf::kWarps * (covf::kZw + covf::kWw);  // [12][13]
-  const int qz = warp, qx = min(lane, kNint - 1);
-  const bool ptq = lane < kNint;
-  const int q = qz * kNint + qx;
-  // l, l' at xi_qx (per lane, in registers); at eta_qz the warp reads the
-  // parameter tables directly (uniform across the warp)
-  const double *lz = tb.l[qz], *dz = tb.d[qz];
-  double xl[kNl], xd[kNl];
-#pragma unroll
-  for (int i = 0; i < kNl; i++) {
-    xl[i] = tb.l[qx][i];
-    xd[i] = tb.d[qx][i];
+  for (int k = tid; k < kNint * kNl; k += covf::kThreads) {
+    tl_s[k] = tb.l[k / kNl][k % kNl];
+    td_s[k] = tb.d[k / kNl][k % kNl];
   }
-  for (int ei = blockIdx.x; ei < n_elem; ei += gridDim.x) {
-    // ---- the element's 15 raw blocks (16-byte cp.async)
-    {
+  const bool ptq = tid < kNq;
+  const int q = ptq ? tid : 0, qx = q % kNint, qz = q / kNint;
+  const int my_elems = (n_elem - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int ntask = max(my_elems, 0) * 9;     // tasks (element, combined block)
+
+  // copies the raw blocks of task k into raw buffer k & 1 (16-byte cp.async)
+  auto fetch = [&](int k) {
+    if (k < ntask) {
+      const int ei = (int)blockIdx.x + (k / 9) * (int)gridDim.x, b = k % 9;
+      int ids[covf::kRawMax], n;
+      cov_raw_of(b, ids, n);
+      double *dst = rawb + (k & 1) * covf::kRaw;
       const double *src = accb + (size_t)ei * cov::kBlocks * cov::kBlk;
-      for (int v = tid; v < covf::kRawAll / 2; v += covf::kThreads)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(raw + 2 * v)),
-                     "l"(src + 2 * v)
+      constexpr int kV = cov::kBlk / 2;  // 16-byte vectors per block
+      for (int v = tid; v < n * kV; v += covf::kThreads) {
+        const int r = v / kV, o = 2 * (v % kV);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst + r * cov::kBlk + o)),
+                     "l"(src + (size_t)ids[r] * cov::kBlk + o)
                      : "memory");
-      asm volatile("cp.async.commit_group;" ::: "memory");
+      }
     }
-    // geometry of this lane's point while the copy is in flight
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+
+  double ax = 0.0, bx = 0.0, az = 0.0, bz = 0.0;  // inverse Jacobian rows at point q
+  double xl[kNl], xd[kNl];                         // l(qx, .), l'(qx, .)
+  double tl = 0.0, tm = 0.0, tr = 0.0;
+  fetch(0);
+  for (int k = 0; k < ntask; k++) {
+    const int ei = (int)blockIdx.x + (k / 9) * (int)gridDim.x, b = k % 9;
     const int4 ie = mv.ieng[elems[ei]];
-    double ax = 0.0, bx = 0.0, az = 0.0, bz = 0.0, wsf[4] = {0.0, 0.0, 0.0, 0.0};
-    if (ptq) {
-      QGeo g;
-      if (!quad_geo(mv, dt, ie, q, false, g)) atomicCAS(err, 0, elems[ei] + 1);
-      ax = g.dzdeta / g.rjac;
-      bx = -g.dzdxi / g.rjac;
-      az = -g.dxdeta / g.rjac;
-      bz = g.dxdxi / g.rjac;
-      const double wq = dt.wts[qx] * dt.wts[qz] * g.rjac;
-#pragma unroll
-      for (int a = 0; a < 4; a++) wsf[a] = dt.sf[4 * q + a] * wq;
-    }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
-    __syncthreads();  // raw blocks visible
-    double tl = 0.0, tm = 0.0, tr = 0.0;
-    for (int b = 0; b < 9; b++) {
-      int ids[covf::kRawMax], nr;
-      cov_raw_of(b, ids, nr);
-      // the combined block reads its raw blocks at r + k kBlk; raw blocks of
-      // one combination are adjacent only for some b, so gather their bases
-      const double *r0 = raw + ids[0] * cov::kBlk;
-      const double *r1 = raw + (nr > 1 ? ids[1] : ids[0]) * cov::kBlk;
-      const double *r2 = raw + (nr > 2 ? ids[2] : ids[0]) * cov::kBlk;
-      auto bval = [&](int i, int jj) -> double {
-        const int ij = jj * kNen + i, ji = i * kNen + jj;  // r[ij] = R[i][jj]
-        switch (b) {
-          case 0: case 1: case 2: return 0.5 * (r0[ij] + r0[ji]);
-          case 3: return r0[ij] + r1[ji];
-          case 4: case 5: return r0[ij] - r1[ji];
-          case 6: return r0[ij];
-          case 7: return r0[ij] + r1[ij];
-          default: return r0[ij] + r1[ij] + r2[ij];
+    __syncthreads();  // task k's raw blocks visible; task k - 1 done with every buffer
+    fetch(k + 1);
+    if (b == 0) {
+      if (k == 0) {
+#pragma unroll
+        for (int i = 0; i < kNl; i++) {
+          xl[i] = tl_s[qx * kNl + i];
+          xd[i] = td_s[qx * kNl + i];
         }
-      };
-      const bool two = b < 6;  // Z_l' and the W's beyond (l, l) needed
-      // ---- Z slice: (i, jx) over the lanes
-      for (int t = lane; t < kNen * kNl; t += 32) {
-        const int i = t / kNl, jx = t % kNl;
+      }
+      tl = tm = tr = 0.0;
+      if (ptq) {
+        QGeo g;
+        if (!quad_geo(mv, dt, ie, q, false, g)) atomicCAS(err, 0, elems[ei] + 1);
+        ax = g.dzdeta / g.rjac;
+        bx = -g.dzdxi / g.rjac;
+        az = -g.dxdeta / g.rjac;
+        bz = g.dxdxi / g.rjac;
+        const double wq = dt.wts[qx] * dt.wts[qz] * g.rjac;
+#pragma unroll
+        for (int a = 0; a < 4; a++) wsf_s[a * kNq + q] = dt.sf[4 * q + a] * wq;
+      }
+    }
+    const double *r = rawb + (k & 1) * covf::kRaw;
+    const bool two = b < 6;  // Z_l' and the W's beyond (l, l) needed
+    // ---- Z stage: task (i, jx)
+    if (tid < kNen * kNl) {
+      const int i = tid / kNl, jx = tid % kNl;
+      double bv[kNl];
+#pragma unroll
+      for (int je = 0; je < kNl; je++) bv[je] = cov_bval(b, r, i, jx + kNl * je);
+      double *ol = zl + (i * kNl + jx) * kNint, *od = zd + (i * kNl + jx) * kNint;
+#pragma unroll
+      for (int z = 0; z < kNint; z++) {
         double sl = 0.0, sd = 0.0;
 #pragma unroll
         for (int je = 0; je < kNl; je++) {
-          const double v = bval(i, jx + kNl * je);
-          sl = fma(v, lz[je], sl);
-          sd = fma(v, dz[je], sd);
+          sl = fma(bv[je], tb.l[z][je], sl);
+          sd = fma(bv[je], tb.d[z][je], sd);
         }
-        zw[t] = sl;
-        if (two) zw[kNen * kNl + t] = sd;
+        ol[z] = sl;
+        if (two) od[z] = sd;
       }
-      __syncwarp();
-      // ---- W slice: (ix, jx) on lanes 0-24
-      if (lane < kNl * kNl) {
-        const int ix = lane / kNl, jx = lane % kNl;
-        double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
+    }
+    __syncthreads();
+    // ---- W stage: task (ix, jx, qz)
+    for (int t = tid; t < covf::kW; t += covf::kThreads) {
+      const int z = t % kNint, ixjx = t / kNint, ix = ixjx / kNl, jx = ixjx % kNl;
+      double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
 #pragma unroll
-        for (int ie2 = 0; ie2 < kNl; ie2++) {
-          const int zi = (ix + kNl * ie2) * kNl + jx;
-          const double a = zw[zi];
-          w0 = fma(lz[ie2], a, w0);
-          if (two) {
-            const double c = zw[kNen * kNl + zi];
-            w1 = fma(lz[ie2], c, w1);
-            w2 = fma(dz[ie2], a, w2);
-            w3 = fma(dz[ie2], c, w3);
-          }
-        }
-        ww[lane] = w0;
+      for (int ie2 = 0; ie2 < kNl; ie2++) {
+        const int zi = ((ix + kNl * ie2) * kNl + jx) * kNint + z;
+        const double a = zl[zi];
+        const double el = tl_s[z * kNl + ie2], ed = td_s[z * kNl + ie2];
+        w0 = fma(el, a, w0);
         if (two) {
-          ww[25 + lane] = w1;
-          ww[50 + lane] = w2;
-          ww[75 + lane] = w3;
+          const double c = zd[zi];
+          w1 = fma(el, c, w1);
+          w2 = fma(ed, a, w2);
+          w3 = fma(ed, c, w3);
         }
       }
-      __syncwarp();
-      // ---- forms at the lane's point
-      if (ptq) {
-        // sum_jx x2[jx] sum_ix x1[ix] W[ix][jx]
-        auto fw = [&](const double *W, const double *x1, const double *x2) -> double {
-          double f = 0.0;
-#pragma unroll
-          for (int jx = 0; jx < kNl; jx++) {
-            double h = 0.0;
-#pragma unroll
-            for (int ix = 0; ix < kNl; ix++) h = fma(x1[ix], W[ix * kNl + jx], h);
-            f = fma(x2[jx], h, f);
-          }
-          return f;
-        };
-        const double *W0 = ww, *W1 = ww + 25, *W2 = ww + 50, *W3 = ww + 75;
-        if (b < 3) {
-          const double fxx = fw(W0, xd, xd), fxe = fw(W1, xd, xl);
-          const double fee = fw(W3, xl, xl);
-          const double xx = ax * ax * fxx + 2.0 * ax * bx * fxe + bx * bx * fee;
-          const double zz = az * az * fxx + 2.0 * az * bz * fxe + bz * bz * fee;
-          if (b == 0) {
-            tl += xx;
-            tm += 2.0 * xx + zz;
-          } else if (b == 1) {
-            tl += zz;
-            tm += xx + 2.0 * zz;
-          } else {
-            tm += xx + zz;
-          }
-        } else if (b == 3) {
-          const double fxx = fw(W0, xd, xd), fxe = fw(W1, xd, xl);
-          const double fex = fw(W2, xl, xd), fee = fw(W3, xl, xl);
-          tl += ax * az * fxx + ax * bz * fxe + bx * az * fex + bx * bz * fee;  // x^T S z
-          tm += az * ax * fxx + az * bx * fxe + bz * ax * fex + bz * bx * fee;  // z^T S x
-        } else if (b < 6) {
-          const double fxn = fw(W0, xd, xl), fen = fw(W2, xl, xl);
-          const double fnx = fw(W0, xl, xd), fne = fw(W1, xl, xl);
-          if (b == 4) {
-            tl += ax * fxn + bx * fen;  // x^T G1 v
-            tm -= ax * fnx + bx * fne;  // v^T G1 x
-          } else {
-            tl += az * fxn + bz * fen;  // z^T G2 v
-            tm -= az * fnx + bz * fne;  // v^T G2 z
-          }
+      wb[t] = w0;
+      if (two) {
+        wb[covf::kW + t] = w1;
+        wb[2 * covf::kW + t] = w2;
+        wb[3 * covf::kW + t] = w3;
+      }
+    }
+    __syncthreads();
+    // ---- F stage: point q
+    if (ptq) {
+      const double *W0 = wb, *W1 = wb + covf::kW, *W2 = wb + 2 * covf::kW, *W3 = wb + 3 * covf::kW;
+      if (b < 3) {
+        const double fxx = cov_fw(W0, qz, xd, xd), fxe = cov_fw(W1, qz, xd, xl);
+        const double fee = cov_fw(W3, qz, xl, xl);
+        const double xx = ax * ax * fxx + 2.0 * ax * bx * fxe + bx * bx * fee;
+        const double zz = az * az * fxx + 2.0 * az * bz * fxe + bz * bz * fee;
+        if (b == 0) {
+          tl += xx;
+          tm += 2.0 * xx + zz;
+        } else if (b == 1) {
+          tl += zz;
+          tm += xx + 2.0 * zz;
         } else {
-          const double fnn = fw(W0, xl, xl);
-          if (b == 6) {
-            tl += fnn;
-            tm += 2.0 * fnn;
-          } else if (b == 7) {
-            tm += fnn;
-          } else {
-            tr -= fnn;
-          }
+          tm += xx + zz;
+        }
+      } else if (b == 3) {
+        const double fxx = cov_fw(W0, qz, xd, xd), fxe = cov_fw(W1, qz, xd, xl);
+        const double fex = cov_fw(W2, qz, xl, xd), fee = cov_fw(W3, qz, xl, xl);
+        tl += ax * az * fxx + ax * bz * fxe + bx * az * fex + bx * bz * fee;  // x^T S z
+        tm += az * ax * fxx + az * bx * fxe + bz * ax * fex + bz * bx * fee;  // z^T S x
+      } else if (b < 6) {
+        const double fxn = cov_fw(W0, qz, xd, xl), fen = cov_fw(W2, qz, xl, xl);
+        const double fnx = cov_fw(W0, qz, xl, xd), fne = cov_fw(W1, qz, xl, xl);
+        if (b == 4) {
+          tl += ax * fxn + bx * fen;  // x^T G1 v
+          tm -= ax * fnx + bx * fne;  // v^T G1 x
+        } else {
+          tl += az * fxn + bz * fen;  // z^T G2 v
+          tm -= az * fnx + bz * fne;  // v^T G2 z
+        }
+      } else {
+        const double fnn = cov_fw(W0, qz, xl, xl);
+        if (b == 6) {
+          tl += fnn;
+          tm += 2.0 * fnn;
+        } else if (b == 7) {
+          tm += fnn;
+        } else {
+          tr -= fnn;
         }
       }
-      __syncwarp();  // Z / W slices free for the next block
     }
-    // ---- g_{m, anchor a} += sum_q W_q SF_a(q) T_m(q)
-    double v[12];
+    if (b == 8) {
+      // ---- g_{m, anchor a} += sum_q W_q SF_a(q) T_m(q)
+      double v[12];
 #pragma unroll
-    for (int a = 0; a < 4; a++) {
-      const double w = ptq ? wsf[a] : 0.0;
-      v[3 * a + 0] = w * tl;
-      v[3 * a + 1] = w * tm;
-      v[3 * a + 2] = w * tr;
-    }
+      for (int a = 0; a < 4; a++) {
+        const double w = ptq ? wsf_s[a * kNq + q] : 0.0;
+        v[3 * a + 0] = w * tl;
+        v[3 * a + 1] = w * tm;
+        v[3 * a + 2] = w * tr;
+      }
 #pragma unroll
-    for (int kk = 0; kk < 12; kk++) {
-      double x = v[kk];
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-      v[kk] = x;
+      for (int kk = 0; kk < 12; kk++) {
+        double x = v[kk];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        v[kk] = x;
+      }
+      if (lane == 0)
+        for (int kk = 0; kk < 12; kk++) red[kk][warp] = v[kk];
+      __syncthreads();
+      if (tid < 12) {
+        double x = 0.0;
+        for (int w = 0; w < covf::kThreads / 32; w++) x += red[tid][w];
+        const int a = tid / 3, m = tid % 3;
+        const int anchor = (a == 0 ? ie.x : a == 1 ? ie.y : a == 2 ? ie.z : ie.w) - 1;
+        atomicAdd(&grad[(size_t)m * nnpg + anchor], x);
+      }
     }
-    if (lane == 0)
-      for (int kk = 0; kk < 12; kk++) red[kk * covf::kWarps + warp] = v[kk];
-    __syncthreads();  // every warp's point sums; every warp done with the raw blocks
-    if (tid < 12) {
-      double x = 0.0;
-      for (int w = 0; w < covf::kWarps; w++) x += red[tid * covf::kWarps + w];
-      const int a = tid / 3, m = tid % 3;
-      const int anchor = (a == 0 ? ie.x : a == 1 ? ie.y : a == 2 ? ie.z : ie.w) - 1;
-      atomicAdd(&grad[(size_t)m * nnpg + anchor], x);
-    }
-    __syncthreads();  // red read before the next element's sums
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -1015,7 +1032,7 @@ cudaError_t launch_grad_cov_fin(Ctx *c, double *grad, cudaStream_t st) {
   if (!c->cov_pending || c->n_nonpml == 0) return cudaSuccess;
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-  const int grid = std::min(2 * nsm, c->n_nonpml);
+  const int grid = std::min(3 * nsm, c->n_nonpml);
   k_grad_cov_fin<<<grid, covf::kThreads, covf::kSmemBytes, st>>>(
       c->mv, c->dt, c->n_nonpml, c->nnpg, c->d_nonpml, c->d_cov, cov_fin_tables(c->tab), grad,
       c->d_err);

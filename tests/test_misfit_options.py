@@ -11,8 +11,10 @@ for every option set.  Tolerances: bit-identical wherever the arithmetic is
 + - * / sqrt (IRESTP 2, 3 without DTMAX), NaN where the reference's NORM 4
 residual is NaN; where phases are taken (IRESTP 1, DTMAX), 1e-6 of the
 larger of the largest magnitude and w_max^2 = 2.25 (the phase-only residual
-is a difference of unit phasors times w^2), because atan2f / cosf / sinf of
-the device and the host library differ in the last bits."""
+is a difference of unit phasors times w^2), and 1e-4 for the L1 norm with
+phase-only residuals, whose normalisation by |DIF| magnifies the rounding of
+nearly equal phases -- because atan2f / cosf / sinf of the device and the
+host library differ in the last bits."""
 import numpy as np
 import pytest
 
@@ -192,7 +194,9 @@ def test_gpu_misfit_options_match_oracle(case, kw):
         d_rhs = torch.zeros((nsrc, g.ndof), dtype=torch.complex64, device=dev)
         est, mis = ctx.misfit(nsrc, mrdof, yrec, f, py, 23.0, recv, d_sol, obs, w, d_rhs)
         rhs = d_rhs.cpu().numpy()
-        tol = 1e-6 if _phase(kw) else 0
+        # the L1 residual normalises DIF (objfn.f:803-804): with phases its
+        # rounding grows as 1 / |DIF| for nearly equal phases
+        tol = (1e-4 if kw.get("norm") == 1 and kw.get("irestp") == 1 else 1e-6) if _phase(kw) else 0
         for s in range(nsrc):
             e_o, r_o, m_o = _orc(case, s, **kw)
             _same(est[s].reshape(-1).view(np.float32), e_o.reshape(-1).view(np.float32), 0)
