@@ -34,14 +34,19 @@
 // c = 2 gives Re C20, Im C21, Re C22, and c = 1 gives Im C10, -Re C11,
 // Im C12.  M = 128, N = 96, 8 sources (K = 16) per stage, x = hi + lo with
 // D = A_hi B_hi + A_lo B_hi + A_hi B_lo.
-//   loader / MMA   one thread (warp 3): fetches each stage's nodal values
-//                with 2D TMA loads -- per element a precomputed list of
-//                boxes covering its nodes' DOF runs (16-, 4- or 1-node
-//                boxes, 8 source rows each, from u and from lam) -- into a
-//                raw ring of kRawD stages, kRawD - 1 stages ahead, and
-//                issues the MMAs into one of 4 TMEM accumulators of 128
-//                columns (each takes kDrain stages of one pair)
-//   8 converter warps  thread (node, source) reads its node's six complex
+//   loader (warp 7, one thread)  fetches each stage's nodal values with
+//                TMA loads -- per element a precomputed list of boxes, 8
+//                source rows each, from u and from lam -- into a raw ring of
+//                kRawD stages.  GENID numbers an interior element's nodes as
+//                one run of 20 consecutive nodes (its own) and five nodes
+//                four apart (the column shared with the previous element),
+//                so such an element takes two boxes per field: a 20-node 2D
+//                box and a 5-node 3D box with a 4-node stride; other
+//                elements take boxes of 16-, 4- and 1-node runs.
+//   MMA (warp 3, one thread)  issues the MMAs into one of 4 TMEM
+//                accumulators of 128 columns (each takes kDrain stages of
+//                one pair)
+//   7 converter warps  thread (node, source) reads its node's six complex
 //                values from the raw stage and writes them (FP64 -> tf32
 //                hi/lo, signs and swaps above) into one of 3 operand stages
 //   15 epilogue warps  one block each: the warp's TMEM lane quarter holds
@@ -49,6 +54,12 @@
 //                and adds them, weighted (and signed) by the pair, into 25
 //                FP64 registers; at the end of the element it writes (or
 //                adds) the block row to memory.
+// Measured per stage (clock stamps per role): a TMA box costs the issuing
+// thread about 150 cycles whatever its size, so seven boxes per field (16-,
+// 4- and five 1-node runs) took longer than the stage's conversion, and
+// issuing them from the MMA thread serialised loads and MMAs; 16-byte
+// cp.async gathers from one warp were slower still (about 100 cycles per
+// warp instruction).  Hence the loader warp and the two-box plan.
 // Hand-offs are mbarriers (the raw stages complete by TMA transaction
 // bytes); every wait is bounded and a wait that runs out sets the error
 // word and drains the schedule without waiting (the loader stops issuing
@@ -89,23 +100,27 @@ constexpr int kNB = 3;                       // operand stages in the ring
 constexpr int kNodeBytes = 48;               // one node's three complex128 DOFs
 constexpr int kRawField = kNen * kG * kNodeBytes;  // 9600 B: 25 nodes x 8 sources
 constexpr int kRawStage = 2 * kRawField;     // u then lam
-constexpr int kRawD = 5;                     // raw stages (kRawD - 1 fetched ahead)
+constexpr int kRawD = 5;                     // raw stages in the ring
 constexpr int kSmemBytes = kNB * kStage + kRawD * kRawStage;  // 180 KB
 constexpr int kThreads = 768;                // 24 warps
 constexpr int kMmaWarp = 3;
+constexpr int kLoadWarp = 7;
 constexpr int kEpiWarps = 15;
-constexpr int kProdWarps = 8;
-constexpr int kProdThreads = kProdWarps * 32;
+constexpr int kProdWarps = 7;
 constexpr int kDrain = 2;                    // stages per TMEM accumulation (FP32 sums of 2 kDrain kG)
 constexpr int kUnits = 4;                    // TMEM accumulators
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kTmemUnit = 128;          // columns per accumulator (96 used)
 constexpr int kBlocks = 15;
 constexpr int kBlk = kNen * kNen + 1;        // 625 doubles per block, padded to 16 bytes
-constexpr int kBoxNodes[3] = {16, 4, 1};     // TMA box widths (nodes)
+// gather boxes by code: 2D runs of 16, 4, 1 and 20 nodes; 3D: 5 nodes with
+// a stride of 4 nodes (kStrideNodes)
+constexpr int kNCodes = 5;
+constexpr int kBoxNodes[kNCodes] = {16, 4, 1, 20, 5};
+constexpr int kStrideNodes = 4;
 constexpr int kRefNode = 12;                 // the element's centre node: the reference values
-static_assert(kProdThreads == 32 * kG, "one converter thread per (node slot, source)");
-static_assert(kRawField % 128 == 0, "raw regions keep the 128-byte alignment of TMA boxes");
+static_assert(kProdWarps * 32 >= (kNen + 1) * kG, "one converter thread per (node row, source)");
+static_assert(kRawField % 128 == 0, "raw regions start on 128-byte boundaries");
 static_assert(kSmemBytes <= 227 * 1024, "shared memory");
 static_assert(kUnits * kTmemUnit <= kTmemCols, "tensor memory");
 }  // namespace cov
@@ -143,10 +158,11 @@ __device__ __forceinline__ void cov_role(int c, int k, int &blk, int &slot, int 
 // quarter c, and those of component 1 a second time in quarter 3, so the 15
 // epilogue warps take partitions 0 (component 0, five blocks), 1 (component
 // 1, three blocks), 2 (component 2, five blocks) and 3 (component 1, two
-// blocks); with the loader / MMA warp on partition 3 the 8 converter warps
-// spread 1 / 3 / 1 / 3 over the partitions.
-// Returns 0 (epilogue: component c, block k of it), 1 (loader / MMA) or 2
-// (converter number pidx).
+// blocks); the MMA and loader warps sit on partition 3 and the 7 converter
+// warps spread 1 / 3 / 1 / 2 over the partitions.  24 warps at 80 registers
+// fill a partition's 16 K registers (a 25th warp would not fit).
+// Returns 0 (epilogue: component c, block k of it), 1 (MMA), 2 (converter
+// number pidx) or 3 (loader).
 __device__ __forceinline__ int cov_warp_role(int w, int &c, int &k, int &pidx) {
   const int q = w & 3, r = w >> 2;  // partition, rank on it (0..5)
   c = k = pidx = 0;
@@ -169,12 +185,13 @@ __device__ __forceinline__ int cov_warp_role(int w, int &c, int &k, int &pidx) {
     return 2;
   }
   if (r == 0) return 1;  // warp 3
-  if (r < 3) {
+  if (r == 1) return 3;  // warp 7
+  if (r < 4) {
     c = 1;
-    k = 2 + r;  // blocks 3, 4 of component 1, lane quarter 3
+    k = r + 1;  // blocks 3, 4 of component 1, lane quarter 3 (warps 11, 15)
     return 0;
   }
-  pidx = 5 + (r - 3);  // warps 15, 19, 23
+  pidx = 5 + (r - 4);  // warps 19, 23
   return 2;
 }
 
@@ -187,11 +204,12 @@ struct CovArgs {
   long long spin;   // SM clocks a pipeline wait may take before it gives up
 };
 
-// The 2D TMA views of the launch's fields: [field: u, lam][box width code],
-// each a row of 2 NDOF doubles per (pair, source), box = (6 x width doubles,
-// kG rows).
+// The TMA views of the launch's fields: [field: u, lam][box code].  Codes
+// 0-3: 2D, a row of 2 NDOF doubles per (pair, source), box = (6 x width
+// doubles, kG rows); code 4: 3D, (24 doubles = 4 nodes, NDOF / 4 node
+// groups of 192 bytes, rows), box = (6, 5, kG).
 struct CovMaps {
-  CUtensorMap m[2][3];
+  CUtensorMap m[2][cov::kNCodes];
 };
 
 // Per-element gather plan (elements outside the PML, kernel order):
@@ -221,6 +239,26 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map
       " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
       : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                            int z, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(mbar)
+      : "memory");
+}
+
+// the tf32 part of x, rounded to nearest (ties away from zero) on the bit
+// pattern; finite inputs only
+__device__ __forceinline__ uint32_t tf32_hi(float x) {
+  return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
+}
+
+// bytes of one source row of a box
+__device__ __forceinline__ uint32_t cov_box_row_bytes(uint32_t code) {
+  return code == 0 ? 768u : code == 1 ? 192u : code == 2 ? 48u : code == 3 ? 960u : 240u;
 }
 
 __global__ void __launch_bounds__(cov::kThreads, 1)
@@ -280,19 +318,28 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
   const int role = cov_warp_role(warp, rc, rk, rp);
 
   if (role == 2) {
-    // =================== converters (warps 13, 15, 17, 19, 20-23)
-    // Thread pt (0..255) owns node a = 8 ah + a7 and source g = 2 gh + g1 of
-    // every stage (a7 = pt bits 0-2, g1 = bit 3, ah = bits 4-5, gh = bits
-    // 6-7; a >= 25: no node): it reads the node's u and lam values of source
-    // g from the raw stage (the node's box and place in it come from the
-    // element's plan) and writes them (FP64 -> tf32 hi/lo) into A rows
-    // 32c + a (lam; component 1 also at 96 + a) and B rows 32c + a (u) at
-    // K = 2g.  A warp's 32 threads cover the 16 (row mod 8, g mod 2)
-    // shared-memory bank classes twice, so each 8-byte tile store is two
-    // wavefronts.
-    const int pt0 = rp * 32 + lane;
-    const int a = ((pt0 >> 4) & 3) * 8 + (pt0 & 7);
-    const int g = ((pt0 >> 6) & (cov::kG / 2 - 1)) * 2 + ((pt0 >> 3) & 1);
+    // =================== converters (warps 13, 17, 19, 20-23)
+    // A thread owns node row a and source g of every stage (row 25: the
+    // reference values; a = 26: idle): it reads the node's u and lam values
+    // of source g from the raw stage (the node's box and place in it come
+    // from the element's plan) and writes them (FP64 -> tf32 hi/lo) into A
+    // rows 32c + a (lam; component 1 also at 96 + a) and B rows 32c + a (u)
+    // at K = 2g.  Converters 0-3 take rows 0-15 (lanes: a mod 8, g mod 2,
+    // a / 8), 4-5 rows 16-23 (a mod 8, g mod 4) and 6 rows 24-25 with half
+    // its lanes, so a warp's threads cover the 16 (row mod 8, g mod 2)
+    // shared-memory bank classes evenly and each 8-byte tile store is two
+    // wavefronts (four for converter 6).
+    int a, g;
+    if (rp < 4) {
+      a = ((lane >> 4) & 1) * 8 + (lane & 7);
+      g = 2 * rp + ((lane >> 3) & 1);
+    } else if (rp < 6) {
+      a = 16 + (lane & 7);
+      g = 4 * (rp - 4) + (lane >> 3);
+    } else {
+      a = lane < 16 ? 24 + (lane & 1) : kNen + 1;
+      g = (lane >> 1) & 7;
+    }
     const bool node = a < kNen;    // a node's deviation from the reference node
     const bool refw = a == kNen;   // the reference values themselves (row / slot row 25)
     const uint32_t to_a = kmajor_off(a, 2 * g, cov::kALbo);                        // A row a
@@ -308,44 +355,60 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
     uint32_t ni_next = node ? node_info(iei + gridDim.x, a) : 0xFFFFFFFFu;
     uint32_t nr_next = node_info(iei + gridDim.x, cov::kRefNode);
     auto raw_of = [&](uint32_t info, int rs) -> const uint8_t * {
-      const uint32_t code = (info >> 16) & 3u;
-      const uint32_t rowb = (code == 0 ? 16u : code == 1 ? 4u : 1u) * cov::kNodeBytes;
-      return raw + rs * cov::kRawStage + (info & 0xFFFFu) + g * rowb;
+      return raw + rs * cov::kRawStage + (info & 0xFFFFu) + g * cov_box_row_bytes(info >> 16);
     };
     for (uint32_t s = 0; s < total; s++) {
       const int rs = (int)(s % cov::kRawD), bs = (int)(s % cov::kNB);
       mbar_wait(smem_u32(&bar_rfull[rs]), (s / cov::kRawD) & 1u, drain, err, -2000006, ga.spin);
-      mbar_wait(smem_u32(&bar_bempty[bs]), ((s / cov::kNB) & 1u) ^ 1u, drain, err, -2000001,
-                ga.spin);
-      if (node || refw) {
-        const bool gact = g < ga.nsrc - ich * cov::kG;
-        const bool vact = gact && node && ni != 0xFFFFFFFFu;
-        const bool ract = gact && nr != 0xFFFFFFFFu;
+      // every raw value of the stage first (the loads in flight together),
+      // then the raw slot is released and the operand stage awaited
+      const bool gact = g < ga.nsrc - ich * cov::kG;
+      const bool vact = gact && node && ni != 0xFFFFFFFFu;
+      const bool ract = gact && (node || refw) && nr != 0xFFFFFFFFu;
+      float xv[6][2];
+      {
         const uint8_t *src = vact ? raw_of(ni, rs) : raw;
         const uint8_t *rsrc = ract ? raw_of(nr, rs) : raw;
-        uint8_t *st = sm + bs * cov::kStage;
+        double2 rv[6], vv[6];
 #pragma unroll
         for (int j = 0; j < 6; j++) {  // j < 3: u component j; else lam component j - 3
-          const int c = j % 3;
-          const int fo = (j < 3 ? 0 : cov::kRawField) + 16 * c;
-          const double2 r = ract ? *reinterpret_cast<const double2 *>(rsrc + fo)
-                                 : make_double2(0.0, 0.0);
-          double2 v = r;  // reference writers store the reference values
-          if (node) {     // node threads store the deviation (a fixed node's value is 0)
-            const double2 x = vact ? *reinterpret_cast<const double2 *>(src + fo)
-                                   : make_double2(0.0, 0.0);
-            v = make_double2(x.x - r.x, x.y - r.y);
-          }
-          // the sign / swap of the layout: u1 -> (Im, -Re), lam1 -> (-Im, Re)
+          const int fo = (j < 3 ? 0 : cov::kRawField) + 16 * (j % 3);
+          rv[j] = ract ? *reinterpret_cast<const double2 *>(rsrc + fo) : make_double2(0.0, 0.0);
+          vv[j] = vact ? *reinterpret_cast<const double2 *>(src + fo) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+          // node threads store the deviation (a fixed node's value is 0),
+          // reference writers the reference values
+          const double2 v =
+              node ? make_double2(vv[j].x - rv[j].x, vv[j].y - rv[j].y) : rv[j];
           float x0 = (float)v.x, x1 = (float)v.y;
-          if (c == 1) {
+          // the sign / swap of the layout: u1 -> (Im, -Re), lam1 -> (-Im, Re)
+          if (j % 3 == 1) {
             const float t = x0;
             x0 = j < 3 ? x1 : -x1;
             x1 = j < 3 ? -t : t;
           }
-          const uint32_t h0 = to_tf32(x0), h1 = to_tf32(x1);
-          const uint32_t l0 = to_tf32(x0 - __uint_as_float(h0));
-          const uint32_t l1 = to_tf32(x1 - __uint_as_float(h1));
+          xv[j][0] = x0;
+          xv[j][1] = x1;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&bar_rempty[rs]));
+      mbar_wait(smem_u32(&bar_bempty[bs]), ((s / cov::kNB) & 1u) ^ 1u, drain, err, -2000001,
+                ga.spin);
+      if (node || refw) {
+        uint8_t *st = sm + bs * cov::kStage;
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+          const int c = j % 3;
+          // x = hi + lo: hi = x rounded to 10 mantissa bits (integer
+          // round-half-up on the bit pattern), lo = x - hi exactly; the MMA
+          // reads lo's top 19 bits
+          const float x0 = xv[j][0], x1 = xv[j][1];
+          const uint32_t h0 = tf32_hi(x0), h1 = tf32_hi(x1);
+          const uint32_t l0 = __float_as_uint(x0 - __uint_as_float(h0));
+          const uint32_t l1 = __float_as_uint(x1 - __uint_as_float(h1));
           if (j < 3) {  // u -> B row 32c + a, hi then lo
             uint8_t *d = st + to_b + 512 * c;
             *reinterpret_cast<uint2 *>(d) = make_uint2(h0, h1);
@@ -365,7 +428,6 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
       __syncwarp();
       const bool withhold = ga.inject && blockIdx.x == 0 && rp == 0 && s == 0;
       if (lane == 0 && !withhold) mbar_arrive(smem_u32(&bar_bfull[bs]));
-      if (lane == 0) mbar_arrive(smem_u32(&bar_rempty[rs]));
       if (++ich == nch) {
         ich = 0;
         if (++ip == ga.npairs) {
@@ -378,20 +440,15 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
         }
       }
     }
-  } else if (role == 1) {
-    // =================== loader and MMA issuer (the whole warp runs the
-    // schedule; lane 0 issues the TMA loads, MMAs and commits, the other
-    // lanes hold the plan's boxes, one per lane, prefetched an element ahead)
-    const uint32_t sbase = smem_u32(sm);
+  } else if (role == 3) {
+    // =================== loader (lane 0 issues the TMA loads; lane k holds
+    // box k of the element, prefetched an element ahead)
     const uint32_t rbase = smem_u32(raw);
-    const uint64_t adesc = umma_desc(sbase, cov::kALbo, 128);
-    const uint64_t bdesc = umma_desc(sbase, cov::kBLbo, 128);
     if (lane == 0)
       for (int f = 0; f < 2; f++)
-        for (int cd = 0; cd < 3; cd++)
+        for (int cd = 0; cd < cov::kNCodes; cd++)
           asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.m[f][cd]))
                        : "memory");
-    // the boxes of element e: lane k holds box k; n boxes; tx bytes per stage
     auto load_ops = [&](int e, int2 &op, int &n, uint32_t &tx) {
       op = make_int2(0, 0);
       n = 0;
@@ -403,8 +460,6 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
         tx = (uint32_t)__ldg(plan.tx + e);
       }
     };
-    // TMA fetch of stage `issued` (element iei, pair ip, chunk ich) into raw
-    // stage issued % kRawD
     int iei = blockIdx.x, ip = 0, ich = 0;
     int2 op_cur, op_nxt;
     int n_cur, n_nxt;
@@ -412,14 +467,12 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
     load_ops(iei, op_cur, n_cur, tx_cur);
     load_ops(iei + (int)gridDim.x, op_nxt, n_nxt, tx_nxt);
     uint32_t issued = 0;
-    // the drain flag as lane 0 reads it, so that the warp takes one branch
-    auto draining = [&]() -> bool { return __shfl_sync(0xffffffffu, *drain, 0) != 0; };
-    auto issue = [&]() {
+    for (; issued < total; issued++) {
       const int rs = (int)(issued % cov::kRawD);
       if (issued >= (uint32_t)cov::kRawD)
         mbar_wait(smem_u32(&bar_rempty[rs]), ((issued / cov::kRawD) & 1u) ^ 1u, drain, err,
                   -2000007, ga.spin);
-      if (draining()) return;  // no new loads once the CTA drains
+      if (__shfl_sync(0xffffffffu, *drain, 0)) break;  // no new loads once the CTA drains
       const uint32_t full = smem_u32(&bar_rfull[rs]);
       if (lane == 0) mbar_arrive_expect_tx(full, tx_cur);
       const int y = ip * ga.nsrc + ich * cov::kG;
@@ -429,13 +482,17 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
         const int yk = __shfl_sync(0xffffffffu, op_cur.y, k);
         if (lane == 0) {
           const int code = yk & 0xFF;
-          const uint32_t off = (uint32_t)(yk >> 8) * 128u;
-          tma_load_2d(dst0 + off, &maps.m[0][code], x, y, full);
-          tma_load_2d(dst0 + cov::kRawField + off, &maps.m[1][code], x, y, full);
+          const uint32_t d = dst0 + (uint32_t)(yk >> 8) * 128u;
+          if (code == 4) {  // x = 6 n for the first node n: group n / 4, double 6 (n % 4)
+            tma_load_3d(d, &maps.m[0][4], x % 24, x / 24, y, full);
+            tma_load_3d(d + cov::kRawField, &maps.m[1][4], x % 24, x / 24, y, full);
+          } else {
+            tma_load_2d(d, &maps.m[0][code], x, y, full);
+            tma_load_2d(d + cov::kRawField, &maps.m[1][code], x, y, full);
+          }
         }
       }
       __syncwarp();
-      issued++;
       if (++ich == nch) {
         ich = 0;
         if (++ip == ga.npairs) {
@@ -447,14 +504,32 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
           load_ops(iei + (int)gridDim.x, op_nxt, n_nxt, tx_nxt);
         }
       }
-    };
-    while (issued < total && issued < (uint32_t)(cov::kRawD - 1)) issue();
+    }
+    // loads still in flight (a drained CTA may have issued stages nobody
+    // consumed): wait, bounded, for the last phase issued into each raw slot
+    if (lane == 0 && *drain) {
+      for (int r = 0; r < cov::kRawD; r++) {
+        const uint32_t n = issued > (uint32_t)r ? (issued - 1 - (uint32_t)r) / cov::kRawD + 1 : 0u;
+        if (n == 0) continue;
+        const long long t0 = clock64();
+        while (!mbar_try_wait(smem_u32(&bar_rfull[r]), (n - 1) & 1u)) {
+          if (clock64() - t0 > kTcSpinCycles) {
+            atomicCAS(err, 0, -2000008);
+            break;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else if (role == 1) {
+    // =================== MMA issuer (lane 0 issues the MMAs and commits)
+    const uint32_t sbase = smem_u32(sm);
+    const uint64_t adesc = umma_desc(sbase, cov::kALbo, 128);
+    const uint64_t bdesc = umma_desc(sbase, cov::kBLbo, 128);
     uint32_t s = 0, unit = 0;
     for (int ei = blockIdx.x; ei < ga.n_elem; ei += gridDim.x) {
       for (int p = 0; p < ga.npairs; p++) {
         for (int ch = 0; ch < nch; ch++, s++) {
-          // fetch stage s + kRawD - 1 (its raw slot was freed by stage s - 1)
-          if (issued < total && !draining()) issue();
           // a TMEM accumulator takes kDrain stages of one pair (FP32 sums
           // of at most 2 kDrain kG products), then the epilogue adds it in FP64
           const bool first = ch % cov::kDrain == 0;
@@ -491,26 +566,11 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
     if (lane == 0) {
       // every MMA issued above has completed once this commit arrives
       mma_commit(smem_u32(&bar_drain));
-      long long t0 = clock64();
+      const long long t0 = clock64();
       while (!mbar_try_wait(smem_u32(&bar_drain), 0u)) {
         if (clock64() - t0 > kTcSpinCycles) {
           atomicCAS(err, 0, -2000004);
           break;
-        }
-      }
-      // loads still in flight (a drained CTA may have issued stages nobody
-      // consumed): wait, bounded, for the last phase issued into each raw slot
-      if (*drain) {
-        for (int r = 0; r < cov::kRawD; r++) {
-          const uint32_t n = issued > (uint32_t)r ? (issued - 1 - (uint32_t)r) / cov::kRawD + 1 : 0u;
-          if (n == 0) continue;
-          t0 = clock64();
-          while (!mbar_try_wait(smem_u32(&bar_rfull[r]), (n - 1) & 1u)) {
-            if (clock64() - t0 > kTcSpinCycles) {
-              atomicCAS(err, 0, -2000008);
-              break;
-            }
-          }
         }
       }
     }
@@ -883,16 +943,21 @@ static CovFinTabs cov_fin_tables(const Tables &t) {
 }
 
 // Gather plan of the covariance accumulation for every element outside the
-// PML (kernel order): the element's nodes, sorted by first DOF, split into
-// runs of consecutive nodes (GENID numbers an element's new nodes
-// consecutively, so a structured mesh gives one 16-node run, one 4-node run
-// and five single nodes); each run is covered by TMA boxes of 16, 4 and 1
-// nodes, packed one after the other (8 source rows each) into the 9600-byte
-// raw region of a field.
+// PML (kernel order): the element's nodes, sorted by first DOF.  An element
+// whose 25 nodes are one run of 20 consecutive nodes plus five nodes
+// kStrideNodes apart (GENID's numbering of an interior element: its own 20
+// nodes, then the column shared with the element numbered before it) takes
+// two boxes, a 20-node run and a 5-node strided box; any other element has
+// its runs of consecutive nodes covered by boxes of 16, 4 and 1 nodes.  The
+// boxes are packed one after the other (8 source rows each) into the
+// 9600-byte raw region of a field.  The loader's lanes hold one box each,
+// so an element may have at most 32 boxes (set-up refuses a mesh that needs
+// more).
 static void build_cov_plan(const Ctx *c, const std::vector<int> &elems, std::vector<int2> &ops,
                            std::vector<int> &opptr, std::vector<uint32_t> &node,
                            std::vector<int> &tx) {
   const int n = (int)elems.size();
+  const long long ngroups = (long long)c->ndof / 12;  // 4-node groups of the strided view
   opptr.assign(n + 1, 0);
   node.assign((size_t)n * kNen, 0xFFFFFFFFu);
   tx.assign(n, 0);
@@ -904,20 +969,43 @@ static void build_cov_plan(const Ctx *c, const std::vector<int> &elems, std::vec
       if (lme[3 * a] > 0) ord[cnt++] = a;
     std::sort(ord, ord + cnt, [&](int x, int y) { return lme[3 * x] < lme[3 * y]; });
     uint32_t off = 0;  // bytes into the field's raw region
-    for (int i = 0; i < cnt;) {
+    auto box = [&](int code, const int *nodes) {
+      const int w = cov::kBoxNodes[code];
+      ops.push_back(make_int2(2 * (lme[3 * nodes[0]] - 1), code | (int)(off / 128u) << 8));
+      for (int j = 0; j < w; j++)
+        node[(size_t)k * kNen + nodes[j]] = (off + (uint32_t)(j * cov::kNodeBytes)) |
+                                            ((uint32_t)code << 16);
+      off += (uint32_t)(w * cov::kNodeBytes * cov::kG);
+    };
+    // the two-box form
+    bool two = false;
+    if (cnt == kNen) {
+      for (int r0 = 0; r0 + 20 <= kNen && !two; r0++) {
+        bool run = true;
+        for (int j = 1; j < 20 && run; j++) run = lme[3 * ord[r0 + j]] == lme[3 * ord[r0]] + 3 * j;
+        if (!run) continue;
+        int rest[5], nr = 0;
+        for (int j = 0; j < kNen; j++)
+          if (j < r0 || j >= r0 + 20) rest[nr++] = ord[j];
+        bool strided = true;
+        for (int j = 1; j < 5 && strided; j++)
+          strided = lme[3 * rest[j]] == lme[3 * rest[0]] + 3 * cov::kStrideNodes * j;
+        const long long g0 = (long long)(lme[3 * rest[0]] - 1) / 3 / cov::kStrideNodes;
+        if (!strided || g0 + 5 > ngroups) continue;
+        box(3, ord + r0);
+        box(4, rest);
+        two = true;
+      }
+    }
+    for (int i = 0; i < cnt && !two;) {
       int len = 1;
       while (i + len < cnt && lme[3 * ord[i + len]] == lme[3 * ord[i]] + 3 * len) len++;
       // boxes of 16, 4 and 1 nodes over the run
       int done = 0;
       while (done < len) {
         const int code = len - done >= 16 ? 0 : len - done >= 4 ? 1 : 2;
-        const int w = cov::kBoxNodes[code];
-        const int d0 = lme[3 * ord[i + done]];
-        ops.push_back(make_int2(2 * (d0 - 1), code | (int)(off / 128u) << 8));
-        for (int j = 0; j < w; j++) node[(size_t)k * kNen + ord[i + done + j]] =
-            (off + (uint32_t)(j * cov::kNodeBytes)) | ((uint32_t)code << 16);
-        off += (uint32_t)(w * cov::kNodeBytes * cov::kG);
-        done += w;
+        box(code, ord + i + done);
+        done += cov::kBoxNodes[code];
       }
       i += len;
     }
@@ -932,12 +1020,6 @@ static void build_cov_plan(const Ctx *c, const std::vector<int> &elems, std::vec
 // so it runs outside any stream capture.
 cudaError_t prepare_grad_cov(Ctx *c) {
   if (c->d_cov) return cudaSuccess;
-  for (size_t i = 0; i + 2 < c->h_lm.size(); i += 3) {
-    const int d = c->h_lm[i];
-    const bool ok = d > 0 ? (c->h_lm[i + 1] == d + 1 && c->h_lm[i + 2] == d + 2)
-                          : (c->h_lm[i + 1] == 0 && c->h_lm[i + 2] == 0);
-    if (!ok) return cudaErrorNotSupported;
-  }
   void *fn = nullptr;
   cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
@@ -945,6 +1027,12 @@ cudaError_t prepare_grad_cov(Ctx *c) {
       q != cudaDriverEntryPointSuccess || !fn)
     return cudaErrorNotSupported;
   c->tmap_encode = fn;
+  for (size_t i = 0; i + 2 < c->h_lm.size(); i += 3) {
+    const int d = c->h_lm[i];
+    const bool ok = d > 0 ? (c->h_lm[i + 1] == d + 1 && c->h_lm[i + 2] == d + 2)
+                          : (c->h_lm[i + 1] == 0 && c->h_lm[i + 2] == 0);
+    if (!ok) return cudaErrorNotSupported;
+  }
   std::vector<int> elems;
   for (int e = 0; e < c->nelem; e++)
     if (c->h_cdomain[e] != 'A') elems.push_back(e);
@@ -952,6 +1040,8 @@ cudaError_t prepare_grad_cov(Ctx *c) {
   std::vector<int> opptr, tx;
   std::vector<uint32_t> node;
   build_cov_plan(c, elems, ops, opptr, node, tx);
+  for (size_t k = 0; k + 1 < opptr.size(); k++)
+    if (opptr[k + 1] - opptr[k] > 32) return cudaErrorNotSupported;
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(k_grad_cov, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 cov::kSmemBytes + 128)))
@@ -977,24 +1067,36 @@ cudaError_t prepare_grad_cov(Ctx *c) {
   return cudaSuccess;
 }
 
-// The 2D TMA views of one launch's fields: rows of 2 NDOF doubles, one per
-// (pair, source), for each box width.  cudaErrorInvalidValue for a field
-// pointer off a 16-byte boundary.
+// The TMA views of one launch's fields (CovMaps).  cudaErrorInvalidValue
+// for a field pointer off a 16-byte boundary.
 static cudaError_t cov_maps(const Ctx *c, const double *u, const double *lam, int rows,
                             CovMaps &maps) {
   auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(c->tmap_encode);
   const double *base[2] = {u, lam};
+  const cuuint32_t estr[3] = {1, 1, 1};
   for (int f = 0; f < 2; f++) {
     if (reinterpret_cast<uintptr_t>(base[f]) % 16) return cudaErrorInvalidValue;
-    for (int code = 0; code < 3; code++) {
-      const cuuint64_t dim[2] = {(cuuint64_t)2 * c->ndof, (cuuint64_t)rows};
-      const cuuint64_t stride[1] = {(cuuint64_t)c->ndof * 16};
-      const cuuint32_t box[2] = {(cuuint32_t)(6 * cov::kBoxNodes[code]), (cuuint32_t)cov::kG};
-      const cuuint32_t estr[2] = {1, 1};
-      CUresult r = encode(&maps.m[f][code], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
-                          const_cast<double *>(base[f]), dim, stride, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    for (int code = 0; code < cov::kNCodes; code++) {
+      CUresult r;
+      if (code < 4) {
+        const cuuint64_t dim[2] = {(cuuint64_t)2 * c->ndof, (cuuint64_t)rows};
+        const cuuint64_t stride[1] = {(cuuint64_t)c->ndof * 16};
+        const cuuint32_t boxd[2] = {(cuuint32_t)(6 * cov::kBoxNodes[code]), (cuuint32_t)cov::kG};
+        r = encode(&maps.m[f][code], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
+                   const_cast<double *>(base[f]), dim, stride, boxd, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      } else {
+        const cuuint64_t dim[3] = {(cuuint64_t)6 * cov::kStrideNodes, (cuuint64_t)c->ndof / 12,
+                                   (cuuint64_t)rows};
+        const cuuint64_t stride[2] = {(cuuint64_t)cov::kStrideNodes * cov::kNodeBytes,
+                                      (cuuint64_t)c->ndof * 16};
+        const cuuint32_t boxd[3] = {6, 5, (cuuint32_t)cov::kG};
+        r = encode(&maps.m[f][code], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                   const_cast<double *>(base[f]), dim, stride, boxd, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      }
       if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
     }
   }

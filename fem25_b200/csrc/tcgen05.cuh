@@ -77,6 +77,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t phase) {
 // CTA in drain mode.
 __device__ __forceinline__ void mbar_wait(uint32_t mbar, uint32_t phase, volatile int *drain,
                                           int *err, int code, long long limit) {
+  if (mbar_try_wait(mbar, phase)) return;  // the common case: already complete
   if (*drain) return;
   const long long t0 = clock64();
   while (!mbar_try_wait(mbar, phase)) {
