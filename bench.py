@@ -19,6 +19,9 @@ Also reported on the same line:
     covariance form (one-shot call, and its accumulation and contraction
     kernels apart, with an HBM roofline of the accumulation) and in the
     pointwise form (tensor roofline); per-parameter error against FP64
+  * sparse_solve: the GPU multifrontal direct solve of one 400x120 system
+    (the MUMPS hop of the reference): factorisation time and flop rate,
+    solves with A and A^H for 1 and 32 right-hand sides, residual
   * split_precision: the 300x150 jittered workload, 128 sources, 2 of its
     1152 pairs: elem.rhs/s of the three gradient kernels and the per-
     parameter error of both split-precision forms against FP64
@@ -496,6 +499,65 @@ def split_precision_leg(local, dev):
             "units": "elem.rhs = element x source x (omega, py) pair", **res}
 
 
+def sparse_solve_leg(local, dev):
+    """The GPU sparse direct solve on one system of the 400x120 layered mesh
+    (the solver hop the reference hands to MUMPS): analysis, factorisation
+    (time and FP64 flop rate from the fronts' sizes), solves with A and A^H
+    for 1 and 32 right-hand sides, and the residual ||op(A) x - b|| / ||b||
+    (A x by a cuSPARSE product of the same CSR)."""
+    import numpy as np
+    import torch
+    from fem25_b200 import Context, graph_build, synth
+    mesh, pairs, _ = synth.make_config(1)
+    g = graph_build(mesh)
+    ctx = Context(mesh, g, device=local)
+    stream = torch.cuda.current_stream(dev)
+    a = torch.zeros(g.nzero, dtype=torch.complex128, device=dev)
+    f, py = pairs[len(pairs) // 2]
+    ctx.assemble("B", f, py, a, stream=stream)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.sparse_factor(a, stream=stream)  # analysis (host) + first factorisation
+    first = time.perf_counter() - t0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    ctx.sparse_factor(a, stream=stream)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    fac = ev[0].elapsed_time(ev[1]) / 1e3
+    fronts, levels, fbytes, wbytes, kmax, nmax, flops = ctx.sparse_info()
+    crow = torch.from_numpy(g.irptr.astype(np.int64) - 1).to(dev)
+    col = torch.from_numpy(g.jcptr.astype(np.int64) - 1).to(dev)
+    A = torch.sparse_csr_tensor(crow, col, a, (g.ndof, g.ndof))
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(7)
+    solves = {}
+    for nrhs in (1, 32):
+        b = torch.randn((nrhs, g.ndof), dtype=torch.complex128, device=dev, generator=gen)
+        for trans, name in ((0, "A"), (2, "A^H")):
+            x = b.clone()
+            ev[0].record(stream)
+            ctx.sparse_solve(x, trans, stream=stream)
+            ev[1].record(stream)
+            torch.cuda.synchronize()
+            entry = {"ms": ev[0].elapsed_time(ev[1])}
+            if trans == 0:  # residual of A (A^H x checked in the tests)
+                r = (A @ x.T).T - b
+                entry["rel_residual"] = float(torch.linalg.norm(r) / torch.linalg.norm(b))
+            solves[f"{name}, {nrhs} rhs"] = entry
+    del A, a, crow, col
+    ctx.close()
+    torch.cuda.empty_cache()
+    return {"workload": f"one system (f = {f:.2f} Hz) of the 400x120 layered mesh, NDOF {g.ndof}, "
+                        f"NNZ {g.nzero}, complex128",
+            "method": "multifrontal LU, nested dissection of the elements, partial pivoting "
+                      "within each front's fully summed rows",
+            "analysis_s": first - fac, "factor_s": fac, "factor_flops": flops,
+            "factor_tflops": flops / fac / 1e12, "factor_gb": fbytes / 1e9,
+            "work_gb": wbytes / 1e9, "fronts": fronts, "levels": levels,
+            "largest_front": nmax, "solves": solves}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -775,9 +837,10 @@ def main():
     ctx.close()
     torch.cuda.empty_cache()
     ctx = None
-    split = None
+    split = sparse = None
     if not args.no_grad and not args.small and rank == 0:
         split = split_precision_leg(local, dev)
+        sparse = sparse_solve_leg(local, dev)
     pipe = None
     if not args.no_pipeline and not args.small:
         pipe = pipeline_uneven(local, dev, rank, world, max_over_ranks)
@@ -810,7 +873,7 @@ def main():
                         "kernel_ms": kms, "peak_kind": peak_kind,
                         "algorithmic_bytes": "16 B x NNZ per system (complex128 values written)"},
            "cpu_baseline": cpu, "e2e": e2e, "model_update_step": model_update,
-           "gradient": grad, "split_precision": split, "pipeline": pipe,
+           "gradient": grad, "split_precision": split, "sparse_solve": sparse, "pipeline": pipe,
            "gpu_launches": launches_per_step * args.steps, "clocks": clocks}
     if rank == 0:
         print(json.dumps(out))

@@ -35,6 +35,7 @@ UNITS = [
     ("api.cu", []),
     ("misfit_noalloc.cu", ["-fmad=false"]),
     ("dense_solve.cu", []),
+    ("sparse_solve.cu", []),
 ]
 HOST = [("host_setup.cpp", ["-O2", "-ffp-contract=off", "-fPIC", "-fopenmp", "-std=c++17"]),
         ("mesh_io.cpp", ["-O2", "-ffp-contract=off", "-fPIC", "-std=c++17"])]
@@ -77,7 +78,7 @@ def build(verbose=False, extra=()):
             _run(["g++"] + flags + ["-I", os.path.join(ROOT, "include"), "-I", SRC, "-c", "-o", obj, src])
     if _stale(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs +
-             ["-Xcompiler", "-fopenmp", "-lgomp", "-lcusolver"])
+             ["-Xcompiler", "-fopenmp", "-lgomp", "-lcusolver", "-lcublas"])
     return LIB
 
 

@@ -107,6 +107,7 @@ void free_ctx(Ctx *c) {
     if (e) cudaEventDestroy(e);
   if (c->copy_st) cudaStreamDestroy(c->copy_st);
   free_dense(c);
+  free_sparse(c);
 }
 
 int read_err_word(Ctx *c, cudaStream_t st) {
@@ -696,6 +697,30 @@ int fem25_dense_solve_dev(fem25_ctx *h, int nrhs, int trans, double *rhs, void *
   std::string msg;
   int r = dense_solve(c, nrhs, trans, rhs, (cudaStream_t)stream, &msg);
   return r ? fail(c, r, msg) : FEM25_OK;
+}
+
+int fem25_sparse_factor_dev(fem25_ctx *h, const double *csr128, void *stream) {
+  if (!h || !csr128) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  CK(cudaSetDevice(c->device), "set device");
+  std::string msg;
+  int r = sparse_factor(c, csr128, (cudaStream_t)stream, &msg);
+  return r ? fail(c, r, msg) : FEM25_OK;
+}
+
+int fem25_sparse_solve_dev(fem25_ctx *h, int nrhs, int trans, double *rhs, void *stream) {
+  if (!h || !rhs || nrhs <= 0 || trans < 0 || trans > 2) return FEM25_ERR_ARG;
+  Ctx *c = &h->c;
+  CK(cudaSetDevice(c->device), "set device");
+  std::string msg;
+  int r = sparse_solve(c, nrhs, trans, rhs, (cudaStream_t)stream, &msg);
+  return r ? fail(c, r, msg) : FEM25_OK;
+}
+
+int fem25_sparse_info(fem25_ctx *h, long long *out) {
+  if (!h || !out) return FEM25_ERR_ARG;
+  sparse_info(&h->c, out);
+  return FEM25_OK;
 }
 
 int fem25_addblk_dev(fem25_ctx *h, int nsrc, const float *ue, float *sol, void *stream) {

@@ -75,7 +75,8 @@ struct MisfitOpts {
   float2 hfact;            // HDIFFER(IBPHASE, FREQ) of the call
 };
 
-struct DenseLU;  // dense LU of the small-mesh direct solve (dense_solve.cu)
+struct DenseLU;   // dense LU of the small-mesh direct solve (dense_solve.cu)
+struct SparseLU;  // multifrontal LU of the sparse direct solve (sparse_solve.cu)
 
 struct Ctx {
   int device = 0;
@@ -163,6 +164,7 @@ struct Ctx {
   cudaStream_t copy_st = nullptr;
   std::vector<cudaEvent_t> drv_ev;
   DenseLU *dense = nullptr;
+  SparseLU *sparse = nullptr;
   // fem25_assemble_dev with the FMA build of the element kernels
   bool plain_fma = false;
   // bounded waits of the tensor-core gradient kernels: limit in SM clocks
@@ -206,6 +208,10 @@ cudaError_t launch_addblk(Ctx *c, int nsrc, const float *u0, float *sol, cudaStr
 int dense_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *msg);
 int dense_solve(Ctx *c, int nrhs, int trans, double *rhs, cudaStream_t st, std::string *msg);
 void free_dense(Ctx *c);
+int sparse_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *msg);
+int sparse_solve(Ctx *c, int nrhs, int trans, double *rhs, cudaStream_t st, std::string *msg);
+void sparse_info(const Ctx *c, long long *out);
+void free_sparse(Ctx *c);
 cudaError_t launch_grad_plain(Ctx *c, const PairTable &pt, int npairs, int nsrc, const double *u,
                               const double *lam, double *grad, cudaStream_t st);
 cudaError_t prepare_grad_tc(Ctx *c);

@@ -1,0 +1,916 @@
+// Sparse direct solve of one assembled system on the GPU: multifrontal LU
+// with a nested-dissection ordering of the element mesh.  It stands in for
+// the host MUMPS factor / solve hop of the reference (forward solve
+// bielak25.f90:443-446, 545-551; transpose adjoint solve adjgrad.f90:327-341)
+// on meshes far beyond the dense solve's reach, so the assemble -> solve ->
+// misfit -> adjoint -> gradient loop stays on the device at the sizes of the
+// benchmark meshes.
+//
+// Ordering (host, once per context).  The elements are bisected recursively
+// along the longer side of their centroids' bounding box; the DOFs shared by
+// the two halves that no coarser separator has taken form the separator of
+// the tree node, and a leaf (at most kLeafElems elements) keeps every DOF of
+// its elements that no separator took.  Because two DOFs are coupled only
+// through an element they share, a separator splits the matrix graph.  The
+// tree is the elimination tree: front t holds its own DOFs (the "fully
+// summed" rows and columns, eliminated there) and its boundary: the DOFs of
+// its subtree's elements owned by an ancestor, ordered by elimination.
+//
+// Factorisation (device), level by level from the leaves: every front of a
+// level is assembled in a work buffer -- the CSR entries whose first
+// eliminated DOF it owns, plus the update (Schur complement) blocks of its
+// two children (extend-add) -- and partially factored: F11 = P L11 U11 with
+// partial pivoting restricted to the fully summed rows, L21 = F21 U11^-1,
+// U12 = L11^-1 P F12, update = F22 - L21 U12.  Fronts up to kSmallN rows are
+// factored one CTA each in a single launch; larger fronts go to cuSOLVER
+// getrf and cuBLAS trsm / gemm.  The factors (L11\U11 over L21, and U12) are
+// copied to a store kept by the context; the update blocks live until the
+// parent level has consumed them (two work buffers, alternating).
+//
+// Solve (device), one launch per level: forward elimination from the leaves,
+// back substitution from the root, for op(A) = A, A^T (MUMPS ICNTL(9) != 1)
+// or A^H; a CTA per (front, group of right-hand sides).
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <numeric>
+
+#include "ctx.cuh"
+
+namespace fem25 {
+
+namespace sp {
+constexpr int kLeafElems = 2;     // elements per leaf of the dissection
+constexpr int kSmallN = 384;      // fronts up to this many rows: one CTA each
+constexpr int kThreads = 256;
+constexpr int kRhsPerCta = 8;     // right-hand sides per solve CTA
+}  // namespace sp
+
+struct SpFront {
+  int k, m;             // own (fully summed) and boundary DOFs
+  int parent;           // -1: root
+  int child[2];         // -1: none
+  int level;            // depth in the dissection tree (root 0)
+  long long own0;       // first own DOF in own[] (= elimination position)
+  long long bnd0;       // first boundary DOF in bnd[]
+  long long ea0;        // first entry of its extend-add map (ea[], m entries)
+  long long fac0;       // factor store: L block [n][k] (ld n), then U12 [k][m] (ld k)
+  long long work0;      // offset of its n x n front in its level's work buffer
+};
+
+struct SparseLU {
+  bool analysed = false, factored = false;
+  int nfront = 0, nlevel = 0;
+  std::vector<SpFront> fr;
+  std::vector<std::vector<int>> lev;        // front ids per level
+  std::vector<long long> lev_work;          // work elements per level
+  std::vector<long long> lev_ent0;          // first CSR-entry record of each level
+  long long fac_elems = 0, max_work = 0;
+  // device
+  SpFront *d_fr = nullptr;
+  int *d_own = nullptr, *d_bnd = nullptr, *d_ea = nullptr;
+  int *d_lev_fronts = nullptr;              // all levels' front ids, concatenated
+  std::vector<long long> lev_off;           // offset of each level in d_lev_fronts
+  int *d_ent_idx = nullptr;                 // CSR entries by level, and their
+  long long *d_ent_loc = nullptr;           // offsets in the level's work buffer
+  double2 *d_fac = nullptr;                 // factor store
+  int64_t *d_piv = nullptr;                 // pivots (1-based within each front), [NDOF]
+  double2 *d_work[2] = {nullptr, nullptr};
+  int *d_info = nullptr;                    // first zero pivot (front + 1), 0 = none
+  cusolverDnHandle_t sol = nullptr;
+  cusolverDnParams_t par = nullptr;
+  cublasHandle_t blas = nullptr;
+  void *dwork = nullptr;
+  size_t dwork_bytes = 0;
+  std::vector<char> hwork;
+  int *d_getrf_info = nullptr;
+};
+
+// ---------------------------------------------------------------------------
+// symbolic analysis (host)
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Builder {
+  const Ctx *c;
+  std::vector<double> cx, cz;
+  std::vector<int> owner;    // DOF -> front (0-based DOF)
+  std::vector<int> mark;     // scratch stamps per DOF
+  int stamp = 0;
+  std::vector<SpFront> fr;
+  std::vector<std::vector<int>> own_list;   // per front, its own DOFs (ascending)
+  std::vector<std::vector<int>> elems;      // per front, its subtree's elements
+
+  int rec(std::vector<int> &E, int depth) {
+    const int *lm = c->h_lm.data();
+    if ((int)E.size() <= sp::kLeafElems) {
+      std::vector<int> own;
+      for (int e : E)
+        for (int q = 0; q < kNee; q++) {
+          const int d = lm[(size_t)e * kNee + q] - 1;
+          if (d >= 0 && owner[d] == -1) {
+            owner[d] = -3;  // claimed by this leaf (id given below)
+            own.push_back(d);
+          }
+        }
+      std::sort(own.begin(), own.end());
+      const int id = (int)fr.size();
+      for (int d : own) owner[d] = id;
+      SpFront f{};
+      f.k = (int)own.size();
+      f.parent = -1;
+      f.child[0] = f.child[1] = -1;
+      f.level = depth;
+      fr.push_back(f);
+      own_list.push_back(std::move(own));
+      elems.push_back(E);
+      return id;
+    }
+    // bisect along the longer side of the centroids' bounding box
+    double x0 = 1e300, x1 = -1e300, z0 = 1e300, z1 = -1e300;
+    for (int e : E) {
+      x0 = std::min(x0, cx[e]);
+      x1 = std::max(x1, cx[e]);
+      z0 = std::min(z0, cz[e]);
+      z1 = std::max(z1, cz[e]);
+    }
+    const bool alongx = (x1 - x0) >= (z1 - z0);
+    const size_t h = E.size() / 2;
+    std::nth_element(E.begin(), E.begin() + h, E.end(), [&](int a, int b) {
+      const double va = alongx ? cx[a] : cz[a], vb = alongx ? cx[b] : cz[b];
+      return va < vb || (va == vb && a < b);
+    });
+    std::vector<int> E1(E.begin(), E.begin() + h), E2(E.begin() + h, E.end());
+    // separator: free DOFs of both halves
+    ++stamp;
+    for (int e : E1)
+      for (int q = 0; q < kNee; q++) {
+        const int d = lm[(size_t)e * kNee + q] - 1;
+        if (d >= 0) mark[d] = stamp;
+      }
+    std::vector<int> sep;
+    for (int e : E2)
+      for (int q = 0; q < kNee; q++) {
+        const int d = lm[(size_t)e * kNee + q] - 1;
+        if (d >= 0 && mark[d] == stamp && owner[d] == -1) {
+          owner[d] = -2;  // taken by this separator (id given below)
+          sep.push_back(d);
+        }
+      }
+    const int c1 = rec(E1, depth + 1);
+    const int c2 = rec(E2, depth + 1);
+    std::sort(sep.begin(), sep.end());
+    const int id = (int)fr.size();
+    for (int d : sep) owner[d] = id;
+    SpFront f{};
+    f.k = (int)sep.size();
+    f.parent = -1;
+    f.child[0] = c1;
+    f.child[1] = c2;
+    f.level = depth;
+    fr[c1].parent = id;
+    fr[c2].parent = id;
+    fr.push_back(f);
+    own_list.push_back(std::move(sep));
+    elems.push_back(E);
+    return id;
+  }
+};
+
+}  // namespace
+
+// Builds the ordering, the fronts, the extend-add maps and the CSR-entry map;
+// uploads them.  0, or a FEM25 status with *msg.
+static int sparse_analyse(Ctx *c, SparseLU *s, cudaStream_t st, std::string *msg) {
+  const int n = c->ndof;
+  Builder b;
+  b.c = c;
+  b.cx.resize(c->nelem);
+  b.cz.resize(c->nelem);
+  for (int e = 0; e < c->nelem; e++) {
+    double x = 0, z = 0;
+    for (int a = 0; a < 4; a++) {
+      const int p = c->h_ieng[4 * e + a] - 1;
+      x += c->h_x[p];
+      z += c->h_z[p];
+    }
+    b.cx[e] = 0.25 * x;
+    b.cz[e] = 0.25 * z;
+  }
+  b.owner.assign(n, -1);
+  b.mark.assign(n, 0);
+  std::vector<int> E(c->nelem);
+  std::iota(E.begin(), E.end(), 0);
+  b.rec(E, 0);
+  for (int d = 0; d < n; d++)
+    if (b.owner[d] < 0) {
+      *msg = "sparse solve: a DOF belongs to no element";
+      return FEM25_ERR_PATTERN;
+    }
+  const int nf = (int)b.fr.size();
+  // elimination positions (postorder = front id order)
+  std::vector<long long> pos(n);
+  long long p = 0;
+  for (int t = 0; t < nf; t++) {
+    b.fr[t].own0 = p;
+    for (int d : b.own_list[t]) pos[d] = p++;
+  }
+  // boundaries: DOFs of the subtree's elements owned by an ancestor (id > t)
+  std::vector<std::vector<int>> bnd(nf);
+  {
+    std::vector<int> seen(n, -1);
+    for (int t = 0; t < nf; t++) {
+      std::vector<int> &B = bnd[t];
+      for (int e : b.elems[t])
+        for (int q = 0; q < kNee; q++) {
+          const int d = c->h_lm[(size_t)e * kNee + q] - 1;
+          if (d >= 0 && b.owner[d] > t && seen[d] != t) {
+            seen[d] = t;
+            B.push_back(d);
+          }
+        }
+      std::sort(B.begin(), B.end(), [&](int x, int y) { return pos[x] < pos[y]; });
+      b.fr[t].m = (int)B.size();
+      b.elems[t].clear();
+      b.elems[t].shrink_to_fit();
+    }
+  }
+  // index of DOF d in front t (own: by position; boundary: by search)
+  auto local = [&](int t, int d) -> int {
+    const SpFront &f = b.fr[t];
+    if (b.owner[d] == t) return (int)(pos[d] - f.own0);
+    const std::vector<int> &B = bnd[t];
+    auto it = std::lower_bound(B.begin(), B.end(), d,
+                               [&](int x, int y) { return pos[x] < pos[y]; });
+    if (it == B.end() || *it != d) return -1;
+    return f.k + (int)(it - B.begin());
+  };
+  // levels, offsets
+  int nlev = 0;
+  for (auto &f : b.fr) nlev = std::max(nlev, f.level + 1);
+  s->lev.assign(nlev, {});
+  s->lev_work.assign(nlev, 0);
+  long long bnd_tot = 0, fac = 0;
+  for (int t = 0; t < nf; t++) {
+    SpFront &f = b.fr[t];
+    const long long nn = (long long)f.k + f.m;
+    f.bnd0 = bnd_tot;
+    f.ea0 = bnd_tot;
+    bnd_tot += f.m;
+    f.fac0 = fac;
+    fac += nn * f.k + (long long)f.k * f.m;
+    f.work0 = s->lev_work[f.level];
+    s->lev_work[f.level] += nn * nn;
+    s->lev[f.level].push_back(t);
+  }
+  s->fac_elems = fac;
+  s->max_work = 0;
+  for (long long w : s->lev_work) s->max_work = std::max(s->max_work, w);
+  // extend-add maps: child boundary DOF -> index in the parent's front
+  std::vector<int> ea(bnd_tot), own_all(n), bnd_all(bnd_tot);
+  for (int t = 0; t < nf; t++) {
+    const SpFront &f = b.fr[t];
+    std::copy(b.own_list[t].begin(), b.own_list[t].end(), own_all.begin() + f.own0);
+    std::copy(bnd[t].begin(), bnd[t].end(), bnd_all.begin() + f.bnd0);
+    for (int i = 0; i < f.m; i++) {
+      const int li = f.parent >= 0 ? local(f.parent, bnd[t][i]) : -1;
+      if (li < 0) {
+        *msg = "sparse solve: a boundary DOF is missing from the parent front";
+        return FEM25_ERR_PATTERN;
+      }
+      ea[f.ea0 + i] = li;
+    }
+  }
+  // CSR entries -> (front, local offset), grouped by level
+  std::vector<int> jc(c->nzero);
+  cudaError_t e;
+  if ((e = cudaMemcpy(jc.data(), c->d_jcptr, sizeof(int) * c->nzero, cudaMemcpyDeviceToHost))) {
+    *msg = std::string("sparse solve: ") + cudaGetErrorString(e);
+    return FEM25_ERR_CUDA;
+  }
+  // two passes over the rows in chunks: count the entries of each level per
+  // chunk, then place each entry at its level's and chunk's next slot
+  const int nchunk = 256;
+  const int rows_per = (n + nchunk - 1) / nchunk;
+  std::vector<long long> cnt((size_t)nchunk * nlev, 0);
+  int bad = 0;
+  auto entry_front = [&](int i, int j) { return pos[i] <= pos[j] ? b.owner[i] : b.owner[j]; };
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int ch = 0; ch < nchunk; ch++) {
+    long long *cc = cnt.data() + (size_t)ch * nlev;
+    const int i1 = std::min(n, (ch + 1) * rows_per);
+    for (int i = ch * rows_per; i < i1; i++)
+      for (int q = c->h_irptr[i] - 1; q < c->h_irptr[i + 1] - 1; q++)
+        cc[b.fr[entry_front(i, jc[q] - 1)].level]++;
+  }
+  s->lev_ent0.assign(nlev + 1, 0);
+  std::vector<long long> cur((size_t)nchunk * nlev);
+  {
+    long long acc = 0;
+    for (int l = 0; l < nlev; l++) {
+      s->lev_ent0[l] = acc;
+      for (int ch = 0; ch < nchunk; ch++) {
+        cur[(size_t)ch * nlev + l] = acc;
+        acc += cnt[(size_t)ch * nlev + l];
+      }
+    }
+    s->lev_ent0[nlev] = acc;
+  }
+  std::vector<int> sidx(c->nzero);
+  std::vector<long long> sloc(c->nzero);
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : bad)
+  for (int ch = 0; ch < nchunk; ch++) {
+    long long *cc = cur.data() + (size_t)ch * nlev;
+    const int i1 = std::min(n, (ch + 1) * rows_per);
+    for (int i = ch * rows_per; i < i1; i++)
+      for (int q = c->h_irptr[i] - 1; q < c->h_irptr[i + 1] - 1; q++) {
+        const int j = jc[q] - 1;
+        const int t = entry_front(i, j);
+        const int li = local(t, i), lj = local(t, j);
+        if (li < 0 || lj < 0) {
+          bad++;
+          continue;
+        }
+        const long long nn = (long long)b.fr[t].k + b.fr[t].m;
+        const long long o = cc[b.fr[t].level]++;
+        sidx[o] = q;
+        sloc[o] = b.fr[t].work0 + li + (long long)lj * nn;
+      }
+  }
+  if (bad) {
+    *msg = "sparse solve: a matrix entry couples DOFs of no common front";
+    return FEM25_ERR_PATTERN;
+  }
+  std::vector<int>().swap(jc);
+  // level front lists, concatenated
+  std::vector<int> lf;
+  s->lev_off.assign(nlev + 1, 0);
+  for (int l = 0; l < nlev; l++) {
+    s->lev_off[l] = (long long)lf.size();
+    lf.insert(lf.end(), s->lev[l].begin(), s->lev[l].end());
+  }
+  s->lev_off[nlev] = (long long)lf.size();
+  // upload
+  auto up = [&](void **d, const void *h, size_t bytes) -> cudaError_t {
+    cudaError_t r = cudaMalloc(d, bytes ? bytes : 16);
+    if (r == cudaSuccess && bytes) r = cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice);
+    return r;
+  };
+  if ((e = up((void **)&s->d_fr, b.fr.data(), sizeof(SpFront) * nf)) ||
+      (e = up((void **)&s->d_own, own_all.data(), sizeof(int) * n)) ||
+      (e = up((void **)&s->d_bnd, bnd_all.data(), sizeof(int) * bnd_tot)) ||
+      (e = up((void **)&s->d_ea, ea.data(), sizeof(int) * bnd_tot)) ||
+      (e = up((void **)&s->d_lev_fronts, lf.data(), sizeof(int) * lf.size())) ||
+      (e = up((void **)&s->d_ent_idx, sidx.data(), sizeof(int) * sidx.size())) ||
+      (e = up((void **)&s->d_ent_loc, sloc.data(), sizeof(long long) * sloc.size()))) {
+    *msg = std::string("sparse solve: ") + cudaGetErrorString(e) + " (symbolic tables)";
+    return FEM25_ERR_ALLOC;
+  }
+  s->fr = std::move(b.fr);
+  s->nfront = nf;
+  s->nlevel = nlev;
+  s->analysed = true;
+  (void)st;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// numeric factorisation (device)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cfms(double2 acc, double2 a, double2 b) {  // acc - a b
+  return make_double2(acc.x - a.x * b.x + a.y * b.y, acc.y - a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+  const double d = b.x * b.x + b.y * b.y;
+  return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+
+// CSR entries of one level into their fronts' work buffers
+__global__ void k_sp_assemble(long long n, const int *__restrict__ idx,
+                              const long long *__restrict__ loc, const double2 *__restrict__ csr,
+                              double2 *__restrict__ work) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    work[loc[i]] = csr[idx[i]];
+}
+
+// extend-add of child slot `slot` of every front of the level: one CTA per front
+__global__ void k_sp_extend_add(const int *__restrict__ fronts, const SpFront *__restrict__ fr,
+                                const int *__restrict__ ea, const double2 *__restrict__ wchild,
+                                double2 *__restrict__ work, int slot) {
+  const SpFront f = fr[fronts[blockIdx.x]];
+  const int ch = f.child[slot];
+  if (ch < 0) return;
+  const SpFront g = fr[ch];
+  const long long nf = (long long)f.k + f.m, ng = (long long)g.k + g.m;
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int j = threadIdx.x >> 5; j < g.m; j += nw) {
+    const double2 *src = wchild + g.work0 + g.k + (long long)(g.k + j) * ng;
+    double2 *dst = work + f.work0 + (long long)ea[g.ea0 + j] * nf;
+    for (int i = lane; i < g.m; i += 32) {
+      const double2 v = src[i];
+      double2 *o = dst + ea[g.ea0 + i];
+      o->x += v.x;
+      o->y += v.y;
+    }
+  }
+}
+
+// partial LU of one small front per CTA (right-looking, pivoting within the
+// fully summed rows), in place in the work buffer; pivots 1-based
+__global__ void __launch_bounds__(sp::kThreads) k_sp_factor_small(
+    const int *__restrict__ fronts, int nfr, const SpFront *__restrict__ fr,
+    double2 *__restrict__ work, int64_t *__restrict__ piv, int *__restrict__ info) {
+  __shared__ double red_v[sp::kThreads / 32];
+  __shared__ int red_i[sp::kThreads / 32];
+  __shared__ int pivrow;
+  const int b = blockIdx.x;
+  if (b >= nfr) return;
+  const int t = fronts[b];
+  const SpFront f = fr[t];
+  const int k = f.k, n = f.k + f.m;
+  double2 *F = work + f.work0;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int j = 0; j < k; j++) {
+    // pivot: largest |F(r, j)| over the fully summed rows r in [j, k)
+    double best = -1.0;
+    int bi = j;
+    for (int r = j + tid; r < k; r += blockDim.x) {
+      const double2 v = F[r + (long long)j * n];
+      const double a = fabs(v.x) + fabs(v.y);
+      if (a > best) {
+        best = a;
+        bi = r;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (lane == 0) {
+      red_v[warp] = best;
+      red_i[warp] = bi;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double bb = -1.0;
+      int ii = j;
+      for (int w = 0; w < (int)(blockDim.x / 32); w++)
+        if (red_v[w] > bb || (red_v[w] == bb && red_i[w] < ii)) {
+          bb = red_v[w];
+          ii = red_i[w];
+        }
+      pivrow = ii;
+      piv[f.own0 + j] = ii + 1;
+      if (bb <= 0.0) atomicCAS(info, 0, t + 1);
+    }
+    __syncthreads();
+    const int pr = pivrow;
+    if (pr != j)
+      for (int cidx = tid; cidx < n; cidx += blockDim.x) {
+        double2 *a = F + j + (long long)cidx * n, *bq = F + pr + (long long)cidx * n;
+        const double2 x = *a;
+        *a = *bq;
+        *bq = x;
+      }
+    __syncthreads();
+    const double2 d = F[j + (long long)j * n];
+    const bool zero = d.x == 0.0 && d.y == 0.0;
+    // column j below the diagonal: L(r, j) = F(r, j) / F(j, j)
+    for (int r = j + 1 + tid; r < n; r += blockDim.x) {
+      double2 *a = F + r + (long long)j * n;
+      *a = zero ? make_double2(0.0, 0.0) : cdiv(*a, d);
+    }
+    __syncthreads();
+    // rank-1 update of the trailing block: a warp per column
+    for (int cc = j + 1 + warp; cc < n; cc += (int)(blockDim.x >> 5)) {
+      const double2 u = F[j + (long long)cc * n];
+      double2 *col = F + (long long)cc * n;
+      const double2 *lj = F + (long long)j * n;
+      for (int r = j + 1 + lane; r < n; r += 32) col[r] = cfms(col[r], lj[r], u);
+    }
+    __syncthreads();
+  }
+}
+
+// a library-factored front's zero pivot into the status word
+__global__ void k_sp_getrf_status(const int *getrf_info, int *info, int front) {
+  if (*getrf_info > 0) atomicCAS(info, 0, front + 1);
+}
+
+// row interchanges of a front's pivots on columns [c0, c1) (laswp)
+__global__ void k_sp_laswp(double2 *F, int n, int k, int c0, int c1, const int64_t *piv) {
+  for (int cidx = c0 + blockIdx.x * blockDim.x + threadIdx.x; cidx < c1;
+       cidx += gridDim.x * blockDim.x)
+    for (int j = 0; j < k; j++) {
+      const int p = (int)piv[j] - 1;
+      if (p != j) {
+        double2 *a = F + j + (long long)cidx * n, *b = F + p + (long long)cidx * n;
+        const double2 x = *a;
+        *a = *b;
+        *b = x;
+      }
+    }
+}
+
+// factors of the level's fronts to the store: the first k columns (L11\U11
+// over L21, n x k) and U12 (rows 0..k-1 of columns k..n-1, k x m, ld k)
+__global__ void k_sp_store(const int *__restrict__ fronts, const SpFront *__restrict__ fr,
+                           const double2 *__restrict__ work, double2 *__restrict__ fac) {
+  const SpFront f = fr[fronts[blockIdx.x]];
+  const long long n = (long long)f.k + f.m;
+  const double2 *F = work + f.work0;
+  double2 *L = fac + f.fac0, *U = L + n * f.k;
+  for (long long q = threadIdx.x; q < n * f.k; q += blockDim.x) L[q] = F[q];
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int j = threadIdx.x >> 5; j < f.m; j += nw)
+    for (int i = lane; i < f.k; i += 32) U[i + (long long)j * f.k] = F[i + (f.k + j) * n];
+}
+
+// ---------------------------------------------------------------------------
+// solve (device): x is [nrhs][NDOF]
+// ---------------------------------------------------------------------------
+// forward step of one front for op(A) = A: pivots, L11 solve, boundary update
+__global__ void __launch_bounds__(sp::kThreads) k_sp_fwd(
+    const int *__restrict__ fronts, const SpFront *__restrict__ fr,
+    const int *__restrict__ own, const int *__restrict__ bnd, const double2 *__restrict__ fac,
+    const int64_t *__restrict__ piv, double2 *__restrict__ x, int ndof, int nrhs) {
+  const SpFront f = fr[fronts[blockIdx.x]];
+  const int r0 = blockIdx.y * sp::kRhsPerCta, nr = min(sp::kRhsPerCta, nrhs - r0);
+  if (nr <= 0 || f.k == 0) return;
+  const long long n = (long long)f.k + f.m;
+  const int *ow = own + f.own0;
+  const double2 *L = fac + f.fac0;
+  const int tid = threadIdx.x;
+  // row interchanges (sequential in j, one thread per right-hand side)
+  if (tid < nr) {
+    double2 *xr = x + (long long)(r0 + tid) * ndof;
+    for (int j = 0; j < f.k; j++) {
+      const int p = (int)piv[f.own0 + j] - 1;
+      if (p != j) {
+        const double2 t = xr[ow[j]];
+        xr[ow[j]] = xr[ow[p]];
+        xr[ow[p]] = t;
+      }
+    }
+  }
+  __syncthreads();
+  // L11 (unit lower), column by column
+  for (int j = 0; j < f.k; j++) {
+    for (int s = 0; s < nr; s++) {
+      double2 *xr = x + (long long)(r0 + s) * ndof;
+      const double2 xj = xr[ow[j]];
+      for (int r = j + 1 + tid; r < f.k; r += blockDim.x)
+        xr[ow[r]] = cfms(xr[ow[r]], L[r + j * n], xj);
+    }
+    __syncthreads();
+  }
+  // boundary rows: x_b -= L21 x_own (other fronts of the level may add to the
+  // same boundary DOF: atomics)
+  for (int q = tid; q < f.m * nr; q += blockDim.x) {
+    const int r = q % f.m, s = q / f.m;
+    const double2 *xr = x + (long long)(r0 + s) * ndof;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int j = 0; j < f.k; j++) acc = cfms(acc, L[f.k + r + j * n], xr[ow[j]]);
+    double *o = reinterpret_cast<double *>(x + (long long)(r0 + s) * ndof + bnd[f.bnd0 + r]);
+    atomicAdd(o, acc.x);
+    atomicAdd(o + 1, acc.y);
+  }
+}
+
+// backward step of one front for op(A) = A: x_own -= U12 x_bnd, U11 solve
+__global__ void __launch_bounds__(sp::kThreads) k_sp_bwd(
+    const int *__restrict__ fronts, const SpFront *__restrict__ fr,
+    const int *__restrict__ own, const int *__restrict__ bnd, const double2 *__restrict__ fac,
+    double2 *__restrict__ x, int ndof, int nrhs) {
+  const SpFront f = fr[fronts[blockIdx.x]];
+  const int r0 = blockIdx.y * sp::kRhsPerCta, nr = min(sp::kRhsPerCta, nrhs - r0);
+  if (nr <= 0 || f.k == 0) return;
+  const long long n = (long long)f.k + f.m;
+  const int *ow = own + f.own0;
+  const double2 *L = fac + f.fac0, *U = L + n * f.k;
+  const int tid = threadIdx.x;
+  for (int q = tid; q < f.k * nr; q += blockDim.x) {
+    const int i = q % f.k, s = q / f.k;
+    double2 *xr = x + (long long)(r0 + s) * ndof;
+    double2 acc = xr[ow[i]];
+    for (int cc = 0; cc < f.m; cc++) acc = cfms(acc, U[i + (long long)cc * f.k], xr[bnd[f.bnd0 + cc]]);
+    xr[ow[i]] = acc;
+  }
+  __syncthreads();
+  for (int j = f.k - 1; j >= 0; j--) {
+    for (int s = tid; s < nr; s += blockDim.x) {
+      double2 *xr = x + (long long)(r0 + s) * ndof;
+      xr[ow[j]] = cdiv(xr[ow[j]], L[j + j * n]);
+    }
+    __syncthreads();
+    for (int s = 0; s < nr; s++) {
+      double2 *xr = x + (long long)(r0 + s) * ndof;
+      const double2 xj = xr[ow[j]];
+      for (int r = tid; r < j; r += blockDim.x) xr[ow[r]] = cfms(xr[ow[r]], L[r + j * n], xj);
+    }
+    __syncthreads();
+  }
+}
+
+// forward step for op(A) = A^T (conj = 0) or A^H (conj = 1): U11^T solve,
+// boundary update with U12^T
+__global__ void __launch_bounds__(sp::kThreads) k_sp_fwd_t(
+    const int *__restrict__ fronts, const SpFront *__restrict__ fr,
+    const int *__restrict__ own, const int *__restrict__ bnd, const double2 *__restrict__ fac,
+    double2 *__restrict__ x, int ndof, int nrhs, int conj) {
+  const SpFront f = fr[fronts[blockIdx.x]];
+  const int r0 = blockIdx.y * sp::kRhsPerCta, nr = min(sp::kRhsPerCta, nrhs - r0);
+  if (nr <= 0 || f.k == 0) return;
+  const long long n = (long long)f.k + f.m;
+  const int *ow = own + f.own0;
+  const double2 *L = fac + f.fac0, *U = L + n * f.k;
+  const int tid = threadIdx.x;
+  auto op = [&](double2 v) { return conj ? cconj(v) : v; };
+  for (int j = 0; j < f.k; j++) {
+    for (int s = tid; s < nr; s += blockDim.x) {
+      double2 *xr = x + (long long)(r0 + s) * ndof;
+      xr[ow[j]] = cdiv(xr[ow[j]], op(L[j + j * n]));
+    }
+    __syncthreads();
+    for (int s = 0; s < nr; s++) {
+      double2 *xr = x + (long long)(r0 + s) * ndof;
+      const double2 xj = xr[ow[j]];
+      for (int r = j + 1 + tid; r < f.k; r += blockDim.x)
+        xr[ow[r]] = cfms(xr[ow[r]], op(L[j + (long long)r * n]), xj);  // U(j, r)
+    }
+    __syncthreads();
+  }
+  for (int q = tid; q < f.m * nr; q += blockDim.x) {
+    const int cc = q % f.m, s = q / f.m;
+    const double2 *xr = x + (long long)(r0 + s) * ndof;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int i = 0; i < f.k; i++) acc = cfms(acc, op(U[i + (long long)cc * f.k]), xr[ow[i]]);
+    double *o = reinterpret_cast<double *>(x + (long long)(r0 + s) * ndof + bnd[f.bnd0 + cc]);
+    atomicAdd(o, acc.x);
+    atomicAdd(o + 1, acc.y);
+  }
+}
+
+// backward step for A^T / A^H: x_own -= L21^T x_bnd, L11^T solve, inverse
+// row interchanges
+__global__ void __launch_bounds__(sp::kThreads) k_sp_bwd_t(
+    const int *__restrict__ fronts, const SpFront *__restrict__ fr,
+    const int *__restrict__ own, const int *__restrict__ bnd, const double2 *__restrict__ fac,
+    const int64_t *__restrict__ piv, double2 *__restrict__ x, int ndof, int nrhs, int conj) {
+  const SpFront f = fr[fronts[blockIdx.x]];
+  const int r0 = blockIdx.y * sp::kRhsPerCta, nr = min(sp::kRhsPerCta, nrhs - r0);
+  if (nr <= 0 || f.k == 0) return;
+  const long long n = (long long)f.k + f.m;
+  const int *ow = own + f.own0;
+  const double2 *L = fac + f.fac0;
+  const int tid = threadIdx.x;
+  auto op = [&](double2 v) { return conj ? cconj(v) : v; };
+  for (int q = tid; q < f.k * nr; q += blockDim.x) {
+    const int i = q % f.k, s = q / f.k;
+    double2 *xr = x + (long long)(r0 + s) * ndof;
+    double2 acc = xr[ow[i]];
+    for (int r = 0; r < f.m; r++) acc = cfms(acc, op(L[f.k + r + (long long)i * n]), xr[bnd[f.bnd0 + r]]);
+    xr[ow[i]] = acc;
+  }
+  __syncthreads();
+  for (int j = f.k - 1; j >= 0; j--) {
+    for (int s = 0; s < nr; s++) {
+      double2 *xr = x + (long long)(r0 + s) * ndof;
+      const double2 xj = xr[ow[j]];
+      for (int r = tid; r < j; r += blockDim.x)
+        xr[ow[r]] = cfms(xr[ow[r]], op(L[j + (long long)r * n]), xj);  // L(j, r)
+    }
+    __syncthreads();
+  }
+  if (tid < nr) {
+    double2 *xr = x + (long long)(r0 + tid) * ndof;
+    for (int j = f.k - 1; j >= 0; j--) {
+      const int p = (int)piv[f.own0 + j] - 1;
+      if (p != j) {
+        const double2 t = xr[ow[j]];
+        xr[ow[j]] = xr[ow[p]];
+        xr[ow[p]] = t;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host drivers
+// ---------------------------------------------------------------------------
+void free_sparse(Ctx *c) {
+  SparseLU *s = c->sparse;
+  if (!s) return;
+  void *ptrs[] = {s->d_fr,      s->d_own,     s->d_bnd,     s->d_ea,      s->d_lev_fronts,
+                  s->d_ent_idx, s->d_ent_loc, s->d_fac,     s->d_piv,     s->d_work[0],
+                  s->d_work[1], s->d_info,    s->dwork,     s->d_getrf_info};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (s->par) cusolverDnDestroyParams(s->par);
+  if (s->sol) cusolverDnDestroy(s->sol);
+  if (s->blas) cublasDestroy(s->blas);
+  delete s;
+  c->sparse = nullptr;
+}
+
+void sparse_info(const Ctx *c, long long *out) {
+  const SparseLU *s = c->sparse;
+  out[0] = s ? s->nfront : 0;
+  out[1] = s ? s->nlevel : 0;
+  out[2] = s ? s->fac_elems * 16 : 0;
+  out[3] = s ? s->max_work * 16 : 0;
+  int kmax = 0, nmax = 0;
+  double flops = 0.0;  // real flops: 8 per complex multiply-add
+  if (s)
+    for (const SpFront &f : s->fr) {
+      kmax = std::max(kmax, f.k);
+      nmax = std::max(nmax, f.k + f.m);
+      const double k = f.k, m = f.m;
+      flops += 8.0 / 3.0 * k * k * k + 8.0 * k * k * m + 8.0 * k * m * m;
+    }
+  out[4] = kmax;
+  out[5] = nmax;
+  out[6] = (long long)flops;
+}
+
+#define SPCK(expr, what)                                                   \
+  do {                                                                     \
+    cudaError_t e_ = (expr);                                               \
+    if (e_ != cudaSuccess) {                                               \
+      *msg = std::string("sparse solve: ") + (what) + ": " + cudaGetErrorString(e_); \
+      return e_ == cudaErrorMemoryAllocation ? FEM25_ERR_ALLOC : FEM25_ERR_CUDA;     \
+    }                                                                      \
+  } while (0)
+
+int sparse_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *msg) {
+  if (!c->sparse) c->sparse = new SparseLU();
+  SparseLU *s = c->sparse;
+  s->factored = false;
+  if (!s->analysed) {
+    const int r = sparse_analyse(c, s, st, msg);
+    if (r) return r;
+  }
+  if (!s->sol) {
+    if (cusolverDnCreate(&s->sol) != CUSOLVER_STATUS_SUCCESS ||
+        cusolverDnCreateParams(&s->par) != CUSOLVER_STATUS_SUCCESS ||
+        cublasCreate(&s->blas) != CUBLAS_STATUS_SUCCESS) {
+      *msg = "sparse solve: cuSOLVER / cuBLAS handle creation failed";
+      return FEM25_ERR_CUDA;
+    }
+  }
+  if (cusolverDnSetStream(s->sol, st) != CUSOLVER_STATUS_SUCCESS ||
+      cublasSetStream(s->blas, st) != CUBLAS_STATUS_SUCCESS) {
+    *msg = "sparse solve: cannot set the library stream";
+    return FEM25_ERR_CUDA;
+  }
+  if (!s->d_fac) {
+    SPCK(cudaMalloc(&s->d_fac, sizeof(double2) * std::max(s->fac_elems, 1LL)), "factor store");
+    SPCK(cudaMalloc(&s->d_piv, sizeof(int64_t) * std::max(c->ndof, 1)), "pivots");
+    SPCK(cudaMalloc(&s->d_work[0], sizeof(double2) * std::max(s->max_work, 1LL)), "work");
+    SPCK(cudaMalloc(&s->d_work[1], sizeof(double2) * std::max(s->max_work, 1LL)), "work");
+    SPCK(cudaMalloc(&s->d_info, sizeof(int)), "status");
+    SPCK(cudaMalloc(&s->d_getrf_info, sizeof(int)), "status");
+  }
+  SPCK(cudaMemsetAsync(s->d_info, 0, sizeof(int), st), "status");
+  const double2 *csr = reinterpret_cast<const double2 *>(csr128);
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  for (int l = s->nlevel - 1; l >= 0; l--) {
+    double2 *W = s->d_work[l & 1], *Wc = s->d_work[(l + 1) & 1];
+    const int nfl = (int)s->lev[l].size();
+    const int *dfr = s->d_lev_fronts + s->lev_off[l];
+    SPCK(cudaMemsetAsync(W, 0, sizeof(double2) * s->lev_work[l], st), "work");
+    const long long ne = s->lev_ent0[l + 1] - s->lev_ent0[l];
+    if (ne > 0) {
+      const int grid = (int)std::min<long long>((ne + 255) / 256, (long long)nsm * 16);
+      k_sp_assemble<<<grid, 256, 0, st>>>(ne, s->d_ent_idx + s->lev_ent0[l],
+                                          s->d_ent_loc + s->lev_ent0[l], csr, W);
+    }
+    if (l + 1 < s->nlevel)
+      for (int slot = 0; slot < 2; slot++)
+        k_sp_extend_add<<<nfl, 256, 0, st>>>(dfr, s->d_fr, s->d_ea, Wc, W, slot);
+    SPCK(cudaGetLastError(), "assembly");
+    // small fronts: one CTA each; large ones: dense library calls
+    std::vector<int> small, large;
+    for (int t : s->lev[l]) (s->fr[t].k + s->fr[t].m <= sp::kSmallN ? small : large).push_back(t);
+    if (!small.empty()) {
+      if (small.size() == s->lev[l].size()) {
+        k_sp_factor_small<<<nfl, sp::kThreads, 0, st>>>(dfr, nfl, s->d_fr, W, s->d_piv, s->d_info);
+      } else {
+        // a level mixing both kinds: its small fronts' ids go to a scratch list
+        int *d_small = nullptr;
+        SPCK(cudaMallocAsync(&d_small, sizeof(int) * small.size(), st), "front list");
+        SPCK(cudaMemcpyAsync(d_small, small.data(), sizeof(int) * small.size(),
+                             cudaMemcpyHostToDevice, st), "front list");
+        k_sp_factor_small<<<(int)small.size(), sp::kThreads, 0, st>>>(d_small, (int)small.size(),
+                                                                      s->d_fr, W, s->d_piv,
+                                                                      s->d_info);
+        SPCK(cudaFreeAsync(d_small, st), "front list");
+      }
+      SPCK(cudaGetLastError(), "small fronts");
+    }
+    for (int t : large) {
+      const SpFront &f = s->fr[t];
+      const int64_t n = (int64_t)f.k + f.m, k = f.k, m = f.m;
+      if (k == 0) continue;
+      double2 *F = W + f.work0;
+      size_t dbytes = 0, hbytes = 0;
+      if (cusolverDnXgetrf_bufferSize(s->sol, s->par, k, k, CUDA_C_64F, F, n, CUDA_C_64F, &dbytes,
+                                      &hbytes) != CUSOLVER_STATUS_SUCCESS) {
+        *msg = "sparse solve: getrf workspace query failed";
+        return FEM25_ERR_CUDA;
+      }
+      if (dbytes > s->dwork_bytes) {
+        if (s->dwork) SPCK(cudaFree(s->dwork), "workspace");
+        s->dwork = nullptr;
+        SPCK(cudaMalloc(&s->dwork, dbytes), "workspace");
+        s->dwork_bytes = dbytes;
+      }
+      if (hbytes > s->hwork.size()) s->hwork.resize(hbytes);
+      int64_t *ipiv = s->d_piv + f.own0;
+      if (cusolverDnXgetrf(s->sol, s->par, k, k, CUDA_C_64F, F, n, ipiv, CUDA_C_64F, s->dwork,
+                           dbytes, hbytes ? s->hwork.data() : nullptr, hbytes,
+                           s->d_getrf_info) != CUSOLVER_STATUS_SUCCESS) {
+        *msg = "sparse solve: getrf failed";
+        return FEM25_ERR_CUDA;
+      }
+      // a zero pivot of this front: recorded as the front's id in the status word
+      k_sp_getrf_status<<<1, 1, 0, st>>>(s->d_getrf_info, s->d_info, t);
+      if (m > 0) {
+        k_sp_laswp<<<(int)std::min<int64_t>((m + 127) / 128, 1024), 128, 0, st>>>(
+            F, (int)n, (int)k, (int)k, (int)n, ipiv);
+        SPCK(cudaGetLastError(), "laswp");
+        const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0),
+                              mone = make_cuDoubleComplex(-1.0, 0.0);
+        cuDoubleComplex *A = reinterpret_cast<cuDoubleComplex *>(F);
+        if (cublasZtrsm(s->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                        CUBLAS_DIAG_UNIT, (int)k, (int)m, &one, A, (int)n, A + k * n, (int)n) ||
+            cublasZtrsm(s->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                        CUBLAS_DIAG_NON_UNIT, (int)m, (int)k, &one, A, (int)n, A + k, (int)n) ||
+            cublasZgemm(s->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)m, (int)k, &mone, A + k,
+                        (int)n, A + k * n, (int)n, &one, A + k + k * n, (int)n)) {
+          *msg = "sparse solve: trsm / gemm failed";
+          return FEM25_ERR_CUDA;
+        }
+      }
+    }
+    k_sp_store<<<nfl, 256, 0, st>>>(dfr, s->d_fr, W, s->d_fac);
+    SPCK(cudaGetLastError(), "factor store");
+  }
+  // zero pivots of any front
+  int info = 0;
+  SPCK(cudaMemcpyAsync(&info, s->d_info, sizeof(int), cudaMemcpyDeviceToHost, st), "status");
+  SPCK(cudaStreamSynchronize(st), "factorisation");
+  if (info != 0) {
+    *msg = "sparse solve: zero pivot in front " + std::to_string(info - 1) +
+           " (matrix singular to working precision)";
+    return FEM25_ERR_ARG;
+  }
+  s->factored = true;
+  return 0;
+}
+
+int sparse_solve(Ctx *c, int nrhs, int trans, double *rhs, cudaStream_t st, std::string *msg) {
+  SparseLU *s = c->sparse;
+  if (!s || !s->factored) {
+    *msg = "sparse solve: no factorisation (call fem25_sparse_factor_dev first)";
+    return FEM25_ERR_ARG;
+  }
+  double2 *x = reinterpret_cast<double2 *>(rhs);
+  const int nchunk = (nrhs + sp::kRhsPerCta - 1) / sp::kRhsPerCta;
+  for (int l = s->nlevel - 1; l >= 0; l--) {
+    const dim3 grid((unsigned)s->lev[l].size(), (unsigned)nchunk);
+    const int *dfr = s->d_lev_fronts + s->lev_off[l];
+    if (trans == 0)
+      k_sp_fwd<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac, s->d_piv,
+                                              x, c->ndof, nrhs);
+    else
+      k_sp_fwd_t<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac, x,
+                                                c->ndof, nrhs, trans == 2);
+  }
+  for (int l = 0; l < s->nlevel; l++) {
+    const dim3 grid((unsigned)s->lev[l].size(), (unsigned)nchunk);
+    const int *dfr = s->d_lev_fronts + s->lev_off[l];
+    if (trans == 0)
+      k_sp_bwd<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac, x,
+                                              c->ndof, nrhs);
+    else
+      k_sp_bwd_t<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac,
+                                                s->d_piv, x, c->ndof, nrhs, trans == 2);
+  }
+  SPCK(cudaGetLastError(), "solve");
+  return 0;
+}
+
+}  // namespace fem25

@@ -71,6 +71,9 @@ def lib():
         L.fem25_addblk_dev.argtypes = [vp, i, vp, vp, vp]
         L.fem25_dense_factor_dev.argtypes = [vp, vp, vp]
         L.fem25_dense_solve_dev.argtypes = [vp, i, i, vp, vp]
+        L.fem25_sparse_factor_dev.argtypes = [vp, vp, vp]
+        L.fem25_sparse_solve_dev.argtypes = [vp, i, i, vp, vp]
+        L.fem25_sparse_info.argtypes = [vp, vp]
         L.fem25_gradient_dev.argtypes = [vp, i, vp, vp, i, vp, vp, i, vp, vp]
         L.fem25_gradient_accumulate_dev.argtypes = [vp, i, vp, vp, i, vp, vp, vp]
         L.fem25_gradient_finalize_dev.argtypes = [vp, vp, vp]
@@ -357,6 +360,23 @@ class Context:
     def dense_factor(self, csr128, stream=None):
         """LU of the assembled complex128 CSR (device) for the small-mesh solve."""
         self._check(lib().fem25_dense_factor_dev(self.h, _ptr(csr128), _stream(stream)))
+
+    def sparse_factor(self, csr128, stream=None):
+        """Multifrontal LU of a complex128 CSR (device) -- fem25_sparse_factor_dev."""
+        self._check(lib().fem25_sparse_factor_dev(self.h, _ptr(csr128), _stream(stream)))
+
+    def sparse_solve(self, rhs, trans=0, stream=None):
+        """op(A) X = B in place, rhs complex128 [nrhs, NDOF] (device); trans 0: A,
+        1: A^T, 2: A^H -- fem25_sparse_solve_dev."""
+        nrhs = 1 if rhs.dim() == 1 else rhs.shape[0]
+        self._check(lib().fem25_sparse_solve_dev(self.h, nrhs, trans, _ptr(rhs), _stream(stream)))
+
+    def sparse_info(self):
+        """(fronts, levels, factor bytes, work bytes, largest k, largest front
+        order, flops of one factorisation) -- fem25_sparse_info."""
+        out = np.zeros(7, np.int64)
+        self._check(lib().fem25_sparse_info(self.h, out.ctypes.data))
+        return tuple(int(v) for v in out)
 
     def dense_solve(self, rhs, trans=0, stream=None):
         """op(A) X = B in place; rhs complex128 [nrhs][NDOF] on the device;

@@ -139,6 +139,19 @@ MODULE FEM25GPU
        IMPORT :: C_INT, C_PTR
        TYPE(C_PTR), VALUE :: CTX, STREAM
      END FUNCTION
+     ! sparse direct solve on the GPU in place of CMUMPS (bielak25.f90:334-335,
+     ! 443-446, 545-551; adjgrad.f90:327-341); CSR128 and RHS are device buffers
+     INTEGER(C_INT) FUNCTION FEM25_SPARSE_FACTOR_DEV(CTX, CSR128, STREAM) &
+                    BIND(C, NAME='fem25_sparse_factor_dev')
+       IMPORT :: C_INT, C_PTR
+       TYPE(C_PTR), VALUE :: CTX, CSR128, STREAM
+     END FUNCTION
+     INTEGER(C_INT) FUNCTION FEM25_SPARSE_SOLVE_DEV(CTX, NRHS, TRANS, RHS, STREAM) &
+                    BIND(C, NAME='fem25_sparse_solve_dev')
+       IMPORT :: C_INT, C_PTR
+       TYPE(C_PTR), VALUE :: CTX, RHS, STREAM
+       INTEGER(C_INT), VALUE :: NRHS, TRANS
+     END FUNCTION
   END INTERFACE
 
 CONTAINS

@@ -184,6 +184,25 @@ int fem25_asmb_peff(fem25_ctx *ctx, int ndof, const float *cdist, const float *u
 int fem25_dense_factor_dev(fem25_ctx *ctx, const double *csr128, void *stream);
 int fem25_dense_solve_dev(fem25_ctx *ctx, int nrhs, int trans, double *rhs, void *stream);
 
+/* ---- sparse direct solve on the GPU (any mesh size) -------------------------
+ * The same hop as fem25_dense_*, for meshes of any size (replaces the host
+ * MUMPS factor / solve, bielak25.f90:443-446, 545-551, and the transpose
+ * adjoint solve, adjgrad.f90:327-341): multifrontal LU of the complex128 CSR
+ * (device) with a nested-dissection ordering of the elements, partial
+ * pivoting within each front's fully summed rows, the factors kept by the
+ * context (fem25_sparse_info reports their size).  The first call analyses
+ * the mesh (host, seconds for millions of DOFs) and allocates; every call
+ * synchronises the stream and returns FEM25_ERR_ARG for a zero pivot.
+ * fem25_sparse_solve_dev solves op(A) X = B in place for nrhs complex128
+ * columns [nrhs][NDOF] on the device; trans = 0: A, 1: A^T, 2: A^H.
+ * fem25_sparse_info fills out[7] = {fronts, levels, factor bytes, work-buffer
+ * bytes, largest front's fully summed DOFs, largest front's order, real
+ * flops of one factorisation (8 per complex multiply-add)}; zeros before the
+ * first factorisation. */
+int fem25_sparse_factor_dev(fem25_ctx *ctx, const double *csr128, void *stream);
+int fem25_sparse_solve_dev(fem25_ctx *ctx, int nrhs, int trans, double *rhs, void *stream);
+int fem25_sparse_info(fem25_ctx *ctx, long long *out);
+
 /* Drop-in for ADDBLK (bielak_utils.f:1116-1125; callers funcgradh.f90:248,
  * srcrec.f90:694, fgh_window.f90:437, qpmfree.f90:378): after the solve, the
  * background field is added back on the exterior ('E') DOFs,
