@@ -22,14 +22,17 @@
 // two children (extend-add) -- and partially factored: F11 = P L11 U11 with
 // partial pivoting restricted to the fully summed rows, L21 = F21 U11^-1,
 // U12 = L11^-1 P F12, update = F22 - L21 U12.  Fronts up to kSmallN rows are
-// factored one CTA each in a single launch; larger fronts go to cuSOLVER
-// getrf and cuBLAS trsm / gemm.  The factors (L11\U11 over L21, and U12) are
-// copied to a store kept by the context; the update blocks live until the
-// parent level has consumed them (two work buffers, alternating).
+// factored one CTA each in a single launch per level (blocked by panels of
+// kNb columns factored in shared memory, rank-kNb trailing updates); larger
+// fronts (the top levels of the tree) go to cuSOLVER getrf and cuBLAS trsm /
+// gemm.  The factors (L11\U11 over L21, and U12) are copied to a store kept
+// by the context; the update blocks live until the parent level has consumed
+// them (two work buffers, alternating).
 //
-// Solve (device), one launch per level: forward elimination from the leaves,
-// back substitution from the root, for op(A) = A, A^T (MUMPS ICNTL(9) != 1)
-// or A^H; a CTA per (front, group of right-hand sides).
+// Solve (device), level by level: forward elimination from the leaves, back
+// substitution from the root, for op(A) = A, A^T (MUMPS ICNTL(9) != 1) or
+// A^H; a CTA per (front, group of right-hand sides) up to kSmallN rows,
+// gathered dense blocks and cuBLAS trsm / gemm for the larger fronts.
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 
@@ -43,7 +46,8 @@ namespace fem25 {
 
 namespace sp {
 constexpr int kLeafElems = 2;     // elements per leaf of the dissection
-constexpr int kSmallN = 384;      // fronts up to this many rows: one CTA each
+constexpr int kSmallN = 1024;     // fronts up to this many rows: one CTA each
+constexpr int kNb = 8;            // panel width of the one-CTA factorisation
 constexpr int kThreads = 256;
 constexpr int kRhsPerCta = 8;     // right-hand sides per solve CTA
 }  // namespace sp
@@ -64,7 +68,8 @@ struct SparseLU {
   bool analysed = false, factored = false;
   int nfront = 0, nlevel = 0;
   std::vector<SpFront> fr;
-  std::vector<std::vector<int>> lev;        // front ids per level
+  std::vector<std::vector<int>> lev;        // front ids per level, one-CTA fronts first
+  std::vector<int> lev_nsmall, lev_nmax_small;  // per level: one-CTA fronts, their largest order
   std::vector<long long> lev_work;          // work elements per level
   std::vector<long long> lev_ent0;          // first CSR-entry record of each level
   long long fac_elems = 0, max_work = 0;
@@ -86,6 +91,10 @@ struct SparseLU {
   size_t dwork_bytes = 0;
   std::vector<char> hwork;
   int *d_getrf_info = nullptr;
+  // solve scratch of the library-path fronts: own rows and boundary rows of
+  // the right-hand sides, [nrhs][k] and [nrhs][m]
+  double2 *d_sx = nullptr, *d_sy = nullptr;
+  size_t sx_cap = 0, sy_cap = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -344,6 +353,19 @@ static int sparse_analyse(Ctx *c, SparseLU *s, cudaStream_t st, std::string *msg
     return FEM25_ERR_PATTERN;
   }
   std::vector<int>().swap(jc);
+  // one-CTA fronts first in each level's list
+  s->lev_nsmall.assign(nlev, 0);
+  s->lev_nmax_small.assign(nlev, 0);
+  for (int l = 0; l < nlev; l++) {
+    std::stable_partition(s->lev[l].begin(), s->lev[l].end(), [&](int t) {
+      return b.fr[t].k + b.fr[t].m <= sp::kSmallN;
+    });
+    for (int t : s->lev[l])
+      if (b.fr[t].k + b.fr[t].m <= sp::kSmallN) {
+        s->lev_nsmall[l]++;
+        s->lev_nmax_small[l] = std::max(s->lev_nmax_small[l], b.fr[t].k + b.fr[t].m);
+      }
+  }
   // level front lists, concatenated
   std::vector<int> lf;
   s->lev_off.assign(nlev + 1, 0);
@@ -410,7 +432,7 @@ __global__ void k_sp_extend_add(const int *__restrict__ fronts, const SpFront *_
   const SpFront g = fr[ch];
   const long long nf = (long long)f.k + f.m, ng = (long long)g.k + g.m;
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int j = threadIdx.x >> 5; j < g.m; j += nw) {
+  for (int j = blockIdx.y * nw + (threadIdx.x >> 5); j < g.m; j += gridDim.y * nw) {
     const double2 *src = wchild + g.work0 + g.k + (long long)(g.k + j) * ng;
     double2 *dst = work + f.work0 + (long long)ea[g.ea0 + j] * nf;
     for (int i = lane; i < g.m; i += 32) {
@@ -422,82 +444,145 @@ __global__ void k_sp_extend_add(const int *__restrict__ fronts, const SpFront *_
   }
 }
 
-// partial LU of one small front per CTA (right-looking, pivoting within the
-// fully summed rows), in place in the work buffer; pivots 1-based
-__global__ void __launch_bounds__(sp::kThreads) k_sp_factor_small(
+// Partial LU of one front per CTA, blocked by panels of kNb columns: the
+// panel (rows jb..n-1) is factored in shared memory with partial pivoting
+// restricted to the fully summed rows, its row interchanges are applied to
+// the front's other columns, the panel's U block (rows jb..jb+nb-1) is
+// solved with the panel's unit lower triangle, and the trailing block is
+// updated by a rank-nb product: a warp per pair of columns, their U values
+// in registers, the panel rows read from shared memory.  In place in the
+// work buffer; pivots 1-based within the front.
+__global__ void __launch_bounds__(sp::kThreads) k_sp_factor_blk(
     const int *__restrict__ fronts, int nfr, const SpFront *__restrict__ fr,
     double2 *__restrict__ work, int64_t *__restrict__ piv, int *__restrict__ info) {
+  extern __shared__ double2 P[];  // panel: P[r + c * pr], r < pr = n - jb, c < nb
   __shared__ double red_v[sp::kThreads / 32];
   __shared__ int red_i[sp::kThreads / 32];
-  __shared__ int pivrow;
+  __shared__ int swp[sp::kNb];
   const int b = blockIdx.x;
   if (b >= nfr) return;
   const int t = fronts[b];
   const SpFront f = fr[t];
   const int k = f.k, n = f.k + f.m;
   double2 *F = work + f.work0;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int j = 0; j < k; j++) {
-    // pivot: largest |F(r, j)| over the fully summed rows r in [j, k)
-    double best = -1.0;
-    int bi = j;
-    for (int r = j + tid; r < k; r += blockDim.x) {
-      const double2 v = F[r + (long long)j * n];
-      const double a = fabs(v.x) + fabs(v.y);
-      if (a > best) {
-        best = a;
-        bi = r;
-      }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ob > best || (ob == best && oi < bi)) {
-        best = ob;
-        bi = oi;
-      }
-    }
-    if (lane == 0) {
-      red_v[warp] = best;
-      red_i[warp] = bi;
-    }
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = (int)(blockDim.x >> 5);
+  for (int jb = 0; jb < k; jb += sp::kNb) {
+    const int nb = min(sp::kNb, k - jb), pr = n - jb, kr = k - jb;
+    // 1. the panel to shared memory
+    for (int c = 0; c < nb; c++)
+      for (int r = tid; r < pr; r += blockDim.x) P[r + c * pr] = F[jb + r + (long long)(jb + c) * n];
     __syncthreads();
-    if (tid == 0) {
-      double bb = -1.0;
-      int ii = j;
-      for (int w = 0; w < (int)(blockDim.x / 32); w++)
-        if (red_v[w] > bb || (red_v[w] == bb && red_i[w] < ii)) {
-          bb = red_v[w];
-          ii = red_i[w];
+    // 2. unblocked LU of the panel; pivots among its first kr rows
+    for (int j = 0; j < nb; j++) {
+      double best = -1.0;
+      int bi = j;
+      for (int r = j + tid; r < kr; r += blockDim.x) {
+        const double2 v = P[r + j * pr];
+        const double a = fabs(v.x) + fabs(v.y);
+        if (a > best) {
+          best = a;
+          bi = r;
         }
-      pivrow = ii;
-      piv[f.own0 + j] = ii + 1;
-      if (bb <= 0.0) atomicCAS(info, 0, t + 1);
-    }
-    __syncthreads();
-    const int pr = pivrow;
-    if (pr != j)
-      for (int cidx = tid; cidx < n; cidx += blockDim.x) {
-        double2 *a = F + j + (long long)cidx * n, *bq = F + pr + (long long)cidx * n;
-        const double2 x = *a;
-        *a = *bq;
-        *bq = x;
       }
-    __syncthreads();
-    const double2 d = F[j + (long long)j * n];
-    const bool zero = d.x == 0.0 && d.y == 0.0;
-    // column j below the diagonal: L(r, j) = F(r, j) / F(j, j)
-    for (int r = j + 1 + tid; r < n; r += blockDim.x) {
-      double2 *a = F + r + (long long)j * n;
-      *a = zero ? make_double2(0.0, 0.0) : cdiv(*a, d);
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      if (lane == 0) {
+        red_v[warp] = best;
+        red_i[warp] = bi;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        double bb = -1.0;
+        int ii = j;
+        for (int w = 0; w < nw; w++)
+          if (red_v[w] > bb || (red_v[w] == bb && red_i[w] < ii)) {
+            bb = red_v[w];
+            ii = red_i[w];
+          }
+        swp[j] = ii;
+        piv[f.own0 + jb + j] = jb + ii + 1;
+        if (bb <= 0.0) atomicCAS(info, 0, t + 1);
+      }
+      __syncthreads();
+      const int pj = swp[j];
+      if (pj != j)
+        for (int c = tid; c < nb; c += blockDim.x) {
+          const double2 x = P[j + c * pr];
+          P[j + c * pr] = P[pj + c * pr];
+          P[pj + c * pr] = x;
+        }
+      __syncthreads();
+      const double2 d = P[j + j * pr];
+      const bool zero = d.x == 0.0 && d.y == 0.0;
+      for (int r = j + 1 + tid; r < pr; r += blockDim.x)
+        P[r + j * pr] = zero ? make_double2(0.0, 0.0) : cdiv(P[r + j * pr], d);
+      __syncthreads();
+      for (int c = j + 1; c < nb; c++) {
+        const double2 u = P[j + c * pr];
+        for (int r = j + 1 + tid; r < pr; r += blockDim.x)
+          P[r + c * pr] = cfms(P[r + c * pr], P[r + j * pr], u);
+      }
+      __syncthreads();
+    }
+    // 3. the panel back; 4. its interchanges on the other columns
+    for (int c = 0; c < nb; c++)
+      for (int r = tid; r < pr; r += blockDim.x) F[jb + r + (long long)(jb + c) * n] = P[r + c * pr];
+    for (int c = tid; c < n - nb; c += blockDim.x) {
+      double2 *col = F + (long long)(c < jb ? c : c + nb) * n + jb;
+      for (int j = 0; j < nb; j++) {
+        const int pj = swp[j];
+        if (pj != j) {
+          const double2 x = col[j];
+          col[j] = col[pj];
+          col[pj] = x;
+        }
+      }
     }
     __syncthreads();
-    // rank-1 update of the trailing block: a warp per column
-    for (int cc = j + 1 + warp; cc < n; cc += (int)(blockDim.x >> 5)) {
-      const double2 u = F[j + (long long)cc * n];
-      double2 *col = F + (long long)cc * n;
-      const double2 *lj = F + (long long)j * n;
-      for (int r = j + 1 + lane; r < n; r += 32) col[r] = cfms(col[r], lj[r], u);
+    // 5. the U block: unit lower solve with the panel's top nb x nb triangle
+    for (int cc = jb + nb + tid; cc < n; cc += blockDim.x) {
+      double2 *col = F + (long long)cc * n + jb;
+      double2 x[sp::kNb];
+#pragma unroll
+      for (int i = 0; i < sp::kNb; i++) x[i] = i < nb ? col[i] : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int i = 1; i < sp::kNb; i++)
+#pragma unroll
+        for (int j = 0; j < i; j++) x[i] = cfms(x[i], P[i + j * pr], x[j]);
+#pragma unroll
+      for (int i = 0; i < sp::kNb; i++)
+        if (i < nb) col[i] = x[i];
+    }
+    __syncthreads();
+    // 6. trailing update, rows and columns from jb + nb
+    const int c0 = jb + nb;
+    for (int cp = c0 + 2 * warp; cp < n; cp += 2 * nw) {
+      const bool two = cp + 1 < n;
+      double2 u0[sp::kNb], u1[sp::kNb];
+#pragma unroll
+      for (int j = 0; j < sp::kNb; j++) {
+        u0[j] = j < nb ? F[jb + j + (long long)cp * n] : make_double2(0.0, 0.0);
+        u1[j] = (two && j < nb) ? F[jb + j + (long long)(cp + 1) * n] : make_double2(0.0, 0.0);
+      }
+      double2 *col0 = F + (long long)cp * n, *col1 = col0 + n;
+      for (int r = c0 + lane; r < n; r += 32) {
+        double2 a0 = col0[r], a1 = two ? col1[r] : make_double2(0.0, 0.0);
+        const double2 *pl = P + (r - jb);
+#pragma unroll
+        for (int j = 0; j < sp::kNb; j++) {
+          const double2 l = j < nb ? pl[j * pr] : make_double2(0.0, 0.0);
+          a0 = cfms(a0, l, u0[j]);
+          a1 = cfms(a1, l, u1[j]);
+        }
+        col0[r] = a0;
+        if (two) col1[r] = a1;
+      }
     }
     __syncthreads();
   }
@@ -531,9 +616,10 @@ __global__ void k_sp_store(const int *__restrict__ fronts, const SpFront *__rest
   const long long n = (long long)f.k + f.m;
   const double2 *F = work + f.work0;
   double2 *L = fac + f.fac0, *U = L + n * f.k;
-  for (long long q = threadIdx.x; q < n * f.k; q += blockDim.x) L[q] = F[q];
+  const long long stride = (long long)gridDim.y * blockDim.x;
+  for (long long q = blockIdx.y * blockDim.x + threadIdx.x; q < n * f.k; q += stride) L[q] = F[q];
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int j = threadIdx.x >> 5; j < f.m; j += nw)
+  for (int j = blockIdx.y * nw + (threadIdx.x >> 5); j < f.m; j += gridDim.y * nw)
     for (int i = lane; i < f.k; i += 32) U[i + (long long)j * f.k] = F[i + (f.k + j) * n];
 }
 
@@ -706,6 +792,46 @@ __global__ void __launch_bounds__(sp::kThreads) k_sp_bwd_t(
   }
 }
 
+// library path of the solve: the rows of one front's own or boundary DOFs
+// gathered into a dense block [nrhs][len] (ld len), scattered back (mode 0:
+// set, 1: subtract), and the front's row interchanges (inverse: reverse order)
+__global__ void k_sp_gather(const int *__restrict__ idx, int len, const double2 *__restrict__ x,
+                            int ndof, int nrhs, double2 *__restrict__ blk) {
+  const long long tot = (long long)len * nrhs;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < tot;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % len), r = (int)(q / len);
+    blk[q] = x[(long long)r * ndof + idx[i]];
+  }
+}
+
+__global__ void k_sp_scatter(const int *__restrict__ idx, int len, const double2 *__restrict__ blk,
+                             int ndof, int nrhs, double2 *__restrict__ x, int sub) {
+  const long long tot = (long long)len * nrhs;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < tot;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % len), r = (int)(q / len);
+    double2 *o = x + (long long)r * ndof + idx[i];
+    const double2 v = blk[q];
+    *o = sub ? make_double2(o->x - v.x, o->y - v.y) : v;
+  }
+}
+
+__global__ void k_sp_swap_rows(double2 *blk, int len, int nrhs, const int64_t *piv, int inverse) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrhs; r += gridDim.x * blockDim.x) {
+    double2 *col = blk + (long long)r * len;
+    for (int jj = 0; jj < len; jj++) {
+      const int j = inverse ? len - 1 - jj : jj;
+      const int p = (int)piv[j] - 1;
+      if (p != j) {
+        const double2 t = col[j];
+        col[j] = col[p];
+        col[p] = t;
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host drivers
 // ---------------------------------------------------------------------------
@@ -714,7 +840,8 @@ void free_sparse(Ctx *c) {
   if (!s) return;
   void *ptrs[] = {s->d_fr,      s->d_own,     s->d_bnd,     s->d_ea,      s->d_lev_fronts,
                   s->d_ent_idx, s->d_ent_loc, s->d_fac,     s->d_piv,     s->d_work[0],
-                  s->d_work[1], s->d_info,    s->dwork,     s->d_getrf_info};
+                  s->d_work[1], s->d_info,    s->dwork,     s->d_getrf_info, s->d_sx,
+                  s->d_sy};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (s->par) cusolverDnDestroyParams(s->par);
@@ -762,6 +889,9 @@ int sparse_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *ms
     if (r) return r;
   }
   if (!s->sol) {
+    SPCK(cudaFuncSetAttribute(k_sp_factor_blk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(sizeof(double2) * sp::kSmallN * sp::kNb)),
+         "kernel attributes");
     if (cusolverDnCreate(&s->sol) != CUSOLVER_STATUS_SUCCESS ||
         cusolverDnCreateParams(&s->par) != CUSOLVER_STATUS_SUCCESS ||
         cublasCreate(&s->blas) != CUBLAS_STATUS_SUCCESS) {
@@ -797,29 +927,21 @@ int sparse_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *ms
       k_sp_assemble<<<grid, 256, 0, st>>>(ne, s->d_ent_idx + s->lev_ent0[l],
                                           s->d_ent_loc + s->lev_ent0[l], csr, W);
     }
+    // more CTAs per front where the level has few fronts
+    const unsigned ysplit = (unsigned)std::max(1, std::min(64, 2 * nsm / std::max(nfl, 1)));
     if (l + 1 < s->nlevel)
       for (int slot = 0; slot < 2; slot++)
-        k_sp_extend_add<<<nfl, 256, 0, st>>>(dfr, s->d_fr, s->d_ea, Wc, W, slot);
+        k_sp_extend_add<<<dim3(nfl, ysplit), 256, 0, st>>>(dfr, s->d_fr, s->d_ea, Wc, W, slot);
     SPCK(cudaGetLastError(), "assembly");
-    // small fronts: one CTA each; large ones: dense library calls
-    std::vector<int> small, large;
-    for (int t : s->lev[l]) (s->fr[t].k + s->fr[t].m <= sp::kSmallN ? small : large).push_back(t);
-    if (!small.empty()) {
-      if (small.size() == s->lev[l].size()) {
-        k_sp_factor_small<<<nfl, sp::kThreads, 0, st>>>(dfr, nfl, s->d_fr, W, s->d_piv, s->d_info);
-      } else {
-        // a level mixing both kinds: its small fronts' ids go to a scratch list
-        int *d_small = nullptr;
-        SPCK(cudaMallocAsync(&d_small, sizeof(int) * small.size(), st), "front list");
-        SPCK(cudaMemcpyAsync(d_small, small.data(), sizeof(int) * small.size(),
-                             cudaMemcpyHostToDevice, st), "front list");
-        k_sp_factor_small<<<(int)small.size(), sp::kThreads, 0, st>>>(d_small, (int)small.size(),
-                                                                      s->d_fr, W, s->d_piv,
-                                                                      s->d_info);
-        SPCK(cudaFreeAsync(d_small, st), "front list");
-      }
+    // one CTA per front up to kSmallN rows; larger fronts: dense library calls
+    const int nsmall = s->lev_nsmall[l];
+    if (nsmall > 0) {
+      const size_t sm = sizeof(double2) * (size_t)s->lev_nmax_small[l] * sp::kNb;
+      k_sp_factor_blk<<<nsmall, sp::kThreads, sm, st>>>(dfr, nsmall, s->d_fr, W, s->d_piv,
+                                                         s->d_info);
       SPCK(cudaGetLastError(), "small fronts");
     }
+    std::vector<int> large(s->lev[l].begin() + nsmall, s->lev[l].end());
     for (int t : large) {
       const SpFront &f = s->fr[t];
       const int64_t n = (int64_t)f.k + f.m, k = f.k, m = f.m;
@@ -865,7 +987,7 @@ int sparse_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *ms
         }
       }
     }
-    k_sp_store<<<nfl, 256, 0, st>>>(dfr, s->d_fr, W, s->d_fac);
+    k_sp_store<<<dim3(nfl, ysplit), 256, 0, st>>>(dfr, s->d_fr, W, s->d_fac);
     SPCK(cudaGetLastError(), "factor store");
   }
   // zero pivots of any front
@@ -881,35 +1003,126 @@ int sparse_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *ms
   return 0;
 }
 
+// One front of the library path: the forward (fwd = 1) or backward step of
+// op(A) X = B with the front's factors, through gathered dense blocks.
+static int solve_front_lib(Ctx *c, SparseLU *s, const SpFront &f, double2 *x, int nrhs, int trans,
+                           bool fwd, cudaStream_t st, std::string *msg) {
+  const int k = f.k, m = f.m, n = k + m, ndof = c->ndof;
+  if (k == 0) return 0;
+  const size_t need_x = (size_t)k * nrhs, need_y = (size_t)std::max(m, 1) * nrhs;
+  if (need_x > s->sx_cap) {
+    if (s->d_sx) SPCK(cudaFree(s->d_sx), "solve scratch");
+    s->d_sx = nullptr;
+    SPCK(cudaMalloc(&s->d_sx, sizeof(double2) * need_x), "solve scratch");
+    s->sx_cap = need_x;
+  }
+  if (need_y > s->sy_cap) {
+    if (s->d_sy) SPCK(cudaFree(s->d_sy), "solve scratch");
+    s->d_sy = nullptr;
+    SPCK(cudaMalloc(&s->d_sy, sizeof(double2) * need_y), "solve scratch");
+    s->sy_cap = need_y;
+  }
+  const int *own = s->d_own + f.own0, *bnd = s->d_bnd + f.bnd0;
+  const int64_t *piv = s->d_piv + f.own0;
+  cuDoubleComplex *X = reinterpret_cast<cuDoubleComplex *>(s->d_sx);
+  cuDoubleComplex *Y = reinterpret_cast<cuDoubleComplex *>(s->d_sy);
+  const cuDoubleComplex *F = reinterpret_cast<const cuDoubleComplex *>(s->d_fac + f.fac0);
+  const cuDoubleComplex *U12 = F + (size_t)n * k;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), mone = make_cuDoubleComplex(-1.0, 0.0),
+                        zero = make_cuDoubleComplex(0.0, 0.0);
+  const cublasOperation_t op = trans == 1 ? CUBLAS_OP_T : CUBLAS_OP_C;
+  const int g = 256, gb = (int)std::min<long long>(((long long)std::max(k, m) * nrhs + g - 1) / g, 4096);
+  k_sp_gather<<<gb, g, 0, st>>>(own, k, x, ndof, nrhs, s->d_sx);
+  bool ok = true;
+  if (trans == 0 && fwd) {
+    k_sp_swap_rows<<<(nrhs + 63) / 64, 64, 0, st>>>(s->d_sx, k, nrhs, piv, 0);
+    ok = !cublasZtrsm(s->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                      CUBLAS_DIAG_UNIT, k, nrhs, &one, F, n, X, k);
+    if (ok && m > 0)
+      ok = !cublasZgemm(s->blas, CUBLAS_OP_N, CUBLAS_OP_N, m, nrhs, k, &one, F + k, n, X, k, &zero,
+                        Y, m);
+  } else if (trans == 0) {
+    if (m > 0) {
+      k_sp_gather<<<gb, g, 0, st>>>(bnd, m, x, ndof, nrhs, s->d_sy);
+      ok = !cublasZgemm(s->blas, CUBLAS_OP_N, CUBLAS_OP_N, k, nrhs, m, &mone, U12, k, Y, m, &one,
+                        X, k);
+    }
+    if (ok)
+      ok = !cublasZtrsm(s->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                        CUBLAS_DIAG_NON_UNIT, k, nrhs, &one, F, n, X, k);
+  } else if (fwd) {
+    ok = !cublasZtrsm(s->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, op, CUBLAS_DIAG_NON_UNIT,
+                      k, nrhs, &one, F, n, X, k);
+    if (ok && m > 0)
+      ok = !cublasZgemm(s->blas, op, CUBLAS_OP_N, m, nrhs, k, &one, U12, k, X, k, &zero, Y, m);
+  } else {
+    if (m > 0) {
+      k_sp_gather<<<gb, g, 0, st>>>(bnd, m, x, ndof, nrhs, s->d_sy);
+      ok = !cublasZgemm(s->blas, op, CUBLAS_OP_N, k, nrhs, m, &mone, F + k, n, Y, m, &one, X, k);
+    }
+    if (ok)
+      ok = !cublasZtrsm(s->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, op, CUBLAS_DIAG_UNIT, k,
+                        nrhs, &one, F, n, X, k);
+    if (ok) k_sp_swap_rows<<<(nrhs + 63) / 64, 64, 0, st>>>(s->d_sx, k, nrhs, piv, 1);
+  }
+  if (!ok) {
+    *msg = "sparse solve: trsm / gemm failed";
+    return FEM25_ERR_CUDA;
+  }
+  k_sp_scatter<<<gb, g, 0, st>>>(own, k, s->d_sx, ndof, nrhs, x, 0);
+  if (fwd && m > 0) k_sp_scatter<<<gb, g, 0, st>>>(bnd, m, s->d_sy, ndof, nrhs, x, 1);
+  SPCK(cudaGetLastError(), "solve");
+  return 0;
+}
+
 int sparse_solve(Ctx *c, int nrhs, int trans, double *rhs, cudaStream_t st, std::string *msg) {
   SparseLU *s = c->sparse;
   if (!s || !s->factored) {
     *msg = "sparse solve: no factorisation (call fem25_sparse_factor_dev first)";
     return FEM25_ERR_ARG;
   }
+  if (cublasSetStream(s->blas, st) != CUBLAS_STATUS_SUCCESS) {
+    *msg = "sparse solve: cannot set the library stream";
+    return FEM25_ERR_CUDA;
+  }
   double2 *x = reinterpret_cast<double2 *>(rhs);
   const int nchunk = (nrhs + sp::kRhsPerCta - 1) / sp::kRhsPerCta;
-  for (int l = s->nlevel - 1; l >= 0; l--) {
-    const dim3 grid((unsigned)s->lev[l].size(), (unsigned)nchunk);
-    const int *dfr = s->d_lev_fronts + s->lev_off[l];
-    if (trans == 0)
-      k_sp_fwd<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac, s->d_piv,
-                                              x, c->ndof, nrhs);
-    else
-      k_sp_fwd_t<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac, x,
-                                                c->ndof, nrhs, trans == 2);
+  // fronts up to kSmallN rows: one CTA each per level (atomics on the shared
+  // boundary rows); larger fronts: dense library calls, one front at a time
+  for (int pass = 0; pass < 2; pass++) {
+    const bool fwd = pass == 0;
+    for (int li = 0; li < s->nlevel; li++) {
+      const int l = fwd ? s->nlevel - 1 - li : li;
+      const int nsmall = s->lev_nsmall[l];
+      const int *dfr = s->d_lev_fronts + s->lev_off[l];
+      if (!fwd)  // root side first going back: the large fronts of the level
+        for (size_t q = nsmall; q < s->lev[l].size(); q++) {
+          const int r = solve_front_lib(c, s, s->fr[s->lev[l][q]], x, nrhs, trans, fwd, st, msg);
+          if (r) return r;
+        }
+      if (nsmall > 0) {
+        const dim3 grid((unsigned)nsmall, (unsigned)nchunk);
+        if (fwd && trans == 0)
+          k_sp_fwd<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac,
+                                                  s->d_piv, x, c->ndof, nrhs);
+        else if (fwd)
+          k_sp_fwd_t<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac, x,
+                                                    c->ndof, nrhs, trans == 2);
+        else if (trans == 0)
+          k_sp_bwd<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac, x,
+                                                  c->ndof, nrhs);
+        else
+          k_sp_bwd_t<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac,
+                                                    s->d_piv, x, c->ndof, nrhs, trans == 2);
+        SPCK(cudaGetLastError(), "solve");
+      }
+      if (fwd)
+        for (size_t q = nsmall; q < s->lev[l].size(); q++) {
+          const int r = solve_front_lib(c, s, s->fr[s->lev[l][q]], x, nrhs, trans, fwd, st, msg);
+          if (r) return r;
+        }
+    }
   }
-  for (int l = 0; l < s->nlevel; l++) {
-    const dim3 grid((unsigned)s->lev[l].size(), (unsigned)nchunk);
-    const int *dfr = s->d_lev_fronts + s->lev_off[l];
-    if (trans == 0)
-      k_sp_bwd<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac, x,
-                                              c->ndof, nrhs);
-    else
-      k_sp_bwd_t<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac,
-                                                s->d_piv, x, c->ndof, nrhs, trans == 2);
-  }
-  SPCK(cudaGetLastError(), "solve");
   return 0;
 }
 
