@@ -29,10 +29,10 @@
 // by the context; the update blocks live until the parent level has consumed
 // them (two work buffers, alternating).
 //
-// Solve (device), level by level: forward elimination from the leaves, back
-// substitution from the root, for op(A) = A, A^T (MUMPS ICNTL(9) != 1) or
-// A^H; a CTA per (front, group of right-hand sides) up to kSmallN rows,
-// gathered dense blocks and cuBLAS trsm / gemm for the larger fronts.
+// Solve (device), one launch per level: forward elimination from the leaves,
+// back substitution from the root, for op(A) = A, A^T (MUMPS ICNTL(9) != 1)
+// or A^H; a CTA per (front, group of right-hand sides), the triangles solved
+// in blocks of 32 rows.
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 
@@ -70,6 +70,7 @@ struct SparseLU {
   std::vector<SpFront> fr;
   std::vector<std::vector<int>> lev;        // front ids per level, one-CTA fronts first
   std::vector<int> lev_nsmall, lev_nmax_small;  // per level: one-CTA fronts, their largest order
+  std::vector<int> lev_kmax, lev_mmax;          // per level: largest own and boundary counts
   std::vector<long long> lev_work;          // work elements per level
   std::vector<long long> lev_ent0;          // first CSR-entry record of each level
   long long fac_elems = 0, max_work = 0;
@@ -91,10 +92,6 @@ struct SparseLU {
   size_t dwork_bytes = 0;
   std::vector<char> hwork;
   int *d_getrf_info = nullptr;
-  // solve scratch of the library-path fronts: own rows and boundary rows of
-  // the right-hand sides, [nrhs][k] and [nrhs][m]
-  double2 *d_sx = nullptr, *d_sy = nullptr;
-  size_t sx_cap = 0, sy_cap = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -356,6 +353,12 @@ static int sparse_analyse(Ctx *c, SparseLU *s, cudaStream_t st, std::string *msg
   // one-CTA fronts first in each level's list
   s->lev_nsmall.assign(nlev, 0);
   s->lev_nmax_small.assign(nlev, 0);
+  s->lev_kmax.assign(nlev, 0);
+  s->lev_mmax.assign(nlev, 0);
+  for (int t = 0; t < nf; t++) {
+    s->lev_kmax[b.fr[t].level] = std::max(s->lev_kmax[b.fr[t].level], b.fr[t].k);
+    s->lev_mmax[b.fr[t].level] = std::max(s->lev_mmax[b.fr[t].level], b.fr[t].m);
+  }
   for (int l = 0; l < nlev; l++) {
     std::stable_partition(s->lev[l].begin(), s->lev[l].end(), [&](int t) {
       return b.fr[t].k + b.fr[t].m <= sp::kSmallN;
@@ -626,23 +629,57 @@ __global__ void k_sp_store(const int *__restrict__ fronts, const SpFront *__rest
 // ---------------------------------------------------------------------------
 // solve (device): x is [nrhs][NDOF]
 // ---------------------------------------------------------------------------
-// forward step of one front for op(A) = A: pivots, L11 solve, boundary update
-__global__ void __launch_bounds__(sp::kThreads) k_sp_fwd(
-    const int *__restrict__ fronts, const SpFront *__restrict__ fr,
-    const int *__restrict__ own, const int *__restrict__ bnd, const double2 *__restrict__ fac,
-    const int64_t *__restrict__ piv, double2 *__restrict__ x, int ndof, int nrhs) {
-  const SpFront f = fr[fronts[blockIdx.x]];
-  const int r0 = blockIdx.y * sp::kRhsPerCta, nr = min(sp::kRhsPerCta, nrhs - r0);
+// The triangular solves of one front, blocked by 32 rows: warp 0 solves the
+// 32 x 32 diagonal triangle of a block with the block's right-hand-side
+// values in registers (lane = row; values passed on by shuffles), the CTA
+// then updates the rows still to come with the solved block (kept in shared
+// memory): two CTA barriers per 32 rows.  Row r of the own block is the DOF
+// own[r]; the right-hand sides [r0, r0 + nr) of x (one CTA per group of
+// kRhsPerCta).
+//   op(A) = A    forward: interchanges, L11 (unit lower), x_b -= L21 x_own
+//                backward: x_own -= U12 x_b, U11 (upper)
+//   A^T / A^H    forward: U11^op (lower), x_b -= U12^op x_own
+//                backward: x_own -= L21^op x_b, L11^op (unit upper), inverse
+//                interchanges
+// The boundary rows x_b of a front belong to ancestors; fronts of one level
+// may share them, so the forward updates add with atomics.
+struct SolveArgs {
+  const int *fronts;
+  const SpFront *fr;
+  const int *own, *bnd;
+  const double2 *fac;
+  const int64_t *piv;
+  double2 *x;
+  int ndof, nrhs, trans;  // trans 0: A, 1: A^T, 2: A^H
+};
+
+__device__ __forceinline__ double2 sp_op(double2 v, int trans) {
+  return trans == 2 ? cconj(v) : v;
+}
+
+// element (i, j) of op(T) for the front's F11 (ld n) or L21 rows: op(T)(i, j)
+// = T(i, j) for A, T(j, i) (conjugated for A^H) for A^T / A^H
+__device__ __forceinline__ double2 sp_el(const double2 *T, long long n, int i, int j, int trans) {
+  return trans == 0 ? T[i + (long long)j * n] : sp_op(T[j + (long long)i * n], trans);
+}
+
+template <int R>
+__global__ void __launch_bounds__(sp::kThreads) k_sp_solve_fwd(SolveArgs a) {
+  __shared__ double2 xs[32][R];
+  __shared__ double2 tb[32][33];  // the block's diagonal triangle, op applied
+  const SpFront f = a.fr[a.fronts[blockIdx.x]];
+  const int r0 = blockIdx.y * R, nr = min(R, a.nrhs - r0);
   if (nr <= 0 || f.k == 0) return;
   const long long n = (long long)f.k + f.m;
-  const int *ow = own + f.own0;
-  const double2 *L = fac + f.fac0;
-  const int tid = threadIdx.x;
-  // row interchanges (sequential in j, one thread per right-hand side)
-  if (tid < nr) {
-    double2 *xr = x + (long long)(r0 + tid) * ndof;
-    for (int j = 0; j < f.k; j++) {
-      const int p = (int)piv[f.own0 + j] - 1;
+  const int k = f.k, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int *ow = a.own + f.own0;
+  const double2 *F = a.fac + f.fac0;          // F11 and L21, ld n
+  double2 *x = a.x + (long long)r0 * a.ndof;
+  const int tr = a.trans;
+  if (tr == 0 && tid < nr) {  // row interchanges of P
+    double2 *xr = x + (long long)tid * a.ndof;
+    for (int j = 0; j < k; j++) {
+      const int p = (int)a.piv[f.own0 + j] - 1;
       if (p != j) {
         const double2 t = xr[ow[j]];
         xr[ow[j]] = xr[ow[p]];
@@ -651,182 +688,202 @@ __global__ void __launch_bounds__(sp::kThreads) k_sp_fwd(
     }
   }
   __syncthreads();
-  // L11 (unit lower), column by column
-  for (int j = 0; j < f.k; j++) {
-    for (int s = 0; s < nr; s++) {
-      double2 *xr = x + (long long)(r0 + s) * ndof;
-      const double2 xj = xr[ow[j]];
-      for (int r = j + 1 + tid; r < f.k; r += blockDim.x)
-        xr[ow[r]] = cfms(xr[ow[r]], L[r + j * n], xj);
+  // lower triangle T: L11 (unit) for A, U11^op (non-unit) for A^T / A^H
+  for (int jb = 0; jb < k; jb += 32) {
+    const int nb = min(32, k - jb);
+    for (int q = tid; q < nb * nb; q += blockDim.x) {
+      const int i = q % nb, j = q / nb;
+      if (i > j) tb[i][j] = sp_el(F, n, jb + i, jb + j, tr);
+      if (i == j && tr != 0) tb[i][i] = cdiv(make_double2(1.0, 0.0), sp_el(F, n, jb + i, jb + i, tr));
     }
     __syncthreads();
-  }
-  // boundary rows: x_b -= L21 x_own (other fronts of the level may add to the
-  // same boundary DOF: atomics)
-  for (int q = tid; q < f.m * nr; q += blockDim.x) {
-    const int r = q % f.m, s = q / f.m;
-    const double2 *xr = x + (long long)(r0 + s) * ndof;
-    double2 acc = make_double2(0.0, 0.0);
-    for (int j = 0; j < f.k; j++) acc = cfms(acc, L[f.k + r + j * n], xr[ow[j]]);
-    double *o = reinterpret_cast<double *>(x + (long long)(r0 + s) * ndof + bnd[f.bnd0 + r]);
-    atomicAdd(o, acc.x);
-    atomicAdd(o + 1, acc.y);
-  }
-}
-
-// backward step of one front for op(A) = A: x_own -= U12 x_bnd, U11 solve
-__global__ void __launch_bounds__(sp::kThreads) k_sp_bwd(
-    const int *__restrict__ fronts, const SpFront *__restrict__ fr,
-    const int *__restrict__ own, const int *__restrict__ bnd, const double2 *__restrict__ fac,
-    double2 *__restrict__ x, int ndof, int nrhs) {
-  const SpFront f = fr[fronts[blockIdx.x]];
-  const int r0 = blockIdx.y * sp::kRhsPerCta, nr = min(sp::kRhsPerCta, nrhs - r0);
-  if (nr <= 0 || f.k == 0) return;
-  const long long n = (long long)f.k + f.m;
-  const int *ow = own + f.own0;
-  const double2 *L = fac + f.fac0, *U = L + n * f.k;
-  const int tid = threadIdx.x;
-  for (int q = tid; q < f.k * nr; q += blockDim.x) {
-    const int i = q % f.k, s = q / f.k;
-    double2 *xr = x + (long long)(r0 + s) * ndof;
-    double2 acc = xr[ow[i]];
-    for (int cc = 0; cc < f.m; cc++) acc = cfms(acc, U[i + (long long)cc * f.k], xr[bnd[f.bnd0 + cc]]);
-    xr[ow[i]] = acc;
-  }
-  __syncthreads();
-  for (int j = f.k - 1; j >= 0; j--) {
-    for (int s = tid; s < nr; s += blockDim.x) {
-      double2 *xr = x + (long long)(r0 + s) * ndof;
-      xr[ow[j]] = cdiv(xr[ow[j]], L[j + j * n]);
+    if (warp == 0) {
+      double2 v[R];
+#pragma unroll
+      for (int s = 0; s < R; s++)
+        v[s] = (lane < nb && s < nr) ? x[(long long)s * a.ndof + ow[jb + lane]] : make_double2(0.0, 0.0);
+      for (int i = 0; i < nb; i++) {
+        if (tr != 0 && lane == i) {
+          const double2 d = tb[i][i];  // reciprocal of the diagonal
+#pragma unroll
+          for (int s = 0; s < R; s++) v[s] = cmul(v[s], d);
+        }
+        const double2 tli = (lane > i && lane < nb) ? tb[lane][i] : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int s = 0; s < R; s++) {
+          const double2 xi = make_double2(__shfl_sync(0xffffffffu, v[s].x, i),
+                                          __shfl_sync(0xffffffffu, v[s].y, i));
+          if (lane > i && lane < nb) v[s] = cfms(v[s], tli, xi);
+        }
+      }
+      if (lane < nb)
+#pragma unroll
+        for (int s = 0; s < R; s++)
+          if (s < nr) {
+            x[(long long)s * a.ndof + ow[jb + lane]] = v[s];
+            xs[lane][s] = v[s];
+          }
     }
     __syncthreads();
-    for (int s = 0; s < nr; s++) {
-      double2 *xr = x + (long long)(r0 + s) * ndof;
-      const double2 xj = xr[ow[j]];
-      for (int r = tid; r < j; r += blockDim.x) xr[ow[r]] = cfms(xr[ow[r]], L[r + j * n], xj);
+    for (int r = jb + nb + tid; r < k; r += blockDim.x) {
+      double2 acc[R];
+#pragma unroll
+      for (int s = 0; s < R; s++)
+        acc[s] = s < nr ? x[(long long)s * a.ndof + ow[r]] : make_double2(0.0, 0.0);
+      for (int i = 0; i < nb; i++) {
+        const double2 t = sp_el(F, n, r, jb + i, tr);
+#pragma unroll
+        for (int s = 0; s < R; s++) acc[s] = cfms(acc[s], t, xs[i][s]);
+      }
+#pragma unroll
+      for (int s = 0; s < R; s++)
+        if (s < nr) x[(long long)s * a.ndof + ow[r]] = acc[s];
     }
     __syncthreads();
   }
 }
 
-// forward step for op(A) = A^T (conj = 0) or A^H (conj = 1): U11^T solve,
-// boundary update with U12^T
-__global__ void __launch_bounds__(sp::kThreads) k_sp_fwd_t(
-    const int *__restrict__ fronts, const SpFront *__restrict__ fr,
-    const int *__restrict__ own, const int *__restrict__ bnd, const double2 *__restrict__ fac,
-    double2 *__restrict__ x, int ndof, int nrhs, int conj) {
-  const SpFront f = fr[fronts[blockIdx.x]];
-  const int r0 = blockIdx.y * sp::kRhsPerCta, nr = min(sp::kRhsPerCta, nrhs - r0);
-  if (nr <= 0 || f.k == 0) return;
+// The rectangular part of a front's solve step, spread over CTAs of
+// kThreads rows each (blockIdx.y: row tile, blockIdx.z: group of
+// right-hand sides):
+//   fwd: boundary rows   x_b -= L21 x_own (A), U12^op x_own (A^T / A^H),
+//        added with atomics (fronts of a level share boundary rows)
+//   bwd: own rows        x_own -= U12 x_b (A), L21^op x_b (A^T / A^H)
+// The right-hand-side values of the summed index pass through shared memory
+// in chunks of kThreads, so each thread's dot product streams its matrix row.
+template <int R>
+__global__ void __launch_bounds__(sp::kThreads) k_sp_solve_rect(SolveArgs a, int fwd) {
+  __shared__ double2 xc[sp::kThreads][R];
+  const SpFront f = a.fr[a.fronts[blockIdx.x]];
+  const int r0 = blockIdx.z * R, nr = min(R, a.nrhs - r0);
+  const int rows = fwd ? f.m : f.k, cols = fwd ? f.k : f.m;
+  const int row0 = blockIdx.y * blockDim.x;
+  if (nr <= 0 || row0 >= rows || cols == 0) return;
   const long long n = (long long)f.k + f.m;
-  const int *ow = own + f.own0;
-  const double2 *L = fac + f.fac0, *U = L + n * f.k;
-  const int tid = threadIdx.x;
-  auto op = [&](double2 v) { return conj ? cconj(v) : v; };
-  for (int j = 0; j < f.k; j++) {
-    for (int s = tid; s < nr; s += blockDim.x) {
-      double2 *xr = x + (long long)(r0 + s) * ndof;
-      xr[ow[j]] = cdiv(xr[ow[j]], op(L[j + j * n]));
+  const int k = f.k, tid = threadIdx.x, tr = a.trans;
+  const double2 *F = a.fac + f.fac0, *U12 = F + n * k;
+  const int *rowidx = (fwd ? a.bnd + f.bnd0 : a.own + f.own0);
+  const int *colidx = (fwd ? a.own + f.own0 : a.bnd + f.bnd0);
+  double2 *x = a.x + (long long)r0 * a.ndof;
+  const int r = row0 + tid;
+  double2 acc[R];
+#pragma unroll
+  for (int s = 0; s < R; s++) acc[s] = make_double2(0.0, 0.0);
+  for (int c0 = 0; c0 < cols; c0 += blockDim.x) {
+    const int nc = min((int)blockDim.x, cols - c0);
+    __syncthreads();
+    if (tid < nc) {
+      const int d = colidx[c0 + tid];
+#pragma unroll
+      for (int s = 0; s < R; s++)
+        xc[tid][s] = s < nr ? x[(long long)s * a.ndof + d] : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    for (int s = 0; s < nr; s++) {
-      double2 *xr = x + (long long)(r0 + s) * ndof;
-      const double2 xj = xr[ow[j]];
-      for (int r = j + 1 + tid; r < f.k; r += blockDim.x)
-        xr[ow[r]] = cfms(xr[ow[r]], op(L[j + (long long)r * n]), xj);  // U(j, r)
+    if (r < rows) {
+#pragma unroll 4
+      for (int j = 0; j < nc; j++) {
+        const int c = c0 + j;
+        // element (r, c) of the rectangular block
+        double2 t;
+        if (fwd)
+          t = tr == 0 ? F[k + r + (long long)c * n] : sp_op(U12[c + (long long)r * k], tr);
+        else
+          t = tr == 0 ? U12[r + (long long)c * k] : sp_op(F[k + c + (long long)r * n], tr);
+#pragma unroll
+        for (int s = 0; s < R; s++) acc[s] = cfms(acc[s], t, xc[j][s]);
+      }
     }
-    __syncthreads();
   }
-  for (int q = tid; q < f.m * nr; q += blockDim.x) {
-    const int cc = q % f.m, s = q / f.m;
-    const double2 *xr = x + (long long)(r0 + s) * ndof;
-    double2 acc = make_double2(0.0, 0.0);
-    for (int i = 0; i < f.k; i++) acc = cfms(acc, op(U[i + (long long)cc * f.k]), xr[ow[i]]);
-    double *o = reinterpret_cast<double *>(x + (long long)(r0 + s) * ndof + bnd[f.bnd0 + cc]);
-    atomicAdd(o, acc.x);
-    atomicAdd(o + 1, acc.y);
-  }
+  if (r >= rows) return;
+  const int d = rowidx[r];
+#pragma unroll
+  for (int s = 0; s < R; s++)
+    if (s < nr) {
+      double2 *o = x + (long long)s * a.ndof + d;
+      if (fwd) {  // acc = -(product)
+        atomicAdd(reinterpret_cast<double *>(o), acc[s].x);
+        atomicAdd(reinterpret_cast<double *>(o) + 1, acc[s].y);
+      } else {
+        *o = make_double2(o->x + acc[s].x, o->y + acc[s].y);
+      }
+    }
 }
 
-// backward step for A^T / A^H: x_own -= L21^T x_bnd, L11^T solve, inverse
-// row interchanges
-__global__ void __launch_bounds__(sp::kThreads) k_sp_bwd_t(
-    const int *__restrict__ fronts, const SpFront *__restrict__ fr,
-    const int *__restrict__ own, const int *__restrict__ bnd, const double2 *__restrict__ fac,
-    const int64_t *__restrict__ piv, double2 *__restrict__ x, int ndof, int nrhs, int conj) {
-  const SpFront f = fr[fronts[blockIdx.x]];
-  const int r0 = blockIdx.y * sp::kRhsPerCta, nr = min(sp::kRhsPerCta, nrhs - r0);
+template <int R>
+__global__ void __launch_bounds__(sp::kThreads) k_sp_solve_bwd(SolveArgs a) {
+  __shared__ double2 xs[32][R];
+  __shared__ double2 tb[32][33];  // the block's diagonal triangle, op applied
+  const SpFront f = a.fr[a.fronts[blockIdx.x]];
+  const int r0 = blockIdx.y * R, nr = min(R, a.nrhs - r0);
   if (nr <= 0 || f.k == 0) return;
   const long long n = (long long)f.k + f.m;
-  const int *ow = own + f.own0;
-  const double2 *L = fac + f.fac0;
-  const int tid = threadIdx.x;
-  auto op = [&](double2 v) { return conj ? cconj(v) : v; };
-  for (int q = tid; q < f.k * nr; q += blockDim.x) {
-    const int i = q % f.k, s = q / f.k;
-    double2 *xr = x + (long long)(r0 + s) * ndof;
-    double2 acc = xr[ow[i]];
-    for (int r = 0; r < f.m; r++) acc = cfms(acc, op(L[f.k + r + (long long)i * n]), xr[bnd[f.bnd0 + r]]);
-    xr[ow[i]] = acc;
-  }
-  __syncthreads();
-  for (int j = f.k - 1; j >= 0; j--) {
-    for (int s = 0; s < nr; s++) {
-      double2 *xr = x + (long long)(r0 + s) * ndof;
-      const double2 xj = xr[ow[j]];
-      for (int r = tid; r < j; r += blockDim.x)
-        xr[ow[r]] = cfms(xr[ow[r]], op(L[j + (long long)r * n]), xj);  // L(j, r)
+  const int k = f.k, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int *ow = a.own + f.own0;
+  const double2 *F = a.fac + f.fac0;
+  double2 *x = a.x + (long long)r0 * a.ndof;
+  const int tr = a.trans;
+  // upper triangle T: U11 (non-unit) for A, L11^op (unit) for A^T / A^H;
+  // blocks of 32 rows from the bottom
+  for (int jb = ((k - 1) / 32) * 32; jb >= 0; jb -= 32) {
+    const int nb = min(32, k - jb);
+    for (int q = tid; q < nb * nb; q += blockDim.x) {
+      const int i = q % nb, j = q / nb;
+      if (i < j) tb[i][j] = sp_el(F, n, jb + i, jb + j, tr);
+      if (i == j && tr == 0) tb[i][i] = cdiv(make_double2(1.0, 0.0), sp_el(F, n, jb + i, jb + i, tr));
+    }
+    __syncthreads();
+    if (warp == 0) {
+      double2 v[R];
+#pragma unroll
+      for (int s = 0; s < R; s++)
+        v[s] = (lane < nb && s < nr) ? x[(long long)s * a.ndof + ow[jb + lane]] : make_double2(0.0, 0.0);
+      for (int i = nb - 1; i >= 0; i--) {
+        if (tr == 0 && lane == i) {
+          const double2 d = tb[i][i];  // reciprocal of the diagonal
+#pragma unroll
+          for (int s = 0; s < R; s++) v[s] = cmul(v[s], d);
+        }
+        const double2 tli = lane < i ? tb[lane][i] : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int s = 0; s < R; s++) {
+          const double2 xi = make_double2(__shfl_sync(0xffffffffu, v[s].x, i),
+                                          __shfl_sync(0xffffffffu, v[s].y, i));
+          if (lane < i) v[s] = cfms(v[s], tli, xi);
+        }
+      }
+      if (lane < nb)
+#pragma unroll
+        for (int s = 0; s < R; s++)
+          if (s < nr) {
+            x[(long long)s * a.ndof + ow[jb + lane]] = v[s];
+            xs[lane][s] = v[s];
+          }
+    }
+    __syncthreads();
+    for (int r = tid; r < jb; r += blockDim.x) {
+      double2 acc[R];
+#pragma unroll
+      for (int s = 0; s < R; s++)
+        acc[s] = s < nr ? x[(long long)s * a.ndof + ow[r]] : make_double2(0.0, 0.0);
+      for (int i = 0; i < nb; i++) {
+        const double2 t = sp_el(F, n, r, jb + i, tr);
+#pragma unroll
+        for (int s = 0; s < R; s++) acc[s] = cfms(acc[s], t, xs[i][s]);
+      }
+#pragma unroll
+      for (int s = 0; s < R; s++)
+        if (s < nr) x[(long long)s * a.ndof + ow[r]] = acc[s];
     }
     __syncthreads();
   }
-  if (tid < nr) {
-    double2 *xr = x + (long long)(r0 + tid) * ndof;
-    for (int j = f.k - 1; j >= 0; j--) {
-      const int p = (int)piv[f.own0 + j] - 1;
+  if (tr != 0 && tid < nr) {  // inverse row interchanges
+    double2 *xr = x + (long long)tid * a.ndof;
+    for (int j = k - 1; j >= 0; j--) {
+      const int p = (int)a.piv[f.own0 + j] - 1;
       if (p != j) {
         const double2 t = xr[ow[j]];
         xr[ow[j]] = xr[ow[p]];
         xr[ow[p]] = t;
-      }
-    }
-  }
-}
-
-// library path of the solve: the rows of one front's own or boundary DOFs
-// gathered into a dense block [nrhs][len] (ld len), scattered back (mode 0:
-// set, 1: subtract), and the front's row interchanges (inverse: reverse order)
-__global__ void k_sp_gather(const int *__restrict__ idx, int len, const double2 *__restrict__ x,
-                            int ndof, int nrhs, double2 *__restrict__ blk) {
-  const long long tot = (long long)len * nrhs;
-  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < tot;
-       q += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(q % len), r = (int)(q / len);
-    blk[q] = x[(long long)r * ndof + idx[i]];
-  }
-}
-
-__global__ void k_sp_scatter(const int *__restrict__ idx, int len, const double2 *__restrict__ blk,
-                             int ndof, int nrhs, double2 *__restrict__ x, int sub) {
-  const long long tot = (long long)len * nrhs;
-  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < tot;
-       q += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(q % len), r = (int)(q / len);
-    double2 *o = x + (long long)r * ndof + idx[i];
-    const double2 v = blk[q];
-    *o = sub ? make_double2(o->x - v.x, o->y - v.y) : v;
-  }
-}
-
-__global__ void k_sp_swap_rows(double2 *blk, int len, int nrhs, const int64_t *piv, int inverse) {
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrhs; r += gridDim.x * blockDim.x) {
-    double2 *col = blk + (long long)r * len;
-    for (int jj = 0; jj < len; jj++) {
-      const int j = inverse ? len - 1 - jj : jj;
-      const int p = (int)piv[j] - 1;
-      if (p != j) {
-        const double2 t = col[j];
-        col[j] = col[p];
-        col[p] = t;
       }
     }
   }
@@ -840,8 +897,7 @@ void free_sparse(Ctx *c) {
   if (!s) return;
   void *ptrs[] = {s->d_fr,      s->d_own,     s->d_bnd,     s->d_ea,      s->d_lev_fronts,
                   s->d_ent_idx, s->d_ent_loc, s->d_fac,     s->d_piv,     s->d_work[0],
-                  s->d_work[1], s->d_info,    s->dwork,     s->d_getrf_info, s->d_sx,
-                  s->d_sy};
+                  s->d_work[1], s->d_info,    s->dwork,     s->d_getrf_info};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (s->par) cusolverDnDestroyParams(s->par);
@@ -1003,76 +1059,25 @@ int sparse_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *ms
   return 0;
 }
 
-// One front of the library path: the forward (fwd = 1) or backward step of
-// op(A) X = B with the front's factors, through gathered dense blocks.
-static int solve_front_lib(Ctx *c, SparseLU *s, const SpFront &f, double2 *x, int nrhs, int trans,
-                           bool fwd, cudaStream_t st, std::string *msg) {
-  const int k = f.k, m = f.m, n = k + m, ndof = c->ndof;
-  if (k == 0) return 0;
-  const size_t need_x = (size_t)k * nrhs, need_y = (size_t)std::max(m, 1) * nrhs;
-  if (need_x > s->sx_cap) {
-    if (s->d_sx) SPCK(cudaFree(s->d_sx), "solve scratch");
-    s->d_sx = nullptr;
-    SPCK(cudaMalloc(&s->d_sx, sizeof(double2) * need_x), "solve scratch");
-    s->sx_cap = need_x;
+// the level-by-level launches of one solve, R right-hand sides per CTA
+template <int R>
+static void sparse_solve_levels(const SparseLU *s, SolveArgs a, cudaStream_t st) {
+  const unsigned nchunk = (unsigned)((a.nrhs + R - 1) / R);
+  auto tiles = [](int rows) { return (unsigned)std::max(1, (rows + sp::kThreads - 1) / sp::kThreads); };
+  for (int l = s->nlevel - 1; l >= 0; l--) {  // forward, from the leaves
+    a.fronts = s->d_lev_fronts + s->lev_off[l];
+    const unsigned nfl = (unsigned)s->lev[l].size();
+    k_sp_solve_fwd<R><<<dim3(nfl, nchunk), sp::kThreads, 0, st>>>(a);
+    if (s->lev_mmax[l] > 0)
+      k_sp_solve_rect<R><<<dim3(nfl, tiles(s->lev_mmax[l]), nchunk), sp::kThreads, 0, st>>>(a, 1);
   }
-  if (need_y > s->sy_cap) {
-    if (s->d_sy) SPCK(cudaFree(s->d_sy), "solve scratch");
-    s->d_sy = nullptr;
-    SPCK(cudaMalloc(&s->d_sy, sizeof(double2) * need_y), "solve scratch");
-    s->sy_cap = need_y;
+  for (int l = 0; l < s->nlevel; l++) {  // backward, from the root
+    a.fronts = s->d_lev_fronts + s->lev_off[l];
+    const unsigned nfl = (unsigned)s->lev[l].size();
+    if (s->lev_mmax[l] > 0)
+      k_sp_solve_rect<R><<<dim3(nfl, tiles(s->lev_kmax[l]), nchunk), sp::kThreads, 0, st>>>(a, 0);
+    k_sp_solve_bwd<R><<<dim3(nfl, nchunk), sp::kThreads, 0, st>>>(a);
   }
-  const int *own = s->d_own + f.own0, *bnd = s->d_bnd + f.bnd0;
-  const int64_t *piv = s->d_piv + f.own0;
-  cuDoubleComplex *X = reinterpret_cast<cuDoubleComplex *>(s->d_sx);
-  cuDoubleComplex *Y = reinterpret_cast<cuDoubleComplex *>(s->d_sy);
-  const cuDoubleComplex *F = reinterpret_cast<const cuDoubleComplex *>(s->d_fac + f.fac0);
-  const cuDoubleComplex *U12 = F + (size_t)n * k;
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), mone = make_cuDoubleComplex(-1.0, 0.0),
-                        zero = make_cuDoubleComplex(0.0, 0.0);
-  const cublasOperation_t op = trans == 1 ? CUBLAS_OP_T : CUBLAS_OP_C;
-  const int g = 256, gb = (int)std::min<long long>(((long long)std::max(k, m) * nrhs + g - 1) / g, 4096);
-  k_sp_gather<<<gb, g, 0, st>>>(own, k, x, ndof, nrhs, s->d_sx);
-  bool ok = true;
-  if (trans == 0 && fwd) {
-    k_sp_swap_rows<<<(nrhs + 63) / 64, 64, 0, st>>>(s->d_sx, k, nrhs, piv, 0);
-    ok = !cublasZtrsm(s->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
-                      CUBLAS_DIAG_UNIT, k, nrhs, &one, F, n, X, k);
-    if (ok && m > 0)
-      ok = !cublasZgemm(s->blas, CUBLAS_OP_N, CUBLAS_OP_N, m, nrhs, k, &one, F + k, n, X, k, &zero,
-                        Y, m);
-  } else if (trans == 0) {
-    if (m > 0) {
-      k_sp_gather<<<gb, g, 0, st>>>(bnd, m, x, ndof, nrhs, s->d_sy);
-      ok = !cublasZgemm(s->blas, CUBLAS_OP_N, CUBLAS_OP_N, k, nrhs, m, &mone, U12, k, Y, m, &one,
-                        X, k);
-    }
-    if (ok)
-      ok = !cublasZtrsm(s->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
-                        CUBLAS_DIAG_NON_UNIT, k, nrhs, &one, F, n, X, k);
-  } else if (fwd) {
-    ok = !cublasZtrsm(s->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, op, CUBLAS_DIAG_NON_UNIT,
-                      k, nrhs, &one, F, n, X, k);
-    if (ok && m > 0)
-      ok = !cublasZgemm(s->blas, op, CUBLAS_OP_N, m, nrhs, k, &one, U12, k, X, k, &zero, Y, m);
-  } else {
-    if (m > 0) {
-      k_sp_gather<<<gb, g, 0, st>>>(bnd, m, x, ndof, nrhs, s->d_sy);
-      ok = !cublasZgemm(s->blas, op, CUBLAS_OP_N, k, nrhs, m, &mone, F + k, n, Y, m, &one, X, k);
-    }
-    if (ok)
-      ok = !cublasZtrsm(s->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, op, CUBLAS_DIAG_UNIT, k,
-                        nrhs, &one, F, n, X, k);
-    if (ok) k_sp_swap_rows<<<(nrhs + 63) / 64, 64, 0, st>>>(s->d_sx, k, nrhs, piv, 1);
-  }
-  if (!ok) {
-    *msg = "sparse solve: trsm / gemm failed";
-    return FEM25_ERR_CUDA;
-  }
-  k_sp_scatter<<<gb, g, 0, st>>>(own, k, s->d_sx, ndof, nrhs, x, 0);
-  if (fwd && m > 0) k_sp_scatter<<<gb, g, 0, st>>>(bnd, m, s->d_sy, ndof, nrhs, x, 1);
-  SPCK(cudaGetLastError(), "solve");
-  return 0;
 }
 
 int sparse_solve(Ctx *c, int nrhs, int trans, double *rhs, cudaStream_t st, std::string *msg) {
@@ -1081,48 +1086,13 @@ int sparse_solve(Ctx *c, int nrhs, int trans, double *rhs, cudaStream_t st, std:
     *msg = "sparse solve: no factorisation (call fem25_sparse_factor_dev first)";
     return FEM25_ERR_ARG;
   }
-  if (cublasSetStream(s->blas, st) != CUBLAS_STATUS_SUCCESS) {
-    *msg = "sparse solve: cannot set the library stream";
-    return FEM25_ERR_CUDA;
-  }
-  double2 *x = reinterpret_cast<double2 *>(rhs);
-  const int nchunk = (nrhs + sp::kRhsPerCta - 1) / sp::kRhsPerCta;
-  // fronts up to kSmallN rows: one CTA each per level (atomics on the shared
-  // boundary rows); larger fronts: dense library calls, one front at a time
-  for (int pass = 0; pass < 2; pass++) {
-    const bool fwd = pass == 0;
-    for (int li = 0; li < s->nlevel; li++) {
-      const int l = fwd ? s->nlevel - 1 - li : li;
-      const int nsmall = s->lev_nsmall[l];
-      const int *dfr = s->d_lev_fronts + s->lev_off[l];
-      if (!fwd)  // root side first going back: the large fronts of the level
-        for (size_t q = nsmall; q < s->lev[l].size(); q++) {
-          const int r = solve_front_lib(c, s, s->fr[s->lev[l][q]], x, nrhs, trans, fwd, st, msg);
-          if (r) return r;
-        }
-      if (nsmall > 0) {
-        const dim3 grid((unsigned)nsmall, (unsigned)nchunk);
-        if (fwd && trans == 0)
-          k_sp_fwd<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac,
-                                                  s->d_piv, x, c->ndof, nrhs);
-        else if (fwd)
-          k_sp_fwd_t<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac, x,
-                                                    c->ndof, nrhs, trans == 2);
-        else if (trans == 0)
-          k_sp_bwd<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac, x,
-                                                  c->ndof, nrhs);
-        else
-          k_sp_bwd_t<<<grid, sp::kThreads, 0, st>>>(dfr, s->d_fr, s->d_own, s->d_bnd, s->d_fac,
-                                                    s->d_piv, x, c->ndof, nrhs, trans == 2);
-        SPCK(cudaGetLastError(), "solve");
-      }
-      if (fwd)
-        for (size_t q = nsmall; q < s->lev[l].size(); q++) {
-          const int r = solve_front_lib(c, s, s->fr[s->lev[l][q]], x, nrhs, trans, fwd, st, msg);
-          if (r) return r;
-        }
-    }
-  }
+  SolveArgs a{nullptr, s->d_fr, s->d_own, s->d_bnd, s->d_fac, s->d_piv,
+              reinterpret_cast<double2 *>(rhs), c->ndof, nrhs, trans};
+  if (nrhs == 1)
+    sparse_solve_levels<1>(s, a, st);
+  else
+    sparse_solve_levels<sp::kRhsPerCta>(s, a, st);
+  SPCK(cudaGetLastError(), "solve");
   return 0;
 }
 
