@@ -50,6 +50,7 @@ constexpr int kSmallN = 1024;     // fronts up to this many rows: one CTA each
 constexpr int kNb = 8;            // panel width of the one-CTA factorisation
 constexpr int kThreads = 256;
 constexpr int kRhsPerCta = 8;     // right-hand sides per solve CTA
+constexpr int kLanes = 8;         // streams for the library-factored fronts of a level
 }  // namespace sp
 
 struct SpFront {
@@ -62,6 +63,19 @@ struct SpFront {
   long long ea0;        // first entry of its extend-add map (ea[], m entries)
   long long fac0;       // factor store: L block [n][k] (ld n), then U12 [k][m] (ld k)
   long long work0;      // offset of its n x n front in its level's work buffer
+};
+
+// one stream of the library path with its own handles and workspace
+struct SpLane {
+  cudaStream_t st = nullptr;
+  cudaEvent_t done = nullptr;
+  cusolverDnHandle_t sol = nullptr;
+  cusolverDnParams_t par = nullptr;
+  cublasHandle_t blas = nullptr;
+  void *dwork = nullptr;
+  size_t dwork_bytes = 0;
+  std::vector<char> hwork;
+  int *d_getrf_info = nullptr;
 };
 
 struct SparseLU {
@@ -85,13 +99,8 @@ struct SparseLU {
   int64_t *d_piv = nullptr;                 // pivots (1-based within each front), [NDOF]
   double2 *d_work[2] = {nullptr, nullptr};
   int *d_info = nullptr;                    // first zero pivot (front + 1), 0 = none
-  cusolverDnHandle_t sol = nullptr;
-  cusolverDnParams_t par = nullptr;
-  cublasHandle_t blas = nullptr;
-  void *dwork = nullptr;
-  size_t dwork_bytes = 0;
-  std::vector<char> hwork;
-  int *d_getrf_info = nullptr;
+  SpLane lane[sp::kLanes];
+  cudaEvent_t level_ready = nullptr;
 };
 
 // ---------------------------------------------------------------------------
@@ -455,7 +464,7 @@ __global__ void k_sp_extend_add(const int *__restrict__ fronts, const SpFront *_
 // updated by a rank-nb product: a warp per pair of columns, their U values
 // in registers, the panel rows read from shared memory.  In place in the
 // work buffer; pivots 1-based within the front.
-__global__ void __launch_bounds__(sp::kThreads) k_sp_factor_blk(
+__global__ void __launch_bounds__(sp::kThreads, 2) k_sp_factor_blk(
     const int *__restrict__ fronts, int nfr, const SpFront *__restrict__ fr,
     double2 *__restrict__ work, int64_t *__restrict__ piv, int *__restrict__ info) {
   extern __shared__ double2 P[];  // panel: P[r + c * pr], r < pr = n - jb, c < nb
@@ -563,28 +572,21 @@ __global__ void __launch_bounds__(sp::kThreads) k_sp_factor_blk(
         if (i < nb) col[i] = x[i];
     }
     __syncthreads();
-    // 6. trailing update, rows and columns from jb + nb
+    // 6. trailing update, rows and columns from jb + nb: a warp per column
     const int c0 = jb + nb;
-    for (int cp = c0 + 2 * warp; cp < n; cp += 2 * nw) {
-      const bool two = cp + 1 < n;
-      double2 u0[sp::kNb], u1[sp::kNb];
+    for (int cp = c0 + warp; cp < n; cp += nw) {
+      double2 u[sp::kNb];
 #pragma unroll
-      for (int j = 0; j < sp::kNb; j++) {
-        u0[j] = j < nb ? F[jb + j + (long long)cp * n] : make_double2(0.0, 0.0);
-        u1[j] = (two && j < nb) ? F[jb + j + (long long)(cp + 1) * n] : make_double2(0.0, 0.0);
-      }
-      double2 *col0 = F + (long long)cp * n, *col1 = col0 + n;
+      for (int j = 0; j < sp::kNb; j++)
+        u[j] = j < nb ? F[jb + j + (long long)cp * n] : make_double2(0.0, 0.0);
+      double2 *col = F + (long long)cp * n;
       for (int r = c0 + lane; r < n; r += 32) {
-        double2 a0 = col0[r], a1 = two ? col1[r] : make_double2(0.0, 0.0);
+        double2 acc = col[r];
         const double2 *pl = P + (r - jb);
 #pragma unroll
-        for (int j = 0; j < sp::kNb; j++) {
-          const double2 l = j < nb ? pl[j * pr] : make_double2(0.0, 0.0);
-          a0 = cfms(a0, l, u0[j]);
-          a1 = cfms(a1, l, u1[j]);
-        }
-        col0[r] = a0;
-        if (two) col1[r] = a1;
+        for (int j = 0; j < sp::kNb; j++)
+          if (j < nb) acc = cfms(acc, pl[j * pr], u[j]);
+        col[r] = acc;
       }
     }
     __syncthreads();
@@ -897,12 +899,19 @@ void free_sparse(Ctx *c) {
   if (!s) return;
   void *ptrs[] = {s->d_fr,      s->d_own,     s->d_bnd,     s->d_ea,      s->d_lev_fronts,
                   s->d_ent_idx, s->d_ent_loc, s->d_fac,     s->d_piv,     s->d_work[0],
-                  s->d_work[1], s->d_info,    s->dwork,     s->d_getrf_info};
+                  s->d_work[1], s->d_info};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  if (s->par) cusolverDnDestroyParams(s->par);
-  if (s->sol) cusolverDnDestroy(s->sol);
-  if (s->blas) cublasDestroy(s->blas);
+  for (SpLane &ln : s->lane) {
+    if (ln.dwork) cudaFree(ln.dwork);
+    if (ln.d_getrf_info) cudaFree(ln.d_getrf_info);
+    if (ln.par) cusolverDnDestroyParams(ln.par);
+    if (ln.sol) cusolverDnDestroy(ln.sol);
+    if (ln.blas) cublasDestroy(ln.blas);
+    if (ln.done) cudaEventDestroy(ln.done);
+    if (ln.st) cudaStreamDestroy(ln.st);
+  }
+  if (s->level_ready) cudaEventDestroy(s->level_ready);
   delete s;
   c->sparse = nullptr;
 }
@@ -944,21 +953,24 @@ int sparse_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *ms
     const int r = sparse_analyse(c, s, st, msg);
     if (r) return r;
   }
-  if (!s->sol) {
+  if (!s->level_ready) {
     SPCK(cudaFuncSetAttribute(k_sp_factor_blk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)(sizeof(double2) * sp::kSmallN * sp::kNb)),
          "kernel attributes");
-    if (cusolverDnCreate(&s->sol) != CUSOLVER_STATUS_SUCCESS ||
-        cusolverDnCreateParams(&s->par) != CUSOLVER_STATUS_SUCCESS ||
-        cublasCreate(&s->blas) != CUBLAS_STATUS_SUCCESS) {
-      *msg = "sparse solve: cuSOLVER / cuBLAS handle creation failed";
-      return FEM25_ERR_CUDA;
+    SPCK(cudaEventCreateWithFlags(&s->level_ready, cudaEventDisableTiming), "events");
+    for (SpLane &ln : s->lane) {
+      SPCK(cudaStreamCreateWithFlags(&ln.st, cudaStreamNonBlocking), "streams");
+      SPCK(cudaEventCreateWithFlags(&ln.done, cudaEventDisableTiming), "events");
+      SPCK(cudaMalloc(&ln.d_getrf_info, sizeof(int)), "status");
+      if (cusolverDnCreate(&ln.sol) != CUSOLVER_STATUS_SUCCESS ||
+          cusolverDnCreateParams(&ln.par) != CUSOLVER_STATUS_SUCCESS ||
+          cublasCreate(&ln.blas) != CUBLAS_STATUS_SUCCESS ||
+          cusolverDnSetStream(ln.sol, ln.st) != CUSOLVER_STATUS_SUCCESS ||
+          cublasSetStream(ln.blas, ln.st) != CUBLAS_STATUS_SUCCESS) {
+        *msg = "sparse solve: cuSOLVER / cuBLAS handle creation failed";
+        return FEM25_ERR_CUDA;
+      }
     }
-  }
-  if (cusolverDnSetStream(s->sol, st) != CUSOLVER_STATUS_SUCCESS ||
-      cublasSetStream(s->blas, st) != CUBLAS_STATUS_SUCCESS) {
-    *msg = "sparse solve: cannot set the library stream";
-    return FEM25_ERR_CUDA;
   }
   if (!s->d_fac) {
     SPCK(cudaMalloc(&s->d_fac, sizeof(double2) * std::max(s->fac_elems, 1LL)), "factor store");
@@ -966,7 +978,6 @@ int sparse_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *ms
     SPCK(cudaMalloc(&s->d_work[0], sizeof(double2) * std::max(s->max_work, 1LL)), "work");
     SPCK(cudaMalloc(&s->d_work[1], sizeof(double2) * std::max(s->max_work, 1LL)), "work");
     SPCK(cudaMalloc(&s->d_info, sizeof(int)), "status");
-    SPCK(cudaMalloc(&s->d_getrf_info, sizeof(int)), "status");
   }
   SPCK(cudaMemsetAsync(s->d_info, 0, sizeof(int), st), "status");
   const double2 *csr = reinterpret_cast<const double2 *>(csr128);
@@ -998,50 +1009,66 @@ int sparse_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *ms
       SPCK(cudaGetLastError(), "small fronts");
     }
     std::vector<int> large(s->lev[l].begin() + nsmall, s->lev[l].end());
-    for (int t : large) {
+    // the level's large fronts spread over the lanes' streams, joined back
+    // into the caller's stream before the factors are stored
+    const int nl = (int)std::min<size_t>(large.size(), sp::kLanes);
+    if (nl > 0) {
+      SPCK(cudaEventRecord(s->level_ready, st), "events");
+      for (int q = 0; q < nl; q++)
+        SPCK(cudaStreamWaitEvent(s->lane[q].st, s->level_ready, 0), "events");
+    }
+    for (size_t q = 0; q < large.size(); q++) {
+      const int t = large[q];
+      SpLane &ln = s->lane[q % sp::kLanes];
       const SpFront &f = s->fr[t];
       const int64_t n = (int64_t)f.k + f.m, k = f.k, m = f.m;
       if (k == 0) continue;
       double2 *F = W + f.work0;
       size_t dbytes = 0, hbytes = 0;
-      if (cusolverDnXgetrf_bufferSize(s->sol, s->par, k, k, CUDA_C_64F, F, n, CUDA_C_64F, &dbytes,
+      if (cusolverDnXgetrf_bufferSize(ln.sol, ln.par, k, k, CUDA_C_64F, F, n, CUDA_C_64F, &dbytes,
                                       &hbytes) != CUSOLVER_STATUS_SUCCESS) {
         *msg = "sparse solve: getrf workspace query failed";
         return FEM25_ERR_CUDA;
       }
-      if (dbytes > s->dwork_bytes) {
-        if (s->dwork) SPCK(cudaFree(s->dwork), "workspace");
-        s->dwork = nullptr;
-        SPCK(cudaMalloc(&s->dwork, dbytes), "workspace");
-        s->dwork_bytes = dbytes;
+      if (dbytes > ln.dwork_bytes) {
+        // the lane's earlier calls may still use the old workspace
+        SPCK(cudaStreamSynchronize(ln.st), "workspace");
+        if (ln.dwork) SPCK(cudaFree(ln.dwork), "workspace");
+        ln.dwork = nullptr;
+        SPCK(cudaMalloc(&ln.dwork, dbytes), "workspace");
+        ln.dwork_bytes = dbytes;
       }
-      if (hbytes > s->hwork.size()) s->hwork.resize(hbytes);
+      if (hbytes > ln.hwork.size()) ln.hwork.resize(hbytes);
       int64_t *ipiv = s->d_piv + f.own0;
-      if (cusolverDnXgetrf(s->sol, s->par, k, k, CUDA_C_64F, F, n, ipiv, CUDA_C_64F, s->dwork,
-                           dbytes, hbytes ? s->hwork.data() : nullptr, hbytes,
-                           s->d_getrf_info) != CUSOLVER_STATUS_SUCCESS) {
+      if (cusolverDnXgetrf(ln.sol, ln.par, k, k, CUDA_C_64F, F, n, ipiv, CUDA_C_64F, ln.dwork,
+                           dbytes, hbytes ? ln.hwork.data() : nullptr, hbytes,
+                           ln.d_getrf_info) != CUSOLVER_STATUS_SUCCESS) {
         *msg = "sparse solve: getrf failed";
         return FEM25_ERR_CUDA;
       }
       // a zero pivot of this front: recorded as the front's id in the status word
-      k_sp_getrf_status<<<1, 1, 0, st>>>(s->d_getrf_info, s->d_info, t);
+      k_sp_getrf_status<<<1, 1, 0, ln.st>>>(ln.d_getrf_info, s->d_info, t);
       if (m > 0) {
-        k_sp_laswp<<<(int)std::min<int64_t>((m + 127) / 128, 1024), 128, 0, st>>>(
+        k_sp_laswp<<<(int)std::min<int64_t>((m + 127) / 128, 1024), 128, 0, ln.st>>>(
             F, (int)n, (int)k, (int)k, (int)n, ipiv);
         SPCK(cudaGetLastError(), "laswp");
         const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0),
                               mone = make_cuDoubleComplex(-1.0, 0.0);
         cuDoubleComplex *A = reinterpret_cast<cuDoubleComplex *>(F);
-        if (cublasZtrsm(s->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+        if (cublasZtrsm(ln.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
                         CUBLAS_DIAG_UNIT, (int)k, (int)m, &one, A, (int)n, A + k * n, (int)n) ||
-            cublasZtrsm(s->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+            cublasZtrsm(ln.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
                         CUBLAS_DIAG_NON_UNIT, (int)m, (int)k, &one, A, (int)n, A + k, (int)n) ||
-            cublasZgemm(s->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)m, (int)k, &mone, A + k,
+            cublasZgemm(ln.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)m, (int)k, &mone, A + k,
                         (int)n, A + k * n, (int)n, &one, A + k + k * n, (int)n)) {
           *msg = "sparse solve: trsm / gemm failed";
           return FEM25_ERR_CUDA;
         }
       }
+    }
+    for (int q = 0; q < nl; q++) {
+      SPCK(cudaEventRecord(s->lane[q].done, s->lane[q].st), "events");
+      SPCK(cudaStreamWaitEvent(st, s->lane[q].done, 0), "events");
     }
     k_sp_store<<<dim3(nfl, ysplit), 256, 0, st>>>(dfr, s->d_fr, W, s->d_fac);
     SPCK(cudaGetLastError(), "factor store");
