@@ -257,6 +257,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
       int dn[tc::kNodeItems];        // first DOF of the item's node (0: fixed)
       int dref = 0;                  // first DOF of the element's centre node
       double2 vn[tc::kNodeItems][3];  // the stage being gathered
+      double2 rn[tc::kNodeItems][3];  // its centre-node values (same combo and field)
       int ei = blockIdx.x, b = 0;
 #define FEM25_TC_LOAD_DOFS(EI)                                                   \
   do {                                                                            \
@@ -271,12 +272,16 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     const int nitems_ = min(tc::kC, ga.ncombo - c0_) * 2 * kNen;                  \
     const double2 *ub_ = u + (size_t)c0_ * ga.ndof, *lb_ = lam + (size_t)c0_ * ga.ndof; \
     _Pragma("unroll") for (int j = 0; j < tc::kNodeItems; j++) {                  \
-      const bool act_ = meta[j] >= 0 && (meta[j] & 7) < nitems_ / (2 * kNen) && dn[j] > 0; \
+      const bool cact_ = meta[j] >= 0 && (meta[j] & 7) < nitems_ / (2 * kNen);    \
+      const bool act_ = cact_ && dn[j] > 0, ract_ = cact_ && dref > 0;            \
       const int off_ = act_ ? (meta[j] & 7) * ga.ndof + dn[j] - 1 : 0;            \
+      const int roff_ = ract_ ? (meta[j] & 7) * ga.ndof + dref - 1 : 0;           \
       const double2 *p_ = ((meta[j] & 8) ? lb_ : ub_) + off_;                     \
+      const double2 *q_ = ((meta[j] & 8) ? lb_ : ub_) + roff_;                    \
       _Pragma("unroll") for (int i = 0; i < 3; i++) {                             \
-        const double2 x_ = __ldg(p_ + i);                                         \
+        const double2 x_ = __ldg(p_ + i), r_ = __ldg(q_ + i);                     \
         vn[j][i] = act_ ? x_ : make_double2(0.0, 0.0);                            \
+        rn[j][i] = ract_ ? r_ : make_double2(0.0, 0.0);                           \
       }                                                                           \
     }                                                                             \
   } while (0)
@@ -295,17 +300,11 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         // derivative rows -- so derivatives are formed from the deviations
         // alone (smooth fields lose no digits to cancellation) and values
         // are centre + interpolated deviation.
-        const int c0s = b * tc::kC, ncs = min(tc::kC, ga.ncombo - c0s);
 #pragma unroll
         for (int j = 0; j < tc::kNodeItems; j++) {
           if (meta[j] >= 0) {
             const int row0 = (meta[j] & 7) * 12 + ((meta[j] >> 3) & 1) * 6, a = meta[j] >> 4;
-            const bool ract = (meta[j] & 7) < ncs && dref > 0;
-            const double2 *rp = ((meta[j] & 8) ? lam : u) +
-                                (ract ? (size_t)(c0s + (meta[j] & 7)) * ga.ndof + dref - 1 : 0);
-            double2 rv[3];
-#pragma unroll
-            for (int i = 0; i < 3; i++) rv[i] = ract ? __ldg(rp + i) : make_double2(0.0, 0.0);
+            const double2 *rv = rn[j];  // centre values, gathered with the stage
             // B1 columns a and 28 + a hold hi, B2 column a (virtual column
             // 56 + a of the stage) holds lo
             const uint32_t o0 = kmajor_off(row0, a, tc::kBLbo);
@@ -325,15 +324,17 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
                 const uint32_t dr = (uint32_t)(((row >> 3) - (row0 >> 3)) * 128 + ((row & 7) - (row0 & 7)) * 16);
                 const double rx = ri == 0 ? rv[i].x : rv[i].y;
                 const float x = (float)((ri == 0 ? vn[j][i].x : vn[j][i].y) - rx);
-                const uint32_t hi = to_tf32(x);
-                const uint32_t lo = to_tf32(x - __uint_as_float(hi));
+                // hi: x rounded to 10 mantissa bits on the bit pattern; lo =
+                // x - hi exactly, of which the MMA reads the top 19 bits
+                const uint32_t hi = (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
+                const uint32_t lo = __float_as_uint(x - __uint_as_float(hi));
                 *reinterpret_cast<uint32_t *>(bh + o0 + dr) = hi;
                 *reinterpret_cast<uint32_t *>(bh + o1 + dr) = hi;
                 *reinterpret_cast<uint32_t *>(bh + o2 + dr) = lo;
                 if (a == tc::kRefNode) {
                   const float xr = (float)rx;
-                  const uint32_t hr = to_tf32(xr);
-                  const uint32_t lr = to_tf32(xr - __uint_as_float(hr));
+                  const uint32_t hr = (__float_as_uint(xr) + 0x1000u) & 0xFFFFE000u;
+                  const uint32_t lr = __float_as_uint(xr - __uint_as_float(hr));
                   *reinterpret_cast<uint32_t *>(bh + r0 + dr) = hr;
                   *reinterpret_cast<uint32_t *>(bh + r1 + dr) = hr;
                   *reinterpret_cast<uint32_t *>(bh + r2 + dr) = lr;
