@@ -97,7 +97,7 @@ void free_ctx(Ctx *c) {
                   c->d_elem_wts, c->d_fmat, c->d_cadj_col0, c->d_cadj_pair_col, c->d_cadj_pair_elem,
                   c->d_cadj_dptr, c->d_cadj_dent, c->d_cadj_w, c->d_nonpml, c->d_cdist, c->d_prim, c->d_desc,
                   c->d_tc_tab, c->d_qp, c->d_qs, c->d_cov, c->d_cov_ops, c->d_cov_opptr,
-                  c->d_cov_tx, c->d_cov_node, c->d_maskg, c->d_avg_work, c->d_post_mrdof,
+                  c->d_cov_tx, c->d_cov_node, c->d_cov_exps, c->d_maskg, c->d_avg_work, c->d_post_mrdof,
                   c->d_post_bits, c->d_hvec, c->d_hgrad};
   for (void *p : ptrs)
     if (p) cudaFree(p);

@@ -155,6 +155,7 @@ struct Ctx {
   int *d_cov_opptr = nullptr, *d_cov_tx = nullptr;
   uint32_t *d_cov_node = nullptr;
   void *tmap_encode = nullptr;
+  int *d_cov_exps = nullptr;  // per launch: the pairs' field-scale exponents
   // cached COMPLEX*8 device buffer of fem25_asmble_driver, and its pipeline:
   // element chunk k = [drv_elem[k], drv_elem[k+1]) completes the CSR rows
   // [drv_row[k], drv_row[k+1]), whose values are gathered and copied to the

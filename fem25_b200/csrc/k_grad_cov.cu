@@ -195,7 +195,21 @@ __device__ __forceinline__ int cov_warp_role(int w, int &c, int &k, int &pidx) {
   return 2;
 }
 
+// Scaling.  FP32 sums of products of small fields underflow: solved fields
+// in SI units (displacements per newton ~1e-10, adjoint fields ~1e-20) give
+// products near FP32's smallest normal numbers, where the split's low parts
+// are flushed.  Each pair's u and lam therefore enter the tensor cores scaled
+// by powers of two that bring their largest sampled component to [1, 2)
+// (exact in FP64), and the epilogue multiplies the pair's weight back.
+constexpr int kExpBias = 4096;    // exponents stored with this offset (0: all zero)
+constexpr int kScaleStride = 13;  // every 13th complex value of a field is sampled
+
+__device__ __forceinline__ double cov_scale_of(int e) {
+  return e == 0 ? 1.0 : ldexp(1.0, kExpBias - e);
+}
+
 struct CovArgs {
+  const int *exps;  // [pair][u, lam]: sampled binary exponents (+ kExpBias)
   int npairs, nsrc, ndof, n_elem;
   int add;          // 1: add into the accumulators, 0: overwrite them
   int inject;       // 1: converter warp 0 of CTA 0 withholds its first stage
@@ -364,6 +378,8 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
       // then the raw slot is released and the operand stage awaited
       const bool gact = g < ga.nsrc - ich * cov::kG;
       const bool vact = gact && node && ni != 0xFFFFFFFFu;
+      const double su = cov_scale_of(__ldg(ga.exps + 2 * ip)),
+                   sl = cov_scale_of(__ldg(ga.exps + 2 * ip + 1));
       const bool ract = gact && (node || refw) && nr != 0xFFFFFFFFu;
       float xv[6][2];
       {
@@ -380,8 +396,9 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
         for (int j = 0; j < 6; j++) {
           // node threads store the deviation (a fixed node's value is 0),
           // reference writers the reference values
-          const double2 v =
-              node ? make_double2(vv[j].x - rv[j].x, vv[j].y - rv[j].y) : rv[j];
+          const double sc = j < 3 ? su : sl;
+          const double2 v = node ? make_double2((vv[j].x - rv[j].x) * sc, (vv[j].y - rv[j].y) * sc)
+                                 : make_double2(rv[j].x * sc, rv[j].y * sc);
           float x0 = (float)v.x, x1 = (float)v.y;
           // the sign / swap of the layout: u1 -> (Im, -Re), lam1 -> (-Im, Re)
           if (j % 3 == 1) {
@@ -594,6 +611,8 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
         const double2 pr = pt.p[p];
         double w = wt == 0 ? 1.0 : wt == 1 ? pr.y * pr.y : wt == 2 ? pr.x * pr.x : pr.y;
         if (neg) w = -w;
+        // the pair's scaling undone
+        w /= cov_scale_of(__ldg(ga.exps + 2 * p)) * cov_scale_of(__ldg(ga.exps + 2 * p + 1));
         for (int ch = 0; ch < nch; ch += cov::kDrain, unit++) {
           const int ts = (int)(unit % cov::kUnits);
           mbar_wait(smem_u32(&bar_tfull[ts]), (unit / cov::kUnits) & 1u, drain, err, -2000005,
@@ -651,6 +670,32 @@ __global__ void __launch_bounds__(cov::kThreads, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cov::kTmemCols)
                  : "memory");
+  }
+}
+
+// Per pair: the binary exponent (+ kExpBias) of the largest real or
+// imaginary part among every kScaleStride-th complex value of u (exps[2p])
+// and of lam (exps[2p + 1]) over the pair's sources; 0 if all are zero.
+__global__ void k_cov_scale(const double2 *__restrict__ u, const double2 *__restrict__ lam,
+                            long long per_pair, int *__restrict__ exps) {
+  const int p = blockIdx.y;
+  const double2 *up = u + (long long)p * per_pair, *lp = lam + (long long)p * per_pair;
+  int eu = 0, el = 0;
+  const long long step = (long long)gridDim.x * blockDim.x * kScaleStride;
+  for (long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * kScaleStride;
+       i < per_pair; i += step) {
+    const double2 a = up[i], b = lp[i];
+    const double ma = fmax(fabs(a.x), fabs(a.y)), mb = fmax(fabs(b.x), fabs(b.y));
+    if (ma > 0.0) eu = max(eu, ilogb(ma) + kExpBias);
+    if (mb > 0.0) el = max(el, ilogb(mb) + kExpBias);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    eu = max(eu, __shfl_xor_sync(0xffffffffu, eu, o));
+    el = max(el, __shfl_xor_sync(0xffffffffu, el, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(exps + 2 * p, eu);
+    atomicMax(exps + 2 * p + 1, el);
   }
 }
 
@@ -1059,6 +1104,7 @@ cudaError_t prepare_grad_cov(Ctx *c) {
       (e = up((void **)&c->d_cov_node, node.data(), node.size() * sizeof(uint32_t))) ||
       (e = up((void **)&c->d_cov_tx, tx.data(), tx.size() * sizeof(int))))
     return e;
+  if ((e = cudaMalloc((void **)&c->d_cov_exps, sizeof(int) * 2 * kMaxPairs))) return e;
   const size_t n = (size_t)std::max(c->n_nonpml, 1) * cov::kBlocks * cov::kBlk;
   double *d = nullptr;
   if ((e = cudaMalloc(&d, n * sizeof(double)))) return e;
@@ -1110,7 +1156,14 @@ cudaError_t launch_grad_cov(Ctx *c, const PairTable &pt, int npairs, int nsrc, c
   CovMaps maps;
   cudaError_t e = cov_maps(c, u, lam, npairs * nsrc, maps);
   if (e != cudaSuccess) return e;
+  // the pairs' field scales
+  if ((e = cudaMemsetAsync(c->d_cov_exps, 0, sizeof(int) * 2 * npairs, st))) return e;
+  k_cov_scale<<<dim3(64, npairs), 256, 0, st>>>(reinterpret_cast<const double2 *>(u),
+                                                 reinterpret_cast<const double2 *>(lam),
+                                                 (long long)nsrc * c->ndof, c->d_cov_exps);
+  if ((e = cudaGetLastError())) return e;
   CovArgs ga;
+  ga.exps = c->d_cov_exps;
   ga.npairs = npairs;
   ga.nsrc = nsrc;
   ga.ndof = c->ndof;
