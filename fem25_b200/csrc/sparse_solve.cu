@@ -464,7 +464,7 @@ __global__ void k_sp_extend_add(const int *__restrict__ fronts, const SpFront *_
 // updated by a rank-nb product: a warp per pair of columns, their U values
 // in registers, the panel rows read from shared memory.  In place in the
 // work buffer; pivots 1-based within the front.
-__global__ void __launch_bounds__(sp::kThreads, 2) k_sp_factor_blk(
+__global__ void __launch_bounds__(sp::kThreads) k_sp_factor_blk(
     const int *__restrict__ fronts, int nfr, const SpFront *__restrict__ fr,
     double2 *__restrict__ work, int64_t *__restrict__ piv, int *__restrict__ info) {
   extern __shared__ double2 P[];  // panel: P[r + c * pr], r < pr = n - jb, c < nb
@@ -572,21 +572,29 @@ __global__ void __launch_bounds__(sp::kThreads, 2) k_sp_factor_blk(
         if (i < nb) col[i] = x[i];
     }
     __syncthreads();
-    // 6. trailing update, rows and columns from jb + nb: a warp per column
+    // 6. trailing update, rows and columns from jb + nb: a warp per pair of
+    // columns (each panel value read from shared memory feeds two columns)
     const int c0 = jb + nb;
-    for (int cp = c0 + warp; cp < n; cp += nw) {
-      double2 u[sp::kNb];
+    for (int cp = c0 + 2 * warp; cp < n; cp += 2 * nw) {
+      const bool two = cp + 1 < n;
+      double2 u0[sp::kNb], u1[sp::kNb];
 #pragma unroll
-      for (int j = 0; j < sp::kNb; j++)
-        u[j] = j < nb ? F[jb + j + (long long)cp * n] : make_double2(0.0, 0.0);
-      double2 *col = F + (long long)cp * n;
+      for (int j = 0; j < sp::kNb; j++) {
+        u0[j] = j < nb ? F[jb + j + (long long)cp * n] : make_double2(0.0, 0.0);
+        u1[j] = (two && j < nb) ? F[jb + j + (long long)(cp + 1) * n] : make_double2(0.0, 0.0);
+      }
+      double2 *col0 = F + (long long)cp * n, *col1 = col0 + n;
       for (int r = c0 + lane; r < n; r += 32) {
-        double2 acc = col[r];
+        double2 a0 = col0[r], a1 = two ? col1[r] : make_double2(0.0, 0.0);
         const double2 *pl = P + (r - jb);
 #pragma unroll
-        for (int j = 0; j < sp::kNb; j++)
-          if (j < nb) acc = cfms(acc, pl[j * pr], u[j]);
-        col[r] = acc;
+        for (int j = 0; j < sp::kNb; j++) {
+          const double2 l = j < nb ? pl[j * pr] : make_double2(0.0, 0.0);
+          a0 = cfms(a0, l, u0[j]);
+          a1 = cfms(a1, l, u1[j]);
+        }
+        col0[r] = a0;
+        if (two) col1[r] = a1;
       }
     }
     __syncthreads();
