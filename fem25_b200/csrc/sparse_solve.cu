@@ -48,6 +48,7 @@ namespace sp {
 constexpr int kLeafElems = 2;     // elements per leaf of the dissection
 constexpr int kSmallN = 1024;     // fronts up to this many rows: one CTA each
 constexpr int kNb = 8;            // panel width of the one-CTA factorisation
+constexpr int kFacThreads = 256;  // threads of the one-CTA factorisation (128 measured slower)
 constexpr int kThreads = 256;
 constexpr int kRhsPerCta = 8;     // right-hand sides per solve CTA
 constexpr int kLanes = 8;         // streams for the library-factored fronts of a level
@@ -464,12 +465,12 @@ __global__ void k_sp_extend_add(const int *__restrict__ fronts, const SpFront *_
 // updated by a rank-nb product: a warp per pair of columns, their U values
 // in registers, the panel rows read from shared memory.  In place in the
 // work buffer; pivots 1-based within the front.
-__global__ void __launch_bounds__(sp::kThreads) k_sp_factor_blk(
+__global__ void __launch_bounds__(sp::kFacThreads) k_sp_factor_blk(
     const int *__restrict__ fronts, int nfr, const SpFront *__restrict__ fr,
     double2 *__restrict__ work, int64_t *__restrict__ piv, int *__restrict__ info) {
   extern __shared__ double2 P[];  // panel: P[r + c * pr], r < pr = n - jb, c < nb
-  __shared__ double red_v[sp::kThreads / 32];
-  __shared__ int red_i[sp::kThreads / 32];
+  __shared__ double red_v[sp::kFacThreads / 32];
+  __shared__ int red_i[sp::kFacThreads / 32];
   __shared__ int swp[sp::kNb];
   const int b = blockIdx.x;
   if (b >= nfr) return;
@@ -1012,7 +1013,7 @@ int sparse_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *ms
     const int nsmall = s->lev_nsmall[l];
     if (nsmall > 0) {
       const size_t sm = sizeof(double2) * (size_t)s->lev_nmax_small[l] * sp::kNb;
-      k_sp_factor_blk<<<nsmall, sp::kThreads, sm, st>>>(dfr, nsmall, s->d_fr, W, s->d_piv,
+      k_sp_factor_blk<<<nsmall, sp::kFacThreads, sm, st>>>(dfr, nsmall, s->d_fr, W, s->d_piv,
                                                          s->d_info);
       SPCK(cudaGetLastError(), "small fronts");
     }
