@@ -434,6 +434,12 @@ def pipeline_uneven(local, dev, rank=0, world=1, max_over_ranks=None):
         out.update({"plain_fp64_s": plain_total, "plain_fp64_fma_s": plain_total_fma,
                     "speedup_measured": plain_total / t_job,
                     "speedup_measured_vs_fma_plain": plain_total_fma / t_job,
+                    # the pointwise form keeps <= 1e-6 in lambda on solved fields too
+                    "speedup_pointwise_estimate": plain_total / max(
+                        t_job - npairs * t_acc - t_fin + npairs * t_gpw, 1e-9),
+                    "speedup_pointwise_note": "the measured graph with each pair's covariance "
+                                              "accumulation (and the contraction) replaced by "
+                                              "the pointwise kernel's measured time per pair",
                     "sample": f"batched: all {npairs} systems and pairs measured in one graph; "
                               f"plain: assembly of 1 system per frequency ({len(sel)}) and the "
                               f"FP64 gradient of 1 pair x {nsrc} sources, scaled to {npairs} "
