@@ -15,9 +15,10 @@ wavelengths (measured: 4.2e-6, 7.1e-9 and 3.5e-9 at h = 1e-4, 2e-5, 5e-6); split
 precision vs the FP64 gradient, per parameter (2-norm): the pointwise form
 <= 1e-6 for lambda, mu and rho; the covariance form <= 1e-6 for mu and rho
 and <= 1e-5 for lambda.  Its lambda error (2.3e-6 here, 3.8e-6 with 32
-sources per pair) comes from the FP32 sums over sources in tensor memory,
-amplified by the lambda gradient's divergence: for shear-dominated solved
-fields the divergence is a small difference of large derivatives."""
+sources per pair) is the split operands' precision (about 22 bits of each
+deviation) amplified twice by the lambda gradient's divergence, a small
+difference of large derivatives for shear-dominated solved fields; the
+pointwise form forms each divergence in FP64 and amplifies it once."""
 import numpy as np
 import pytest
 
