@@ -230,14 +230,21 @@ int fem25_addblk_dev(fem25_ctx *ctx, int nsrc, const float *ue, float *sol, void
  *                               contracted once in FP64.  Equivalent to
  *                               fem25_gradient_accumulate_dev followed by
  *                               fem25_gradient_finalize_dev, so it also adds
- *                               any accumulation still pending on the context;
+ *                               any accumulation still pending on the context.
+ *                               Within 1e-6 of FP64 per parameter on smooth
+ *                               fields; on solved point-source fields mu and
+ *                               rho stay within 1e-6 while lambda, whose
+ *                               divergence terms cancel for shear-dominated
+ *                               fields, can reach a few 1e-6;
  *   FEM25_PREC_TF32X3_POINTWISE split-precision tensor cores interpolating
  *                               both fields at the 169 points per (pair,
- *                               source), no accumulator memory; faster for
- *                               one-shot calls with few (pair, source)
- *                               fields, as the covariance form's contraction
- *                               is a fixed cost per call (about 40 fields on
- *                               a 48 000-element mesh break even).
+ *                               source), no accumulator memory; within 1e-6
+ *                               of FP64 for lambda, mu and rho on smooth and
+ *                               solved fields; faster for one-shot calls
+ *                               with few (pair, source) fields, as the
+ *                               covariance form's contraction is a fixed
+ *                               cost per call (about 40 fields on a
+ *                               48 000-element mesh break even).
  * Pairs are passed to the kernels by value, 64 per launch; the call only
  * enqueues work and may be recorded into a CUDA graph once the first
  * split-precision call of that kind on the context (which allocates or
