@@ -19,7 +19,7 @@ Errors follow the reference's IERR convention: a nonzero status raises
 no CPU fallback: without the CUDA library every call fails.
 """
 from .lib import (FEM25_PREC_FP64, FEM25_PREC_TF32X3, FEM25_PREC_TF32X3_POINTWISE, Context,
-                  Fem25Error, graph_build, lib, fazmod, mesh_struct, read_mesh)
+                  Fem25Error, graph_build, lib, fazmod, mesh_struct, read_mesh, sparse_plan)
 
 __all__ = ["Context", "Fem25Error", "fazmod", "graph_build", "lib", "mesh_struct", "read_mesh",
-           "FEM25_PREC_FP64", "FEM25_PREC_TF32X3", "FEM25_PREC_TF32X3_POINTWISE"]
+           "sparse_plan", "FEM25_PREC_FP64", "FEM25_PREC_TF32X3", "FEM25_PREC_TF32X3_POINTWISE"]

@@ -717,6 +717,16 @@ int fem25_sparse_solve_dev(fem25_ctx *h, int nrhs, int trans, double *rhs, void 
   return r ? fail(c, r, msg) : FEM25_OK;
 }
 
+int fem25_sparse_plan(const fem25_mesh *m, const fem25_graph *g, long long *out) {
+  if (!m || !g || !out || !m->ieng || !m->xlocs || !m->zlocs) return FEM25_ERR_ARG;
+  if (g->g.nelem != m->nelem) return FEM25_ERR_ARG;
+  std::string msg;
+  const int r = sparse_plan_info(m->nelem, g->g.ndof, g->g.lm.data(), m->ieng, m->xlocs,
+                                 m->zlocs, out, &msg);
+  if (r) std::fprintf(stderr, "fem25gpu: %s\n", msg.c_str());
+  return r;
+}
+
 int fem25_sparse_info(fem25_ctx *h, long long *out) {
   if (!h || !out) return FEM25_ERR_ARG;
   sparse_info(&h->c, out);

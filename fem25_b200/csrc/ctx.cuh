@@ -212,6 +212,8 @@ void free_dense(Ctx *c);
 int sparse_factor(Ctx *c, const double *csr128, cudaStream_t st, std::string *msg);
 int sparse_solve(Ctx *c, int nrhs, int trans, double *rhs, cudaStream_t st, std::string *msg);
 void sparse_info(const Ctx *c, long long *out);
+int sparse_plan_info(int nelem, int ndof, const int *lm, const int *ieng, const double *x,
+                     const double *z, long long *out, std::string *msg);
 void free_sparse(Ctx *c);
 cudaError_t launch_grad_plain(Ctx *c, const PairTable &pt, int npairs, int nsrc, const double *u,
                               const double *lam, double *grad, cudaStream_t st);

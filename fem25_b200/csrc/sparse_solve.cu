@@ -110,7 +110,7 @@ struct SparseLU {
 namespace {
 
 struct Builder {
-  const Ctx *c;
+  const int *lm_all;  // LM(3,25,NELEM), 1-based DOFs
   std::vector<double> cx, cz;
   std::vector<int> owner;    // DOF -> front (0-based DOF)
   std::vector<int> mark;     // scratch stamps per DOF
@@ -120,7 +120,7 @@ struct Builder {
   std::vector<std::vector<int>> elems;      // per front, its subtree's elements
 
   int rec(std::vector<int> &E, int depth) {
-    const int *lm = c->h_lm.data();
+    const int *lm = lm_all;
     if ((int)E.size() <= sp::kLeafElems) {
       std::vector<int> own;
       for (int e : E)
@@ -197,27 +197,39 @@ struct Builder {
 
 }  // namespace
 
-// Builds the ordering, the fronts, the extend-add maps and the CSR-entry map;
-// uploads them.  0, or a FEM25 status with *msg.
-static int sparse_analyse(Ctx *c, SparseLU *s, cudaStream_t st, std::string *msg) {
-  const int n = c->ndof;
+// The dissection of a mesh (host only): the fronts with their own and
+// boundary DOFs, elimination positions, levels and the offsets of every
+// front's work and factor blocks.
+struct FrontPlan {
+  std::vector<SpFront> fr;
+  std::vector<std::vector<int>> own, bnd;
+  std::vector<long long> pos;
+  std::vector<int> owner;
+  std::vector<std::vector<int>> lev;
+  std::vector<long long> lev_work;
+  long long fac_elems = 0, bnd_tot = 0;
+  int nlev = 0;
+};
+
+static int plan_fronts(int nelem, int n, const int *lm, const int *ieng, const double *xa,
+                       const double *za, FrontPlan *pl, std::string *msg) {
   Builder b;
-  b.c = c;
-  b.cx.resize(c->nelem);
-  b.cz.resize(c->nelem);
-  for (int e = 0; e < c->nelem; e++) {
+  b.lm_all = lm;
+  b.cx.resize(nelem);
+  b.cz.resize(nelem);
+  for (int e = 0; e < nelem; e++) {
     double x = 0, z = 0;
     for (int a = 0; a < 4; a++) {
-      const int p = c->h_ieng[4 * e + a] - 1;
-      x += c->h_x[p];
-      z += c->h_z[p];
+      const int p = ieng[4 * e + a] - 1;
+      x += xa[p];
+      z += za[p];
     }
     b.cx[e] = 0.25 * x;
     b.cz[e] = 0.25 * z;
   }
   b.owner.assign(n, -1);
   b.mark.assign(n, 0);
-  std::vector<int> E(c->nelem);
+  std::vector<int> E(nelem);
   std::iota(E.begin(), E.end(), 0);
   b.rec(E, 0);
   for (int d = 0; d < n; d++)
@@ -227,21 +239,23 @@ static int sparse_analyse(Ctx *c, SparseLU *s, cudaStream_t st, std::string *msg
     }
   const int nf = (int)b.fr.size();
   // elimination positions (postorder = front id order)
-  std::vector<long long> pos(n);
+  std::vector<long long> &pos = pl->pos;
+  pos.assign(n, 0);
   long long p = 0;
   for (int t = 0; t < nf; t++) {
     b.fr[t].own0 = p;
     for (int d : b.own_list[t]) pos[d] = p++;
   }
   // boundaries: DOFs of the subtree's elements owned by an ancestor (id > t)
-  std::vector<std::vector<int>> bnd(nf);
+  std::vector<std::vector<int>> &bnd = pl->bnd;
+  bnd.assign(nf, {});
   {
     std::vector<int> seen(n, -1);
     for (int t = 0; t < nf; t++) {
       std::vector<int> &B = bnd[t];
       for (int e : b.elems[t])
         for (int q = 0; q < kNee; q++) {
-          const int d = c->h_lm[(size_t)e * kNee + q] - 1;
+          const int d = lm[(size_t)e * kNee + q] - 1;
           if (d >= 0 && b.owner[d] > t && seen[d] != t) {
             seen[d] = t;
             B.push_back(d);
@@ -253,6 +267,86 @@ static int sparse_analyse(Ctx *c, SparseLU *s, cudaStream_t st, std::string *msg
       b.elems[t].shrink_to_fit();
     }
   }
+  // levels, offsets
+  int nlev = 0;
+  for (auto &f : b.fr) nlev = std::max(nlev, f.level + 1);
+  pl->lev.assign(nlev, {});
+  pl->lev_work.assign(nlev, 0);
+  long long bnd_tot = 0, fac = 0;
+  for (int t = 0; t < nf; t++) {
+    SpFront &f = b.fr[t];
+    const long long nn = (long long)f.k + f.m;
+    f.bnd0 = bnd_tot;
+    f.ea0 = bnd_tot;
+    bnd_tot += f.m;
+    f.fac0 = fac;
+    fac += nn * f.k + (long long)f.k * f.m;
+    f.work0 = pl->lev_work[f.level];
+    pl->lev_work[f.level] += nn * nn;
+    pl->lev[f.level].push_back(t);
+  }
+  pl->fac_elems = fac;
+  pl->bnd_tot = bnd_tot;
+  pl->nlev = nlev;
+  pl->fr = std::move(b.fr);
+  pl->own = std::move(b.own_list);
+  pl->owner = std::move(b.owner);
+  return 0;
+}
+
+// fronts, levels, factor bytes, largest level work bytes, largest own count,
+// largest front order, real flops of one factorisation (8 per complex
+// multiply-add)
+static void plan_stats(const std::vector<SpFront> &fr, long long fac_elems,
+                       const std::vector<long long> &lev_work, long long *out) {
+  int kmax = 0, nmax = 0, nlev = 0;
+  double flops = 0.0;
+  for (const SpFront &f : fr) {
+    kmax = std::max(kmax, f.k);
+    nmax = std::max(nmax, f.k + f.m);
+    nlev = std::max(nlev, f.level + 1);
+    const double k = f.k, m = f.m;
+    flops += 8.0 / 3.0 * k * k * k + 8.0 * k * k * m + 8.0 * k * m * m;
+  }
+  long long wmax = 0;
+  for (long long w : lev_work) wmax = std::max(wmax, w);
+  out[0] = (long long)fr.size();
+  out[1] = nlev;
+  out[2] = fac_elems * 16;
+  out[3] = wmax * 16;
+  out[4] = kmax;
+  out[5] = nmax;
+  out[6] = (long long)flops;
+}
+
+int sparse_plan_info(int nelem, int ndof, const int *lm, const int *ieng, const double *x,
+                     const double *z, long long *out, std::string *msg) {
+  FrontPlan pl;
+  const int r = plan_fronts(nelem, ndof, lm, ieng, x, z, &pl, msg);
+  if (r) return r;
+  plan_stats(pl.fr, pl.fac_elems, pl.lev_work, out);
+  return 0;
+}
+
+// Builds the ordering, the fronts, the extend-add maps and the CSR-entry map;
+// uploads them.  0, or a FEM25 status with *msg.
+static int sparse_analyse(Ctx *c, SparseLU *s, cudaStream_t st, std::string *msg) {
+  const int n = c->ndof;
+  FrontPlan pl;
+  {
+    const int r = plan_fronts(c->nelem, n, c->h_lm.data(), c->h_ieng.data(), c->h_x.data(),
+                              c->h_z.data(), &pl, msg);
+    if (r) return r;
+  }
+  const int nf = (int)pl.fr.size();
+  const int nlev = pl.nlev;
+  const std::vector<long long> &pos = pl.pos;
+  const std::vector<std::vector<int>> &bnd = pl.bnd;
+  struct {
+    std::vector<SpFront> &fr;
+    std::vector<std::vector<int>> &own_list;
+    std::vector<int> &owner;
+  } b{pl.fr, pl.own, pl.owner};
   // index of DOF d in front t (own: by position; boundary: by search)
   auto local = [&](int t, int d) -> int {
     const SpFront &f = b.fr[t];
@@ -263,27 +357,12 @@ static int sparse_analyse(Ctx *c, SparseLU *s, cudaStream_t st, std::string *msg
     if (it == B.end() || *it != d) return -1;
     return f.k + (int)(it - B.begin());
   };
-  // levels, offsets
-  int nlev = 0;
-  for (auto &f : b.fr) nlev = std::max(nlev, f.level + 1);
-  s->lev.assign(nlev, {});
-  s->lev_work.assign(nlev, 0);
-  long long bnd_tot = 0, fac = 0;
-  for (int t = 0; t < nf; t++) {
-    SpFront &f = b.fr[t];
-    const long long nn = (long long)f.k + f.m;
-    f.bnd0 = bnd_tot;
-    f.ea0 = bnd_tot;
-    bnd_tot += f.m;
-    f.fac0 = fac;
-    fac += nn * f.k + (long long)f.k * f.m;
-    f.work0 = s->lev_work[f.level];
-    s->lev_work[f.level] += nn * nn;
-    s->lev[f.level].push_back(t);
-  }
-  s->fac_elems = fac;
+  s->lev = pl.lev;
+  s->lev_work = pl.lev_work;
+  s->fac_elems = pl.fac_elems;
   s->max_work = 0;
   for (long long w : s->lev_work) s->max_work = std::max(s->max_work, w);
+  const long long bnd_tot = pl.bnd_tot;
   // extend-add maps: child boundary DOF -> index in the parent's front
   std::vector<int> ea(bnd_tot), own_all(n), bnd_all(bnd_tot);
   for (int t = 0; t < nf; t++) {
@@ -927,22 +1006,11 @@ void free_sparse(Ctx *c) {
 
 void sparse_info(const Ctx *c, long long *out) {
   const SparseLU *s = c->sparse;
-  out[0] = s ? s->nfront : 0;
-  out[1] = s ? s->nlevel : 0;
-  out[2] = s ? s->fac_elems * 16 : 0;
-  out[3] = s ? s->max_work * 16 : 0;
-  int kmax = 0, nmax = 0;
-  double flops = 0.0;  // real flops: 8 per complex multiply-add
-  if (s)
-    for (const SpFront &f : s->fr) {
-      kmax = std::max(kmax, f.k);
-      nmax = std::max(nmax, f.k + f.m);
-      const double k = f.k, m = f.m;
-      flops += 8.0 / 3.0 * k * k * k + 8.0 * k * k * m + 8.0 * k * m * m;
-    }
-  out[4] = kmax;
-  out[5] = nmax;
-  out[6] = (long long)flops;
+  if (!s) {
+    for (int i = 0; i < 7; i++) out[i] = 0;
+    return;
+  }
+  plan_stats(s->fr, s->fac_elems, s->lev_work, out);
 }
 
 #define SPCK(expr, what)                                                   \

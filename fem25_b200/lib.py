@@ -74,6 +74,7 @@ def lib():
         L.fem25_sparse_factor_dev.argtypes = [vp, vp, vp]
         L.fem25_sparse_solve_dev.argtypes = [vp, i, i, vp, vp]
         L.fem25_sparse_info.argtypes = [vp, vp]
+        L.fem25_sparse_plan.argtypes = [vp, vp, vp]
         L.fem25_gradient_dev.argtypes = [vp, i, vp, vp, i, vp, vp, i, vp, vp]
         L.fem25_gradient_accumulate_dev.argtypes = [vp, i, vp, vp, i, vp, vp, vp]
         L.fem25_gradient_finalize_dev.argtypes = [vp, vp, vp]
@@ -200,6 +201,27 @@ def graph_build(mesh, cache=None):
     L.fem25_graph_free(h)
     return Graph(nnp=nnp.value, ndof=ndof.value, nzero=nz.value, ien=ien, lm=lm, irptr=irptr,
                  jcptr=jcptr, cnp=cnp)
+
+
+def sparse_plan(mesh):
+    """The nested dissection fem25_sparse_factor_dev would use for ``mesh``,
+    planned on the host (fem25_sparse_plan): (fronts, levels, factor bytes,
+    largest level work bytes, largest own count, largest front order, flops
+    of one factorisation)."""
+    L = lib()
+    mk = _MeshKeep(mesh)
+    h = C.c_void_p()
+    r = L.fem25_graph_build(mk.ptr, C.byref(h))
+    if r:
+        raise Fem25Error(r, "graph build failed")
+    out = np.zeros(7, np.int64)
+    try:
+        r = L.fem25_sparse_plan(mk.ptr, h, out.ctypes.data)
+    finally:
+        L.fem25_graph_free(h)
+    if r:
+        raise Fem25Error(r, "sparse plan failed")
+    return tuple(int(v) for v in out)
 
 
 def fazmod(xlatmin, xlonmin, xlatmax, xlonmax):

@@ -202,6 +202,11 @@ int fem25_dense_solve_dev(fem25_ctx *ctx, int nrhs, int trans, double *rhs, void
 int fem25_sparse_factor_dev(fem25_ctx *ctx, const double *csr128, void *stream);
 int fem25_sparse_solve_dev(fem25_ctx *ctx, int nrhs, int trans, double *rhs, void *stream);
 int fem25_sparse_info(fem25_ctx *ctx, long long *out);
+/* The nested dissection that fem25_sparse_factor_dev would use for a mesh and
+ * its graph (fem25_graph_build), computed on the host without a device or a
+ * context: out[7] as fem25_sparse_info.  For planning memory (the factor
+ * store and the two work buffers) before a context exists. */
+int fem25_sparse_plan(const fem25_mesh *mesh, const fem25_graph *graph, long long *out);
 
 /* Drop-in for ADDBLK (bielak_utils.f:1116-1125; callers funcgradh.f90:248,
  * srcrec.f90:694, fgh_window.f90:437, qpmfree.f90:378): after the solve, the
