@@ -367,6 +367,9 @@ def smooth_fields(mesh: Mesh, g, pairs, nsrc: int, seed: int, device="cpu", spee
     xt = torch.from_numpy(x).to(device)
     zt = torch.from_numpy(z).to(device)
     out = torch.empty((len(pairs), nsrc, g.ndof), dtype=torch.complex128, device=device)
+    # modes are summed in chunks of 16 rows ([16, NDOF] per chunk), a handful
+    # of launches per source instead of several per mode
+    chunk = 16
     for p, (f, _py) in enumerate(pairs):
         k0 = TWOPI * f / speed
         for s in range(nsrc):
@@ -374,8 +377,11 @@ def smooth_fields(mesh: Mesh, g, pairs, nsrc: int, seed: int, device="cpu", spee
             kz = (torch.randn(nmodes, generator=gen, dtype=torch.float64) / corr_len).to(device)
             b = (torch.rand(nmodes, generator=gen, dtype=torch.float64) * TWOPI).to(device)
             phi = torch.zeros(g.ndof, dtype=torch.float64, device=device)
-            for m in range(nmodes):
-                phi += torch.cos(kx[m] * xt + kz[m] * zt + b[m])
+            for m0 in range(0, nmodes, chunk):
+                sl = slice(m0, min(nmodes, m0 + chunk))
+                arg = torch.outer(kx[sl], xt)
+                arg.addcmul_(kz[sl, None], zt[None, :]).add_(b[sl, None])
+                phi += torch.cos_(arg).sum(0)
             phi *= math.sqrt(2.0 / nmodes)
             amp = torch.exp(sigma_amp * torch.randn(g.ndof, generator=gen,
                                                     dtype=torch.float64).to(device))
