@@ -28,7 +28,7 @@ Also reported on the same line:
   * pipeline: the uneven-batch workload (600x200 jittered mesh with
     topography, 24 frequencies 0.1-2.4 Hz x ceil(16 f / 0.1) ky = 4800 systems,
     64 sources): batched assembly + split-precision covariance accumulation per
-    pair + one contraction, measured in one CUDA graph over all 4800 pairs,
+    two pairs + one contraction, measured in one CUDA graph over all 4800 pairs,
     against the plain per-(omega, py) FP64 assembly (reference arithmetic and
     FMA build) + FP64 gradient per pair (sampled, scaled); sharded over ranks
     with one NCCL all-reduce when N > 1
@@ -251,9 +251,10 @@ def pipeline_uneven(local, dev, rank=0, world=1, max_over_ranks=None):
     Batched split-precision side, measured end to end: one CUDA graph holds
     the batched assembly of every system of this rank (ring of 8 complex128
     slots), one covariance accumulation (fem25_gradient_accumulate_dev) per
-    pair with that pair's 64 source fields (a pool of 2 field sets of the
-    adjoint-gradient kind, cycled: the operator and the kernels do not depend
-    on the values), and the contraction (fem25_gradient_finalize_dev); the
+    two pairs with their 64 source fields each (two pairs' solutions held at
+    a time; a pool of 2 field sets of the adjoint-gradient kind, reused: the
+    operator and the kernels do not depend on the values), and the
+    contraction (fem25_gradient_finalize_dev); the
     graph is replayed once under CUDA events.  With several ranks the pairs
     are sharded longest-processing-time first and the FP64 gradients summed
     by one NCCL all-reduce, timed apart.
@@ -360,9 +361,16 @@ def pipeline_uneven(local, dev, rank=0, world=1, max_over_ranks=None):
     ctx.gradient_accumulate([gp[0]], [gp[1]], nsrc, u1, l1, stream=stream)
     ctx.gradient_finalize(gsum, stream=stream)
     torch.cuda.synchronize()
-    # the accumulation of one pair and the contraction, eager, for the record
-    t_acc = timed(lambda: ctx.gradient_accumulate([gp[0]], [gp[1]], nsrc, u1, l1, stream=stream),
-                  reps=3)
+    # the accumulation (per pair, in the graph's grouping) and the
+    # contraction, eager, for the record
+    acc_group = 2
+    gf = [p[0] for p in pool_pairs[:acc_group]]
+    gy = [p[1] for p in pool_pairs[:acc_group]]
+    t_acc1 = timed(lambda: ctx.gradient_accumulate([gp[0]], [gp[1]], nsrc, u1, l1, stream=stream),
+                   reps=3)
+    t_acc = timed(lambda: ctx.gradient_accumulate(gf, gy, nsrc, pool_u[:acc_group],
+                                                  pool_l[:acc_group], stream=stream),
+                  reps=3) / acc_group
     t_fin = timed(lambda: ctx.gradient_finalize(gsum, stream=stream))
     ctx.sync_status(stream)
     gsum.zero_()
@@ -377,10 +385,13 @@ def pipeline_uneven(local, dev, rank=0, world=1, max_over_ranks=None):
             cur = torch.cuda.current_stream(dev)
             if mine:
                 ctx.assemble_batch("B", mine_f, mine_p, ring, sst, nslots, stream=cur)
-            for j, k in enumerate(mine):
-                q = k % len(pool_pairs)
-                ctx.gradient_accumulate([freqs[k]], [pys[k]], nsrc, pool_u[q:q + 1],
-                                        pool_l[q:q + 1], stream=cur)
+            # the pairs' fields two at a time (two pairs' solutions held), so
+            # each element's FP64 accumulators are read and written once per
+            # two pairs
+            for j in range(0, len(mine), acc_group):
+                ks = mine[j:j + acc_group]
+                ctx.gradient_accumulate([freqs[k] for k in ks], [pys[k] for k in ks], nsrc,
+                                        pool_u[:len(ks)], pool_l[:len(ks)], stream=cur)
             ctx.gradient_finalize(gsum, stream=cur)
     stream.wait_stream(side)
     torch.cuda.synchronize()
@@ -409,16 +420,22 @@ def pipeline_uneven(local, dev, rank=0, world=1, max_over_ranks=None):
     del graph, ring, pool_u, pool_l
     ctx.close()
     torch.cuda.empty_cache()
-    n_launch = (len(set(mine_f)) * 2 + -(-len(mine) // nslots) + len(mine) + 1)
+    # kernel nodes: PML deltas (2 per frequency), streaming launches (one per
+    # ring of systems), per accumulation call the field-scale and covariance
+    # kernels, the contraction
+    n_launch = (len(set(mine_f)) * 2 + -(-len(mine) // nslots) + 2 * -(-len(mine) // acc_group)
+                + 1)
     units = mesh.nelem * nsrc
     out = {"workload": f"uneven batch: 600x200 jittered deg-4 mesh with topography, strip 4 "
                        f"({mesh.nelem} elements, NDOF {ndof}, NNZ {nz}), "
                        f"24 f x ceil(16 f/0.1) ky = {npairs} systems, {nsrc} sources",
            "batched_measured_s": t_job, "batched_graph_s": t_graph,
            "batched_form": "one CUDA graph: batched assembly of every system + one covariance "
-                           "accumulation per (omega, py) pair (64 sources) + one contraction",
+                           "accumulation per two (omega, py) pairs (64 sources each) + one "
+                           "contraction",
            "pairs_this_rank": len(mine), "allreduce_s": t_allreduce,
-           "gradient_tf32x3_s_per_pair": t_acc, "gradient_tf32x3_contraction_s": t_fin,
+           "gradient_tf32x3_s_per_pair": t_acc, "gradient_tf32x3_pairs_per_call": acc_group,
+           "gradient_tf32x3_s_one_pair_per_call": t_acc1, "gradient_tf32x3_contraction_s": t_fin,
            "gradient_tf32x3_elem_rhs_per_s": units / t_acc,
            "plain_assembly_s_per_system": t_pasm, "plain_assembly_fma_s_per_system": t_pasm_fma,
            "gradient_fp64_s_per_pair": t_g64, "gradient_tf32x3_pointwise_s_per_pair": t_gpw,
