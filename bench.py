@@ -868,6 +868,14 @@ def main():
                                        "peak_kind": hkind,
                                        "algorithmic_bytes": "u and lambda read once, "
                                                             f"{fbytes / 1e9:.2f} GB per launch"}
+        # the launch's output too: 15 FP64 blocks of 25 x 25 per non-PML
+        # element, written once (the timed launches follow a contraction, so
+        # they overwrite the accumulators instead of adding to them)
+        bbytes = nelem_phys * 15 * 625 * 8.0
+        gbs_all = (fbytes + bbytes) / (acc_ms / 1e3) / 1e9
+        grad["covariance_roofline"].update({
+            "block_bytes": bbytes, "achieved_fields_and_blocks": gbs_all,
+            "frac_fields_and_blocks": gbs_all / hpk})
         # the pointwise kernel against the tensor roofline: the metric's fixed
         # 547 200 flop per elem.rhs over a 3xTF32 peak (bf16 burst / 2 / 3)
         bpk, bkind = bf16_peak()
