@@ -146,14 +146,17 @@ class CpuSampler:
         self.workers = workers or os.cpu_count()
         self.pool = mp.get_context("spawn").Pool(self.workers)
         r = self.pool.map(_cpu_worker, [(cfg_idx, w, 64) for w in range(self.workers)])
-        self.nelem, self.ndof, self.nz = r[0][1:]
+        self.nelem, self.ndof, self.nz = r[0][1:4]
         self.t_elem = max(sum(x[0] for x in r) / (64.0 * self.workers), 1e-9)
+        # whether any worker process had this library's libfem25gpu.so mapped
+        self.product_loaded = any(x[4] for x in r)
 
     def sample(self, seconds):
         per = int(max(16, min(self.nelem, seconds / self.t_elem)))
         t0 = time.perf_counter()
-        self.pool.map(_cpu_worker, [(self.cfg, w, per) for w in range(self.workers)])
+        r = self.pool.map(_cpu_worker, [(self.cfg, w, per) for w in range(self.workers)])
         wall = time.perf_counter() - t0
+        self.product_loaded = self.product_loaded or any(x[4] for x in r)
         done = per * self.workers
         return {"value": done / self.nelem / wall, "unit": UNIT, "cores": self.workers,
                 "kind": "port", "wall_s": wall,
@@ -184,7 +187,16 @@ def _cpu_worker(arg):
     lo = (w * 997) % max(1, mesh.nelem - per)
     t0 = time.perf_counter()
     oracle.asmble(mesh, g, "B", f, py, elo=lo, ehi=min(mesh.nelem, lo + per), out=(None, cdist))
-    return time.perf_counter() - t0, mesh.nelem, g.ndof, g.nzero
+    return time.perf_counter() - t0, mesh.nelem, g.ndof, g.nzero, _product_mapped()
+
+
+def _product_mapped():
+    """True if this process has libfem25gpu.so mapped (Linux /proc)."""
+    try:
+        with open("/proc/self/maps") as f:
+            return "libfem25gpu" in f.read()
+    except OSError:
+        return False
 
 
 def run_reference(args, rank):
@@ -202,6 +214,7 @@ def run_reference(args, rank):
         vals.append(base["value"])
         walls.append(base["wall_s"])
     smp.close()
+    product_loaded = smp.product_loaded or _product_mapped()
     v = statistics.mean(vals)
     base["value"] = v
     nsys = 512
@@ -217,7 +230,8 @@ def run_reference(args, rank):
            "config": headline_config(smp.nelem, smp.ndof, smp.nz, nsys),
            "parallelism": f"{smp.workers} host processes on rank 0",
            "cpu_baseline": base,
-           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "product_library_loaded": product_loaded}
     print(json.dumps(out))
 
 
